@@ -1,0 +1,218 @@
+/*
+ * rtdl_b200.h -- C ABI of librtdl_b200.so, the B200-native RTDL neighbor backend.
+ *
+ * The entry points are the ones RTDL's ctypes layer binds for its OptiX
+ * neighbor path, renamed from rtdl_optix_* to rtdl_b200_* with the same
+ * argument order, meaning, ownership and error convention, so a Python or C
+ * caller switches backends by changing the symbol prefix.  Citations are to
+ * rubaolee/rtdl (paths within that project).
+ *
+ * Conventions shared by every int-returning entry point
+ * (src/native/optix/rtdl_optix_core.cpp:58-66, rtdl_optix_api.cpp:4084-4100):
+ *   - returns 0 on success, 1 on failure with a NUL-terminated message copied
+ *     into error_out (truncated to error_size); nothing is thrown across the ABI;
+ *   - *rows_out / *row_count_out are zeroed before any work; empty query or
+ *     search sets return 0 rows;
+ *   - rows are owned by the caller and released with rtdl_b200_free_rows
+ *     (rtdl_optix_api.cpp:5698); inputs are borrowed for the call only;
+ *   - validation messages match the reference: "radius must be non-negative",
+ *     "k_max must be positive", "... exceeds uint32 limit".
+ * Row order equals the reference's cpu_python_reference
+ * (src/rtdsl/reference.py:349-434): rows grouped by query_id (stable in query
+ * input order), within a query by (distance, neighbor_id, search input order).
+ * Row sets and distances are bit-identical to that reference: the device
+ * decides in FP32 and re-decides every case within the error band in FP64,
+ * and each emitted distance is sqrt((dx*dx + dy*dy) + dz*dz) in FP64 with no
+ * fused multiply-add.
+ */
+#ifndef RTDL_B200_H
+#define RTDL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(RTDL_B200_BUILD) && defined(__GNUC__)
+#define RTDL_B200_API __attribute__((visibility("default")))
+#else
+#define RTDL_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Point and row records: same layouts as src/native/optix/rtdl_optix_prelude.h
+ * :103-106 (RtdlPoint), :138-141 (RtdlPoint3D), :254-260
+ * (RtdlFixedRadiusNeighborRow, 16 B) and :289-295 (RtdlKnnNeighborRow, 24 B). */
+typedef struct RtdlPoint {
+  uint32_t id;
+  double x, y;
+} RtdlPoint;
+
+typedef struct RtdlPoint3D {
+  uint32_t id;
+  double x, y, z;
+} RtdlPoint3D;
+
+typedef struct RtdlFixedRadiusNeighborRow {
+  uint32_t query_id, neighbor_id;
+  double distance;
+} RtdlFixedRadiusNeighborRow;
+
+typedef struct RtdlKnnNeighborRow {
+  uint32_t query_id, neighbor_id;
+  double distance;
+  uint32_t neighbor_rank;
+} RtdlKnnNeighborRow;
+
+/* Version triple (the reference exports rtdl_optix_get_version,
+ * rtdl_optix_api.cpp:1-7). */
+RTDL_B200_API int rtdl_b200_get_version(int* major, int* minor, int* patch);
+
+/* Makes `device` current for the calling thread's later calls (the library
+ * links the CUDA runtime statically, so it keeps its own current device).
+ * No counterpart in the reference, which drives one GPU. */
+RTDL_B200_API int rtdl_b200_set_device(int device);
+
+/* ---- plain per-call launches ------------------------------------------- */
+
+/* Replaces rtdl_optix_run_fixed_radius_neighbors (rtdl_optix_api.cpp:4076-4105). */
+RTDL_B200_API int rtdl_b200_run_fixed_radius_neighbors(
+    const RtdlPoint* query_points, size_t query_count,
+    const RtdlPoint* search_points, size_t search_count,
+    double radius, size_t k_max,
+    RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out,
+    char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_run_fixed_radius_neighbors_3d (rtdl_optix_api.cpp:4107-4150). */
+RTDL_B200_API int rtdl_b200_run_fixed_radius_neighbors_3d(
+    const RtdlPoint3D* query_points, size_t query_count,
+    const RtdlPoint3D* search_points, size_t search_count,
+    double radius, size_t k_max,
+    RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out,
+    char* error_out, size_t error_size);
+
+/* bounded_knn_rows with ranks assigned on the device.  The reference builds
+ * these rows in Python from the FRN rows (src/rtdsl/optix_runtime.py:15834-15862);
+ * the rows equal src/rtdsl/reference.py:406-434. */
+RTDL_B200_API int rtdl_b200_run_bounded_knn_rows(
+    const RtdlPoint* query_points, size_t query_count,
+    const RtdlPoint* search_points, size_t search_count,
+    double radius, size_t k_max,
+    RtdlKnnNeighborRow** rows_out, size_t* row_count_out,
+    char* error_out, size_t error_size);
+
+RTDL_B200_API int rtdl_b200_run_bounded_knn_rows_3d(
+    const RtdlPoint3D* query_points, size_t query_count,
+    const RtdlPoint3D* search_points, size_t search_count,
+    double radius, size_t k_max,
+    RtdlKnnNeighborRow** rows_out, size_t* row_count_out,
+    char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_run_k_closest_hits (rtdl_optix_api.cpp:4971-4997). */
+RTDL_B200_API int rtdl_b200_run_k_closest_hits(
+    const RtdlPoint* query_points, size_t query_count,
+    const RtdlPoint* search_points, size_t search_count,
+    size_t k,
+    RtdlKnnNeighborRow** rows_out, size_t* row_count_out,
+    char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_run_k_closest_hits_3d (rtdl_optix_api.cpp:4999-5025). */
+RTDL_B200_API int rtdl_b200_run_k_closest_hits_3d(
+    const RtdlPoint3D* query_points, size_t query_count,
+    const RtdlPoint3D* search_points, size_t search_count,
+    size_t k,
+    RtdlKnnNeighborRow** rows_out, size_t* row_count_out,
+    char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_free_rows (rtdl_optix_api.cpp:5698). */
+RTDL_B200_API void rtdl_b200_free_rows(void* rows);
+
+/* ---- prepared scenes (resident BVH on the device) ---------------------- */
+
+/* Replaces rtdl_optix_prepare_fixed_radius_neighbors_3d (rtdl_optix_api.cpp:4152-4171).
+ * The scene is an LBVH over the search points kept resident on the device;
+ * max_radius is validated like the reference (must be positive) and recorded,
+ * and later calls must use radius <= max_radius. */
+RTDL_B200_API int rtdl_b200_prepare_fixed_radius_neighbors_3d(
+    const RtdlPoint3D* search_points, size_t search_count,
+    double max_radius,
+    void** prepared_out,
+    char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_run_prepared_fixed_radius_neighbors_3d (rtdl_optix_api.cpp:4173-4186). */
+RTDL_B200_API int rtdl_b200_run_prepared_fixed_radius_neighbors_3d(
+    void* prepared,
+    const RtdlPoint3D* query_points, size_t query_count,
+    double radius, size_t k_max,
+    RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out,
+    char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_destroy_prepared_fixed_radius_neighbors_3d (rtdl_optix_api.cpp:4432). */
+RTDL_B200_API void rtdl_b200_destroy_prepared_fixed_radius_neighbors_3d(void* prepared);
+
+/* ---- scenes of either dimension (new: the reference only prepares 3D FRN) --
+ * A scene is an LBVH built on the device over 2D or 3D search points.  One
+ * scene serves FRN, bounded KNN, KNN and nearest-distance calls. */
+
+/* dimension is 2 (points are RtdlPoint) or 3 (RtdlPoint3D).  points_on_device
+ * != 0 means `points` is a device pointer.  stream may be NULL (the library's
+ * own stream). */
+RTDL_B200_API int rtdl_b200_scene_create(
+    const void* points, size_t count, int dimension, int points_on_device,
+    void* stream, void** scene_out,
+    char* error_out, size_t error_size);
+
+RTDL_B200_API void rtdl_b200_scene_destroy(void* scene);
+
+/* Host-buffer call on a scene.  predicate: 0 = fixed_radius_neighbors
+ * (RtdlFixedRadiusNeighborRow rows), 1 = bounded_knn_rows and 2 = knn_rows
+ * (RtdlKnnNeighborRow rows).  `limit` is k_max (0, 1) or k (2); radius is
+ * ignored for knn_rows.  overflow_out (optional, query_count bytes, query
+ * input order) receives 1 where a query had more than k_max neighbors inside
+ * the radius (the rows still hold the k_max nearest). */
+RTDL_B200_API int rtdl_b200_scene_query(
+    void* scene, const void* query_points, size_t query_count,
+    int predicate, double radius, size_t limit,
+    void** rows_out, size_t* row_count_out, uint8_t* overflow_out,
+    char* error_out, size_t error_size);
+
+/* Device-resident call: query points, rows and flags live in device memory
+ * and the work is enqueued on `stream`; no host buffer is touched.  Rows
+ * beyond rows_capacity are not written; *row_count_out receives the full row
+ * count, so a caller whose capacity was too small retries with more.
+ * overflow_dev (optional) receives one byte per query (query input order). */
+RTDL_B200_API int rtdl_b200_scene_query_device(
+    void* scene, const void* query_points_dev, size_t query_count,
+    int predicate, double radius, size_t limit,
+    void* rows_dev, size_t rows_capacity, size_t* row_count_out,
+    uint8_t* overflow_dev, void* stream,
+    char* error_out, size_t error_size);
+
+/* Directed nearest-distance reduction (Hausdorff).  For every query the exact
+ * nearest (distance, neighbor_id) of knn_rows(k=1); then the witness is the
+ * maximum of (distance, -query_id, -neighbor_id) over all queries, the rule of
+ * examples/v2_0/research_benchmarks/hausdorff_xhd/rtdl_hausdorff_distance_app.py:108-130,
+ * reduced on the device in FP64.  nearest_distance_out / nearest_id_out are
+ * optional host arrays of query_count entries in query input order. */
+RTDL_B200_API int rtdl_b200_scene_directed_hausdorff(
+    void* scene, const void* query_points, size_t query_count,
+    double* distance_out, uint32_t* source_id_out, uint32_t* target_id_out,
+    double* nearest_distance_out, uint32_t* nearest_id_out,
+    char* error_out, size_t error_size);
+
+/* Phase timings of the last call on this thread, in milliseconds (device
+ * events).  Mirrors rtdl_optix_fixed_radius_neighbors_3d_get_last_phase_timings
+ * (src/rtdsl/optix_runtime.py:4916, 5029-5106).  Fills up to `capacity`
+ * (name, value) pairs; returns the number of phases. */
+RTDL_B200_API int rtdl_b200_get_last_phase_timings(const char** names_out, double* values_ms_out, int capacity);
+
+/* Tuning knobs (leaf size, threads per block); the autotuner sets these.
+ * Returns 0 on success. */
+RTDL_B200_API int rtdl_b200_set_tuning(int leaf_size, int block_threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTDL_B200_H */

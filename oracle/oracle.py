@@ -1,0 +1,235 @@
+"""ctypes wrapper over the CPU restatement in ``nn_oracle.c`` (test infrastructure).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+import this module.  It is the checker, never the product: the CUDA backend
+(``rtdl_b200``) does not import it.
+
+The semantics restate ``src/rtdsl/reference.py:349-434`` and ``:882-890`` of
+rubaolee/rtdl (see the header of ``nn_oracle.c`` for the line-by-line mapping).
+Inputs are numpy columns; outputs are numpy structured arrays whose dtypes
+match the reference ABI rows ``RtdlFixedRadiusNeighborRow`` {u32, u32, f64}
+and ``RtdlKnnNeighborRow`` {u32, u32, f64, u32}
+(``src/native/optix/rtdl_optix_prelude.h:254-295``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libnn_oracle.so"
+REF_LIB_PATH = HERE / "_ref" / "librtdl_oracle.so"
+
+FRN_ROW_DTYPE = np.dtype(
+    {"names": ["query_id", "neighbor_id", "distance"], "formats": ["<u4", "<u4", "<f8"], "offsets": [0, 4, 8], "itemsize": 16}
+)
+KNN_ROW_DTYPE = np.dtype(
+    {
+        "names": ["query_id", "neighbor_id", "distance", "neighbor_rank"],
+        "formats": ["<u4", "<u4", "<f8", "<u4"],
+        "offsets": [0, 4, 8, 16],
+        "itemsize": 24,
+    }
+)
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile ``libnn_oracle.so`` (and the reference's own oracle when its tree is present)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+    ref_root = os.environ.get("RTDL_REFERENCE_ROOT", "/root/reference")
+    if Path(ref_root, "src", "native", "rtdl_oracle.cpp").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={ref_root}"], check=True)
+    return LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        build()
+    lib = ctypes.CDLL(str(LIB_PATH))
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    f64p = ctypes.POINTER(ctypes.c_double)
+    lib.nn_oracle_rows.argtypes = [
+        u32p, f64p, f64p, f64p, ctypes.c_size_t,
+        u32p, f64p, f64p, f64p, ctypes.c_size_t,
+        ctypes.c_int, ctypes.c_double, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+        ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t), u32p,
+    ]
+    lib.nn_oracle_rows.restype = ctypes.c_int
+    lib.nn_oracle_nearest.argtypes = [
+        u32p, f64p, f64p, f64p, ctypes.c_size_t,
+        u32p, f64p, f64p, f64p, ctypes.c_size_t,
+        ctypes.c_int, f64p, u32p,
+    ]
+    lib.nn_oracle_nearest.restype = ctypes.c_int
+    lib.nn_oracle_free.argtypes = [ctypes.c_void_p]
+    lib.nn_oracle_free.restype = None
+    _lib = lib
+    return lib
+
+
+def _columns(points):
+    """Accepts an (n, 2|3) float array plus ids, or a dict with id/x/y[/z]."""
+    ids = np.ascontiguousarray(points["id"], dtype=np.uint32)
+    x = np.ascontiguousarray(points["x"], dtype=np.float64)
+    y = np.ascontiguousarray(points["y"], dtype=np.float64)
+    z = points.get("z") if isinstance(points, dict) else (points["z"] if "z" in points.dtype.names else None)
+    z = None if z is None else np.ascontiguousarray(z, dtype=np.float64)
+    return ids, x, y, z
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return ctypes.cast(None, ctypes.POINTER(ctype))
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def _call_rows(query, search, mode, radius, k, ranked, threads, want_counts):
+    lib = _load()
+    qid, qx, qy, qz = _columns(query)
+    sid, sx, sy, sz = _columns(search)
+    if (qz is None) != (sz is None):
+        raise ValueError("query and search sets must have the same dimension")
+    rows_ptr = ctypes.c_void_p()
+    count = ctypes.c_size_t()
+    counts = np.zeros(len(qid), dtype=np.uint32) if want_counts else None
+    status = lib.nn_oracle_rows(
+        _ptr(qid, ctypes.c_uint32), _ptr(qx, ctypes.c_double), _ptr(qy, ctypes.c_double), _ptr(qz, ctypes.c_double), len(qid),
+        _ptr(sid, ctypes.c_uint32), _ptr(sx, ctypes.c_double), _ptr(sy, ctypes.c_double), _ptr(sz, ctypes.c_double), len(sid),
+        mode, float(radius), int(k), int(ranked), int(threads),
+        ctypes.byref(rows_ptr), ctypes.byref(count), _ptr(counts, ctypes.c_uint32),
+    )
+    if status != 0:
+        raise RuntimeError("nn_oracle_rows failed (out of memory)")
+    dtype = KNN_ROW_DTYPE if ranked else FRN_ROW_DTYPE
+    n = count.value
+    try:
+        if n:
+            buf = (ctypes.c_char * (n * dtype.itemsize)).from_address(rows_ptr.value)
+            rows = np.frombuffer(buf, dtype=dtype).copy()
+        else:
+            rows = np.zeros(0, dtype=dtype)
+    finally:
+        lib.nn_oracle_free(rows_ptr)
+    return (rows, counts) if want_counts else rows
+
+
+def fixed_radius_neighbors(query, search, *, radius, k_max, threads=1, ranked=False, with_counts=False):
+    """FRN rows (``reference.py:349-376``); ``ranked=True`` gives bounded_knn_rows (``:406-434``)."""
+    return _call_rows(query, search, 0, radius, k_max, ranked, threads, with_counts)
+
+
+def knn_rows(query, search, *, k, threads=1):
+    """KNN rows (``reference.py:379-403``)."""
+    return _call_rows(query, search, 1, 0.0, k, True, threads, False)
+
+
+def nearest(query, search, *, threads=1):
+    """Per-query nearest (distance, neighbor_id) in query-input order (knn_rows with k=1)."""
+    lib = _load()
+    qid, qx, qy, qz = _columns(query)
+    sid, sx, sy, sz = _columns(search)
+    dist = np.zeros(len(qid), dtype=np.float64)
+    nid = np.zeros(len(qid), dtype=np.uint32)
+    status = lib.nn_oracle_nearest(
+        _ptr(qid, ctypes.c_uint32), _ptr(qx, ctypes.c_double), _ptr(qy, ctypes.c_double), _ptr(qz, ctypes.c_double), len(qid),
+        _ptr(sid, ctypes.c_uint32), _ptr(sx, ctypes.c_double), _ptr(sy, ctypes.c_double), _ptr(sz, ctypes.c_double), len(sid),
+        int(threads), _ptr(dist, ctypes.c_double), _ptr(nid, ctypes.c_uint32),
+    )
+    if status != 0:
+        raise RuntimeError("nn_oracle_nearest failed")
+    return dist, nid
+
+
+def directed_hausdorff(query, search, *, threads=1):
+    """Directed Hausdorff witness: max over queries of (distance, -query_id, -neighbor_id).
+
+    Follows ``examples/v2_0/research_benchmarks/hausdorff_xhd/rtdl_hausdorff_distance_app.py:108-130``.
+    """
+    dist, nid = nearest(query, search, threads=threads)
+    qid = np.asarray(query["id"], dtype=np.uint32)
+    order = np.lexsort((nid.astype(np.int64), qid.astype(np.int64), -dist))
+    best = order[0]
+    return {"distance": float(dist[best]), "source_id": int(qid[best]), "target_id": int(nid[best]), "row_count": int(len(qid))}
+
+
+# --- the reference's own native oracle (compiled from its sources into _ref/) ---------------
+
+class _RefPoint3D(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint32), ("x", ctypes.c_double), ("y", ctypes.c_double), ("z", ctypes.c_double)]
+
+
+class _RefPoint2D(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint32), ("x", ctypes.c_double), ("y", ctypes.c_double)]
+
+
+def reference_library_available() -> bool:
+    return REF_LIB_PATH.exists()
+
+
+_ref_lib = None
+
+
+def _load_ref():
+    global _ref_lib
+    if _ref_lib is None:
+        lib = ctypes.CDLL(str(REF_LIB_PATH))
+        for name in ("rtdl_oracle_run_fixed_radius_neighbors_3d", "rtdl_oracle_run_fixed_radius_neighbors"):
+            fn = getattr(lib, name)
+            fn.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_double,
+                           ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t),
+                           ctypes.c_char_p, ctypes.c_size_t]
+            fn.restype = ctypes.c_int
+        for name in ("rtdl_oracle_run_k_closest_hits_3d", "rtdl_oracle_run_k_closest_hits"):
+            fn = getattr(lib, name)
+            fn.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32,
+                           ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t), ctypes.c_char_p, ctypes.c_size_t]
+            fn.restype = ctypes.c_int
+        lib.rtdl_oracle_free_rows.argtypes = [ctypes.c_void_p]
+        lib.rtdl_oracle_free_rows.restype = None
+        _ref_lib = lib
+    return _ref_lib
+
+
+def pack_reference_points(points):
+    """numpy columns -> ctypes array of the reference's RtdlPoint / RtdlPoint3D."""
+    ids, x, y, z = _columns(points)
+    if z is None:
+        arr = (_RefPoint2D * len(ids))()
+        view = np.frombuffer(arr, dtype=np.dtype({"names": ["id", "x", "y"], "formats": ["<u4", "<f8", "<f8"], "offsets": [0, 8, 16], "itemsize": 24}))
+        view["id"], view["x"], view["y"] = ids, x, y
+    else:
+        arr = (_RefPoint3D * len(ids))()
+        view = np.frombuffer(arr, dtype=np.dtype({"names": ["id", "x", "y", "z"], "formats": ["<u4", "<f8", "<f8", "<f8"], "offsets": [0, 8, 16, 24], "itemsize": 32}))
+        view["id"], view["x"], view["y"], view["z"] = ids, x, y, z
+    return arr, len(ids), z is not None
+
+
+def reference_fixed_radius_neighbors(packed_query, packed_search, *, radius, k_max):
+    """One call of the reference's native ``rtdl_oracle_run_fixed_radius_neighbors[_3d]``
+    (``src/native/oracle/rtdl_oracle_api.cpp:900-1023``).  Releases the GIL (ctypes)."""
+    lib = _load_ref()
+    qarr, nq, is3d = packed_query
+    sarr, ns, _ = packed_search
+    fn = lib.rtdl_oracle_run_fixed_radius_neighbors_3d if is3d else lib.rtdl_oracle_run_fixed_radius_neighbors
+    rows = ctypes.c_void_p()
+    count = ctypes.c_size_t()
+    err = ctypes.create_string_buffer(4096)
+    status = fn(ctypes.addressof(qarr), nq, ctypes.addressof(sarr), ns, float(radius), int(k_max),
+                ctypes.byref(rows), ctypes.byref(count), err, len(err))
+    if status != 0:
+        raise RuntimeError(err.value.decode())
+    try:
+        n = count.value
+        out = np.frombuffer((ctypes.c_char * (n * 16)).from_address(rows.value), dtype=FRN_ROW_DTYPE).copy() if n else np.zeros(0, FRN_ROW_DTYPE)
+    finally:
+        lib.rtdl_oracle_free_rows(rows)
+    return out

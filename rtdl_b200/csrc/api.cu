@@ -1,0 +1,592 @@
+// api.cu -- the C ABI of librtdl_b200.so (declared in include/rtdl_b200.h).
+//
+// Every entry point follows the reference's native-call convention
+// (rubaolee/rtdl src/native/optix/rtdl_optix_core.cpp:58-66): exceptions are
+// caught at the boundary and turned into status 1 plus a message.
+// Device memory comes from the stream-ordered allocator with the release
+// threshold raised, so repeated calls reuse pooled memory without OS calls.
+// Rows handed to the caller live in pinned host buffers from a small pool, so
+// the device-to-host copy runs at full PCIe rate; rtdl_b200_free_rows returns
+// them to the pool.
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace rtdl_b200 {
+
+Tuning& tuning() {
+  static Tuning t;
+  return t;
+}
+
+void ensure_pool_configured(int device) {
+  static std::mutex m;
+  static std::vector<bool> done;
+  std::lock_guard<std::mutex> g(m);
+  if ((int)done.size() <= device) done.resize(device + 1, false);
+  if (done[device]) return;
+  cudaMemPool_t pool;
+  RTDL_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t threshold = UINT64_MAX;
+  RTDL_CUDA_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+  done[device] = true;
+}
+
+void* dev_alloc(size_t bytes, cudaStream_t s) {
+  if (bytes == 0) bytes = 16;
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, bytes, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw std::runtime_error("device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+  }
+  return p;
+}
+
+void dev_free(void* p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
+namespace {
+
+thread_local std::vector<std::pair<const char*, double>> g_last_timings;
+
+}  // namespace
+
+PhaseTimer::PhaseTimer(cudaStream_t s) : stream(s) {}
+PhaseTimer::~PhaseTimer() {
+  for (auto& m : marks) cudaEventDestroy(m.second);
+}
+void PhaseTimer::mark(const char* name) {
+  cudaEvent_t e;
+  RTDL_CUDA_CHECK(cudaEventCreate(&e));
+  RTDL_CUDA_CHECK(cudaEventRecord(e, stream));
+  marks.emplace_back(name, e);
+}
+void PhaseTimer::publish() {
+  g_last_timings.clear();
+  double total = 0.0;
+  for (size_t i = 1; i < marks.size(); ++i) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, marks[i - 1].second, marks[i].second) != cudaSuccess) {
+      cudaGetLastError();
+      ms = 0.f;
+    }
+    g_last_timings.emplace_back(marks[i].first, (double)ms);
+    total += ms;
+  }
+  g_last_timings.emplace_back("total", total);
+}
+
+namespace {
+
+// Pinned host buffers for returned rows.
+class PinnedPool {
+ public:
+  void* get(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    {
+      std::lock_guard<std::mutex> g(m_);
+      auto it = free_.lower_bound(bytes);
+      if (it != free_.end() && it->first <= 2 * bytes + (4u << 20)) {
+        void* p = it->second;
+        cached_ -= it->first;
+        live_[p] = it->first;
+        free_.erase(it);
+        return p;
+      }
+    }
+    const size_t rounded = (bytes + (2u << 20) - 1) & ~((size_t)(2u << 20) - 1);
+    void* p = nullptr;
+    if (cudaMallocHost(&p, rounded) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    std::lock_guard<std::mutex> g(m_);
+    live_[p] = rounded;
+    return p;
+  }
+  bool put(void* p) {
+    std::lock_guard<std::mutex> g(m_);
+    auto it = live_.find(p);
+    if (it == live_.end()) return false;
+    const size_t sz = it->second;
+    live_.erase(it);
+    if (cached_ + sz > limit()) {
+      cudaFreeHost(p);
+    } else {
+      free_.emplace(sz, p);
+      cached_ += sz;
+    }
+    return true;
+  }
+
+ private:
+  static size_t limit() {
+    static size_t lim = [] {
+      const char* env = std::getenv("RTDL_B200_PINNED_POOL_MB");
+      return (size_t)(env ? std::atoll(env) : 8192) << 20;
+    }();
+    return lim;
+  }
+  std::mutex m_;
+  std::multimap<size_t, void*> free_;
+  std::unordered_map<void*, size_t> live_;
+  size_t cached_ = 0;
+};
+
+PinnedPool& pinned_pool() {
+  static PinnedPool* p = new PinnedPool();  // never destroyed: outlives static teardown order
+  return *p;
+}
+
+cudaStream_t library_stream() {
+  static std::mutex m;
+  static std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  RTDL_CUDA_CHECK(cudaGetDevice(&dev));
+  ensure_pool_configured(dev);
+  std::lock_guard<std::mutex> g(m);
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s;
+  RTDL_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  streams[dev] = s;
+  return s;
+}
+
+void set_error(const char* msg, char* error_out, size_t error_size) {
+  if (!error_out || error_size == 0) return;
+  std::strncpy(error_out, msg, error_size - 1);
+  error_out[error_size - 1] = '\0';
+}
+
+template <typename Fn>
+int guarded(Fn&& fn, char* error_out, size_t error_size) {
+  try {
+    if (error_out && error_size) error_out[0] = '\0';
+    fn();
+    return 0;
+  } catch (const std::exception& ex) {
+    set_error(ex.what(), error_out, error_size);
+    return 1;
+  } catch (...) {
+    set_error("unknown native error", error_out, error_size);
+    return 1;
+  }
+}
+
+size_t record_size(int dim) { return dim == 3 ? sizeof(RtdlPoint3D) : sizeof(RtdlPoint); }
+
+void* upload(const void* host, size_t bytes, cudaStream_t s) {
+  void* d = dev_alloc(bytes, s);
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, s));
+  return d;
+}
+
+// Downloads `bytes` of device rows into a caller-owned host buffer.
+void* download_rows(const void* d_rows, size_t bytes, cudaStream_t s) {
+  void* host = pinned_pool().get(bytes);
+  bool pinned = host != nullptr;
+  if (!pinned) {
+    host = std::malloc(bytes ? bytes : 1);
+    if (!host) throw std::runtime_error("host allocation of rows failed");
+  }
+  if (bytes) {
+    cudaError_t e = cudaMemcpyAsync(host, d_rows, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      if (pinned) pinned_pool().put(host);
+      else std::free(host);
+      throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e) + " while downloading rows");
+    }
+  }
+  return host;
+}
+
+void validate_common(double radius, size_t limit, size_t nq, size_t ns, bool has_radius, const char* what,
+                     const char* limit_name) {
+  if (has_radius && !(radius >= 0.0))
+    throw std::runtime_error(std::string(what) + " radius must be non-negative");
+  if (limit == 0) throw std::runtime_error(std::string(what) + " " + limit_name + " must be positive");
+  if (nq > (size_t)UINT32_MAX) throw std::runtime_error(std::string(what) + " query_count exceeds uint32 limit");
+  if (ns > (size_t)UINT32_MAX) throw std::runtime_error(std::string(what) + " search_count exceeds uint32 limit");
+  if (limit > (size_t)UINT32_MAX)
+    throw std::runtime_error(std::string(what) + " " + limit_name + " exceeds uint32 limit");
+}
+
+// Plain per-call launch: upload, build, query, download.
+void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim, int predicate, double radius,
+                   size_t limit, void** rows_out, size_t* row_count_out) {
+  cudaStream_t s = library_stream();
+  PhaseTimer timer(s);
+  timer.mark("begin");
+  const size_t rec = record_size(dim);
+  void* d_search = upload(sp, rec * ns, s);
+  void* d_query = upload(q, rec * nq, s);
+  timer.mark("upload");
+  Scene* sc = nullptr;
+  void* d_rows = nullptr;
+  try {
+    sc = build_scene(d_search, (uint32_t)ns, dim, s, tuning().leaf_size);
+    timer.mark("build");
+    QueryResult r = run_query(sc, d_query, (uint32_t)nq, predicate, radius, (uint32_t)limit, nullptr, 0, &d_rows,
+                              nullptr, s, &timer);
+    const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
+    void* host = download_rows(d_rows, row_size * r.rows, s);
+    timer.mark("download");
+    timer.publish();
+    *rows_out = host;
+    *row_count_out = (size_t)r.rows;
+  } catch (...) {
+    dev_free(d_rows, s);
+    destroy_scene(sc);
+    dev_free(d_search, s);
+    dev_free(d_query, s);
+    cudaStreamSynchronize(s);
+    throw;
+  }
+  dev_free(d_rows, s);
+  destroy_scene(sc);
+  dev_free(d_search, s);
+  dev_free(d_query, s);
+}
+
+struct PreparedHandle {
+  Scene* scene;
+  int dim;
+};
+
+}  // namespace
+}  // namespace rtdl_b200
+
+using namespace rtdl_b200;
+
+extern "C" {
+
+int rtdl_b200_get_version(int* major, int* minor, int* patch) {
+  if (major) *major = 0;
+  if (minor) *minor = 1;
+  if (patch) *patch = 0;
+  return 0;
+}
+
+int rtdl_b200_set_device(int device) {
+  return cudaSetDevice(device) == cudaSuccess ? 0 : 1;
+}
+
+int rtdl_b200_set_tuning(int leaf_size, int block_threads) {
+  if (leaf_size < 1 || leaf_size > 32) return 1;
+  if (block_threads != 64 && block_threads != 128 && block_threads != 256) return 1;
+  tuning().leaf_size = leaf_size;
+  tuning().block_threads = block_threads;
+  return 0;
+}
+
+int rtdl_b200_get_last_phase_timings(const char** names_out, double* values_ms_out, int capacity) {
+  const int n = (int)g_last_timings.size();
+  for (int i = 0; i < n && i < capacity; ++i) {
+    if (names_out) names_out[i] = g_last_timings[i].first;
+    if (values_ms_out) values_ms_out[i] = g_last_timings[i].second;
+  }
+  return n;
+}
+
+void rtdl_b200_free_rows(void* rows) {
+  if (!rows) return;
+  if (!pinned_pool().put(rows)) std::free(rows);
+}
+
+int rtdl_b200_run_fixed_radius_neighbors(const RtdlPoint* query_points, size_t query_count,
+                                         const RtdlPoint* search_points, size_t search_count, double radius,
+                                         size_t k_max, RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out,
+                                         char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    validate_common(radius, k_max, query_count, search_count, true, "fixed_radius_neighbors", "k_max");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || search_count == 0) return;
+    run_rows_call(query_points, query_count, search_points, search_count, 2, kFrn, radius, k_max,
+                  reinterpret_cast<void**>(rows_out), row_count_out);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_fixed_radius_neighbors_3d(const RtdlPoint3D* query_points, size_t query_count,
+                                            const RtdlPoint3D* search_points, size_t search_count, double radius,
+                                            size_t k_max, RtdlFixedRadiusNeighborRow** rows_out,
+                                            size_t* row_count_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    validate_common(radius, k_max, query_count, search_count, true, "fixed_radius_neighbors", "k_max");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || search_count == 0) return;
+    run_rows_call(query_points, query_count, search_points, search_count, 3, kFrn, radius, k_max,
+                  reinterpret_cast<void**>(rows_out), row_count_out);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_bounded_knn_rows(const RtdlPoint* query_points, size_t query_count, const RtdlPoint* search_points,
+                                   size_t search_count, double radius, size_t k_max, RtdlKnnNeighborRow** rows_out,
+                                   size_t* row_count_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    validate_common(radius, k_max, query_count, search_count, true, "bounded_knn_rows", "k_max");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || search_count == 0) return;
+    run_rows_call(query_points, query_count, search_points, search_count, 2, kBounded, radius, k_max,
+                  reinterpret_cast<void**>(rows_out), row_count_out);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_bounded_knn_rows_3d(const RtdlPoint3D* query_points, size_t query_count,
+                                      const RtdlPoint3D* search_points, size_t search_count, double radius,
+                                      size_t k_max, RtdlKnnNeighborRow** rows_out, size_t* row_count_out,
+                                      char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    validate_common(radius, k_max, query_count, search_count, true, "bounded_knn_rows", "k_max");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || search_count == 0) return;
+    run_rows_call(query_points, query_count, search_points, search_count, 3, kBounded, radius, k_max,
+                  reinterpret_cast<void**>(rows_out), row_count_out);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_k_closest_hits(const RtdlPoint* query_points, size_t query_count, const RtdlPoint* search_points,
+                                 size_t search_count, size_t k, RtdlKnnNeighborRow** rows_out, size_t* row_count_out,
+                                 char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    validate_common(0.0, k, query_count, search_count, false, "knn_rows", "k");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || search_count == 0) return;
+    run_rows_call(query_points, query_count, search_points, search_count, 2, kKnn, 0.0, k,
+                  reinterpret_cast<void**>(rows_out), row_count_out);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_k_closest_hits_3d(const RtdlPoint3D* query_points, size_t query_count,
+                                    const RtdlPoint3D* search_points, size_t search_count, size_t k,
+                                    RtdlKnnNeighborRow** rows_out, size_t* row_count_out, char* error_out,
+                                    size_t error_size) {
+  return guarded([&]() {
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    validate_common(0.0, k, query_count, search_count, false, "knn_rows", "k");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || search_count == 0) return;
+    run_rows_call(query_points, query_count, search_points, search_count, 3, kKnn, 0.0, k,
+                  reinterpret_cast<void**>(rows_out), row_count_out);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_scene_create(const void* points, size_t count, int dimension, int points_on_device, void* stream,
+                           void** scene_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!scene_out) throw std::runtime_error("scene_out must not be null");
+    *scene_out = nullptr;
+    if (dimension != 2 && dimension != 3) throw std::runtime_error("dimension must be 2 or 3");
+    if (!points && count != 0) throw std::runtime_error("points pointer must not be null when count is nonzero");
+    if (count > (size_t)UINT32_MAX) throw std::runtime_error("search_count exceeds uint32 limit");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : library_stream();
+    int dev = 0;
+    RTDL_CUDA_CHECK(cudaGetDevice(&dev));
+    ensure_pool_configured(dev);
+    const void* d_points = points;
+    void* owned = nullptr;
+    if (!points_on_device && count) {
+      owned = upload(points, record_size(dimension) * count, s);
+      d_points = owned;
+    }
+    Scene* sc = nullptr;
+    try {
+      sc = build_scene(d_points, (uint32_t)count, dimension, s, tuning().leaf_size);
+      unsigned int bad = 0;
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      if (bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+    } catch (...) {
+      destroy_scene(sc);
+      dev_free(owned, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(owned, s);
+    *scene_out = sc;
+  }, error_out, error_size);
+}
+
+void rtdl_b200_scene_destroy(void* scene) {
+  Scene* sc = static_cast<Scene*>(scene);
+  if (!sc) return;
+  cudaStream_t s = sc->stream;
+  destroy_scene(sc);
+  if (s) cudaStreamSynchronize(s);
+}
+
+int rtdl_b200_scene_query(void* scene, const void* query_points, size_t query_count, int predicate, double radius,
+                          size_t limit, void** rows_out, size_t* row_count_out, uint8_t* overflow_out,
+                          char* error_out, size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(scene);
+    if (!sc) throw std::runtime_error("scene must not be null");
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    if (predicate < 0 || predicate > 2) throw std::runtime_error("predicate must be 0, 1 or 2");
+    const char* what = predicate == kFrn ? "fixed_radius_neighbors" : predicate == kBounded ? "bounded_knn_rows" : "knn_rows";
+    validate_common(radius, limit, query_count, sc->n, predicate != kKnn, what, predicate == kKnn ? "k" : "k_max");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0) return;
+    if (!query_points) throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    cudaStream_t s = sc->stream;
+    PhaseTimer timer(s);
+    timer.mark("begin");
+    void* d_query = upload(query_points, record_size(sc->dim) * query_count, s);
+    uint8_t* d_overflow = overflow_out ? static_cast<uint8_t*>(dev_alloc(query_count, s)) : nullptr;
+    if (d_overflow) RTDL_CUDA_CHECK(cudaMemsetAsync(d_overflow, 0, query_count, s));
+    timer.mark("upload");
+    void* d_rows = nullptr;
+    try {
+      QueryResult r = run_query(sc, d_query, (uint32_t)query_count, predicate, radius, (uint32_t)limit, nullptr, 0,
+                                &d_rows, d_overflow, s, &timer);
+      const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
+      if (d_overflow) RTDL_CUDA_CHECK(cudaMemcpyAsync(overflow_out, d_overflow, query_count, cudaMemcpyDeviceToHost, s));
+      void* host = download_rows(d_rows, row_size * r.rows, s);
+      timer.mark("download");
+      timer.publish();
+      *rows_out = host;
+      *row_count_out = (size_t)r.rows;
+    } catch (...) {
+      dev_free(d_rows, s);
+      dev_free(d_query, s);
+      dev_free(d_overflow, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(d_rows, s);
+    dev_free(d_query, s);
+    dev_free(d_overflow, s);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_scene_query_device(void* scene, const void* query_points_dev, size_t query_count, int predicate,
+                                 double radius, size_t limit, void* rows_dev, size_t rows_capacity,
+                                 size_t* row_count_out, uint8_t* overflow_dev, void* stream, char* error_out,
+                                 size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(scene);
+    if (!sc) throw std::runtime_error("scene must not be null");
+    if (!row_count_out) throw std::runtime_error("row_count_out must not be null");
+    if (predicate < 0 || predicate > 2) throw std::runtime_error("predicate must be 0, 1 or 2");
+    const char* what = predicate == kFrn ? "fixed_radius_neighbors" : predicate == kBounded ? "bounded_knn_rows" : "knn_rows";
+    validate_common(radius, limit, query_count, sc->n, predicate != kKnn, what, predicate == kKnn ? "k" : "k_max");
+    *row_count_out = 0;
+    if (query_count == 0) return;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sc->stream;
+    PhaseTimer timer(s);
+    QueryResult r = run_query(sc, query_points_dev, (uint32_t)query_count, predicate, radius, (uint32_t)limit,
+                              rows_dev, rows_capacity, nullptr, overflow_dev, s, &timer);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    timer.publish();
+    *row_count_out = (size_t)r.rows;
+  }, error_out, error_size);
+}
+
+int rtdl_b200_scene_directed_hausdorff(void* scene, const void* query_points, size_t query_count,
+                                       double* distance_out, uint32_t* source_id_out, uint32_t* target_id_out,
+                                       double* nearest_distance_out, uint32_t* nearest_id_out, char* error_out,
+                                       size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(scene);
+    if (!sc) throw std::runtime_error("scene must not be null");
+    if (query_count > (size_t)UINT32_MAX) throw std::runtime_error("query_count exceeds uint32 limit");
+    if (query_count == 0 || sc->n == 0) throw std::runtime_error("Hausdorff distance requires non-empty point sets");
+    cudaStream_t s = sc->stream;
+    PhaseTimer timer(s);
+    timer.mark("begin");
+    void* d_query = upload(query_points, record_size(sc->dim) * query_count, s);
+    double* d_nd = nearest_distance_out ? static_cast<double*>(dev_alloc(sizeof(double) * query_count, s)) : nullptr;
+    uint32_t* d_ni = nearest_id_out ? static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * query_count, s)) : nullptr;
+    timer.mark("upload");
+    try {
+      HausdorffResult h = run_directed_hausdorff(sc, d_query, (uint32_t)query_count, d_nd, d_ni, s, &timer);
+      if (d_nd) RTDL_CUDA_CHECK(cudaMemcpyAsync(nearest_distance_out, d_nd, sizeof(double) * query_count, cudaMemcpyDeviceToHost, s));
+      if (d_ni) RTDL_CUDA_CHECK(cudaMemcpyAsync(nearest_id_out, d_ni, sizeof(uint32_t) * query_count, cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      timer.mark("download");
+      timer.publish();
+      if (distance_out) *distance_out = h.distance;
+      if (source_id_out) *source_id_out = h.source_id;
+      if (target_id_out) *target_id_out = h.target_id;
+    } catch (...) {
+      dev_free(d_query, s);
+      dev_free(d_nd, s);
+      dev_free(d_ni, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(d_query, s);
+    dev_free(d_nd, s);
+    dev_free(d_ni, s);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_prepare_fixed_radius_neighbors_3d(const RtdlPoint3D* search_points, size_t search_count,
+                                                double max_radius, void** prepared_out, char* error_out,
+                                                size_t error_size) {
+  return guarded([&]() {
+    if (!prepared_out) throw std::runtime_error("prepared_out must not be null");
+    if (!search_points && search_count != 0)
+      throw std::runtime_error("search_points pointer must not be null when search_count is nonzero");
+    if (!(max_radius > 0.0)) throw std::runtime_error("fixed_radius_neighbors_3d max_radius must be positive");
+    if (search_count > (size_t)UINT32_MAX)
+      throw std::runtime_error("fixed_radius_neighbors_3d search_count exceeds uint32 limit");
+    *prepared_out = nullptr;
+    void* scene = nullptr;
+    char err[1024];
+    if (rtdl_b200_scene_create(search_points, search_count, 3, 0, nullptr, &scene, err, sizeof(err)) != 0)
+      throw std::runtime_error(err);
+    static_cast<Scene*>(scene)->max_radius = max_radius;
+    *prepared_out = scene;
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_prepared_fixed_radius_neighbors_3d(void* prepared, const RtdlPoint3D* query_points,
+                                                     size_t query_count, double radius, size_t k_max,
+                                                     RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out,
+                                                     char* error_out, size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(prepared);
+    if (!sc) throw std::runtime_error("prepared handle must not be null");
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    validate_common(radius, k_max, query_count, sc->n, true, "fixed_radius_neighbors_3d", "k_max");
+    if (sc->dim != 3) throw std::runtime_error("prepared scene is not 3D");
+    // same tolerance as the reference (rtdl_optix_workloads.cpp:15629-15631)
+    if (radius > sc->max_radius + 1.0e-7)
+      throw std::runtime_error("fixed_radius_neighbors_3d radius exceeds prepared max_radius");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || sc->n == 0) return;
+    char err[1024];
+    void* rows = nullptr;
+    if (rtdl_b200_scene_query(sc, query_points, query_count, kFrn, radius, k_max, &rows, row_count_out, nullptr, err,
+                              sizeof(err)) != 0)
+      throw std::runtime_error(err);
+    *rows_out = static_cast<RtdlFixedRadiusNeighborRow*>(rows);
+  }, error_out, error_size);
+}
+
+void rtdl_b200_destroy_prepared_fixed_radius_neighbors_3d(void* prepared) { rtdl_b200_scene_destroy(prepared); }
+
+}  // extern "C"

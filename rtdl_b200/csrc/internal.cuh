@@ -1,0 +1,178 @@
+// internal.cuh -- shared declarations of librtdl_b200 (device structures,
+// launch helpers and the host-side plumbing every translation unit uses).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/rtdl_b200.h"
+
+namespace rtdl_b200 {
+
+#define RTDL_CUDA_CHECK(call)                                                          \
+  do {                                                                                 \
+    cudaError_t _e = (call);                                                           \
+    if (_e != cudaSuccess)                                                             \
+      throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(_e) + \
+                               " at " #call);                                          \
+  } while (0)
+
+constexpr int kSmCount = 148;          // B200: 2 dies x 74 SMs
+constexpr int kMaxList = 64;           // per-query list capacity held in shared memory
+constexpr int kStackDepth = 64;        // traversal stack; Karras depth <= 30 code bits + 32 index bits
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// ---- reductions over an input point set ------------------------------------
+// Min/max use an order-preserving uint encoding of the float bits.
+struct PointStats {
+  unsigned int lo[3];
+  unsigned int hi[3];
+  unsigned long long max_abs_bits;  // bits of the largest |coordinate| (double)
+  unsigned int inexact;             // a coordinate is not exactly representable in FP32
+  unsigned int bad;                 // non-finite or |coordinate| > kMaxCoordinate
+  unsigned int ids_unsorted;        // ids decrease somewhere in input order
+  unsigned int pad;
+};
+constexpr double kMaxCoordinate = 1.0e18;
+
+__host__ __device__ inline unsigned int float_to_ordered(float f) {
+#ifdef __CUDA_ARCH__
+  unsigned int b = __float_as_uint(f);
+#else
+  unsigned int b;
+  memcpy(&b, &f, 4);
+#endif
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__host__ __device__ inline float ordered_to_float(unsigned int o) {
+  unsigned int b = (o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o;
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(b);
+#else
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+#endif
+}
+
+// ---- a built scene (LBVH over the search points) ---------------------------
+// Node layout: 4 x float4 = 64 B, both children's boxes in the parent so one
+// visit tests two children with two coalesced 32-B reads.
+//   n[0] = {c0.lo.xyz, c0.ref}  n[1] = {c0.hi.xyz, c0.cnt}
+//   n[2] = {c1.lo.xyz, c1.ref}  n[3] = {c1.hi.xyz, c1.cnt}
+// cnt == 0: ref is an internal node index; cnt > 0: a leaf bucket of cnt
+// consecutive sorted points starting at ref.
+struct SceneView {
+  const float4* pts;      // n sorted points: x, y, z (0 for 2D), w = record id bits
+  const uint32_t* perm;   // sorted index -> search input index
+  const double* pts64;    // 3 doubles per sorted point (exact coordinates), used when inexact
+  const float4* nodes;    // 4 float4 per internal node
+  int root_ref;
+  int root_cnt;           // > 0 when the whole scene is a single leaf
+  uint32_t n;
+  const unsigned int* inexact;  // device flag: scene coordinates are not all FP32-exact
+};
+
+struct Scene {
+  int dim = 3;
+  int device = 0;
+  uint32_t n = 0;
+  double max_radius = 0.0;  // prepared-FRN contract only
+  int root_ref = 0, root_cnt = 0;
+  int leaf_size = 8;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  float4* pts = nullptr;
+  uint32_t* perm = nullptr;
+  double* pts64 = nullptr;
+  float4* nodes = nullptr;
+  PointStats* stats = nullptr;  // device copy of the build statistics
+  SceneView view() const {
+    SceneView v;
+    v.pts = pts;
+    v.perm = perm;
+    v.pts64 = pts64;
+    v.nodes = nodes;
+    v.root_ref = root_ref;
+    v.root_cnt = root_cnt;
+    v.n = n;
+    v.inexact = stats ? &stats->inexact : nullptr;
+    return v;
+  }
+};
+
+// ---- tuning ---------------------------------------------------------------
+struct Tuning {
+  int leaf_size = 8;
+  int block_threads = 128;
+};
+Tuning& tuning();
+
+// ---- phase timing (CUDA events, read after the call's final sync) ----------
+struct PhaseTimer {
+  cudaStream_t stream;
+  std::vector<std::pair<const char*, cudaEvent_t>> marks;
+  explicit PhaseTimer(cudaStream_t s);
+  ~PhaseTimer();
+  void mark(const char* name);
+  void publish();  // after a sync: converts to milliseconds for get_last_phase_timings
+};
+
+// ---- stream-ordered allocation (pooled: no OS calls after warm-up) --------
+void* dev_alloc(size_t bytes, cudaStream_t s);
+void dev_free(void* p, cudaStream_t s);
+void ensure_pool_configured(int device);
+
+// ---- sort / scan (sort_scan.cu) -------------------------------------------
+// Exclusive scan of `counts` (optionally gathered through `order`, or identity
+// when *identity_flag != 0) into out[0..n] (u64); out[n] is the total.
+void scan_counts_u64(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag,
+                     uint32_t n, unsigned long long* out, cudaStream_t s);
+// Stable LSD radix sort of (key, value) pairs over bits [begin_bit, end_bit),
+// 8 bits per pass.  The result is left in keys/vals.  When *skip_flag != 0
+// (device memory) every pass returns immediately and the input stays in place.
+void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int begin_bit, int end_bit,
+                      const unsigned int* skip_flag, cudaStream_t s);
+void iota_u32(uint32_t* out, uint32_t n, cudaStream_t s);
+
+// ---- scene build (lbvh.cu) -------------------------------------------------
+// `points` is a device AoS of RtdlPoint (dim 2) or RtdlPoint3D (dim 3).
+Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, int leaf_size);
+void destroy_scene(Scene* sc);
+// Converts AoS points to float4 (w = id bits) and accumulates statistics.
+void prep_points(const void* points_dev, uint32_t n, int dim, float4* out, PointStats* stats, cudaStream_t s);
+void reset_stats(PointStats* stats, cudaStream_t s);
+// 32-bit Morton codes relative to the box held in `box_stats` (clamped).
+void morton_codes(const float4* pts, uint32_t n, int dim, const PointStats* box_stats, uint32_t* codes,
+                  cudaStream_t s);
+
+// ---- queries (query.cu) -----------------------------------------------------
+enum Predicate { kFrn = 0, kBounded = 1, kKnn = 2 };
+
+struct QueryResult {
+  unsigned long long rows = 0;   // total rows
+  unsigned int heavy = 0;        // queries resolved by the generic path
+};
+
+// Runs a neighbor query on a scene.  All buffers are device buffers; rows are
+// written as RtdlFixedRadiusNeighborRow (kFrn) or RtdlKnnNeighborRow.  When
+// rows_dev is null the rows are only counted.  When alloc_rows is set, a
+// device buffer of exactly the row count is allocated into *rows_alloc.
+QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius,
+                      uint32_t limit, void* rows_dev, size_t rows_capacity, void** rows_alloc,
+                      uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer);
+
+struct HausdorffResult {
+  double distance;
+  uint32_t source_id, target_id;
+};
+HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint32_t nq, double* nearest_dist_dev,
+                                       uint32_t* nearest_id_dev, cudaStream_t s, PhaseTimer* timer);
+
+inline unsigned int div_up(unsigned long long a, unsigned long long b) { return (unsigned int)((a + b - 1) / b); }
+
+}  // namespace rtdl_b200

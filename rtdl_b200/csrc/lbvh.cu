@@ -1,0 +1,397 @@
+// lbvh.cu -- on-device LBVH over the search points.
+//
+// Build steps, all on one stream with no host round trip:
+//   1. prep:    AoS FP64 records (RtdlPoint / RtdlPoint3D) -> float4 {x, y, z, id}
+//               plus set statistics (box, largest |coordinate|, FP32
+//               exactness, finiteness, id order);
+//   2. morton:  30-bit (3D, 10 bits per axis) or 32-bit (2D, 16 bits per
+//               axis) codes relative to the set's box;
+//   3. sort:    stable radix sort of (code, input index) pairs (sort_scan.cu);
+//   4. gather:  points into code order (coalesced float4 stores); exact FP64
+//               coordinates alongside when the set is not FP32-exact;
+//   5. karras:  one thread per internal node finds its key range and split
+//               (Karras 2012, "Maximizing Parallelism in the Construction of
+//               BVHs, Octrees, and k-d Trees"; equal codes are split on the
+//               index, so duplicates are handled);
+//   6. refit:   bottom-up boxes, one thread per leaf, an atomic arrival
+//               counter per node lets the second child to arrive continue;
+//   7. pack:    64-B nodes holding both children's boxes; subtrees of at most
+//               leaf_size points become leaf buckets (contiguous point ranges).
+#include "internal.cuh"
+
+namespace rtdl_b200 {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kLeafFlag = 0x40000000;  // child is a single point (Karras leaf)
+
+inline unsigned int grid_for(uint64_t n, int threads = kThreads) {
+  uint64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  const uint64_t cap = (uint64_t)kSmCount * 16;
+  return (unsigned int)(b < cap ? b : cap);
+}
+
+template <int DIM>
+__global__ void k_prep(const double* __restrict__ raw, uint32_t n, float4* __restrict__ out,
+                       PointStats* __restrict__ st) {
+  constexpr int kStride = DIM == 3 ? 4 : 3;  // record size in doubles (id occupies the first slot)
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  double max_abs = 0.0;
+  unsigned int inexact = 0, bad = 0, unsorted = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double* r = raw + i * kStride;
+    const uint32_t id = *reinterpret_cast<const uint32_t*>(r);
+    double c[3] = {r[1], r[2], DIM == 3 ? r[3] : 0.0};
+    float f[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double v = c[a];
+      const double av = fabs(v);
+      if (!(av <= kMaxCoordinate)) bad = 1;  // also catches NaN
+      f[a] = __double2float_rn(v);
+      if ((double)f[a] != v) inexact = 1;
+      lo[a] = fminf(lo[a], f[a]);
+      hi[a] = fmaxf(hi[a], f[a]);
+      max_abs = fmax(max_abs, av);
+    }
+    if (i > 0) {
+      const uint32_t prev = *reinterpret_cast<const uint32_t*>(raw + (i - 1) * kStride);
+      if (id < prev) unsorted = 1;
+    }
+    out[i] = make_float4(f[0], f[1], f[2], __uint_as_float(id));
+  }
+  // warp reduction, then one set of atomics per warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+      hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+    }
+    max_abs = fmax(max_abs, __shfl_xor_sync(0xffffffffu, max_abs, o));
+    inexact |= __shfl_xor_sync(0xffffffffu, inexact, o);
+    bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    unsorted |= __shfl_xor_sync(0xffffffffu, unsorted, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (lo[a] <= hi[a]) {
+        atomicMin(&st->lo[a], float_to_ordered(lo[a]));
+        atomicMax(&st->hi[a], float_to_ordered(hi[a]));
+      }
+    }
+    atomicMax(&st->max_abs_bits, (unsigned long long)__double_as_longlong(max_abs));
+    if (inexact) atomicOr(&st->inexact, 1u);
+    if (bad) atomicOr(&st->bad, 1u);
+    if (unsorted) atomicOr(&st->ids_unsorted, 1u);
+  }
+}
+
+__global__ void k_reset_stats(PointStats* st) {
+  if (threadIdx.x == 0) {
+    for (int a = 0; a < 3; ++a) {
+      st->lo[a] = 0xFFFFFFFFu;
+      st->hi[a] = 0u;
+    }
+    st->max_abs_bits = 0ull;
+    st->inexact = 0u;
+    st->bad = 0u;
+    st->ids_unsorted = 0u;
+    st->pad = 0u;
+  }
+}
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {  // 10 bits -> every third bit
+  v &= 0x3FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__device__ __forceinline__ uint32_t spread16(uint32_t v) {  // 16 bits -> every other bit
+  v &= 0xFFFFu;
+  v = (v | (v << 8)) & 0x00FF00FFu;
+  v = (v | (v << 4)) & 0x0F0F0F0Fu;
+  v = (v | (v << 2)) & 0x33333333u;
+  v = (v | (v << 1)) & 0x55555555u;
+  return v;
+}
+
+__global__ void k_morton(const float4* __restrict__ pts, uint32_t n, int dim, const PointStats* __restrict__ box,
+                         uint32_t* __restrict__ codes) {
+  float lo[3], scale[3];
+  const float cells = dim == 3 ? 1023.0f : 65535.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const unsigned int ol = box->lo[a], oh = box->hi[a];
+    const bool empty = ol == 0xFFFFFFFFu;
+    const float l = empty ? 0.f : ordered_to_float(ol);
+    const float h = empty ? 0.f : ordered_to_float(oh);
+    lo[a] = l;
+    const float ext = h - l;
+    scale[a] = (ext > 0.f && isfinite(ext)) ? cells / ext : 0.f;
+  }
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float4 p = pts[i];
+    const float c[3] = {p.x, p.y, p.z};
+    uint32_t q[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float t = (c[a] - lo[a]) * scale[a];
+      t = fminf(fmaxf(t, 0.f), cells);
+      q[a] = (uint32_t)t;
+    }
+    codes[i] = dim == 3 ? (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2])
+                        : (spread16(q[0]) << 1) | spread16(q[1]);
+  }
+}
+
+template <int DIM>
+__global__ void k_gather(const float4* __restrict__ in, const double* __restrict__ raw, const uint32_t* __restrict__ perm,
+                         uint32_t n, float4* __restrict__ out, double* __restrict__ out64,
+                         const PointStats* __restrict__ st) {
+  constexpr int kStride = DIM == 3 ? 4 : 3;
+  const bool want64 = st->inexact != 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t src = perm[i];
+    out[i] = in[src];
+    if (want64) {
+      const double* r = raw + (uint64_t)src * kStride;
+      out64[3 * i + 0] = r[1];
+      out64[3 * i + 1] = r[2];
+      out64[3 * i + 2] = DIM == 3 ? r[3] : 0.0;
+    }
+  }
+}
+
+// Common-prefix length of the (code, index) keys of sorted positions i and j;
+// -1 outside [0, n).
+__device__ __forceinline__ int prefix_len(const uint32_t* __restrict__ codes, int64_t n, int64_t i, int64_t j) {
+  if (j < 0 || j >= n) return -1;
+  const uint32_t a = codes[i], b = codes[j];
+  if (a != b) return __clz(a ^ b);
+  return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+}
+
+__global__ void k_karras(const uint32_t* __restrict__ codes, uint32_t n, int* __restrict__ child_l,
+                         int* __restrict__ child_r, int* __restrict__ first, int* __restrict__ last,
+                         int* __restrict__ parent_int, int* __restrict__ parent_leaf) {
+  const int64_t nn = n;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn - 1; i += (int64_t)gridDim.x * blockDim.x) {
+    const int d = (prefix_len(codes, nn, i, i + 1) - prefix_len(codes, nn, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = prefix_len(codes, nn, i, i - d);
+    int64_t lmax = 2;
+    while (prefix_len(codes, nn, i, i + lmax * d) > dmin) lmax <<= 1;
+    int64_t l = 0;
+    for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
+      if (prefix_len(codes, nn, i, i + (l + t) * d) > dmin) l += t;
+    const int64_t j = i + l * d;
+    const int dnode = prefix_len(codes, nn, i, j);
+    int64_t s = 0;
+    int64_t t = l;
+    do {
+      t = (t + 1) >> 1;
+      if (prefix_len(codes, nn, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int64_t gamma = i + s * d + (d < 0 ? -1 : 0);
+    const int64_t lo = i < j ? i : j;
+    const int64_t hi = i < j ? j : i;
+    int cl, cr;
+    if (lo == gamma) {
+      cl = (int)gamma | kLeafFlag;
+      parent_leaf[gamma] = (int)i;
+    } else {
+      cl = (int)gamma;
+      parent_int[gamma] = (int)i;
+    }
+    if (hi == gamma + 1) {
+      cr = (int)(gamma + 1) | kLeafFlag;
+      parent_leaf[gamma + 1] = (int)i;
+    } else {
+      cr = (int)(gamma + 1);
+      parent_int[gamma + 1] = (int)i;
+    }
+    child_l[i] = cl;
+    child_r[i] = cr;
+    first[i] = (int)lo;
+    last[i] = (int)hi;
+  }
+}
+
+__device__ __forceinline__ void child_box(int c, const float4* __restrict__ pts, const float4* boxes, float4& lo,
+                                          float4& hi) {
+  if (c & kLeafFlag) {
+    const float4 p = pts[c & ~kLeafFlag];
+    lo = p;
+    hi = p;
+  } else {
+    lo = __ldcg(&boxes[2 * c]);
+    hi = __ldcg(&boxes[2 * c + 1]);
+  }
+}
+
+__global__ void k_refit(uint32_t n, const float4* __restrict__ pts, const int* __restrict__ child_l,
+                        const int* __restrict__ child_r, const int* __restrict__ parent_int,
+                        const int* __restrict__ parent_leaf, unsigned int* __restrict__ arrivals, float4* boxes) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    int p = parent_leaf[i];
+    while (p >= 0) {
+      __threadfence();
+      if (atomicAdd(&arrivals[p], 1u) == 0u) break;  // the sibling subtree is not finished yet
+      __threadfence();
+      float4 al, ah, bl, bh;
+      child_box(child_l[p], pts, boxes, al, ah);
+      child_box(child_r[p], pts, boxes, bl, bh);
+      const float4 lo = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.f);
+      const float4 hi = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.f);
+      __stcg(&boxes[2 * p], lo);
+      __stcg(&boxes[2 * p + 1], hi);
+      p = parent_int[p];
+    }
+  }
+}
+
+__global__ void k_pack(uint32_t n, const float4* __restrict__ pts, const int* __restrict__ child_l,
+                       const int* __restrict__ child_r, const int* __restrict__ first, const int* __restrict__ last,
+                       const float4* __restrict__ boxes, int leaf_size, float4* __restrict__ nodes) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int cs[2] = {child_l[i], child_r[i]};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int c = cs[k];
+      float4 lo, hi;
+      int ref, cnt;
+      if (c & kLeafFlag) {
+        const int p = c & ~kLeafFlag;
+        lo = pts[p];
+        hi = lo;
+        ref = p;
+        cnt = 1;
+      } else {
+        lo = boxes[2 * c];
+        hi = boxes[2 * c + 1];
+        const int count = last[c] - first[c] + 1;
+        if (count <= leaf_size) {
+          ref = first[c];
+          cnt = count;
+        } else {
+          ref = c;
+          cnt = 0;
+        }
+      }
+      nodes[4 * i + 2 * k] = make_float4(lo.x, lo.y, lo.z, __int_as_float(ref));
+      nodes[4 * i + 2 * k + 1] = make_float4(hi.x, hi.y, hi.z, __int_as_float(cnt));
+    }
+  }
+}
+
+}  // namespace
+
+void reset_stats(PointStats* stats, cudaStream_t s) {
+  k_reset_stats<<<1, 32, 0, s>>>(stats);
+  RTDL_CUDA_CHECK(cudaGetLastError());
+}
+
+void prep_points(const void* points_dev, uint32_t n, int dim, float4* out, PointStats* stats, cudaStream_t s) {
+  if (n == 0) return;
+  const double* raw = static_cast<const double*>(points_dev);
+  if (dim == 3)
+    k_prep<3><<<grid_for(n), kThreads, 0, s>>>(raw, n, out, stats);
+  else
+    k_prep<2><<<grid_for(n), kThreads, 0, s>>>(raw, n, out, stats);
+  RTDL_CUDA_CHECK(cudaGetLastError());
+}
+
+void morton_codes(const float4* pts, uint32_t n, int dim, const PointStats* box_stats, uint32_t* codes, cudaStream_t s) {
+  if (n == 0) return;
+  k_morton<<<grid_for(n), kThreads, 0, s>>>(pts, n, dim, box_stats, codes);
+  RTDL_CUDA_CHECK(cudaGetLastError());
+}
+
+Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, int leaf_size) {
+  if (dim != 2 && dim != 3) throw std::runtime_error("dimension must be 2 or 3");
+  if (n > 0x3FFFFFFFu) throw std::runtime_error("search_count exceeds the scene limit of 2^30 points");
+  if (leaf_size < 1) leaf_size = 1;
+  if (leaf_size > 32) leaf_size = 32;
+  Scene* sc = new Scene();
+  sc->dim = dim;
+  sc->n = n;
+  sc->stream = s;
+  sc->leaf_size = leaf_size;
+  RTDL_CUDA_CHECK(cudaGetDevice(&sc->device));
+  sc->stats = static_cast<PointStats*>(dev_alloc(sizeof(PointStats), s));
+  reset_stats(sc->stats, s);
+  if (n == 0) return sc;
+  const double* raw = static_cast<const double*>(points_dev);
+  float4* pts_in = static_cast<float4*>(dev_alloc(sizeof(float4) * n, s));
+  prep_points(points_dev, n, dim, pts_in, sc->stats, s);
+  uint32_t* codes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
+  morton_codes(pts_in, n, dim, sc->stats, codes, s);
+  sc->perm = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
+  iota_u32(sc->perm, n, s);
+  radix_sort_pairs(codes, sc->perm, n, 0, dim == 3 ? 30 : 32, nullptr, s);
+  sc->pts = static_cast<float4*>(dev_alloc(sizeof(float4) * n, s));
+  sc->pts64 = static_cast<double*>(dev_alloc(sizeof(double) * 3 * (size_t)n, s));
+  if (dim == 3)
+    k_gather<3><<<grid_for(n), kThreads, 0, s>>>(pts_in, raw, sc->perm, n, sc->pts, sc->pts64, sc->stats);
+  else
+    k_gather<2><<<grid_for(n), kThreads, 0, s>>>(pts_in, raw, sc->perm, n, sc->pts, sc->pts64, sc->stats);
+  RTDL_CUDA_CHECK(cudaGetLastError());
+  dev_free(pts_in, s);
+  if (n >= 2) {
+    const uint32_t ni = n - 1;
+    int* child_l = static_cast<int*>(dev_alloc(sizeof(int) * ni, s));
+    int* child_r = static_cast<int*>(dev_alloc(sizeof(int) * ni, s));
+    int* first = static_cast<int*>(dev_alloc(sizeof(int) * ni, s));
+    int* last = static_cast<int*>(dev_alloc(sizeof(int) * ni, s));
+    int* parent_int = static_cast<int*>(dev_alloc(sizeof(int) * ni, s));
+    int* parent_leaf = static_cast<int*>(dev_alloc(sizeof(int) * n, s));
+    unsigned int* arrivals = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * ni, s));
+    float4* boxes = static_cast<float4*>(dev_alloc(sizeof(float4) * 2 * (size_t)ni, s));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(arrivals, 0, sizeof(unsigned int) * ni, s));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(parent_int, 0xFF, sizeof(int) * ni, s));  // root keeps -1
+    k_karras<<<grid_for(ni), kThreads, 0, s>>>(codes, n, child_l, child_r, first, last, parent_int, parent_leaf);
+    k_refit<<<grid_for(n), kThreads, 0, s>>>(n, sc->pts, child_l, child_r, parent_int, parent_leaf, arrivals, boxes);
+    sc->nodes = static_cast<float4*>(dev_alloc(sizeof(float4) * 4 * (size_t)ni, s));
+    k_pack<<<grid_for(ni), kThreads, 0, s>>>(n, sc->pts, child_l, child_r, first, last, boxes, leaf_size, sc->nodes);
+    RTDL_CUDA_CHECK(cudaGetLastError());
+    dev_free(child_l, s);
+    dev_free(child_r, s);
+    dev_free(first, s);
+    dev_free(last, s);
+    dev_free(parent_int, s);
+    dev_free(parent_leaf, s);
+    dev_free(arrivals, s);
+    dev_free(boxes, s);
+  }
+  dev_free(codes, s);
+  if (n <= (uint32_t)leaf_size) {
+    sc->root_ref = 0;
+    sc->root_cnt = (int)n;
+  } else {
+    sc->root_ref = 0;
+    sc->root_cnt = 0;
+  }
+  return sc;
+}
+
+void destroy_scene(Scene* sc) {
+  if (!sc) return;
+  cudaStream_t s = sc->stream;
+  dev_free(sc->pts, s);
+  dev_free(sc->perm, s);
+  dev_free(sc->pts64, s);
+  dev_free(sc->nodes, s);
+  dev_free(sc->stats, s);
+  if (sc->own_stream && s) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  delete sc;
+}
+
+}  // namespace rtdl_b200

@@ -1,0 +1,273 @@
+// sort_scan.cu -- device prefix scans and a stable LSD radix sort, written for
+// this library (no CUB): the LBVH build sorts Morton codes with it, the query
+// path sorts queries into Morton order and into query-id order, and row
+// offsets come from the scan.
+//
+// Scan: reduce-then-scan over 2,048-element tiles (256 threads x 8 items), a
+// single-block pass over the tile sums, then a downsweep.  Deterministic and
+// free of inter-block waits.
+// Radix sort: 8-bit digits; per pass a tile histogram kernel, a scan of the
+// (digit, tile) histogram and a scatter kernel that ranks keys stably inside
+// the tile with __match_any_sync and per-warp digit counters.
+#include "internal.cuh"
+
+namespace rtdl_b200 {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kSortWarps = kSortThreads / 32;
+
+__device__ __forceinline__ uint32_t load_count(const uint32_t* counts, const uint32_t* order,
+                                               const unsigned int* identity_flag, uint32_t i) {
+  if (order == nullptr || (identity_flag != nullptr && *identity_flag)) return counts[i];
+  return counts[order[i]];
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim == kScanThreads).
+template <typename T>
+__device__ T block_exclusive_scan(T v, T* total) {
+  __shared__ T warp_sums[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) warp_sums[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    T w = lane < kScanThreads / 32 ? warp_sums[lane] : T(0);
+    T wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < kScanThreads / 32) warp_sums[lane] = wi - w;
+    if (lane == kScanThreads / 32 - 1) warp_sums[0] = warp_sums[0];  // keep ordering explicit
+    if (lane == kScanThreads / 32 - 1) *total = wi;
+  }
+  __syncthreads();
+  T r = warp_sums[warp] + inc - v;
+  __syncthreads();
+  return r;
+}
+
+template <typename Out>
+__global__ void k_scan_reduce(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag,
+                              uint32_t n, Out* block_sums) {
+  __shared__ Out total;
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  Out s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    uint64_t idx = base + i;
+    if (idx < n) s += (Out)load_count(counts, order, identity_flag, (uint32_t)idx);
+  }
+  block_exclusive_scan<Out>(s, &total);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+// One block of 1,024 threads scans the tile sums in place (exclusive) and
+// writes the grand total to *grand_total.
+template <typename Out>
+__global__ void k_scan_tile_sums(Out* sums, uint32_t num, Out* grand_total) {
+  __shared__ Out warp_sums[32];
+  __shared__ Out carry_s;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry_s = 0;
+  __syncthreads();
+  for (uint32_t chunk = 0; chunk < num; chunk += blockDim.x) {
+    uint32_t i = chunk + threadIdx.x;
+    Out v = i < num ? sums[i] : Out(0);
+    Out inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      Out y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) warp_sums[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      Out w = warp_sums[lane];
+      Out wi = w;
+      for (int o = 1; o < 32; o <<= 1) {
+        Out y = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      warp_sums[lane] = wi - w;
+    }
+    __syncthreads();
+    Out carry = carry_s;
+    Out excl = carry + warp_sums[warp] + inc - v;
+    if (i < num) sums[i] = excl;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry_s = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *grand_total = carry_s;
+}
+
+template <typename Out>
+__global__ void k_scan_down(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag,
+                            uint32_t n, const Out* block_prefix, Out* out) {
+  __shared__ Out total;
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  Out s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    uint64_t idx = base + i;
+    v[i] = idx < n ? load_count(counts, order, identity_flag, (uint32_t)idx) : 0u;
+    s += (Out)v[i];
+  }
+  Out run = block_exclusive_scan<Out>(s, &total) + block_prefix[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    uint64_t idx = base + i;
+    if (idx < n) out[idx] = run;
+    run += (Out)v[i];
+  }
+}
+
+template <typename Out>
+void scan_impl(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag, uint32_t n,
+               Out* out, cudaStream_t s) {
+  uint32_t tiles = div_up(n, kScanTile);
+  if (tiles == 0) tiles = 1;
+  Out* sums = static_cast<Out*>(dev_alloc(sizeof(Out) * tiles, s));
+  k_scan_reduce<Out><<<tiles, kScanThreads, 0, s>>>(counts, order, identity_flag, n, sums);
+  k_scan_tile_sums<Out><<<1, 1024, 0, s>>>(sums, tiles, out + n);
+  k_scan_down<Out><<<tiles, kScanThreads, 0, s>>>(counts, order, identity_flag, n, sums, out);
+  RTDL_CUDA_CHECK(cudaGetLastError());
+  dev_free(sums, s);
+}
+
+__global__ void k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift, uint32_t* hist,
+                             uint32_t num_tiles, const unsigned int* skip) {
+  if (skip != nullptr && *skip) return;
+  __shared__ unsigned int h[256];
+  const int t = threadIdx.x;
+  h[t] = 0;
+  __syncthreads();
+  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+  for (int i = 0; i < kSortItems; ++i) {
+    uint64_t idx = base + (uint64_t)i * kSortThreads + t;
+    if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[(uint64_t)t * num_tiles + blockIdx.x] = h[t];
+}
+
+__global__ void k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                                uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
+                                int shift, const uint32_t* __restrict__ hist_scanned, uint32_t num_tiles,
+                                const unsigned int* skip) {
+  if (skip != nullptr && *skip) return;
+  __shared__ unsigned int base_off[256];
+  __shared__ unsigned int warp_cnt[kSortWarps][256];
+  __shared__ unsigned int run[256];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  base_off[t] = hist_scanned[(uint64_t)t * num_tiles + blockIdx.x];
+  run[t] = 0;
+  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+  const unsigned int lt_mask = (1u << lane) - 1u;
+  for (int i = 0; i < kSortItems; ++i) {
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) warp_cnt[w][t] = 0;
+    __syncthreads();
+    const uint64_t idx = base + (uint64_t)i * kSortThreads + t;
+    const bool valid = idx < n;
+    const uint32_t key = valid ? keys_in[idx] : 0u;
+    const uint32_t d = (key >> shift) & 255u;
+    const unsigned int vmask = __ballot_sync(0xffffffffu, valid);
+    const unsigned int peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u) & vmask;
+    const unsigned int rank = __popc(peers & lt_mask);
+    if (valid && rank == 0) warp_cnt[warp][d] = __popc(peers);
+    __syncthreads();
+    {
+      unsigned int r = run[t];
+#pragma unroll
+      for (int w = 0; w < kSortWarps; ++w) {
+        unsigned int c = warp_cnt[w][t];
+        warp_cnt[w][t] = r;
+        r += c;
+      }
+      run[t] = r;
+    }
+    __syncthreads();
+    if (valid) {
+      const unsigned int pos = base_off[d] + warp_cnt[warp][d] + rank;
+      keys_out[pos] = key;
+      vals_out[pos] = vals_in[idx];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_iota(uint32_t* out, uint32_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)i;
+}
+
+}  // namespace
+
+void scan_counts_u64(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag, uint32_t n,
+                     unsigned long long* out, cudaStream_t s) {
+  scan_impl<unsigned long long>(counts, order, identity_flag, n, out, s);
+}
+
+void iota_u32(uint32_t* out, uint32_t n, cudaStream_t s) {
+  if (n == 0) return;
+  unsigned int blocks = div_up(n, 256);
+  if (blocks > 8 * kSmCount * 4) blocks = 8 * kSmCount * 4;
+  k_iota<<<blocks, 256, 0, s>>>(out, n);
+  RTDL_CUDA_CHECK(cudaGetLastError());
+}
+
+void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int begin_bit, int end_bit,
+                      const unsigned int* skip_flag, cudaStream_t s) {
+  if (n <= 1 || end_bit <= begin_bit) return;
+  int passes = (end_bit - begin_bit + 7) / 8;
+  if (passes & 1) ++passes;  // even pass count leaves the result in the caller's buffers
+  const uint32_t tiles = div_up(n, kSortTile);
+  const uint64_t hist_n = (uint64_t)256 * tiles;
+  if (hist_n + 1 > 0xFFFFFFFFull) throw std::runtime_error("radix sort input too large");
+  uint32_t* keys_alt = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
+  uint32_t* vals_alt = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
+  uint32_t* hist = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (hist_n + 1), s));
+  uint32_t* hist_sums = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (div_up(hist_n, kScanTile) + 1), s));
+  uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
+  const uint32_t htiles = div_up(hist_n, kScanTile);
+  for (int p = 0; p < passes; ++p) {
+    const int shift = begin_bit + 8 * p;
+    if (shift < 32) {
+      k_radix_hist<<<tiles, kSortThreads, 0, s>>>(ki, n, shift, hist, tiles, skip_flag);
+      k_scan_reduce<uint32_t><<<htiles, kScanThreads, 0, s>>>(hist, nullptr, nullptr, (uint32_t)hist_n, hist_sums);
+      k_scan_tile_sums<uint32_t><<<1, 1024, 0, s>>>(hist_sums, htiles, hist + hist_n);
+      k_scan_down<uint32_t><<<htiles, kScanThreads, 0, s>>>(hist, nullptr, nullptr, (uint32_t)hist_n, hist_sums, hist);
+      k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, shift, hist, tiles, skip_flag);
+    } else {
+      // A padding pass beyond the key width: a plain copy keeps the ping-pong even.
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(ko, ki, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(vo, vi, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+    }
+    RTDL_CUDA_CHECK(cudaGetLastError());
+    uint32_t* tk = ki; ki = ko; ko = tk;
+    uint32_t* tv = vi; vi = vo; vo = tv;
+  }
+  dev_free(keys_alt, s);
+  dev_free(vals_alt, s);
+  dev_free(hist, s);
+  dev_free(hist_sums, s);
+}
+
+}  // namespace rtdl_b200

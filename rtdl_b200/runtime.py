@@ -1,0 +1,599 @@
+"""Host runtime of the b200 backend: ``run_b200``, prepared kernels and scenes.
+
+Mirrors the reference's OptiX runtime for the neighbor path
+(rubaolee/rtdl ``src/rtdsl/optix_runtime.py``):
+
+* ``run_b200(kernel, *, result_mode="dict"|"raw", **inputs)`` -- ``run_optix``
+  (``:1275-1331``): same input validation and messages, same result modes;
+* ``prepare_b200(kernel).bind(**inputs).run()/run_raw()`` -- ``prepare_optix``
+  (``:865-1000``);
+* ``B200RowView`` -- ``OptixRowView`` (``:813-848``): owns the native rows,
+  ``close()``, ``to_dict_rows()``, ``to_tuple_rows()``, plus ``to_numpy()``;
+* ``PreparedB200FixedRadiusNeighbors3D`` / ``prepare_b200_fixed_radius_neighbors_3d``
+  -- ``PreparedOptixFixedRadiusNeighbors3D`` (``:2315-2419, 2962``);
+* ``pack_points`` / ``PackedPoints`` -- ``embree_runtime.py:538-542, 987-1037``,
+  with a numpy column fast path (no per-point Python loop).
+
+Everything below calls librtdl_b200.so through ctypes; no computation happens
+in Python and there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from collections.abc import Iterable, Mapping
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from . import dsl
+
+NEIGHBOR_PREDICATES = ("fixed_radius_neighbors", "bounded_knn_rows", "knn_rows")
+PREDICATE_CODE = {"fixed_radius_neighbors": 0, "bounded_knn_rows": 1, "knn_rows": 2}
+
+POINT2D_DTYPE = np.dtype({"names": ["id", "x", "y"], "formats": ["<u4", "<f8", "<f8"], "offsets": [0, 8, 16], "itemsize": 24})
+POINT3D_DTYPE = np.dtype(
+    {"names": ["id", "x", "y", "z"], "formats": ["<u4", "<f8", "<f8", "<f8"], "offsets": [0, 8, 16, 24], "itemsize": 32}
+)
+FRN_ROW_DTYPE = np.dtype(
+    {"names": ["query_id", "neighbor_id", "distance"], "formats": ["<u4", "<u4", "<f8"], "offsets": [0, 4, 8], "itemsize": 16}
+)
+KNN_ROW_DTYPE = np.dtype(
+    {
+        "names": ["query_id", "neighbor_id", "distance", "neighbor_rank"],
+        "formats": ["<u4", "<u4", "<f8", "<u4"],
+        "offsets": [0, 4, 8, 16],
+        "itemsize": 24,
+    }
+)
+
+
+# ---------------------------------------------------------------------------
+# packing
+# ---------------------------------------------------------------------------
+
+@dataclass(frozen=True)
+class PackedPoints:
+    """Points in the ABI record layout (RtdlPoint / RtdlPoint3D), held as a numpy array."""
+
+    records: np.ndarray
+    count: int
+    dimension: int = 2
+
+    @property
+    def address(self) -> int:
+        return int(self.records.ctypes.data) if self.count else 0
+
+
+def _record_fields(record, names):
+    if isinstance(record, Mapping):
+        missing = [n for n in names if n not in record]
+        if missing:
+            raise ValueError(f"point record is missing fields: {', '.join(missing)}")
+        return [record[n] for n in names]
+    if all(hasattr(record, n) for n in names):
+        return [getattr(record, n) for n in names]
+    raise ValueError("point record must be a mapping or dataclass-like object")
+
+
+def _has_fields(record, names) -> bool:
+    if isinstance(record, Mapping):
+        return all(n in record for n in names)
+    return all(hasattr(record, n) for n in names)
+
+
+def pack_points(records=None, *, ids=None, x=None, y=None, z=None, dimension: int | None = None) -> PackedPoints:
+    """Pack point records or numpy columns into the ABI layout.
+
+    Records follow the reference's coercion (``src/rtdsl/runtime.py:263-336``):
+    mappings or objects with ``id, x, y[, z]``.  Columns (``ids``, ``x``, ``y``,
+    ``z``) are packed with numpy only.
+    """
+    if dimension not in (None, 2, 3):
+        raise ValueError("points dimension must be one of: 2, 3")
+    if records is not None:
+        if isinstance(records, PackedPoints):
+            return records
+        if isinstance(records, np.ndarray) and records.dtype.names is not None:
+            names = records.dtype.names
+            dim = dimension or (3 if "z" in names else 2)
+            return pack_points(ids=records["id"], x=records["x"], y=records["y"],
+                               z=records["z"] if dim == 3 else None, dimension=dim)
+        if isinstance(records, (str, bytes)) or not isinstance(records, Iterable):
+            raise ValueError("points input must be an iterable of records")
+        items = list(records)
+        dim = dimension
+        if dim is None:
+            dim = 3 if items and all(_has_fields(r, ("id", "x", "y", "z")) for r in items) else 2
+        dtype = POINT3D_DTYPE if dim == 3 else POINT2D_DTYPE
+        arr = np.zeros(len(items), dtype=dtype)
+        if items:
+            names = ("id", "x", "y", "z") if dim == 3 else ("id", "x", "y")
+            if dim == 3 and not all(_has_fields(r, names) for r in items):
+                raise ValueError("points packed for a 3D layout must provide 3D point records")
+            if dim == 2 and any(isinstance(r, dsl.Point3D) or type(r).__name__ == "Point3D" for r in items):
+                raise ValueError("points packed for a 2D layout must provide 2D point records")
+            cols = list(zip(*(_record_fields(r, names) for r in items)))
+            arr["id"] = np.asarray([int(v) for v in cols[0]], dtype=np.int64).astype(np.uint32)
+            arr["x"] = np.asarray(cols[1], dtype=np.float64)
+            arr["y"] = np.asarray(cols[2], dtype=np.float64)
+            if dim == 3:
+                arr["z"] = np.asarray(cols[3], dtype=np.float64)
+        return PackedPoints(records=arr, count=len(items), dimension=dim)
+    if ids is None or x is None or y is None:
+        raise ValueError("pack_points needs records or ids/x/y columns")
+    dim = dimension or (3 if z is not None else 2)
+    ids_a = np.asarray(ids)
+    n = len(ids_a)
+    if len(x) != n or len(y) != n or (dim == 3 and (z is None or len(z) != n)):
+        raise ValueError("packed points arrays must have identical lengths")
+    if n and (ids_a.min() < 0 or ids_a.max() > 0xFFFFFFFF):
+        raise ValueError("point ids must fit in uint32")
+    arr = np.empty(n, dtype=POINT3D_DTYPE if dim == 3 else POINT2D_DTYPE)
+    arr["id"] = ids_a.astype(np.uint32, copy=False)
+    arr["x"] = np.asarray(x, dtype=np.float64)
+    arr["y"] = np.asarray(y, dtype=np.float64)
+    if dim == 3:
+        arr["z"] = np.asarray(z, dtype=np.float64)
+    return PackedPoints(records=arr, count=n, dimension=dim)
+
+
+def _pack_any(payload, dimension: int | None) -> tuple[int, int, int, object]:
+    """Returns (address, count, dimension, keepalive) for any supported points payload."""
+    cached = getattr(payload, "_rtdl_packed_points", None)
+    if cached is not None:
+        payload = cached
+    if isinstance(payload, PackedPoints):
+        if dimension is not None and payload.dimension != dimension:
+            raise ValueError("packed points payload dimension does not match the kernel input layout")
+        return payload.address, payload.count, payload.dimension, payload
+    # The reference's own PackedPoints (ctypes array of _RtdlPoint/_RtdlPoint3D) has the same layout.
+    if hasattr(payload, "records") and hasattr(payload, "count") and hasattr(payload, "dimension") \
+            and isinstance(getattr(payload, "records"), ctypes.Array):
+        if dimension is not None and payload.dimension != dimension:
+            raise ValueError("packed points payload dimension does not match the kernel input layout")
+        expected = 32 if payload.dimension == 3 else 24
+        if ctypes.sizeof(payload.records._type_) != expected:
+            raise ValueError("packed points records do not have the RtdlPoint/RtdlPoint3D layout")
+        return (ctypes.addressof(payload.records) if payload.count else 0), int(payload.count), int(payload.dimension), payload
+    packed = pack_points(records=payload, dimension=dimension)
+    return packed.address, packed.count, packed.dimension, packed
+
+
+# ---------------------------------------------------------------------------
+# row views
+# ---------------------------------------------------------------------------
+
+@dataclass
+class B200RowView:
+    """Rows owned by librtdl_b200 (pinned host memory); mirrors ``OptixRowView``."""
+
+    rows_address: int
+    row_count: int
+    row_dtype: np.dtype
+    field_names: tuple
+    _closed: bool = False
+
+    def _array(self) -> np.ndarray:
+        if self._closed:
+            raise RuntimeError("row view is closed")
+        if self.row_count == 0:
+            return np.zeros(0, dtype=self.row_dtype)
+        buf = (ctypes.c_char * (self.row_count * self.row_dtype.itemsize)).from_address(self.rows_address)
+        return np.frombuffer(buf, dtype=self.row_dtype)
+
+    def to_numpy(self, copy: bool = True) -> np.ndarray:
+        a = self._array()
+        return a.copy() if copy else a
+
+    def close(self) -> None:
+        if not self._closed:
+            if self.rows_address:
+                _native.load_library().rtdl_b200_free_rows(ctypes.c_void_p(self.rows_address))
+            self._closed = True
+
+    def __len__(self) -> int:
+        return self.row_count
+
+    def to_dict_rows(self, fields: tuple | None = None) -> tuple:
+        names = tuple(fields or self.field_names)
+        a = self._array()
+        cols = [a[n].tolist() for n in names]
+        return tuple(dict(zip(names, vals)) for vals in zip(*cols)) if self.row_count else ()
+
+    def to_tuple_rows(self, fields: tuple | None = None) -> tuple:
+        names = tuple(fields or self.field_names)
+        a = self._array()
+        cols = [a[n].tolist() for n in names]
+        return tuple(zip(*cols)) if self.row_count else ()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _row_view(address: int, count: int, ranked: bool) -> B200RowView:
+    if ranked:
+        return B200RowView(address, count, KNN_ROW_DTYPE, ("query_id", "neighbor_id", "distance", "neighbor_rank"))
+    return B200RowView(address, count, FRN_ROW_DTYPE, ("query_id", "neighbor_id", "distance"))
+
+
+# ---------------------------------------------------------------------------
+# low-level calls (plain per-call launch)
+# ---------------------------------------------------------------------------
+
+def fixed_radius_neighbors(query, search, *, radius: float, k_max: int, dimension: int | None = None,
+                           ranked: bool = False) -> B200RowView:
+    """One plain per-call launch (``rtdl_b200_run_fixed_radius_neighbors[_3d]`` or
+    ``rtdl_b200_run_bounded_knn_rows[_3d]`` when ``ranked``)."""
+    lib = _native.load_library()
+    qa, qn, qd, qk = _pack_any(query, dimension)
+    sa, sn, sd, sk = _pack_any(search, dimension or qd)
+    if qd != sd:
+        raise ValueError("query and search points must have the same dimension")
+    name = ("rtdl_b200_run_bounded_knn_rows" if ranked else "rtdl_b200_run_fixed_radius_neighbors") + ("_3d" if qd == 3 else "")
+    rows = ctypes.c_void_p()
+    count = ctypes.c_size_t()
+    err = _native.error_buffer()
+    status = getattr(lib, name)(qa, qn, sa, sn, float(radius), int(k_max), ctypes.byref(rows), ctypes.byref(count), err, len(err))
+    _native.check_status(status, err)
+    del qk, sk
+    return _row_view(rows.value or 0, count.value, ranked)
+
+
+def knn_rows(query, search, *, k: int, dimension: int | None = None) -> B200RowView:
+    """One plain per-call launch of ``rtdl_b200_run_k_closest_hits[_3d]``."""
+    lib = _native.load_library()
+    qa, qn, qd, qk = _pack_any(query, dimension)
+    sa, sn, sd, sk = _pack_any(search, dimension or qd)
+    if qd != sd:
+        raise ValueError("query and search points must have the same dimension")
+    name = "rtdl_b200_run_k_closest_hits" + ("_3d" if qd == 3 else "")
+    rows = ctypes.c_void_p()
+    count = ctypes.c_size_t()
+    err = _native.error_buffer()
+    status = getattr(lib, name)(qa, qn, sa, sn, int(k), ctypes.byref(rows), ctypes.byref(count), err, len(err))
+    _native.check_status(status, err)
+    del qk, sk
+    return _row_view(rows.value or 0, count.value, True)
+
+
+# ---------------------------------------------------------------------------
+# kernels: run_b200 / prepare_b200
+# ---------------------------------------------------------------------------
+
+def _resolve_kernel(kernel_fn_or_compiled):
+    if hasattr(kernel_fn_or_compiled, "refine_op") and hasattr(kernel_fn_or_compiled, "inputs"):
+        return kernel_fn_or_compiled
+    if callable(kernel_fn_or_compiled):
+        return kernel_fn_or_compiled()
+    raise TypeError("expected an @rt.kernel function or a CompiledKernel")
+
+
+def _validate_kernel(compiled) -> None:
+    # same checks and messages as src/rtdsl/runtime.py:145-149
+    if compiled.precision != "float_approx":
+        raise ValueError("RTDL CPU simulator currently supports only precision='float_approx'")
+    if compiled.candidates is None or compiled.refine_op is None or compiled.emit_op is None:
+        raise ValueError("RTDL CPU simulator requires a fully compiled kernel with traverse/refine/emit")
+
+
+def _layout_dimension(geometry_input) -> int:
+    layout = geometry_input.layout
+    names = set(layout.field_names())
+    if layout.name.endswith("3D") or "z" in names:
+        return 3
+    return 2
+
+
+def _check_inputs(expected, inputs, label="RTDL b200"):
+    missing = [n for n in expected if n not in inputs]
+    unexpected = [n for n in inputs if n not in expected]
+    if missing:
+        raise ValueError(f"missing {label} inputs: {', '.join(sorted(missing))}")
+    if unexpected:
+        raise ValueError(f"unexpected {label} inputs: {', '.join(sorted(unexpected))}")
+
+
+def _call_packed(compiled, packed: dict) -> B200RowView:
+    pred = compiled.refine_op.predicate
+    query = packed[compiled.candidates.left.name]
+    search = packed[compiled.candidates.right.name]
+    if pred.name == "knn_rows":
+        return knn_rows(query, search, k=int(pred.options["k"]))
+    return fixed_radius_neighbors(query, search, radius=float(pred.options["radius"]), k_max=int(pred.options["k_max"]),
+                                  ranked=pred.name == "bounded_knn_rows")
+
+
+class PreparedB200Kernel:
+    """Compiled-once handle; mirrors ``PreparedOptixKernel`` for the neighbor predicates."""
+
+    def __init__(self, kernel_fn_or_compiled):
+        compiled = _resolve_kernel(kernel_fn_or_compiled)
+        _validate_kernel(compiled)
+        pred = compiled.refine_op.predicate.name
+        if pred not in NEIGHBOR_PREDICATES:
+            raise ValueError(f"unsupported predicate for b200 backend: {pred!r}")
+        self.compiled = compiled
+        self.expected_inputs = {item.name: item for item in compiled.inputs}
+        self.predicate_name = pred
+        _native.load_library()
+
+    def bind(self, **inputs) -> "PreparedB200Execution":
+        _check_inputs(self.expected_inputs, inputs)
+        packed = {}
+        for name, payload in inputs.items():
+            dim = _layout_dimension(self.expected_inputs[name])
+            _addr, _n, _d, keep = _pack_any(payload, dim)
+            packed[name] = keep
+        return PreparedB200Execution(self.compiled, packed)
+
+    def run(self, **inputs) -> tuple:
+        return self.bind(**inputs).run()
+
+
+@dataclass
+class PreparedB200Execution:
+    compiled: object
+    packed_inputs: dict
+
+    def run_raw(self) -> B200RowView:
+        return _call_packed(self.compiled, self.packed_inputs)
+
+    def run(self) -> tuple:
+        view = self.run_raw()
+        try:
+            return _project(self.compiled, view)
+        finally:
+            view.close()
+
+
+def _project(compiled, view: B200RowView) -> tuple:
+    fields = tuple(compiled.emit_op.fields)
+    missing = [f for f in fields if f not in view.field_names]
+    if missing:
+        raise ValueError("b200 row is missing emitted fields: " + ", ".join(missing))
+    return view.to_dict_rows(fields)
+
+
+def prepare_b200(kernel_fn_or_compiled) -> PreparedB200Kernel:
+    return PreparedB200Kernel(kernel_fn_or_compiled)
+
+
+def run_b200(kernel_fn_or_compiled, *, result_mode: str = "dict", **inputs):
+    """Execute a neighbor kernel on the B200 backend (mirrors ``run_optix``).
+
+    ``result_mode="dict"`` returns ``tuple[dict, ...]`` projected onto the
+    kernel's emitted fields; ``"raw"`` returns a ``B200RowView`` the caller
+    closes.
+    """
+    compiled = _resolve_kernel(kernel_fn_or_compiled)
+    _validate_kernel(compiled)
+    expected = {item.name: item for item in compiled.inputs}
+    _check_inputs(expected, inputs)
+    if result_mode not in {"dict", "raw"}:
+        raise ValueError("b200 result_mode must be 'dict' or 'raw'")
+    pred = compiled.refine_op.predicate.name
+    if pred not in NEIGHBOR_PREDICATES:
+        raise ValueError(f"unsupported predicate for b200 backend: {pred!r}")
+    execution = PreparedB200Kernel(compiled).bind(**inputs)
+    return execution.run_raw() if result_mode == "raw" else execution.run()
+
+
+# ---------------------------------------------------------------------------
+# scenes (resident LBVH)
+# ---------------------------------------------------------------------------
+
+class B200Scene:
+    """An LBVH built on the device over search points; serves FRN, bounded KNN,
+    KNN and Hausdorff calls until ``close()``."""
+
+    def __init__(self, search_points, *, dimension: int | None = None, stream: int | None = None,
+                 device_points: tuple[int, int] | None = None):
+        lib = _native.load_library()
+        self._lib = lib
+        self._handle = ctypes.c_void_p()
+        err = _native.error_buffer()
+        if device_points is not None:
+            address, count = device_points
+            if dimension not in (2, 3):
+                raise ValueError("device_points needs an explicit dimension")
+            self.dimension, self.count = dimension, int(count)
+            status = lib.rtdl_b200_scene_create(address, self.count, dimension, 1, stream, ctypes.byref(self._handle), err, len(err))
+        else:
+            addr, n, dim, keep = _pack_any(search_points, dimension)
+            self.dimension, self.count = dim, n
+            status = lib.rtdl_b200_scene_create(addr, n, dim, 0, stream, ctypes.byref(self._handle), err, len(err))
+            del keep
+        _native.check_status(status, err)
+        self._closed = False
+
+    @property
+    def handle(self) -> int:
+        return self._handle.value or 0
+
+    def query(self, query_points, *, predicate: str, radius: float = 0.0, limit: int, with_overflow: bool = False):
+        if self._closed:
+            raise RuntimeError("scene is closed")
+        code = PREDICATE_CODE[predicate]
+        addr, n, dim, keep = _pack_any(query_points, self.dimension)
+        rows = ctypes.c_void_p()
+        count = ctypes.c_size_t()
+        overflow = np.zeros(n, dtype=np.uint8) if with_overflow else None
+        err = _native.error_buffer()
+        status = self._lib.rtdl_b200_scene_query(
+            self._handle, addr, n, code, float(radius), int(limit), ctypes.byref(rows), ctypes.byref(count),
+            overflow.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if overflow is not None else None, err, len(err))
+        del keep
+        _native.check_status(status, err)
+        view = _row_view(rows.value or 0, count.value, code != 0)
+        return (view, overflow) if with_overflow else view
+
+    def query_device(self, query_address: int, query_count: int, *, predicate: str, radius: float = 0.0, limit: int,
+                     rows_address: int, rows_capacity: int, overflow_address: int | None = None,
+                     stream: int | None = None) -> int:
+        """Device-resident call; returns the total row count."""
+        count = ctypes.c_size_t()
+        err = _native.error_buffer()
+        status = self._lib.rtdl_b200_scene_query_device(
+            self._handle, query_address, int(query_count), PREDICATE_CODE[predicate], float(radius), int(limit),
+            rows_address, int(rows_capacity), ctypes.byref(count), overflow_address, stream, err, len(err))
+        _native.check_status(status, err)
+        return count.value
+
+    def directed_hausdorff(self, query_points, *, with_nearest: bool = False):
+        if self._closed:
+            raise RuntimeError("scene is closed")
+        addr, n, dim, keep = _pack_any(query_points, self.dimension)
+        dist = ctypes.c_double()
+        src = ctypes.c_uint32()
+        tgt = ctypes.c_uint32()
+        nd = np.zeros(n, dtype=np.float64) if with_nearest else None
+        ni = np.zeros(n, dtype=np.uint32) if with_nearest else None
+        err = _native.error_buffer()
+        status = self._lib.rtdl_b200_scene_directed_hausdorff(
+            self._handle, addr, n, ctypes.byref(dist), ctypes.byref(src), ctypes.byref(tgt),
+            nd.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if nd is not None else None,
+            ni.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)) if ni is not None else None, err, len(err))
+        del keep
+        _native.check_status(status, err)
+        result = {"distance": dist.value, "source_id": int(src.value), "target_id": int(tgt.value), "row_count": n}
+        return (result, nd, ni) if with_nearest else result
+
+    def close(self) -> None:
+        if not getattr(self, "_closed", True):
+            self._lib.rtdl_b200_scene_destroy(self._handle)
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PreparedB200FixedRadiusNeighbors3D:
+    """Prepared 3-D fixed-radius scene; mirrors ``PreparedOptixFixedRadiusNeighbors3D``
+    (``optix_runtime.py:2315-2419``) on top of the C ABI's prepared entry points."""
+
+    def __init__(self, search_points, *, max_radius: float):
+        if max_radius <= 0:
+            raise ValueError("max_radius must be positive")
+        addr, n, dim, keep = _pack_any(search_points, 3)
+        if dim != 3:
+            raise ValueError("prepare_b200_fixed_radius_neighbors_3d requires 3-D points")
+        self._keep = keep
+        self._count = n
+        self._max_radius = float(max_radius)
+        self._handle = ctypes.c_void_p()
+        self._closed = False
+        if n == 0:
+            return
+        lib = _native.load_library()
+        err = _native.error_buffer()
+        status = lib.rtdl_b200_prepare_fixed_radius_neighbors_3d(addr, n, ctypes.c_double(self._max_radius),
+                                                                 ctypes.byref(self._handle), err, len(err))
+        _native.check_status(status, err)
+
+    @property
+    def max_radius(self) -> float:
+        return self._max_radius
+
+    @property
+    def closed(self) -> bool:
+        return self._closed
+
+    def run_raw(self, query_points, *, radius: float, k_max: int) -> B200RowView:
+        if self._closed:
+            raise RuntimeError("prepared b200 fixed-radius-neighbor 3D handle is closed")
+        if radius < 0:
+            raise ValueError("radius must be non-negative")
+        if radius > self._max_radius:
+            raise ValueError("radius must be less than or equal to prepared max_radius")
+        if k_max <= 0:
+            raise ValueError("k_max must be positive")
+        addr, n, dim, keep = _pack_any(query_points, 3)
+        if dim != 3:
+            raise ValueError("PreparedB200FixedRadiusNeighbors3D.run_raw requires 3-D points")
+        if n == 0 or self._count == 0:
+            return _row_view(0, 0, False)
+        lib = _native.load_library()
+        rows = ctypes.c_void_p()
+        count = ctypes.c_size_t()
+        err = _native.error_buffer()
+        status = lib.rtdl_b200_run_prepared_fixed_radius_neighbors_3d(
+            self._handle, addr, n, ctypes.c_double(float(radius)), ctypes.c_size_t(int(k_max)),
+            ctypes.byref(rows), ctypes.byref(count), err, len(err))
+        del keep
+        _native.check_status(status, err)
+        return _row_view(rows.value or 0, count.value, False)
+
+    def run(self, query_points, *, radius: float, k_max: int) -> tuple:
+        view = self.run_raw(query_points, radius=radius, k_max=k_max)
+        try:
+            return view.to_dict_rows()
+        finally:
+            view.close()
+
+    def close(self) -> None:
+        if not self._closed:
+            if self._handle.value:
+                _native.load_library().rtdl_b200_destroy_prepared_fixed_radius_neighbors_3d(self._handle)
+            self._closed = True
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def prepare_b200_fixed_radius_neighbors_3d(search_points, *, max_radius: float) -> PreparedB200FixedRadiusNeighbors3D:
+    return PreparedB200FixedRadiusNeighbors3D(search_points, max_radius=max_radius)
+
+
+def directed_hausdorff(query_points, search_points, *, dimension: int | None = None) -> dict:
+    """Directed Hausdorff witness (max over queries of the exact nearest distance,
+    ties to the smaller query id then neighbor id), reduced on the device."""
+    with B200Scene(search_points, dimension=dimension) as scene:
+        return scene.directed_hausdorff(query_points)
+
+
+def hausdorff_distance(points_a, points_b, *, dimension: int | None = None) -> dict:
+    """Undirected Hausdorff as the reference app reports it
+    (``rtdl_hausdorff_distance_app.py:152``): both directions, the larger wins
+    with the direction name as the tie-break."""
+    ab = directed_hausdorff(points_a, points_b, dimension=dimension)
+    ba = directed_hausdorff(points_b, points_a, dimension=dimension)
+    direction, best = max((("a_to_b", ab), ("b_to_a", ba)), key=lambda item: (float(item[1]["distance"]), item[0]))
+    return {
+        "directed_a_to_b": ab,
+        "directed_b_to_a": ba,
+        "hausdorff_distance": float(best["distance"]),
+        "witness_direction": direction,
+    }
+
+
+def set_tuning(*, leaf_size: int, block_threads: int) -> None:
+    status = _native.load_library().rtdl_b200_set_tuning(int(leaf_size), int(block_threads))
+    if status != 0:
+        raise ValueError("leaf_size must be in [1, 32] and block_threads one of 64, 128, 256")
+
+
+def set_device(device: int) -> None:
+    if _native.load_library().rtdl_b200_set_device(int(device)) != 0:
+        raise RuntimeError(f"cannot select CUDA device {device}")

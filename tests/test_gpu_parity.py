@@ -1,0 +1,235 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's outputs.
+
+Small cases compare against the golden fixtures produced by the reference's
+own cpu_python_reference (bit-exact rows: ids, ranks, FP64 distances and row
+order).  Larger seeded cases compare against the CPU oracle restatement, which
+is itself pinned to those fixtures by tests/test_oracle_golden.py.
+"""
+import numpy as np
+import pytest
+
+import rtdl_b200 as rt
+from oracle import oracle as O
+from tests import golden_cases as G
+
+pytestmark = pytest.mark.gpu
+
+CASES = G.load_cases()
+
+
+def _kernel(predicate, dim, **options):
+    geometry = rt.Points3D if dim == 3 else rt.Points
+    fields = ["query_id", "neighbor_id", "distance"] + ([] if predicate == "fixed_radius_neighbors" else ["neighbor_rank"])
+
+    @rt.kernel(backend="rtdl", precision="float_approx")
+    def k():
+        q = rt.input("query_points", geometry, role="probe")
+        s = rt.input("search_points", geometry, role="build")
+        c = rt.traverse(q, s, accel="bvh")
+        return rt.emit(rt.refine(c, predicate=getattr(rt, predicate)(**options)), fields=fields)
+
+    return k
+
+
+def _as_tuples(rows, ranked):
+    if ranked:
+        return [(r["query_id"], r["neighbor_id"], r["distance"], r["neighbor_rank"]) for r in rows]
+    return [(r["query_id"], r["neighbor_id"], r["distance"]) for r in rows]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_run_b200_matches_reference_golden(gpu, case):
+    dim = case["dimension"]
+    kernel = _kernel(case["predicate"], dim, **case["options"])
+    q = G.points_records(case["query_points"], dim)
+    s = G.points_records(case["search_points"], dim)
+    rows = rt.run_b200(kernel, query_points=q, search_points=s)
+    assert _as_tuples(rows, case["predicate"] != "fixed_radius_neighbors") == G.expected_rows(case)
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c["predicate"] != "knn_rows"][:12], ids=lambda c: c["name"])
+def test_scene_query_matches_golden_with_columns(gpu, case):
+    dim = case["dimension"]
+    q = rt.pack_points(**{k if k != "id" else "ids": v for k, v in G.points_columns(case["query_points"], dim).items()})
+    s = rt.pack_points(**{k if k != "id" else "ids": v for k, v in G.points_columns(case["search_points"], dim).items()})
+    ranked = case["predicate"] == "bounded_knn_rows"
+    with rt.B200Scene(s) as scene:
+        view = scene.query(q, predicate=case["predicate"], radius=case["options"]["radius"], limit=case["options"]["k_max"])
+        got = G.rows_as_tuples(view.to_numpy(), ranked)
+        view.close()
+    assert got == G.expected_rows(case)
+
+
+def test_config1_full_matches_reference_rows(gpu):
+    z = G.load_config1()
+    q, s = G.config1_points()
+    view = rt.runtime.fixed_radius_neighbors(
+        rt.pack_points(ids=q["id"], x=q["x"], y=q["y"]), rt.pack_points(ids=s["id"], x=s["x"], y=s["y"]),
+        radius=0.02, k_max=4096)
+    a = view.to_numpy()
+    view.close()
+    assert len(a) == 20911
+    assert np.array_equal(a["query_id"], z["query_id"])
+    assert np.array_equal(a["neighbor_id"], z["neighbor_id"])
+    assert np.array_equal(a["distance"].view(np.uint64), z["distance"].view(np.uint64))
+
+
+def _clustered(rng, n, centres, sigma=0.01, background=0.1):
+    which = rng.integers(0, len(centres), n)
+    pts = centres[which] + rng.normal(0.0, sigma, (n, 3))
+    bg = rng.random(n) < background
+    pts[bg] = rng.random((int(bg.sum()), 3))
+    return np.clip(pts, 0.0, 1.0).astype(np.float32).astype(np.float64)
+
+
+def _cols(pts, ids=None):
+    ids = np.arange(len(pts), dtype=np.uint32) if ids is None else ids
+    d = {"id": ids, "x": pts[:, 0], "y": pts[:, 1]}
+    if pts.shape[1] == 3:
+        d["z"] = pts[:, 2]
+    return d
+
+
+def _pack(c):
+    return rt.pack_points(ids=c["id"], x=c["x"], y=c["y"], z=c.get("z"))
+
+
+def _assert_same_rows(a, b, ranked):
+    assert len(a) == len(b)
+    for f in ("query_id", "neighbor_id") + (("neighbor_rank",) if ranked else ()):
+        assert np.array_equal(a[f], b[f]), f
+    assert np.array_equal(a["distance"].view(np.uint64), b["distance"].view(np.uint64))
+
+
+@pytest.mark.parametrize("k_max", [1, 8, 32, 64])
+def test_clustered_frn_3d_matches_oracle(gpu, k_max):
+    rng = np.random.default_rng(100 + k_max)
+    centres = rng.random((16, 3))
+    s = _cols(_clustered(rng, 40000, centres))
+    q = _cols(_clustered(rng, 6000, centres))
+    radius = 0.01
+    with rt.B200Scene(_pack(s)) as scene:
+        view, overflow = scene.query(_pack(q), predicate="fixed_radius_neighbors", radius=radius, limit=k_max,
+                                     with_overflow=True)
+        got = view.to_numpy()
+        view.close()
+    exp, counts = O.fixed_radius_neighbors(q, s, radius=radius, k_max=k_max, threads=8, with_counts=True)
+    _assert_same_rows(got, exp, False)
+    assert np.array_equal(overflow.astype(bool), counts > k_max)
+    assert (counts > k_max).any()
+
+
+def test_bounded_knn_and_knn_3d_match_oracle(gpu):
+    rng = np.random.default_rng(5)
+    centres = rng.random((8, 3))
+    s = _cols(_clustered(rng, 30000, centres))
+    q = _cols(_clustered(rng, 4000, centres))
+    with rt.B200Scene(_pack(s)) as scene:
+        v = scene.query(_pack(q), predicate="bounded_knn_rows", radius=0.012, limit=16)
+        _assert_same_rows(v.to_numpy(), O.fixed_radius_neighbors(q, s, radius=0.012, k_max=16, ranked=True, threads=8), True)
+        v.close()
+        for k in (1, 4, 16, 64):
+            v = scene.query(_pack(q), predicate="knn_rows", limit=k)
+            _assert_same_rows(v.to_numpy(), O.knn_rows(q, s, k=k, threads=8), True)
+            v.close()
+
+
+def test_generic_path_large_limits_match_oracle(gpu):
+    rng = np.random.default_rng(9)
+    centres = rng.random((4, 3))
+    s = _cols(_clustered(rng, 5000, centres, sigma=0.02))
+    q = _cols(_clustered(rng, 300, centres, sigma=0.02))
+    with rt.B200Scene(_pack(s)) as scene:
+        v = scene.query(_pack(q), predicate="fixed_radius_neighbors", radius=0.03, limit=300)
+        exp = O.fixed_radius_neighbors(q, s, radius=0.03, k_max=300, threads=8)
+        _assert_same_rows(v.to_numpy(), exp, False)
+        v.close()
+        v = scene.query(_pack(q), predicate="knn_rows", limit=100)
+        _assert_same_rows(v.to_numpy(), O.knn_rows(q, s, k=100, threads=8), True)
+        v.close()
+
+
+def test_inexact_fp64_inputs_and_large_coordinates(gpu):
+    rng = np.random.default_rng(21)
+    for offset, radius in ((0.0, 0.04), (1.0e4, 0.004), (-3.0e6, 0.5)):
+        s = _cols(offset + rng.random((5000, 3)) * (0.3 if offset else 1.0))
+        q = _cols(offset + rng.random((1500, 3)) * (0.3 if offset else 1.0))
+        with rt.B200Scene(_pack(s)) as scene:
+            v = scene.query(_pack(q), predicate="fixed_radius_neighbors", radius=radius, limit=20)
+            _assert_same_rows(v.to_numpy(), O.fixed_radius_neighbors(q, s, radius=radius, k_max=20, threads=8), False)
+            v.close()
+            v = scene.query(_pack(q), predicate="knn_rows", limit=5)
+            _assert_same_rows(v.to_numpy(), O.knn_rows(q, s, k=5, threads=8), True)
+            v.close()
+
+
+def test_duplicates_ties_unsorted_query_ids_2d(gpu):
+    rng = np.random.default_rng(33)
+    grid = np.stack(np.meshgrid(np.arange(40), np.arange(40)), -1).reshape(-1, 2).astype(np.float64) * 0.25
+    s_pts = np.concatenate([grid, grid[:300]])  # coincident duplicates
+    s = _cols(s_pts, ids=rng.integers(0, 500, len(s_pts)).astype(np.uint32))  # duplicate ids too
+    q_pts = grid[rng.integers(0, len(grid), 700)] + rng.integers(-1, 2, (700, 2)) * 0.125
+    q = _cols(q_pts, ids=rng.integers(0, 300, 700).astype(np.uint32))  # unsorted, repeated query ids
+    for radius, k_max in ((0.25, 3), (0.5, 7), (0.0, 4), (0.35355339059327373, 64)):
+        v = rt.runtime.fixed_radius_neighbors(_pack(q), _pack(s), radius=radius, k_max=k_max)
+        _assert_same_rows(v.to_numpy(), O.fixed_radius_neighbors(q, s, radius=radius, k_max=k_max, threads=8), False)
+        v.close()
+    v = rt.runtime.knn_rows(_pack(q), _pack(s), k=9)
+    _assert_same_rows(v.to_numpy(), O.knn_rows(q, s, k=9, threads=8), True)
+    v.close()
+
+
+def test_tiny_and_single_point_scenes(gpu):
+    for ns in (1, 2, 3, 7, 9, 33):
+        rng = np.random.default_rng(ns)
+        s = _cols(rng.random((ns, 3)))
+        q = _cols(rng.random((50, 3)))
+        v = rt.runtime.fixed_radius_neighbors(_pack(q), _pack(s), radius=0.4, k_max=5)
+        _assert_same_rows(v.to_numpy(), O.fixed_radius_neighbors(q, s, radius=0.4, k_max=5), False)
+        v.close()
+        v = rt.runtime.knn_rows(_pack(q), _pack(s), k=4)
+        _assert_same_rows(v.to_numpy(), O.knn_rows(q, s, k=4), True)
+        v.close()
+
+
+def test_prepared_fixed_radius_3d_matches_direct(gpu):
+    rng = np.random.default_rng(4)
+    s = _cols(rng.random((20000, 3)).astype(np.float32).astype(np.float64))
+    q = _cols(rng.random((3000, 3)).astype(np.float32).astype(np.float64))
+    prepared = rt.prepare_b200_fixed_radius_neighbors_3d(_pack(s), max_radius=0.05)
+    try:
+        for radius in (0.02, 0.05):
+            v = prepared.run_raw(_pack(q), radius=radius, k_max=16)
+            _assert_same_rows(v.to_numpy(), O.fixed_radius_neighbors(q, s, radius=radius, k_max=16, threads=8), False)
+            v.close()
+        with pytest.raises(ValueError):
+            prepared.run(_pack(q), radius=0.06, k_max=4)
+    finally:
+        prepared.close()
+
+
+def test_rt_run_facade_and_raw_mode(gpu):
+    case = next(c for c in CASES if c["name"] == "authored_frn_3d")
+    kernel = _kernel("fixed_radius_neighbors", 3, **case["options"])
+    q = G.points_records(case["query_points"], 3)
+    s = G.points_records(case["search_points"], 3)
+    result = rt.run(kernel, {"query_points": q, "search_points": s}, execution=rt.ExecutionPolicy(backend="b200"))
+    assert _as_tuples(result.rows, False) == G.expected_rows(case)
+    assert result.execution_report.accel_kind == "lbvh"
+    raw = rt.run_b200(kernel, result_mode="raw", query_points=q, search_points=s)
+    try:
+        assert raw.to_tuple_rows() == tuple(G.expected_rows(case))
+    finally:
+        raw.close()
+    prepared = rt.prepare_b200(kernel)
+    assert prepared.run(query_points=q, search_points=s) == rt.run_b200(kernel, query_points=q, search_points=s)
+
+
+def test_phase_timings_reported(gpu):
+    rng = np.random.default_rng(1)
+    s = _cols(rng.random((5000, 3)))
+    v = rt.runtime.fixed_radius_neighbors(_pack(s), _pack(s), radius=0.05, k_max=8)
+    v.close()
+    t = rt.last_phase_timings()
+    for phase in ("upload", "build", "traverse", "emit", "download", "total"):
+        assert phase in t and t[phase] >= 0.0

@@ -1,0 +1,78 @@
+"""Pins the CPU oracle (oracle/nn_oracle.c) to the reference's own outputs.
+
+Every golden case was produced by running the reference's cpu_python_reference
+(tests/golden/make_golden.py); the oracle must reproduce each row bit for bit,
+including the FP64 distance and the row order."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import golden_cases as G
+
+CASES = G.load_cases()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_oracle_matches_reference_case(case):
+    dim = case["dimension"]
+    q = G.points_columns(case["query_points"], dim)
+    s = G.points_columns(case["search_points"], dim)
+    opts = case["options"]
+    if case["predicate"] == "knn_rows":
+        rows = O.knn_rows(q, s, k=opts["k"])
+        got = G.rows_as_tuples(rows, True)
+    else:
+        ranked = case["predicate"] == "bounded_knn_rows"
+        rows = O.fixed_radius_neighbors(q, s, radius=opts["radius"], k_max=opts["k_max"], ranked=ranked)
+        got = G.rows_as_tuples(rows, ranked)
+    assert got == G.expected_rows(case)
+
+
+def test_oracle_matches_reference_config1_full():
+    z = G.load_config1()
+    q, s = G.config1_points()
+    rows = O.fixed_radius_neighbors(q, s, radius=0.02, k_max=4096, threads=4)
+    assert len(rows) == 20911 == len(z["query_id"])
+    assert np.array_equal(rows["query_id"], z["query_id"])
+    assert np.array_equal(rows["neighbor_id"], z["neighbor_id"])
+    assert np.array_equal(rows["distance"].view(np.uint64), z["distance"].view(np.uint64))
+
+
+@pytest.mark.parametrize("case", G.load_hausdorff(), ids=lambda c: f"copies{c['copies']}")
+def test_oracle_hausdorff_matches_reference_app(case):
+    a = G.points_columns(case["points_a"], 2)
+    b = G.points_columns(case["points_b"], 2)
+    for key, (q, s) in (("directed_a_to_b", (a, b)), ("directed_b_to_a", (b, a))):
+        got = O.directed_hausdorff(q, s)
+        exp = case[key]
+        assert got["distance"] == float.fromhex(exp["distance"])
+        assert (got["source_id"], got["target_id"], got["row_count"]) == (exp["source_id"], exp["target_id"], exp["row_count"])
+
+
+def test_oracle_threads_do_not_change_rows():
+    rng = np.random.default_rng(7)
+    p = rng.random((3000, 3)).astype(np.float32).astype(np.float64)
+    b = rng.random((2000, 3)).astype(np.float32).astype(np.float64)
+    q = {"id": rng.integers(0, 50, 3000).astype(np.uint32), "x": p[:, 0], "y": p[:, 1], "z": p[:, 2]}
+    s = {"id": np.arange(2000, dtype=np.uint32), "x": b[:, 0], "y": b[:, 1], "z": b[:, 2]}
+    one = O.fixed_radius_neighbors(q, s, radius=0.08, k_max=5, threads=1)
+    many = O.fixed_radius_neighbors(q, s, radius=0.08, k_max=5, threads=8)
+    assert G.rows_as_tuples(one, False) == G.rows_as_tuples(many, False)
+    k1 = O.knn_rows(q, s, k=7, threads=1)
+    k8 = O.knn_rows(q, s, k=7, threads=8)
+    assert G.rows_as_tuples(k1, True) == G.rows_as_tuples(k8, True)
+
+
+@pytest.mark.skipif(not O.reference_library_available(), reason="reference native oracle not built here")
+def test_restatement_agrees_with_reference_native_oracle():
+    """The reference's own C++ oracle (compiled from its sources into oracle/_ref)
+    sorts with a 1e-12 distance tolerance instead of exact ties; on tie-free
+    data both must give the same rows."""
+    rng = np.random.default_rng(11)
+    p = rng.random((800, 3))
+    b = rng.random((1500, 3))
+    q = {"id": np.arange(800, dtype=np.uint32), "x": p[:, 0], "y": p[:, 1], "z": p[:, 2]}
+    s = {"id": np.arange(1500, dtype=np.uint32), "x": b[:, 0], "y": b[:, 1], "z": b[:, 2]}
+    ours = O.fixed_radius_neighbors(q, s, radius=0.12, k_max=6)
+    ref = O.reference_fixed_radius_neighbors(O.pack_reference_points(q), O.pack_reference_points(s), radius=0.12, k_max=6)
+    assert G.rows_as_tuples(ours, False) == G.rows_as_tuples(ref, False)

@@ -1,0 +1,421 @@
+"""Benchmark: neighbor rows/s at 1,048,576 x 1,048,576 3D (exact row set).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload NAME]
+
+One step is one plain per-call launch of the hot path over one batch: build
+the LBVH over the 1,048,576 build points, run fixed-radius neighbors
+(radius 0.00287, k_max 64, mean ~28.5 rows per probe) for 1,048,576 probes and
+write the exact rows (RtdlFixedRadiusNeighborRow, FP64 distances) to HBM.
+Inputs are resident in HBM before timing; L2 is flushed (a 512 MiB write)
+between timed steps; each step is timed with CUDA events on the stream the
+library launches on, and the job time is the max over ranks.
+
+Multi-GPU (torchrun, one process per GPU): every rank holds a replica of the
+build set and answers its own 1,048,576 probes (weak scaling, no data-path
+collective); `value` is the rows of all ranks divided by the slowest rank's
+time.
+
+`e2e` is the same metric through the C ABI entry point
+rtdl_b200_run_fixed_radius_neighbors_3d with pinned host buffers: the timed
+region holds the host-to-device copy of both point sets and the device-to-host
+copy of the rows.
+
+`--impl reference` times the reference's own CPU implementation of the path
+(its native oracle, compiled from its sources into oracle/_ref/, sharded over
+all host cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "neighbor rows/s at 1M x 1M 3D (exact row set)"
+UNIT = "rows/s"
+RADIUS = 0.00287
+K_MAX = 64
+N_BUILD = 1 << 20
+N_PROBE = 1 << 20
+L2_FLUSH_BYTES = 512 << 20
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines
+# ---------------------------------------------------------------------------
+
+def cpu_baseline_port(probe, build, threads: int, budget_s: float = 10.0) -> dict:
+    """The oracle restatement (oracle/nn_oracle.c) on a bounded sample of probes."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(123)
+    n = 64 * threads
+    idx = np.sort(rng.choice(len(probe), n, replace=False))
+    t0 = time.perf_counter()
+    rows = O.fixed_radius_neighbors(probe[idx], build, radius=RADIUS, k_max=K_MAX, threads=threads)
+    dt = time.perf_counter() - t0
+    scale = max(1.0, min(64.0, budget_s / max(dt, 1e-3)))
+    n2 = min(len(probe), int(n * scale))
+    if n2 > n:
+        idx = np.sort(rng.choice(len(probe), n2, replace=False))
+        t0 = time.perf_counter()
+        rows = O.fixed_radius_neighbors(probe[idx], build, radius=RADIUS, k_max=K_MAX, threads=threads)
+        dt = time.perf_counter() - t0
+    return {"value": len(rows) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(idx)} seeded probes x all {len(build)} build points, {len(rows)} rows in {dt:.2f} s"}
+
+
+def cpu_reference_step(probe_idx, packed_build, probe, threads):
+    """One bounded sample of the reference's native oracle, sharded over threads."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+
+    shards = np.array_split(probe_idx, threads)
+    packed = [O.pack_reference_points(probe[s]) for s in shards if len(s)]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        results = list(ex.map(lambda pq: O.reference_fixed_radius_neighbors(pq, packed_build, radius=RADIUS, k_max=K_MAX), packed))
+    dt = time.perf_counter() - t0
+    return sum(len(r) for r in results), dt
+
+
+def run_reference_arm(args) -> int:
+    rank = _env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from rtdl_b200 import workloads
+
+    threads = os.cpu_count() or 1
+    probe, build = workloads.clustered_3d(N_BUILD, N_PROBE)
+    if O.reference_library_available():
+        kind = "reference"
+        packed_build = O.pack_reference_points(build)
+        rng = np.random.default_rng(321)
+        # size one step to ~10 s of CPU work: calibrate on a small sample first
+        probe_idx = np.sort(rng.choice(len(probe), 8 * threads, replace=False))
+        rows, dt = cpu_reference_step(probe_idx, packed_build, probe, threads)
+        per_step = int(min(len(probe), max(8 * threads, 8 * threads * (10.0 / max(dt, 1e-3)))))
+        samples = []
+        for i in range(args.warmup + args.steps):
+            idx = np.sort(rng.choice(len(probe), per_step, replace=False))
+            rows, dt = cpu_reference_step(idx, packed_build, probe, threads)
+            if i >= args.warmup:
+                samples.append((rows, dt))
+        total_rows = sum(r for r, _ in samples)
+        total_t = sum(t for _, t in samples)
+        value = total_rows / total_t
+        sample = (f"{per_step} seeded probes per step x all {len(build)} build points; reference native oracle "
+                  f"(src/native/oracle/rtdl_oracle_api.cpp) sharded over {threads} threads")
+    else:
+        kind = "port"
+        base = cpu_baseline_port(probe, build, threads)
+        value, total_t, sample = base["value"], None, base["sample"]
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": (total_t / max(1, args.steps) * 1e3) if total_t else None,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "clustered_3d_fixed_radius", "build": N_BUILD, "probe": N_PROBE, "radius": RADIUS,
+                   "k_max": K_MAX, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    import rtdl_b200 as rt
+    from rtdl_b200 import _native, workloads
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    rt.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+
+    def allreduce(v: float, op) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    # workload: shared build set, per-rank probe set (rank 0 gets the benchmark's own probes)
+    c = np.random.default_rng(0).random((64, 3))
+    build = workloads.records(workloads._mixture(np.random.default_rng(1), N_BUILD, c))
+    probe = workloads.records(workloads._mixture(np.random.default_rng(2 + 1000 * rank), N_PROBE, c))
+    dev = torch.device("cuda", local)
+    d_build = torch.from_numpy(build.view(np.uint8)).to(dev)
+    d_probe = torch.from_numpy(probe.view(np.uint8)).to(dev)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    overflow = torch.empty(N_PROBE, dtype=torch.uint8, device=dev)
+
+    def one_step(rows_buf, capacity):
+        scene = rt.B200Scene(None, dimension=3, stream=sh, device_points=(d_build.data_ptr(), N_BUILD))
+        try:
+            n = scene.query_device(d_probe.data_ptr(), N_PROBE, predicate="fixed_radius_neighbors", radius=RADIUS,
+                                   limit=K_MAX, rows_address=rows_buf.data_ptr() if rows_buf is not None else None,
+                                   rows_capacity=capacity, overflow_address=overflow.data_ptr(), stream=sh)
+            phases = _native.last_phase_timings()
+        finally:
+            scene.close()
+        return n, phases
+
+    rows_total, _ = one_step(None, 0)
+    rows_buf = torch.empty(rows_total * 16, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        one_step(rows_buf, rows_total)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = _native.launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    step_ms, phase_log = [], []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+        n, phases = one_step(rows_buf, rows_total)
+        with torch.cuda.stream(stream):
+            end.record(stream)
+        end.synchronize()
+        step_ms.append(start.elapsed_time(end))
+        phase_log.append(phases)
+        assert n == rows_total
+    torch.cuda.synchronize()
+    barrier()
+    launches = _native.launch_count() - launches0
+    clocks = sampler.stop()
+    local_ms = sum(step_ms)
+    job_ms = allreduce(local_ms, dist.ReduceOp.MAX if dist else None)
+    all_rows = allreduce(float(rows_total), dist.ReduceOp.SUM if dist else None)
+    value = all_rows * args.steps / (job_ms / 1e3)
+    ms_per_step = job_ms / args.steps
+
+    # phase (kernel) durations from the library's CUDA events on the launching stream
+    def mean_phase(name):
+        vals = [p.get(name, 0.0) for p in phase_log]
+        return sum(vals) / len(vals)
+
+    traverse_ms, emit_ms, prep_ms, scan_ms = (mean_phase("traverse"), mean_phase("emit"), mean_phase("query_prep"),
+                                              mean_phase("scan"))
+    query_ms = mean_phase("total")
+    build_ms = ms_per_step - query_ms
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        hbm_peak, peak_note = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        hbm_peak, peak_note = 6650.0, "fallback"
+    R = rows_total
+    # algorithmic bytes (per launch) of the two query kernels
+    traverse_bytes = N_PROBE * 16 + N_BUILD * 16 + R * 4 + N_PROBE * 5
+    emit_bytes = R * 4 + R * 16 + N_PROBE * (4 + 1 + 1 + 8 + 32)
+    if traverse_ms >= emit_ms:
+        dom, dom_ms, dom_bytes = "k_pass1 (LBVH traversal + FP64 band + per-query list)", traverse_ms, traverse_bytes
+    else:
+        dom, dom_ms, dom_bytes = "k_expand (exact FP64 row emission)", emit_ms, emit_bytes
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    phase_bytes = N_PROBE * 16 + N_BUILD * 16 + R * 16 + N_PROBE * 4 + N_PROBE // 8
+    phase_achieved = phase_bytes / (query_ms / 1e3) / 1e9
+
+    # e2e through the C ABI with pinned host buffers
+    e2e = None
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else min(args.steps, 5)
+    if e2e_steps > 0:
+        import ctypes
+
+        h_build = torch.from_numpy(build.view(np.uint8)).pin_memory()
+        h_probe = torch.from_numpy(probe.view(np.uint8)).pin_memory()
+        lib = _native.load_library()
+
+        def e2e_call():
+            rows = ctypes.c_void_p()
+            count = ctypes.c_size_t()
+            err = _native.error_buffer()
+            st = lib.rtdl_b200_run_fixed_radius_neighbors_3d(h_probe.data_ptr(), N_PROBE, h_build.data_ptr(), N_BUILD,
+                                                             RADIUS, K_MAX, ctypes.byref(rows), ctypes.byref(count), err,
+                                                             len(err))
+            _native.check_status(st, err)
+            lib.rtdl_b200_free_rows(rows)
+            return count.value
+
+        for _ in range(2):
+            e2e_call()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            assert e2e_call() == rows_total
+        t_local = time.perf_counter() - t0
+        barrier()
+        t_job = allreduce(t_local, dist.ReduceOp.MAX if dist else None)
+        e2e = {"value": all_rows * e2e_steps / t_job, "unit": UNIT, "h2d_bytes_per_step": (N_BUILD + N_PROBE) * 32,
+               "d2h_bytes_per_step": rows_total * 16, "ms_per_step": t_job / e2e_steps * 1e3,
+               "entry_point": "rtdl_b200_run_fixed_radius_neighbors_3d (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(probe, build, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 traversal + f64 band recheck and distances",
+            "data": "synthetic",
+            "config": {"workload": "clustered_3d_fixed_radius (plain per-call launch: LBVH build + query + exact rows)",
+                       "build": N_BUILD, "probe_per_gpu": N_PROBE, "radius": RADIUS, "k_max": K_MAX,
+                       "rows_per_gpu": rows_total, "row_bytes": 16, "l2": "flushed between steps (512 MiB write)",
+                       "parallelism": f"query-sharded replicas x{world}"},
+            "phases_ms": {"build": build_ms, "query_prep": prep_ms, "traverse": traverse_ms, "scan": scan_ms,
+                          "emit": emit_ms, "query_total": query_ms},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_note,
+                         "algorithmic_bytes": dom_bytes},
+            "phase_roofline": {"phase": "query+emit", "achieved": phase_achieved, "peak": hbm_peak, "unit": "GB/s",
+                               "frac": phase_achieved / hbm_peak, "algorithmic_bytes": phase_bytes},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

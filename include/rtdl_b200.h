@@ -207,6 +207,10 @@ RTDL_B200_API int rtdl_b200_scene_directed_hausdorff(
  * (name, value) pairs; returns the number of phases. */
 RTDL_B200_API int rtdl_b200_get_last_phase_timings(const char** names_out, double* values_ms_out, int capacity);
 
+/* Number of kernels this library has launched in the process so far (all
+ * devices).  Benchmarks read it before and after a timed region. */
+RTDL_B200_API int rtdl_b200_get_launch_count(unsigned long long* count_out);
+
 /* Tuning knobs (leaf size, threads per block); the autotuner sets these.
  * Returns 0 on success. */
 RTDL_B200_API int rtdl_b200_set_tuning(int leaf_size, int block_threads);

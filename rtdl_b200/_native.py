@@ -85,6 +85,7 @@ SIGNATURES = {
     "rtdl_b200_scene_directed_hausdorff": (_i, [_vp, _vp, _sz, _dp, _u32p, _u32p, _dp, _u32p, _cp, _sz]),
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i]),
+    "rtdl_b200_get_launch_count": (_i, [ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 
 
@@ -125,6 +126,13 @@ def check_status(status: int, error) -> None:
 
 def error_buffer():
     return ctypes.create_string_buffer(4096)
+
+
+def launch_count() -> int:
+    """Kernels launched by librtdl_b200 in this process so far."""
+    v = ctypes.c_ulonglong()
+    load_library().rtdl_b200_get_launch_count(ctypes.byref(v))
+    return int(v.value)
 
 
 def last_phase_timings() -> dict[str, float]:

@@ -8,6 +8,7 @@
 // Rows handed to the caller live in pinned host buffers from a small pool, so
 // the device-to-host copy runs at full PCIe rate; rtdl_b200_free_rows returns
 // them to the pool.
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -19,6 +20,12 @@
 #include "internal.cuh"
 
 namespace rtdl_b200 {
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}  // namespace
+
+void count_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 
 Tuning& tuning() {
   static Tuning t;
@@ -296,6 +303,12 @@ int rtdl_b200_get_last_phase_timings(const char** names_out, double* values_ms_o
     if (values_ms_out) values_ms_out[i] = g_last_timings[i].second;
   }
   return n;
+}
+
+int rtdl_b200_get_launch_count(unsigned long long* count_out) {
+  if (!count_out) return 1;
+  *count_out = g_launches.load(std::memory_order_relaxed);
+  return 0;
 }
 
 void rtdl_b200_free_rows(void* rows) {

@@ -21,6 +21,15 @@ namespace rtdl_b200 {
                                " at " #call);                                          \
   } while (0)
 
+// Counts kernel launches made by this library (reported by
+// rtdl_b200_get_launch_count) and checks the launch status.
+void count_launches(int n);
+#define RTDL_LAUNCHED(n)                              \
+  do {                                                \
+    ::rtdl_b200::count_launches(n);                   \
+    RTDL_CUDA_CHECK(cudaGetLastError());              \
+  } while (0)
+
 constexpr int kSmCount = 148;          // B200: 2 dies x 74 SMs
 constexpr int kMaxList = 64;           // per-query list capacity held in shared memory
 constexpr int kStackDepth = 64;        // traversal stack; Karras depth <= 30 code bits + 32 index bits

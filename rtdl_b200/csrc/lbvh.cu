@@ -293,7 +293,7 @@ __global__ void k_pack(uint32_t n, const float4* __restrict__ pts, const int* __
 
 void reset_stats(PointStats* stats, cudaStream_t s) {
   k_reset_stats<<<1, 32, 0, s>>>(stats);
-  RTDL_CUDA_CHECK(cudaGetLastError());
+  RTDL_LAUNCHED(1);
 }
 
 void prep_points(const void* points_dev, uint32_t n, int dim, float4* out, PointStats* stats, cudaStream_t s) {
@@ -303,13 +303,13 @@ void prep_points(const void* points_dev, uint32_t n, int dim, float4* out, Point
     k_prep<3><<<grid_for(n), kThreads, 0, s>>>(raw, n, out, stats);
   else
     k_prep<2><<<grid_for(n), kThreads, 0, s>>>(raw, n, out, stats);
-  RTDL_CUDA_CHECK(cudaGetLastError());
+  RTDL_LAUNCHED(1);
 }
 
 void morton_codes(const float4* pts, uint32_t n, int dim, const PointStats* box_stats, uint32_t* codes, cudaStream_t s) {
   if (n == 0) return;
   k_morton<<<grid_for(n), kThreads, 0, s>>>(pts, n, dim, box_stats, codes);
-  RTDL_CUDA_CHECK(cudaGetLastError());
+  RTDL_LAUNCHED(1);
 }
 
 Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, int leaf_size) {
@@ -340,7 +340,7 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
     k_gather<3><<<grid_for(n), kThreads, 0, s>>>(pts_in, raw, sc->perm, n, sc->pts, sc->pts64, sc->stats);
   else
     k_gather<2><<<grid_for(n), kThreads, 0, s>>>(pts_in, raw, sc->perm, n, sc->pts, sc->pts64, sc->stats);
-  RTDL_CUDA_CHECK(cudaGetLastError());
+  RTDL_LAUNCHED(1);
   dev_free(pts_in, s);
   if (n >= 2) {
     const uint32_t ni = n - 1;
@@ -358,7 +358,7 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
     k_refit<<<grid_for(n), kThreads, 0, s>>>(n, sc->pts, child_l, child_r, parent_int, parent_leaf, arrivals, boxes);
     sc->nodes = static_cast<float4*>(dev_alloc(sizeof(float4) * 4 * (size_t)ni, s));
     k_pack<<<grid_for(ni), kThreads, 0, s>>>(n, sc->pts, child_l, child_r, first, last, boxes, leaf_size, sc->nodes);
-    RTDL_CUDA_CHECK(cudaGetLastError());
+    RTDL_LAUNCHED(3);
     dev_free(child_l, s);
     dev_free(child_r, s);
     dev_free(first, s);

@@ -659,7 +659,7 @@ QueryPrep prepare_queries(Scene* sc, const void* queries_dev, uint32_t nq, bool 
   reset_stats(qp.qst, s);
   prep_points(queries_dev, nq, sc->dim, qp.qpts, qp.qst, s);
   k_bands<<<1, 32, 0, s>>>(sc->stats, qp.qst, radius, has_radius ? 1 : 0, qp.bands);
-  RTDL_CUDA_CHECK(cudaGetLastError());
+  RTDL_LAUNCHED(1);
   uint32_t* qcodes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   morton_codes(qp.qpts, nq, sc->dim, sc->stats, qcodes, s);
   iota_u32(qp.qorder, nq, s);
@@ -667,6 +667,7 @@ QueryPrep prepare_queries(Scene* sc, const void* queries_dev, uint32_t nq, bool 
   if (want_output_order) {
     qp.oorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
     k_extract_ids<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, qcodes);
+    RTDL_LAUNCHED(1);
     iota_u32(qp.oorder, nq, s);
     radix_sort_pairs(qcodes, qp.oorder, nq, 0, 32, &qp.bands->ids_sorted, s);
   }
@@ -714,6 +715,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
   if (all_heavy) {
     k_mark_all_heavy<<<grid_for(nq, 256), 256, 0, s>>>(qp.qorder, nq, sc->n, limit, counts, flags, temp, heavy_list,
                                                        heavy_m);
+    RTDL_LAUNCHED(1);
     RTDL_CUDA_CHECK(cudaMemcpyAsync(small, &nq, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // nq lives on this host stack frame
   } else {
@@ -744,7 +746,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
       RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
       k_pass1<false><<<blocks, threads, shm, s>>>(P);
     }
-    RTDL_CUDA_CHECK(cudaGetLastError());
+    RTDL_LAUNCHED(1);
   }
   if (timer) timer->mark("traverse");
   scan_counts_u64(counts, qp.oorder, &qp.bands->ids_sorted, nq, offsets, s);
@@ -818,7 +820,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
                                                small + 1);
     k_heavy_sort<<<H, kHeavyThreads, 0, s>>>(d_seg_off, d_seg_size, scratch, sc->perm);
     k_heavy_emit<<<H, kHeavyThreads, 0, s>>>(d_seg_off, heavy_out_off, d_out_cnt, scratch, heavy_out);
-    RTDL_CUDA_CHECK(cudaGetLastError());
+    RTDL_LAUNCHED(3);
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors above are read by the copies
     dev_free(d_seg_off, s);
     dev_free(d_seg_size, s);
@@ -856,7 +858,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
     E.error = small + 1;
     const unsigned int blocks = grid_for((uint64_t)nq * 32, kExpandThreads);
     k_expand<<<blocks, kExpandThreads, 0, s>>>(E);
-    RTDL_CUDA_CHECK(cudaGetLastError());
+    RTDL_LAUNCHED(1);
   }
   if (timer) timer->mark("emit");
   RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
@@ -900,7 +902,7 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   P.error = small + 1;
   const int threads = tuning().block_threads;
   k_pass1<true><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
-  RTDL_CUDA_CHECK(cudaGetLastError());
+  RTDL_LAUNCHED(1);
   if (timer) timer->mark("traverse");
   const unsigned int blocks = grid_for(nq, 256) < 2 * kSmCount ? grid_for(nq, 256) : 2 * kSmCount;
   Witness* partial = static_cast<Witness*>(dev_alloc(sizeof(Witness) * blocks, s));
@@ -908,7 +910,7 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   k_nearest_reduce<<<blocks, 256, 0, s>>>(sc->view(), qp.qpts, static_cast<const double*>(queries_dev), qstride, nq,
                                           temp, nearest_dist_dev, nearest_id_dev, partial);
   k_witness_final<<<1, 32, 0, s>>>(partial, (int)blocks, best);
-  RTDL_CUDA_CHECK(cudaGetLastError());
+  RTDL_LAUNCHED(2);
   Readback* rb = pinned_readback();
   Witness* hw = reinterpret_cast<Witness*>(rb);
   static_assert(sizeof(Witness) <= sizeof(Readback), "readback buffer too small");

@@ -146,7 +146,7 @@ void scan_impl(const uint32_t* counts, const uint32_t* order, const unsigned int
   k_scan_reduce<Out><<<tiles, kScanThreads, 0, s>>>(counts, order, identity_flag, n, sums);
   k_scan_tile_sums<Out><<<1, 1024, 0, s>>>(sums, tiles, out + n);
   k_scan_down<Out><<<tiles, kScanThreads, 0, s>>>(counts, order, identity_flag, n, sums, out);
-  RTDL_CUDA_CHECK(cudaGetLastError());
+  RTDL_LAUNCHED(3);
   dev_free(sums, s);
 }
 
@@ -230,7 +230,7 @@ void iota_u32(uint32_t* out, uint32_t n, cudaStream_t s) {
   unsigned int blocks = div_up(n, 256);
   if (blocks > 8 * kSmCount * 4) blocks = 8 * kSmCount * 4;
   k_iota<<<blocks, 256, 0, s>>>(out, n);
-  RTDL_CUDA_CHECK(cudaGetLastError());
+  RTDL_LAUNCHED(1);
 }
 
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int begin_bit, int end_bit,
@@ -255,6 +255,7 @@ void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int begin_bit,
       k_scan_tile_sums<uint32_t><<<1, 1024, 0, s>>>(hist_sums, htiles, hist + hist_n);
       k_scan_down<uint32_t><<<htiles, kScanThreads, 0, s>>>(hist, nullptr, nullptr, (uint32_t)hist_n, hist_sums, hist);
       k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, shift, hist, tiles, skip_flag);
+      RTDL_LAUNCHED(5);
     } else {
       // A padding pass beyond the key width: a plain copy keeps the ping-pong even.
       RTDL_CUDA_CHECK(cudaMemcpyAsync(ko, ki, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));

@@ -129,7 +129,7 @@ def pack_points(records=None, *, ids=None, x=None, y=None, z=None, dimension: in
         raise ValueError("packed points arrays must have identical lengths")
     if n and (ids_a.min() < 0 or ids_a.max() > 0xFFFFFFFF):
         raise ValueError("point ids must fit in uint32")
-    arr = np.empty(n, dtype=POINT3D_DTYPE if dim == 3 else POINT2D_DTYPE)
+    arr = np.zeros(n, dtype=POINT3D_DTYPE if dim == 3 else POINT2D_DTYPE)  # zeroed padding: deterministic bytes
     arr["id"] = ids_a.astype(np.uint32, copy=False)
     arr["x"] = np.asarray(x, dtype=np.float64)
     arr["y"] = np.asarray(y, dtype=np.float64)

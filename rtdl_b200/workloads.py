@@ -28,7 +28,7 @@ def records(points: np.ndarray, ids: np.ndarray | None = None) -> np.ndarray:
     from .runtime import POINT2D_DTYPE, POINT3D_DTYPE
 
     n, dim = points.shape
-    out = np.empty(n, dtype=POINT3D_DTYPE if dim == 3 else POINT2D_DTYPE)
+    out = np.zeros(n, dtype=POINT3D_DTYPE if dim == 3 else POINT2D_DTYPE)
     out["id"] = np.arange(n, dtype=np.uint32) if ids is None else ids
     out["x"] = points[:, 0]
     out["y"] = points[:, 1]

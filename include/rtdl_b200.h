@@ -207,6 +207,13 @@ RTDL_B200_API int rtdl_b200_scene_directed_hausdorff(
  * (name, value) pairs; returns the number of phases. */
 RTDL_B200_API int rtdl_b200_get_last_phase_timings(const char** names_out, double* values_ms_out, int capacity);
 
+/* Traversal counters of this thread's last query, recorded only when the
+ * environment variable RTDL_B200_STATS is set at load time: nodes visited,
+ * leaf points tested, in-radius candidates, list inserts, list shifts, FP64
+ * band re-decisions, largest leaf-point count of one query.  Returns the
+ * number of counters. */
+RTDL_B200_API int rtdl_b200_get_last_query_stats(unsigned long long* values_out, int capacity);
+
 /* Number of kernels this library has launched in the process so far (all
  * devices).  Benchmarks read it before and after a timed region. */
 RTDL_B200_API int rtdl_b200_get_launch_count(unsigned long long* count_out);

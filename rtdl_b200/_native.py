@@ -86,6 +86,7 @@ SIGNATURES = {
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i]),
     "rtdl_b200_get_launch_count": (_i, [ctypes.POINTER(ctypes.c_ulonglong)]),
+    "rtdl_b200_get_last_query_stats": (_i, [ctypes.POINTER(ctypes.c_ulonglong), _i]),
 }
 
 
@@ -133,6 +134,17 @@ def launch_count() -> int:
     v = ctypes.c_ulonglong()
     load_library().rtdl_b200_get_launch_count(ctypes.byref(v))
     return int(v.value)
+
+
+STAT_NAMES = ("nodes", "leaf_points", "in_radius", "inserts", "shifts", "band_checks", "max_count",
+              "generic_queries", "large_queries")
+
+
+def last_query_stats() -> dict[str, int]:
+    """Traversal counters of this thread's last query (RTDL_B200_STATS must be set)."""
+    vals = (ctypes.c_ulonglong * 16)()
+    n = load_library().rtdl_b200_get_last_query_stats(vals, 16)
+    return {STAT_NAMES[i]: int(vals[i]) for i in range(min(n, len(STAT_NAMES)))}
 
 
 def last_phase_timings() -> dict[str, float]:

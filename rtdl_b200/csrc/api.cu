@@ -305,6 +305,12 @@ int rtdl_b200_get_last_phase_timings(const char** names_out, double* values_ms_o
   return n;
 }
 
+int rtdl_b200_get_last_query_stats(unsigned long long* values_out, int capacity) {
+  const auto& v = last_stats();
+  for (int i = 0; i < (int)v.size() && i < capacity; ++i) values_out[i] = v[i];
+  return (int)v.size();
+}
+
 int rtdl_b200_get_launch_count(unsigned long long* count_out) {
   if (!count_out) return 1;
   *count_out = g_launches.load(std::memory_order_relaxed);

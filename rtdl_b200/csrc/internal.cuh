@@ -182,6 +182,13 @@ struct HausdorffResult {
 HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint32_t nq, double* nearest_dist_dev,
                                        uint32_t* nearest_id_dev, cudaStream_t s, PhaseTimer* timer);
 
+// Traversal counters of the last query on this thread (filled only when the
+// environment variable RTDL_B200_STATS is set): nodes visited, leaf points
+// tested, in-radius candidates, list inserts, list shifts, FP64 band checks,
+// max count of one query, queries on the generic path, queries with 65..128
+// candidates.
+std::vector<unsigned long long>& last_stats();
+
 inline unsigned int div_up(unsigned long long a, unsigned long long b) { return (unsigned int)((a + b - 1) / b); }
 
 }  // namespace rtdl_b200

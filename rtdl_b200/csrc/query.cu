@@ -27,6 +27,8 @@
 //   * Queries needing more than 64 rows with more than 64 candidates (large
 //     k_max, or k > 64) go to a generic block-per-query path (gather, bitonic
 //     sort in global memory, emit).
+#include <cstdlib>
+
 #include "internal.cuh"
 
 namespace rtdl_b200 {
@@ -116,13 +118,35 @@ __device__ __forceinline__ float key_tol(const Ctx& c, float m) {
   return t;
 }
 
-// Exact comparison of two candidates by the reference's sort key.
-__device__ __noinline__ bool exact_before(const Ctx& c, uint32_t ia, uint32_t ib) {
-  const double da = __dsqrt_rn(exact_d2(c, ia)), db = __dsqrt_rn(exact_d2(c, ib));
+__device__ __forceinline__ double exact_d2_at(double ex, double ey, double ez, const float4* pts, const double* pts64,
+                                              int inexact, uint32_t i) {
+  double sx, sy, sz;
+  if (inexact) {
+    const double* p = pts64 + 3ull * i;
+    sx = p[0];
+    sy = p[1];
+    sz = p[2];
+  } else {
+    const float4 p = __ldg(&pts[i]);
+    sx = p.x;
+    sy = p.y;
+    sz = p.z;
+  }
+  const double dx = __dsub_rn(sx, ex), dy = __dsub_rn(sy, ey), dz = __dsub_rn(sz, ez);
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// Exact comparison of two candidates by the reference's sort key.  Out of
+// line and with scalar arguments, so the caller's query context stays in
+// registers.
+__device__ __noinline__ bool exact_before(double ex, double ey, double ez, const float4* pts, const double* pts64,
+                                          const uint32_t* perm, int inexact, uint32_t ia, uint32_t ib) {
+  const double da = __dsqrt_rn(exact_d2_at(ex, ey, ez, pts, pts64, inexact, ia));
+  const double db = __dsqrt_rn(exact_d2_at(ex, ey, ez, pts, pts64, inexact, ib));
   if (da != db) return da < db;
-  const uint32_t na = __float_as_uint(__ldg(&c.pts[ia].w)), nb = __float_as_uint(__ldg(&c.pts[ib].w));
+  const uint32_t na = __float_as_uint(__ldg(&pts[ia].w)), nb = __float_as_uint(__ldg(&pts[ib].w));
   if (na != nb) return na < nb;
-  return __ldg(&c.perm[ia]) < __ldg(&c.perm[ib]);
+  return __ldg(&perm[ia]) < __ldg(&perm[ib]);
 }
 
 // True when candidate a orders strictly before candidate b.  FP32 keys decide
@@ -132,7 +156,7 @@ __device__ __forceinline__ bool before(const Ctx& c, float ka, uint32_t ia, floa
   const float t = key_tol(c, fmaxf(ka, kb));
   if (d > t) return true;
   if (-d > t) return false;
-  return exact_before(c, ia, ib);
+  return exact_before(c.ex, c.ey, c.ez, c.pts, c.pts64, c.perm, c.scene_inexact, ia, ib);
 }
 
 // Every point in a box whose FP32 key lower bound is kbox orders after the
@@ -166,12 +190,17 @@ struct Pass1Params {
   uint32_t* heavy_m;
   unsigned int* heavy_count;
   unsigned int* error;
+  unsigned long long* stats;  // kStatCount counters, only with STATS
 };
+
+// Traversal counters gathered by the STATS instantiation (diagnostics).
+enum Stat { kStatNodes, kStatLeafPoints, kStatInRadius, kStatInserts, kStatShifts, kStatBand, kStatMaxLeafPoints,
+            kStatGenericQueries, kStatLargeQueries, kStatCount };
 
 // One thread per query, queries in Morton order so a warp walks neighbouring
 // subtrees.  KNN == false: radius-limited (fixed_radius_neighbors and
 // bounded_knn_rows); KNN == true: k nearest.
-template <bool KNN>
+template <bool KNN, bool STATS>
 __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
   extern __shared__ uint32_t smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -209,6 +238,7 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
   bool prune = false;  // the list is complete: only candidates ordering before its last entry matter
   float klast = INFINITY;
   uint32_t ilast = kNone;
+  unsigned long long st_nodes = 0, st_points = 0, st_inserts = 0, st_shifts = 0, st_band = 0;
 
   auto insert = [&](float key, uint32_t idx) {
     int pos;
@@ -224,7 +254,9 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
       lkey[pos * 32 + lane] = __float_as_uint(pk);
       lidx[pos * 32 + lane] = pi;
       --pos;
+      if (STATS) ++st_shifts;
     }
+    if (STATS) ++st_inserts;
     lkey[pos * 32 + lane] = __float_as_uint(key);
     lidx[pos * 32 + lane] = idx;
     if (len == L) {
@@ -234,6 +266,7 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
   };
 
   auto visit_leaf = [&](int first, int cnt) {
+    if (STATS) st_points += cnt;
     for (int i = first; i < first + cnt; ++i) {
       const float4 p = __ldg(&S.pts[i]);
       const float dx = p.x - c.qx, dy = p.y - c.qy, dz = p.z - c.qz;
@@ -241,7 +274,10 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
       if (!KNN) {
         if (d2 > B.hi2) continue;
         if (prune && !before(c, d2, (uint32_t)i, klast, ilast)) continue;
-        if (d2 >= B.lo2 && exact_d2(c, (uint32_t)i) > B.r2) continue;
+        if (d2 >= B.lo2) {
+          if (STATS) ++st_band;
+          if (exact_d2(c, (uint32_t)i) > B.r2) continue;
+        }
         ++count;
         if (heavy) continue;
         if (len < L) {
@@ -277,6 +313,7 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
       int cur = S.root_ref;
       while (true) {
         const float4* nd = S.nodes + 4 * (size_t)cur;
+        if (STATS) ++st_nodes;
         const float4 a = __ldg(nd), b = __ldg(nd + 1), e = __ldg(nd + 2), f = __ldg(nd + 3);
         float k0 = box_d2(c.qx, c.qy, c.qz, a, b), k1 = box_d2(c.qx, c.qy, c.qz, e, f);
         int r0 = __float_as_int(a.w), n0 = __float_as_int(b.w);
@@ -319,6 +356,15 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
     }
   }
 
+  if (STATS) {
+    atomicAdd(&P.stats[kStatNodes], st_nodes);
+    atomicAdd(&P.stats[kStatLeafPoints], st_points);
+    atomicAdd(&P.stats[kStatInRadius], (unsigned long long)count);
+    atomicAdd(&P.stats[kStatInserts], st_inserts);
+    atomicAdd(&P.stats[kStatShifts], st_shifts);
+    atomicAdd(&P.stats[kStatBand], st_band);
+    atomicMax(&P.stats[kStatMaxLeafPoints], st_points);
+  }
   uint8_t fl = 0;
   if (!KNN) {
     P.counts[qin] = count < kmax ? count : kmax;
@@ -337,6 +383,430 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
     for (int j = 0; j < len; ++j) dst[j] = lidx[j * 32 + lane];
   }
   P.flags[qin] = fl;
+}
+
+// ---- fixed-radius collect pass ----------------------------------------------
+// One thread per query in Morton order.  The traversal is a while-while loop:
+// a lane walks internal nodes until it holds a leaf bucket, then all lanes
+// test their buckets together.  In-radius candidates are appended unsorted to
+// the query's slab (capacity C); the exact in-radius count is kept, so the
+// overflow flag and the row offsets are exact without any per-query list.
+constexpr int kSlab = 128;  // slab capacity (candidates kept per query)
+
+struct CollectParams {
+  SceneView S;
+  const float4* qpts;
+  const double* qraw;
+  int qstride;
+  const uint32_t* qorder;
+  uint32_t nq;
+  uint32_t kmax;
+  const DevBands* bands;
+  uint32_t* slab;        // nq * kSlab
+  uint32_t* counts;      // min(count, kmax), query input order
+  uint8_t* ncand;        // min(count, kSlab)
+  uint8_t* flags;        // bit0: count > kmax, bit1: count > kSlab (generic path), bit2: count > 64
+  uint32_t* heavy_list;
+  uint32_t* heavy_m;
+  uint32_t* big_list;
+  unsigned int* small;   // [0] heavy count, [1] error bits, [2] big count
+  unsigned long long* stats;
+};
+
+template <bool STATS>
+__global__ void __launch_bounds__(256) k_collect(CollectParams P) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P.nq) return;
+  const uint32_t qin = P.qorder[t];
+  const float4 q = P.qpts[qin];
+  const DevBands B = *P.bands;
+  const SceneView& S = P.S;
+  const int scene_inexact = *S.inexact;
+  double ex = 0.0, ey = 0.0, ez = 0.0;
+  bool have_exact = false;
+  uint32_t* slab = P.slab + (size_t)qin * kSlab;
+  uint32_t count = 0;
+  unsigned long long st_nodes = 0, st_points = 0, st_band = 0;
+
+  int2 stack[kStackDepth];
+  int sp = 0;
+  int ref = S.root_ref, cnt = S.root_cnt;
+  bool alive = S.n > 0;
+  while (alive) {
+    // internal nodes until this lane holds a leaf bucket
+    while (alive && cnt == 0) {
+      const float4* nd = S.nodes + 4 * (size_t)ref;
+      if (STATS) ++st_nodes;
+      const float4 a = __ldg(nd), b = __ldg(nd + 1), e = __ldg(nd + 2), f = __ldg(nd + 3);
+      const bool h0 = box_d2(q.x, q.y, q.z, a, b) <= B.box_hi2;
+      const bool h1 = box_d2(q.x, q.y, q.z, e, f) <= B.box_hi2;
+      if (h0) {
+        if (h1) {
+          if (sp >= kStackDepth) {
+            atomicOr(&P.small[1], 1u);
+            alive = false;
+            break;
+          }
+          stack[sp++] = make_int2(__float_as_int(e.w), __float_as_int(f.w));
+        }
+        ref = __float_as_int(a.w);
+        cnt = __float_as_int(b.w);
+      } else if (h1) {
+        ref = __float_as_int(e.w);
+        cnt = __float_as_int(f.w);
+      } else if (sp > 0) {
+        --sp;
+        ref = stack[sp].x;
+        cnt = stack[sp].y;
+      } else {
+        alive = false;
+      }
+    }
+    if (!alive) break;
+    if (STATS) st_points += cnt;
+    for (int i = ref; i < ref + cnt; ++i) {
+      const float4 p = __ldg(&S.pts[i]);
+      const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+      const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      if (d2 > B.hi2) continue;
+      if (d2 >= B.lo2) {
+        if (STATS) ++st_band;
+        if (!have_exact) {
+          const double* r = P.qraw + (size_t)qin * P.qstride;
+          ex = r[1];
+          ey = r[2];
+          ez = P.qstride == 4 ? r[3] : 0.0;
+          have_exact = true;
+        }
+        if (exact_d2_at(ex, ey, ez, S.pts, S.pts64, scene_inexact, (uint32_t)i) > B.r2) continue;
+      }
+      if (count < (uint32_t)kSlab) slab[count] = (uint32_t)i;
+      ++count;
+    }
+    if (sp > 0) {
+      --sp;
+      ref = stack[sp].x;
+      cnt = stack[sp].y;
+    } else {
+      alive = false;
+    }
+  }
+  if (STATS) {
+    atomicAdd(&P.stats[kStatNodes], st_nodes);
+    atomicAdd(&P.stats[kStatLeafPoints], st_points);
+    atomicAdd(&P.stats[kStatInRadius], (unsigned long long)count);
+    atomicAdd(&P.stats[kStatBand], st_band);
+    atomicMax(&P.stats[kStatMaxLeafPoints], (unsigned long long)count);
+  }
+  const uint32_t kmax = P.kmax;
+  P.counts[qin] = count < kmax ? count : kmax;
+  uint8_t fl = count > kmax ? 1 : 0;
+  if (count > (uint32_t)kSlab) {
+    fl |= 2;
+    const unsigned int h = atomicAdd(&P.small[0], 1u);
+    P.heavy_list[h] = qin;
+    P.heavy_m[h] = count;
+    slab[0] = h;  // the generic path's slot for this query
+  } else if (count > 64) {
+    fl |= 4;
+    P.big_list[atomicAdd(&P.small[2], 1u)] = qin;
+  }
+  P.ncand[qin] = (uint8_t)(count < (uint32_t)kSlab ? count : (uint32_t)kSlab);
+  P.flags[qin] = fl;
+}
+
+// ---- register sorting network --------------------------------------------
+// Batcher's odd-even merge sort, fully unrolled: every index is a compile-time
+// constant, so the array lives in registers and each compare-exchange is one
+// min and one max.
+__device__ __forceinline__ void cmpswap(uint32_t& a, uint32_t& b) {
+  const uint32_t lo = min(a, b), hi = max(a, b);
+  a = lo;
+  b = hi;
+}
+
+// Batcher's odd-even merge sort network as a compile-time table of
+// compare-exchange pairs (for N = 32: 191 pairs, N = 64: 543).
+template <int N>
+struct OddEvenMergeNet {
+  static constexpr int count() {
+    int c = 0;
+    for (int p = 1; p < N; p <<= 1)
+      for (int k = p; k >= 1; k >>= 1)
+        for (int j = k % p; j + k < N; j += 2 * k)
+          for (int i = 0; i < k; ++i)
+            if (i + j + k < N && (i + j) / (2 * p) == (i + j + k) / (2 * p)) ++c;
+    return c;
+  }
+  static constexpr int kSize = count();
+  unsigned char a[kSize];
+  unsigned char b[kSize];
+  constexpr OddEvenMergeNet() : a(), b() {
+    int c = 0;
+    for (int p = 1; p < N; p <<= 1)
+      for (int k = p; k >= 1; k >>= 1)
+        for (int j = k % p; j + k < N; j += 2 * k)
+          for (int i = 0; i < k; ++i)
+            if (i + j + k < N && (i + j) / (2 * p) == (i + j + k) / (2 * p)) {
+              a[c] = (unsigned char)(i + j);
+              b[c] = (unsigned char)(i + j + k);
+              ++c;
+            }
+  }
+};
+
+template <int N>
+__device__ __forceinline__ void sort_network(uint32_t (&e)[N]) {
+  constexpr OddEvenMergeNet<N> net{};
+#pragma unroll
+  for (int t = 0; t < OddEvenMergeNet<N>::kSize; ++t) cmpswap(e[net.a[t]], e[net.b[t]]);
+}
+
+// Emitted row writer shared by the lane-per-query emit kernels.
+struct RowSink {
+  void* rows;
+  unsigned long long capacity;
+  int ranked;
+  __device__ __forceinline__ void put(unsigned long long row, uint32_t qid, uint32_t nid, double dist,
+                                      uint32_t rank) const {
+    if (row >= capacity) return;
+    const unsigned long long db = (unsigned long long)__double_as_longlong(dist);
+    if (!ranked) {
+      reinterpret_cast<uint4*>(rows)[row] = make_uint4(qid, nid, (uint32_t)db, (uint32_t)(db >> 32));
+    } else {
+      uint2* out = reinterpret_cast<uint2*>(static_cast<char*>(rows) + row * 24);
+      out[0] = make_uint2(qid, nid);
+      out[1] = make_uint2((uint32_t)db, (uint32_t)(db >> 32));
+      out[2] = make_uint2(rank, 0u);
+    }
+  }
+};
+
+struct EmitParams {
+  SceneView S;
+  const float4* qpts;
+  const double* qraw;
+  int qstride;
+  const uint32_t* qorder;     // Morton order (all-query emit) or the list of large queries
+  uint32_t nwork;
+  const uint32_t* qrank;      // query input index -> output rank (identity when ids are sorted)
+  const DevBands* bands;
+  const uint32_t* slab;
+  const uint8_t* ncand;
+  const uint8_t* flags;
+  const unsigned long long* offsets;
+  uint32_t kmax;
+  RowSink sink;
+  uint8_t* overflow_out;
+};
+
+// Packed element: FP32 d2 key with its low SHIFT mantissa bits replaced by the
+// slab slot.  Keys closer than two truncated units are re-decided exactly.
+template <int SHIFT>
+__device__ __forceinline__ uint32_t pack_key(float d2, uint32_t slot) {
+  return (__float_as_uint(d2) & ~((1u << SHIFT) - 1u)) | slot;
+}
+
+// FP32-comparable key of candidate i (exact inputs: FP32 d2; inexact inputs:
+// the exact FP64 d2 rounded to FP32, so the key error stays relative).
+__device__ __forceinline__ float cand_key(const SceneView& S, int any_inexact, int scene_inexact, const float4& q,
+                                          double ex, double ey, double ez, uint32_t i) {
+  if (!any_inexact) {
+    const float4 p = __ldg(&S.pts[i]);
+    const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+    return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+  }
+  return __double2float_rn(exact_d2_at(ex, ey, ez, S.pts, S.pts64, scene_inexact, i));
+}
+
+// After the network: the sorted packed keys go to a per-thread column of
+// shared memory ([slot][thread], conflict free) so the register array is dead
+// before any call; neighbours whose truncated keys differ by at most one unit
+// are re-decided exactly (odd-even transposition restricted to those pairs,
+// bounded by n passes), then the rows are written.
+template <int N, int SHIFT>
+__device__ __forceinline__ bool store_sorted(const uint32_t (&e)[N], int n, uint32_t* col, int stride) {
+  bool amb = false;
+#pragma unroll
+  for (int i = 0; i + 1 < N; ++i)
+    if (i + 1 < n) amb |= (e[i + 1] >> SHIFT) - (e[i] >> SHIFT) <= 1u;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    if (i < n) col[i * stride] = e[i];
+  return amb;
+}
+
+template <int SHIFT>
+__device__ __noinline__ void exact_fixup(uint32_t* col, int stride, int n, const uint32_t* slab, SceneView S,
+                                         int inexact, double ex, double ey, double ez) {
+  constexpr uint32_t kMask = (1u << SHIFT) - 1u;
+  for (int pass = 0; pass < n; ++pass) {
+    bool changed = false;
+    for (int parity = 0; parity < 2; ++parity) {
+      for (int i = parity; i + 1 < n; i += 2) {
+        const uint32_t a = col[i * stride], b = col[(i + 1) * stride];
+        if ((b >> SHIFT) - (a >> SHIFT) > 1u) continue;
+        if (exact_before(ex, ey, ez, S.pts, S.pts64, S.perm, inexact, slab[b & kMask], slab[a & kMask])) {
+          col[i * stride] = b;
+          col[(i + 1) * stride] = a;
+          changed = true;
+        }
+      }
+    }
+    if (!changed) break;
+  }
+}
+
+// Exact insertion sort of all n candidates by the reference key (slots in
+// col).  Used when the 64/65 boundary of a large query is ambiguous in FP32.
+__device__ __noinline__ void exact_sort_all(uint32_t* col, int stride, int n, const uint32_t* slab, SceneView S,
+                                            int inexact, double ex, double ey, double ez) {
+  for (int i = 0; i < n; ++i) col[i * stride] = (uint32_t)i;
+  for (int i = 1; i < n; ++i) {
+    const uint32_t v = col[i * stride];
+    int j = i;
+    while (j > 0) {
+      const uint32_t u = col[(j - 1) * stride];
+      if (!exact_before(ex, ey, ez, S.pts, S.pts64, S.perm, inexact, slab[v], slab[u])) break;
+      col[j * stride] = u;
+      --j;
+    }
+    col[j * stride] = v;
+  }
+}
+
+template <int SHIFT>
+__device__ __forceinline__ void emit_rows(const uint32_t* col, int stride, int kk, const uint32_t* slab,
+                                          const SceneView& S, int inexact, double ex, double ey, double ez,
+                                          uint32_t qid, unsigned long long base, const RowSink& sink) {
+  constexpr uint32_t kMask = (1u << SHIFT) - 1u;
+  for (int s = 0; s < kk; ++s) {
+    const uint32_t i = slab[col[s * stride] & kMask];
+    const float4 p = __ldg(&S.pts[i]);
+    const double dist = __dsqrt_rn(exact_d2_at(ex, ey, ez, S.pts, S.pts64, inexact, i));
+    sink.put(base + s, qid, __float_as_uint(p.w), dist, (uint32_t)s + 1);
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void emit_one_query(const EmitParams& P, uint32_t qin, int n, int inexact, int any_inexact,
+                                               uint32_t* col, int stride) {
+  constexpr int SHIFT = 6;
+  const float4 q = P.qpts[qin];
+  const double* r = P.qraw + (size_t)qin * P.qstride;
+  const double ex = r[1], ey = r[2], ez = P.qstride == 4 ? r[3] : 0.0;
+  const uint32_t* slab = P.slab + (size_t)qin * kSlab;
+  bool amb;
+  {
+    uint32_t e[N];
+#pragma unroll
+    for (int s = 0; s < N; ++s)
+      e[s] = s < n ? pack_key<SHIFT>(cand_key(P.S, any_inexact, inexact, q, ex, ey, ez, slab[s]), (uint32_t)s)
+                   : 0xFFFFFFFFu;
+    sort_network<N>(e);
+    amb = store_sorted<N, SHIFT>(e, n, col, stride);
+  }
+  if (amb) exact_fixup<SHIFT>(col, stride, n, slab, P.S, inexact, ex, ey, ez);
+  const int kk = n < (int)P.kmax ? n : (int)P.kmax;
+  emit_rows<SHIFT>(col, stride, kk, slab, P.S, inexact, ex, ey, ez, __float_as_uint(q.w), P.offsets[P.qrank[qin]],
+                   P.sink);
+}
+
+// Lane-per-query emit for queries with at most 64 candidates, in Morton order
+// so a warp's 32 queries are alike; warps whose queries all have <= 32
+// candidates use the 32-wide network.  Dynamic shared memory: 64 words per
+// thread.
+__global__ void __launch_bounds__(128) k_emit_lanes(EmitParams P) {
+  extern __shared__ uint32_t emit_smem[];
+  uint32_t* col = emit_smem + threadIdx.x;
+  const int stride = blockDim.x;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = t < P.nwork;
+  const uint32_t qin = valid ? P.qorder[t] : 0u;
+  const uint8_t fl = valid ? P.flags[qin] : 0;
+  if (valid && P.overflow_out) P.overflow_out[qin] = fl & 1;
+  const bool mine = valid && (fl & 6) == 0;
+  const int n = mine ? (int)P.ncand[qin] : 0;
+  const int inexact = *P.S.inexact;
+  const int any_inexact = P.bands->any_inexact;
+  const unsigned int active = __ballot_sync(0xffffffffu, mine && n > 0);
+  if (!(mine && n > 0)) return;
+  if (__all_sync(active, n <= 32))
+    emit_one_query<32>(P, qin, n, inexact, any_inexact, col, stride);
+  else
+    emit_one_query<64>(P, qin, n, inexact, any_inexact, col, stride);
+}
+
+// Lane-per-query emit for queries with 65..128 candidates: the first 64 are
+// sorted and parked in shared memory, the rest sorted in registers, then a
+// bitonic keep-smallest merge yields the 64 nearest in order.  If the best
+// dropped candidate is within one truncated unit of the last kept one, the
+// cut at 64 is not decided by FP32 and all candidates are sorted exactly.
+// Dynamic shared memory: 128 words per thread.
+__global__ void __launch_bounds__(64) k_emit_big(EmitParams P) {
+  constexpr int SHIFT = 7;
+  constexpr int N = 64;
+  extern __shared__ uint32_t emit_smem[];
+  uint32_t* col = emit_smem + threadIdx.x;
+  const int stride = blockDim.x;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P.nwork) return;
+  const uint32_t qin = P.qorder[t];
+  const int n = (int)P.ncand[qin];
+  const int inexact = *P.S.inexact;
+  const int any_inexact = P.bands->any_inexact;
+  const float4 q = P.qpts[qin];
+  const double* r = P.qraw + (size_t)qin * P.qstride;
+  const double ex = r[1], ey = r[2], ez = P.qstride == 4 ? r[3] : 0.0;
+  const uint32_t* slab = P.slab + (size_t)qin * kSlab;
+  bool amb = false, cut_ambiguous = false;
+  {
+    uint32_t e[N];
+#pragma unroll
+    for (int s = 0; s < N; ++s)
+      e[s] = pack_key<SHIFT>(cand_key(P.S, any_inexact, inexact, q, ex, ey, ez, slab[s]), (uint32_t)s);
+    sort_network<N>(e);
+#pragma unroll
+    for (int s = 0; s < N; ++s) col[s * stride] = e[s];
+  }
+  {
+    uint32_t f[N];
+#pragma unroll
+    for (int s = 0; s < N; ++s)
+      f[s] = s + N < n
+                 ? pack_key<SHIFT>(cand_key(P.S, any_inexact, inexact, q, ex, ey, ez, slab[s + N]), (uint32_t)(s + N))
+                 : 0xFFFFFFFFu;
+    sort_network<N>(f);
+    uint32_t g[N];
+    uint32_t dropped = 0xFFFFFFFFu;  // smallest candidate not kept
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const uint32_t a = col[i * stride], b = f[N - 1 - i];
+      g[i] = min(a, b);  // the 64 smallest, as a bitonic sequence
+      dropped = min(dropped, max(a, b));
+    }
+#pragma unroll
+    for (int k = N / 2; k >= 1; k >>= 1) {
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+        if ((i & k) == 0) cmpswap(g[i], g[i + k]);
+    }
+    cut_ambiguous = (dropped >> SHIFT) - (g[N - 1] >> SHIFT) <= 1u;
+    if (!cut_ambiguous) amb = store_sorted<N, SHIFT>(g, N, col, stride);
+  }
+  if (cut_ambiguous)
+    exact_sort_all(col, stride, n, slab, P.S, inexact, ex, ey, ez);
+  else if (amb)
+    exact_fixup<SHIFT>(col, stride, N, slab, P.S, inexact, ex, ey, ez);
+  const int kk = (int)P.kmax < N ? (int)P.kmax : N;
+  emit_rows<SHIFT>(col, stride, kk, slab, P.S, inexact, ex, ey, ez, __float_as_uint(q.w), P.offsets[P.qrank[qin]],
+                   P.sink);
+}
+
+__global__ void k_invert(const uint32_t* order, uint32_t n, const unsigned int* identity_flag, uint32_t* inv) {
+  const bool ident = *identity_flag != 0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+    inv[ident ? j : order[j]] = (uint32_t)j;
 }
 
 // k > 64 KNN: every query takes the generic path.
@@ -427,6 +897,95 @@ __global__ void __launch_bounds__(kHeavyThreads)
   }
 }
 
+// Generic-path gather for a radius query with more than kSlab candidates: one
+// warp per query walks the BVH with a warp-uniform stack; the lanes test a leaf
+// bucket's points together and append in-radius candidates with a ballot
+// prefix (no atomics).
+__global__ void __launch_bounds__(32)
+    k_heavy_gather_bvh(SceneView S, const float4* qpts, const double* qraw, int qstride, const uint32_t* heavy_list,
+                       const unsigned long long* seg_off, const uint32_t* seg_size, const DevBands* bands,
+                       HeavyEntry* scratch, unsigned int* error) {
+  const int lane = threadIdx.x;
+  const uint32_t h = blockIdx.x;
+  const uint32_t qin = heavy_list[h];
+  const DevBands B = *bands;
+  const Ctx c = make_ctx(S, qpts, qraw, qstride, qin, B);
+  HeavyEntry* seg = scratch + seg_off[h];
+  const uint32_t P2 = seg_size[h];
+  const unsigned int lt_mask = (1u << lane) - 1u;
+  uint32_t cnt = 0;
+  int2 stack[kStackDepth];
+  int sp = 0;
+  int ref = S.root_ref, leaf = S.root_cnt;
+  bool alive = S.n > 0;
+  while (alive) {
+    if (leaf > 0) {
+      bool acc = false;
+      const uint32_t i = (uint32_t)(ref + lane);
+      if (lane < leaf) {
+        const float4 p = __ldg(&S.pts[i]);
+        const float dx = p.x - c.qx, dy = p.y - c.qy, dz = p.z - c.qz;
+        const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        acc = d2 <= B.hi2 && (d2 < B.lo2 || exact_d2(c, i) <= B.r2);
+      }
+      const unsigned int m = __ballot_sync(0xffffffffu, acc);
+      if (acc) {
+        const uint32_t pos = cnt + __popc(m & lt_mask);
+        if (pos < P2) {
+          HeavyEntry en;
+          en.key = (unsigned long long)__double_as_longlong(__dsqrt_rn(exact_d2(c, i)));
+          en.nid = __float_as_uint(__ldg(&S.pts[i].w));
+          en.sidx = i;
+          seg[pos] = en;
+        } else {
+          atomicOr(error, 2u);
+        }
+      }
+      cnt += __popc(m);
+      leaf = 0;
+      if (sp > 0) {
+        --sp;
+        ref = stack[sp].x;
+        leaf = stack[sp].y;
+      } else {
+        alive = false;
+      }
+      continue;
+    }
+    const float4* nd = S.nodes + 4 * (size_t)ref;
+    const float4 a = __ldg(nd), b = __ldg(nd + 1), e = __ldg(nd + 2), f = __ldg(nd + 3);
+    const bool h0 = box_d2(c.qx, c.qy, c.qz, a, b) <= B.box_hi2;
+    const bool h1 = box_d2(c.qx, c.qy, c.qz, e, f) <= B.box_hi2;
+    if (h0) {
+      if (h1) {
+        if (sp >= kStackDepth) {
+          atomicOr(error, 1u);
+          break;
+        }
+        stack[sp++] = make_int2(__float_as_int(e.w), __float_as_int(f.w));
+      }
+      ref = __float_as_int(a.w);
+      leaf = __float_as_int(b.w);
+    } else if (h1) {
+      ref = __float_as_int(e.w);
+      leaf = __float_as_int(f.w);
+    } else if (sp > 0) {
+      --sp;
+      ref = stack[sp].x;
+      leaf = stack[sp].y;
+    } else {
+      alive = false;
+    }
+  }
+  for (uint32_t i = cnt + lane; i < P2; i += 32) {
+    HeavyEntry en;
+    en.key = ~0ull;
+    en.nid = kNone;
+    en.sidx = kNone;
+    seg[i] = en;
+  }
+}
+
 __device__ __forceinline__ bool heavy_greater(const HeavyEntry& a, const HeavyEntry& b, const uint32_t* perm) {
   if (a.key != b.key) return a.key > b.key;
   if (a.nid != b.nid) return a.nid > b.nid;
@@ -485,21 +1044,24 @@ struct ExpandParams {
   int ranked;
   uint8_t* overflow_out;
   unsigned int* error;
+  const uint32_t* work_list;  // optional: process only these queries (input indices)
+  const uint32_t* qrank;      // with work_list: input index -> output rank
 };
 
-// A warp per query in output order writes its rows with the exact FP64 distance.
+// A warp per query writes its rows with the exact FP64 distance: all queries in
+// output order, or the queries of `work_list`.
 __global__ void __launch_bounds__(kExpandThreads) k_expand(ExpandParams P) {
   const int lane = threadIdx.x & 31;
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const bool ids_sorted = P.bands->ids_sorted != 0;
   const bool scene_inexact = *P.S.inexact != 0;
   for (uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < P.nq; j += warps) {
-    const uint32_t qin = ids_sorted ? (uint32_t)j : P.oorder[j];
+    const uint32_t qin = P.work_list ? P.work_list[j] : (ids_sorted ? (uint32_t)j : P.oorder[j]);
     const uint32_t cnt = P.counts[qin];
     const uint8_t fl = P.flags[qin];
     if (P.overflow_out != nullptr && lane == 0) P.overflow_out[qin] = fl & 1;
     if (cnt == 0 || P.rows == nullptr) continue;
-    const unsigned long long base = P.offsets[j];
+    const unsigned long long base = P.offsets[P.work_list ? P.qrank[qin] : (uint32_t)j];
     const uint32_t qid = __float_as_uint(P.qpts[qin].w);
     const double* r = P.qraw + (size_t)qin * P.qstride;
     const double ex = r[1], ey = r[2], ez = P.qstride == 4 ? r[3] : 0.0;
@@ -613,13 +1175,28 @@ __global__ void k_witness_final(const Witness* partial, int n, Witness* out) {
   *out = b;
 }
 
+bool stats_enabled() {
+  static const bool on = std::getenv("RTDL_B200_STATS") != nullptr;
+  return on;
+}
+
+}  // namespace
+
+std::vector<unsigned long long>& last_stats() {
+  thread_local std::vector<unsigned long long> v(kStatCount, 0ull);
+  return v;
+}
+
+namespace {
+
 struct Readback {
   unsigned long long rows;
-  unsigned int heavy;
+  unsigned int heavy;  // these three are copied together from the `small` device counters
   unsigned int error;
+  unsigned int big;
   unsigned int scene_bad;
   unsigned int query_bad;
-  unsigned int pad[2];
+  unsigned int pad;
 };
 
 Readback* pinned_readback() {
@@ -685,6 +1262,247 @@ void free_prep(QueryPrep& qp, cudaStream_t s) {
 
 }  // namespace
 
+namespace {
+
+// Output of the generic (block/warp-per-query) path: sorted candidate indices
+// per query, located through heavy_out_off[h] (h = the query's generic slot).
+struct GenericOut {
+  uint32_t* heavy_out = nullptr;
+  unsigned long long* heavy_out_off = nullptr;
+  void release(cudaStream_t s) {
+    dev_free(heavy_out, s);
+    dev_free(heavy_out_off, s);
+    heavy_out = nullptr;
+    heavy_out_off = nullptr;
+  }
+};
+
+// Runs the generic path for H queries listed in heavy_list with candidate
+// counts heavy_m (read back here).  knn: gather every scene point (brute
+// force); otherwise gather in-radius candidates through the BVH.
+GenericOut run_generic_path(Scene* sc, const QueryPrep& qp, const void* queries_dev, int qstride, uint32_t H,
+                            const uint32_t* heavy_list, const uint32_t* heavy_m, uint32_t limit, bool knn,
+                            unsigned int* error, cudaStream_t s) {
+  GenericOut g;
+  std::vector<uint32_t> hm(H);
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(hm.data(), heavy_m, sizeof(uint32_t) * H, cudaMemcpyDeviceToHost, s));
+  RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+  std::vector<unsigned long long> seg_off(H), out_off(H);
+  std::vector<uint32_t> seg_size(H), out_cnt(H);
+  unsigned long long seg_total = 0, out_total = 0;
+  for (uint32_t h = 0; h < H; ++h) {
+    seg_size[h] = next_pow2(hm[h] ? hm[h] : 1);
+    seg_off[h] = seg_total;
+    seg_total += seg_size[h];
+    out_cnt[h] = hm[h] < limit ? hm[h] : limit;
+    out_off[h] = out_total;
+    out_total += out_cnt[h];
+  }
+  const unsigned long long kScratchLimit = 1ull << 28;  // entries (4 GiB of 16-B sort entries)
+  if (seg_total > kScratchLimit)
+    throw std::runtime_error(
+        "b200 backend: the generic path for limits above 64 needs more than 4 GiB of sort scratch; "
+        "reduce k/k_max or split the query set");
+  unsigned long long* d_seg_off = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * H, s));
+  uint32_t* d_seg_size = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * H, s));
+  g.heavy_out_off = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * H, s));
+  uint32_t* d_out_cnt = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * H, s));
+  HeavyEntry* scratch = static_cast<HeavyEntry*>(dev_alloc(sizeof(HeavyEntry) * seg_total, s));
+  g.heavy_out = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (out_total ? out_total : 1), s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(d_seg_off, seg_off.data(), sizeof(unsigned long long) * H, cudaMemcpyHostToDevice, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(d_seg_size, seg_size.data(), sizeof(uint32_t) * H, cudaMemcpyHostToDevice, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(g.heavy_out_off, out_off.data(), sizeof(unsigned long long) * H,
+                                  cudaMemcpyHostToDevice, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(d_out_cnt, out_cnt.data(), sizeof(uint32_t) * H, cudaMemcpyHostToDevice, s));
+  if (knn)
+    k_heavy_gather<<<H, kHeavyThreads, 0, s>>>(sc->view(), qp.qpts, static_cast<const double*>(queries_dev), qstride,
+                                               heavy_list, d_seg_off, d_seg_size, 1, qp.bands, scratch, error);
+  else
+    k_heavy_gather_bvh<<<H, 32, 0, s>>>(sc->view(), qp.qpts, static_cast<const double*>(queries_dev), qstride,
+                                        heavy_list, d_seg_off, d_seg_size, qp.bands, scratch, error);
+  k_heavy_sort<<<H, kHeavyThreads, 0, s>>>(d_seg_off, d_seg_size, scratch, sc->perm);
+  k_heavy_emit<<<H, kHeavyThreads, 0, s>>>(d_seg_off, g.heavy_out_off, d_out_cnt, scratch, g.heavy_out);
+  RTDL_LAUNCHED(3);
+  RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors above are read by the copies
+  dev_free(d_seg_off, s);
+  dev_free(d_seg_size, s);
+  dev_free(d_out_cnt, s);
+  dev_free(scratch, s);
+  return g;
+}
+
+void check_readback(const Readback& r) {
+  if (r.scene_bad || r.query_bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+  if (r.error & 1u) throw std::runtime_error("BVH traversal stack overflow");
+}
+
+// fixed_radius_neighbors / bounded_knn_rows: collect, scan, emit.
+QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius,
+                             uint32_t kmax, void* rows_dev, size_t rows_capacity, void** rows_alloc,
+                             uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer) {
+  QueryResult res;
+  const int qstride = sc->dim == 3 ? 4 : 3;
+  QueryPrep qp = prepare_queries(sc, queries_dev, nq, true, radius, true, s);
+  uint32_t* qrank = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  k_invert<<<grid_for(nq, 256), 256, 0, s>>>(qp.oorder, nq, &qp.bands->ids_sorted, qrank);
+  RTDL_LAUNCHED(1);
+  if (timer) timer->mark("query_prep");
+  uint32_t* slab = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (size_t)nq * kSlab, s));
+  uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  uint8_t* ncand = static_cast<uint8_t*>(dev_alloc(nq, s));
+  uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq, s));
+  uint32_t* heavy_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  uint32_t* heavy_m = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  uint32_t* big_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  unsigned int* small = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * 4, s));
+  unsigned long long* offsets = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (nq + 1), s));
+  RTDL_CUDA_CHECK(cudaMemsetAsync(small, 0, sizeof(unsigned int) * 4, s));
+  GenericOut g;
+  auto cleanup = [&]() {
+    g.release(s);
+    dev_free(qrank, s);
+    dev_free(slab, s);
+    dev_free(counts, s);
+    dev_free(ncand, s);
+    dev_free(flags, s);
+    dev_free(heavy_list, s);
+    dev_free(heavy_m, s);
+    dev_free(big_list, s);
+    dev_free(small, s);
+    dev_free(offsets, s);
+    free_prep(qp, s);
+  };
+  try {
+    CollectParams C;
+    C.S = sc->view();
+    C.qpts = qp.qpts;
+    C.qraw = static_cast<const double*>(queries_dev);
+    C.qstride = qstride;
+    C.qorder = qp.qorder;
+    C.nq = nq;
+    C.kmax = kmax;
+    C.bands = qp.bands;
+    C.slab = slab;
+    C.counts = counts;
+    C.ncand = ncand;
+    C.flags = flags;
+    C.heavy_list = heavy_list;
+    C.heavy_m = heavy_m;
+    C.big_list = big_list;
+    C.small = small;
+    C.stats = nullptr;
+    const bool stats = stats_enabled();
+    if (stats) {
+      C.stats = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * kStatCount, s));
+      RTDL_CUDA_CHECK(cudaMemsetAsync(C.stats, 0, sizeof(unsigned long long) * kStatCount, s));
+    }
+    const int threads = tuning().block_threads;
+    if (stats)
+      k_collect<true><<<div_up(nq, threads), threads, 0, s>>>(C);
+    else
+      k_collect<false><<<div_up(nq, threads), threads, 0, s>>>(C);
+    RTDL_LAUNCHED(1);
+    if (stats) {
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(last_stats().data(), C.stats, sizeof(unsigned long long) * kStatCount,
+                                      cudaMemcpyDeviceToHost, s));
+      dev_free(C.stats, s);
+    }
+    if (timer) timer->mark("traverse");
+    scan_counts_u64(counts, qp.oorder, &qp.bands->ids_sorted, nq, offsets, s);
+    if (timer) timer->mark("scan");
+    Readback* rb = pinned_readback();
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 3, cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    const Readback r = *rb;
+    check_readback(r);
+    res.rows = r.rows;
+    res.heavy = r.heavy;
+    const uint32_t big = r.big;
+    if (stats) {
+      last_stats()[kStatGenericQueries] = r.heavy;
+      last_stats()[kStatLargeQueries] = r.big;
+    }
+    if (r.heavy > 0) {
+      g = run_generic_path(sc, qp, queries_dev, qstride, r.heavy, heavy_list, heavy_m, kmax, false, small + 1, s);
+      if (timer) timer->mark("generic_path");
+    }
+    if (rows_alloc != nullptr) {
+      const size_t row_size = predicate == kFrn ? 16 : 24;
+      rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
+      rows_capacity = res.rows;
+      *rows_alloc = rows_dev;
+    }
+    EmitParams E;
+    E.S = sc->view();
+    E.qpts = qp.qpts;
+    E.qraw = static_cast<const double*>(queries_dev);
+    E.qstride = qstride;
+    E.qorder = qp.qorder;
+    E.nwork = nq;
+    E.qrank = qrank;
+    E.bands = qp.bands;
+    E.slab = slab;
+    E.ncand = ncand;
+    E.flags = flags;
+    E.offsets = offsets;
+    E.kmax = kmax;
+    E.sink.rows = rows_dev;
+    E.sink.capacity = rows_dev ? rows_capacity : 0;
+    E.sink.ranked = predicate == kFrn ? 0 : 1;
+    E.overflow_out = overflow_dev;
+    k_emit_lanes<<<div_up(nq, 128), 128, 128 * 64 * sizeof(uint32_t), s>>>(E);
+    RTDL_LAUNCHED(1);
+    if (big > 0) {
+      E.qorder = big_list;
+      E.nwork = big;
+      E.overflow_out = nullptr;
+      k_emit_big<<<div_up(big, 64), 64, 64 * kSlab * sizeof(uint32_t), s>>>(E);
+      RTDL_LAUNCHED(1);
+    }
+    if (r.heavy > 0) {
+      ExpandParams X;
+      X.S = sc->view();
+      X.qpts = qp.qpts;
+      X.qraw = static_cast<const double*>(queries_dev);
+      X.qstride = qstride;
+      X.oorder = qp.oorder;
+      X.bands = qp.bands;
+      X.nq = r.heavy;
+      X.L = kSlab;
+      X.counts = counts;
+      X.flags = flags;
+      X.temp = slab;
+      X.heavy_out = g.heavy_out;
+      X.heavy_out_off = g.heavy_out_off;
+      X.offsets = offsets;
+      X.rows = rows_dev;
+      X.capacity = rows_dev ? rows_capacity : 0;
+      X.ranked = predicate == kFrn ? 0 : 1;
+      X.overflow_out = nullptr;
+      X.error = small + 1;
+      X.work_list = heavy_list;
+      X.qrank = qrank;
+      k_expand<<<grid_for((uint64_t)r.heavy * 32, kExpandThreads), kExpandThreads, 0, s>>>(X);
+      RTDL_LAUNCHED(1);
+    }
+    if (timer) timer->mark("emit");
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
+  } catch (...) {
+    cudaStreamSynchronize(s);
+    cleanup();
+    throw;
+  }
+  cleanup();
+  return res;
+}
+
+}  // namespace
+
 QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius, uint32_t limit,
                       void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
                       PhaseTimer* timer) {
@@ -698,6 +1516,9 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
     return res;
   }
   if (timer) timer->mark("start");
+  if (!knn && limit <= (uint32_t)kMaxList)
+    return run_radius_query(sc, queries_dev, nq, predicate, radius, limit, rows_dev, rows_capacity, rows_alloc,
+                            overflow_dev, s, timer);
   QueryPrep qp = prepare_queries(sc, queries_dev, nq, !knn, radius, true, s);
   if (timer) timer->mark("query_prep");
 
@@ -711,55 +1532,9 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
   unsigned int* small = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * 4, s));  // heavy count, error
   unsigned long long* offsets = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (nq + 1), s));
   RTDL_CUDA_CHECK(cudaMemsetAsync(small, 0, sizeof(unsigned int) * 4, s));
-
-  if (all_heavy) {
-    k_mark_all_heavy<<<grid_for(nq, 256), 256, 0, s>>>(qp.qorder, nq, sc->n, limit, counts, flags, temp, heavy_list,
-                                                       heavy_m);
-    RTDL_LAUNCHED(1);
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(small, &nq, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // nq lives on this host stack frame
-  } else {
-    Pass1Params P;
-    P.S = sc->view();
-    P.qpts = qp.qpts;
-    P.qraw = static_cast<const double*>(queries_dev);
-    P.qstride = qstride;
-    P.qorder = qp.qorder;
-    P.nq = nq;
-    P.kmax = limit;
-    P.L = L;
-    P.bands = qp.bands;
-    P.temp = temp;
-    P.counts = counts;
-    P.flags = flags;
-    P.heavy_list = heavy_list;
-    P.heavy_m = heavy_m;
-    P.heavy_count = small;
-    P.error = small + 1;
-    const int threads = tuning().block_threads;
-    const size_t shm = (size_t)threads * L * 8;
-    const unsigned int blocks = div_up(nq, threads);
-    if (knn) {
-      RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-      k_pass1<true><<<blocks, threads, shm, s>>>(P);
-    } else {
-      RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-      k_pass1<false><<<blocks, threads, shm, s>>>(P);
-    }
-    RTDL_LAUNCHED(1);
-  }
-  if (timer) timer->mark("traverse");
-  scan_counts_u64(counts, qp.oorder, &qp.bands->ids_sorted, nq, offsets, s);
-  if (timer) timer->mark("scan");
-
-  Readback* rb = pinned_readback();
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 2, cudaMemcpyDeviceToHost, s));
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-  RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-  const Readback r = *rb;
+  GenericOut g;
   auto cleanup = [&]() {
+    g.release(s);
     dev_free(counts, s);
     dev_free(flags, s);
     dev_free(temp, s);
@@ -769,105 +1544,119 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
     dev_free(offsets, s);
     free_prep(qp, s);
   };
-  if (r.scene_bad || r.query_bad) {
-    cleanup();
-    throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
-  }
-  if (r.error & 1u) {
-    cleanup();
-    throw std::runtime_error("BVH traversal stack overflow");
-  }
-  res.rows = r.rows;
-  res.heavy = r.heavy;
+  try {
+    if (all_heavy) {
+      k_mark_all_heavy<<<grid_for(nq, 256), 256, 0, s>>>(qp.qorder, nq, sc->n, limit, counts, flags, temp,
+                                                         heavy_list, heavy_m);
+      RTDL_LAUNCHED(1);
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(small, &nq, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // nq lives on this host stack frame
+    } else {
+      Pass1Params P;
+      P.S = sc->view();
+      P.qpts = qp.qpts;
+      P.qraw = static_cast<const double*>(queries_dev);
+      P.qstride = qstride;
+      P.qorder = qp.qorder;
+      P.nq = nq;
+      P.kmax = limit;
+      P.L = L;
+      P.bands = qp.bands;
+      P.temp = temp;
+      P.counts = counts;
+      P.flags = flags;
+      P.heavy_list = heavy_list;
+      P.heavy_m = heavy_m;
+      P.heavy_count = small;
+      P.error = small + 1;
+      const int threads = tuning().block_threads;
+      const size_t shm = (size_t)threads * L * 8;
+      const unsigned int blocks = div_up(nq, threads);
+      const bool stats = stats_enabled();
+      P.stats = nullptr;
+      if (stats) {
+        P.stats = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * kStatCount, s));
+        RTDL_CUDA_CHECK(cudaMemsetAsync(P.stats, 0, sizeof(unsigned long long) * kStatCount, s));
+      }
+      auto launch = [&](auto kernel) {
+        RTDL_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        kernel<<<blocks, threads, shm, s>>>(P);
+      };
+      if (knn) {
+        if (stats) launch(k_pass1<true, true>);
+        else launch(k_pass1<true, false>);
+      } else {
+        if (stats) launch(k_pass1<false, true>);
+        else launch(k_pass1<false, false>);
+      }
+      RTDL_LAUNCHED(1);
+      if (stats) {
+        RTDL_CUDA_CHECK(cudaMemcpyAsync(last_stats().data(), P.stats, sizeof(unsigned long long) * kStatCount,
+                                        cudaMemcpyDeviceToHost, s));
+        dev_free(P.stats, s);
+      }
+    }
+    if (timer) timer->mark("traverse");
+    scan_counts_u64(counts, qp.oorder, &qp.bands->ids_sorted, nq, offsets, s);
+    if (timer) timer->mark("scan");
 
-  uint32_t* heavy_out = nullptr;
-  unsigned long long* heavy_out_off = nullptr;
-  if (r.heavy > 0) {
-    const uint32_t H = r.heavy;
-    std::vector<uint32_t> hm(H);
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(hm.data(), heavy_m, sizeof(uint32_t) * H, cudaMemcpyDeviceToHost, s));
+    Readback* rb = pinned_readback();
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 2, cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-    std::vector<unsigned long long> seg_off(H), out_off(H);
-    std::vector<uint32_t> seg_size(H), out_cnt(H);
-    unsigned long long seg_total = 0, out_total = 0;
-    for (uint32_t h = 0; h < H; ++h) {
-      seg_size[h] = next_pow2(hm[h] ? hm[h] : 1);
-      seg_off[h] = seg_total;
-      seg_total += seg_size[h];
-      out_cnt[h] = hm[h] < limit ? hm[h] : limit;
-      out_off[h] = out_total;
-      out_total += out_cnt[h];
+    const Readback r = *rb;
+    check_readback(r);
+    res.rows = r.rows;
+    res.heavy = r.heavy;
+    if (r.heavy > 0) {
+      g = run_generic_path(sc, qp, queries_dev, qstride, r.heavy, heavy_list, heavy_m, limit, knn, small + 1, s);
+      if (timer) timer->mark("generic_path");
     }
-    const unsigned long long kScratchLimit = 1ull << 28;  // entries (4 GiB of 16-B sort entries)
-    if (seg_total > kScratchLimit) {
-      cleanup();
-      throw std::runtime_error(
-          "b200 backend: the generic path for limits above 64 needs more than 4 GiB of sort scratch; "
-          "reduce k/k_max or split the query set");
+    if (rows_alloc != nullptr) {
+      const size_t row_size = predicate == kFrn ? 16 : 24;
+      rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
+      rows_capacity = res.rows;
+      *rows_alloc = rows_dev;
     }
-    unsigned long long* d_seg_off = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * H, s));
-    uint32_t* d_seg_size = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * H, s));
-    heavy_out_off = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * H, s));
-    uint32_t* d_out_cnt = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * H, s));
-    HeavyEntry* scratch = static_cast<HeavyEntry*>(dev_alloc(sizeof(HeavyEntry) * seg_total, s));
-    heavy_out = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (out_total ? out_total : 1), s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(d_seg_off, seg_off.data(), sizeof(unsigned long long) * H, cudaMemcpyHostToDevice, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(d_seg_size, seg_size.data(), sizeof(uint32_t) * H, cudaMemcpyHostToDevice, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(heavy_out_off, out_off.data(), sizeof(unsigned long long) * H, cudaMemcpyHostToDevice, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(d_out_cnt, out_cnt.data(), sizeof(uint32_t) * H, cudaMemcpyHostToDevice, s));
-    k_heavy_gather<<<H, kHeavyThreads, 0, s>>>(sc->view(), qp.qpts, static_cast<const double*>(queries_dev), qstride,
-                                               heavy_list, d_seg_off, d_seg_size, knn ? 1 : 0, qp.bands, scratch,
-                                               small + 1);
-    k_heavy_sort<<<H, kHeavyThreads, 0, s>>>(d_seg_off, d_seg_size, scratch, sc->perm);
-    k_heavy_emit<<<H, kHeavyThreads, 0, s>>>(d_seg_off, heavy_out_off, d_out_cnt, scratch, heavy_out);
-    RTDL_LAUNCHED(3);
-    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors above are read by the copies
-    dev_free(d_seg_off, s);
-    dev_free(d_seg_size, s);
-    dev_free(d_out_cnt, s);
-    dev_free(scratch, s);
-    if (timer) timer->mark("generic_path");
+    if (res.rows > 0 || overflow_dev != nullptr) {
+      ExpandParams E;
+      E.S = sc->view();
+      E.qpts = qp.qpts;
+      E.qraw = static_cast<const double*>(queries_dev);
+      E.qstride = qstride;
+      E.oorder = qp.oorder;
+      E.bands = qp.bands;
+      E.nq = nq;
+      E.L = L;
+      E.counts = counts;
+      E.flags = flags;
+      E.temp = temp;
+      E.heavy_out = g.heavy_out;
+      E.heavy_out_off = g.heavy_out_off;
+      E.offsets = offsets;
+      E.rows = rows_dev;
+      E.capacity = rows_dev ? rows_capacity : 0;
+      E.ranked = predicate == kFrn ? 0 : 1;
+      E.overflow_out = overflow_dev;
+      E.error = small + 1;
+      E.work_list = nullptr;
+      E.qrank = nullptr;
+      const unsigned int blocks = grid_for((uint64_t)nq * 32, kExpandThreads);
+      k_expand<<<blocks, kExpandThreads, 0, s>>>(E);
+      RTDL_LAUNCHED(1);
+    }
+    if (timer) timer->mark("emit");
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
+  } catch (...) {
+    cudaStreamSynchronize(s);
+    cleanup();
+    throw;
   }
-
-  if (rows_alloc != nullptr) {
-    const size_t row_size = predicate == kFrn ? 16 : 24;
-    rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
-    rows_capacity = res.rows;
-    *rows_alloc = rows_dev;
-  }
-  if (res.rows > 0 || overflow_dev != nullptr) {
-    ExpandParams E;
-    E.S = sc->view();
-    E.qpts = qp.qpts;
-    E.qraw = static_cast<const double*>(queries_dev);
-    E.qstride = qstride;
-    E.oorder = qp.oorder;
-    E.bands = qp.bands;
-    E.nq = nq;
-    E.L = L;
-    E.counts = counts;
-    E.flags = flags;
-    E.temp = temp;
-    E.heavy_out = heavy_out;
-    E.heavy_out_off = heavy_out_off;
-    E.offsets = offsets;
-    E.rows = rows_dev;
-    E.capacity = rows_capacity;
-    E.ranked = predicate == kFrn ? 0 : 1;
-    E.overflow_out = overflow_dev;
-    E.error = small + 1;
-    const unsigned int blocks = grid_for((uint64_t)nq * 32, kExpandThreads);
-    k_expand<<<blocks, kExpandThreads, 0, s>>>(E);
-    RTDL_LAUNCHED(1);
-  }
-  if (timer) timer->mark("emit");
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-  RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-  const unsigned int late_error = rb->error;
-  dev_free(heavy_out, s);
-  dev_free(heavy_out_off, s);
   cleanup();
-  if (late_error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
   return res;
 }
 
@@ -901,7 +1690,8 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   P.heavy_count = small;
   P.error = small + 1;
   const int threads = tuning().block_threads;
-  k_pass1<true><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
+  P.stats = nullptr;
+  k_pass1<true, false><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
   RTDL_LAUNCHED(1);
   if (timer) timer->mark("traverse");
   const unsigned int blocks = grid_for(nq, 256) < 2 * kSmCount ? grid_for(nq, 256) : 2 * kSmCount;

@@ -233,3 +233,33 @@ def test_phase_timings_reported(gpu):
     t = rt.last_phase_timings()
     for phase in ("upload", "build", "traverse", "emit", "download", "total"):
         assert phase in t and t[phase] >= 0.0
+
+
+def test_lattice_shell_ties_at_the_cut(gpu):
+    """Integer points on the shells |v|^2 = 25, 26, 27 around each query give
+    groups of exactly equal FP64 distances; with 65..128 candidates per query
+    the k_max cut falls inside a tie group, which must be broken by neighbor id
+    and then search input order, exactly as the reference sorts."""
+    rng = np.random.default_rng(8)
+    r = np.arange(-6, 7)
+    grid = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3)
+    shell = grid[np.isin((grid ** 2).sum(1), (25, 26, 27))].astype(np.float64)
+    centres = np.array([[0.0, 0.0, 0.0], [40.0, 0.0, 0.0], [0.0, 40.0, 0.0]])
+    pts = np.concatenate([c + shell for c in centres])
+    order = rng.permutation(len(pts))
+    pts = pts[order]
+    s = _cols(pts, ids=(rng.integers(0, 60, len(pts))).astype(np.uint32))  # many duplicate ids
+    q = _cols(centres, ids=np.array([7, 3, 5], dtype=np.uint32))
+    # radius^2 = 26: 102 candidates per query (65..128 path); 27: 134 (generic path)
+    for r2, per_query in ((26.0, 102), (27.0, 134)):
+        radius = float(np.nextafter(np.sqrt(r2), np.inf))  # radius * radius >= r2 in FP64
+        for k_max in (10, 30, 40, 64, 100):
+            with rt.B200Scene(_pack(s)) as scene:
+                v, overflow = scene.query(_pack(q), predicate="fixed_radius_neighbors", radius=radius,
+                                          limit=k_max, with_overflow=True)
+                got = v.to_numpy()
+                v.close()
+            exp, counts = O.fixed_radius_neighbors(q, s, radius=radius, k_max=k_max, with_counts=True)
+            assert (counts == per_query).all()
+            _assert_same_rows(got, exp, False)
+            assert np.array_equal(overflow.astype(bool), counts > k_max)

@@ -69,19 +69,26 @@ __host__ __device__ inline float ordered_to_float(unsigned int o) {
 }
 
 // ---- a built scene (LBVH over the search points) ---------------------------
-// Node layout: 4 x float4 = 64 B, both children's boxes in the parent so one
-// visit tests two children with two coalesced 32-B reads.
-//   n[0] = {c0.lo.xyz, c0.ref}  n[1] = {c0.hi.xyz, c0.cnt}
-//   n[2] = {c1.lo.xyz, c1.ref}  n[3] = {c1.hi.xyz, c1.cnt}
-// cnt == 0: ref is an internal node index; cnt > 0: a leaf bucket of cnt
-// consecutive sorted points starting at ref.
+// Node layout: the collapsed tree in depth-first pre-order, 2 x float4 = 32 B
+// per node, traversed without a stack:
+//   n[0] = {lo.xyz, ref}   ref == kInternalNode: an internal node, its left
+//                          child is the next record (descend on overlap);
+//                          ref < 0: leaf bucket, see leaf_first / leaf_count
+//   n[1] = {hi.xyz, rope}  next record when the subtree is done or missed;
+//                          kRopeEnd ends the traversal
+// The root is record 0.
+constexpr int kRopeEnd = -1;
+constexpr int kInternalNode = 0;
+constexpr uint32_t kMaxScenePoints = 1u << 26;  // leaf references keep 26 bits for the first point
+__host__ __device__ inline int leaf_ref(int first, int count) { return ~((first << 5) | (count - 1)); }
+__host__ __device__ inline int leaf_first(int hit) { return (~hit) >> 5; }
+__host__ __device__ inline int leaf_count(int hit) { return ((~hit) & 31) + 1; }
+
 struct SceneView {
   const float4* pts;      // n sorted points: x, y, z (0 for 2D), w = record id bits
   const uint32_t* perm;   // sorted index -> search input index
   const double* pts64;    // 3 doubles per sorted point (exact coordinates), used when inexact
-  const float4* nodes;    // 4 float4 per internal node
-  int root_ref;
-  int root_cnt;           // > 0 when the whole scene is a single leaf
+  const float4* nodes;    // 2 float4 per node, collapsed tree in pre-order
   uint32_t n;
   const unsigned int* inexact;  // device flag: scene coordinates are not all FP32-exact
 };
@@ -91,7 +98,6 @@ struct Scene {
   int device = 0;
   uint32_t n = 0;
   double max_radius = 0.0;  // prepared-FRN contract only
-  int root_ref = 0, root_cnt = 0;
   int leaf_size = 8;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -106,8 +112,6 @@ struct Scene {
     v.perm = perm;
     v.pts64 = pts64;
     v.nodes = nodes;
-    v.root_ref = root_ref;
-    v.root_cnt = root_cnt;
     v.n = n;
     v.inexact = stats ? &stats->inexact : nullptr;
     return v;
@@ -118,6 +122,7 @@ struct Scene {
 struct Tuning {
   int leaf_size = 8;
   int block_threads = 128;
+  int traversal = 0;  // fixed-radius collect: 0 = one warp per 32 queries (packet), 1 = one thread per query
 };
 Tuning& tuning();
 

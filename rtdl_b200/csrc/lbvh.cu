@@ -15,8 +15,18 @@
 //               index, so duplicates are handled);
 //   6. refit:   bottom-up boxes, one thread per leaf, an atomic arrival
 //               counter per node lets the second child to arrive continue;
-//   7. pack:    64-B nodes holding both children's boxes; subtrees of at most
-//               leaf_size points become leaf buckets (contiguous point ranges).
+//   7. compact: the tree the traversal sees keeps an internal node only while
+//               it covers more than leaf_size points; smaller subtrees (and
+//               single points hanging off large nodes) become leaf buckets.
+//               That collapsed tree is written in depth-first pre-order as
+//               32-B records {box, leaf reference or "internal", rope}: the
+//               left child of an internal node is the next record, and the
+//               rope is the record that follows the node's subtree.  A walk
+//               is then stackless and reads nearly consecutive memory.  A
+//               node's pre-order index is 2 L + depth - r, with L the leaf
+//               buckets left of it, depth its depth and r the right turns on
+//               its root path; its rope is the right child of the internal
+//               node whose split equals the node's last point.
 #include "internal.cuh"
 
 namespace rtdl_b200 {
@@ -179,7 +189,8 @@ __device__ __forceinline__ int prefix_len(const uint32_t* __restrict__ codes, in
 
 __global__ void k_karras(const uint32_t* __restrict__ codes, uint32_t n, int* __restrict__ child_l,
                          int* __restrict__ child_r, int* __restrict__ first, int* __restrict__ last,
-                         int* __restrict__ parent_int, int* __restrict__ parent_leaf) {
+                         int* __restrict__ parent_int, int* __restrict__ parent_leaf,
+                         int* __restrict__ right_of_split) {
   const int64_t nn = n;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn - 1; i += (int64_t)gridDim.x * blockDim.x) {
     const int d = (prefix_len(codes, nn, i, i + 1) - prefix_len(codes, nn, i, i - 1)) >= 0 ? 1 : -1;
@@ -219,6 +230,9 @@ __global__ void k_karras(const uint32_t* __restrict__ codes, uint32_t n, int* __
     child_r[i] = cr;
     first[i] = (int)lo;
     last[i] = (int)hi;
+    // node index of the right child: internal nodes keep their index, point
+    // leaves follow the n - 1 internal nodes
+    right_of_split[gamma] = (cr & kLeafFlag) ? (int)(nn - 1) + (cr & ~kLeafFlag) : cr;
   }
 }
 
@@ -255,38 +269,99 @@ __global__ void k_refit(uint32_t n, const float4* __restrict__ pts, const int* _
   }
 }
 
-__global__ void k_pack(uint32_t n, const float4* __restrict__ pts, const int* __restrict__ child_l,
-                       const int* __restrict__ child_r, const int* __restrict__ first, const int* __restrict__ last,
-                       const float4* __restrict__ boxes, int leaf_size, float4* __restrict__ nodes) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const int cs[2] = {child_l[i], child_r[i]};
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int c = cs[k];
-      float4 lo, hi;
-      int ref, cnt;
-      if (c & kLeafFlag) {
-        const int p = c & ~kLeafFlag;
-        lo = pts[p];
-        hi = lo;
-        ref = p;
-        cnt = 1;
-      } else {
-        lo = boxes[2 * c];
-        hi = boxes[2 * c + 1];
-        const int count = last[c] - first[c] + 1;
-        if (count <= leaf_size) {
-          ref = first[c];
-          cnt = count;
-        } else {
-          ref = c;
-          cnt = 0;
-        }
-      }
-      nodes[4 * i + 2 * k] = make_float4(lo.x, lo.y, lo.z, __int_as_float(ref));
-      nodes[4 * i + 2 * k + 1] = make_float4(hi.x, hi.y, hi.z, __int_as_float(cnt));
-    }
+// Karras entities: internal node k for e < n - 1, point e - (n - 1) otherwise.
+struct Ent {
+  const int* child_l;
+  const int* child_r;
+  const int* first;
+  const int* last;
+  const int* parent_int;
+  const int* parent_leaf;
+  uint32_t n;
+  __device__ __forceinline__ bool is_point(int e) const { return e >= (int)n - 1; }
+  __device__ __forceinline__ int lo(int e) const { return is_point(e) ? e - ((int)n - 1) : first[e]; }
+  __device__ __forceinline__ int hi(int e) const { return is_point(e) ? e - ((int)n - 1) : last[e]; }
+  __device__ __forceinline__ int parent(int e) const {
+    return is_point(e) ? parent_leaf[e - ((int)n - 1)] : parent_int[e];
   }
+  __device__ __forceinline__ int child_code(int e) const {  // as stored in child_l / child_r
+    return is_point(e) ? ((e - ((int)n - 1)) | kLeafFlag) : e;
+  }
+};
+
+// Marks the nodes of the collapsed tree (flag bit 0) and its leaf buckets
+// (bit 1); a bucket sets leaf_start at its first point.
+__global__ void k_mark_collapsed(Ent E, int leaf_size, uint8_t* __restrict__ flags, uint32_t* __restrict__ leaf_start) {
+  const int total = 2 * (int)E.n - 1;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int par = e == 0 ? -1 : E.parent(e);
+    const bool in = e == 0 || (par >= 0 && E.hi(par) - E.lo(par) + 1 > leaf_size);
+    uint8_t f = 0;
+    if (in) {
+      f = 1;
+      if (E.is_point(e) || E.hi(e) - E.lo(e) + 1 <= leaf_size) {
+        f |= 2;
+        leaf_start[E.lo(e)] = 1u;
+      }
+    }
+    flags[e] = f;
+  }
+}
+
+// Writes each collapsed-tree node at its pre-order index; the rope field holds
+// the Karras entity of the rope until k_translate_ropes maps it.
+__global__ void k_compact(Ent E, const uint8_t* __restrict__ flags, const uint32_t* __restrict__ leaves_before,
+                          const float4* __restrict__ pts, const float4* __restrict__ boxes,
+                          const int* __restrict__ right_of_split, int* __restrict__ ent2pre,
+                          float4* __restrict__ nodes) {
+  const int total = 2 * (int)E.n - 1;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const uint8_t f = flags[e];
+    if (!(f & 1)) continue;
+    int depth = 0, right = 0;
+    for (int x = e; x != 0;) {
+      const int par = E.parent(x);
+      ++depth;
+      if (E.child_r[par] == E.child_code(x)) ++right;
+      x = par;
+    }
+    const int a = E.lo(e), b = E.hi(e);
+    const int pre = 2 * (int)leaves_before[a] + depth - right;
+    ent2pre[e] = pre;
+    float4 lo, hi;
+    if (E.is_point(e)) {
+      lo = pts[a];
+      hi = lo;
+    } else {
+      lo = boxes[2 * e];
+      hi = boxes[2 * e + 1];
+    }
+    const int ref = (f & 2) ? leaf_ref(a, b - a + 1) : kInternalNode;
+    const int rope_ent = b == (int)E.n - 1 ? kRopeEnd : right_of_split[b];
+    nodes[2 * pre] = make_float4(lo.x, lo.y, lo.z, __int_as_float(ref));
+    nodes[2 * pre + 1] = make_float4(hi.x, hi.y, hi.z, __int_as_float(rope_ent));
+  }
+}
+
+__global__ void k_translate_ropes(const uint32_t* __restrict__ leaves_total, const int* __restrict__ ent2pre,
+                                  float4* __restrict__ nodes) {
+  const int m = 2 * (int)(*leaves_total) - 1;  // nodes of the collapsed tree
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const int r = __float_as_int(nodes[2 * i + 1].w);
+    nodes[2 * i + 1].w = __int_as_float(r == kRopeEnd ? kRopeEnd : ent2pre[r]);
+  }
+}
+
+__global__ void k_narrow_u64(const uint64_t* __restrict__ in, uint64_t n, uint32_t* __restrict__ out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)in[i];
+}
+
+// A one-point scene: a single leaf bucket.
+__global__ void k_single_point(const float4* __restrict__ pts, float4* __restrict__ nodes) {
+  const float4 p = pts[0];
+  nodes[0] = make_float4(p.x, p.y, p.z, __int_as_float(leaf_ref(0, 1)));
+  nodes[1] = make_float4(p.x, p.y, p.z, __int_as_float(kRopeEnd));
 }
 
 }  // namespace
@@ -314,7 +389,8 @@ void morton_codes(const float4* pts, uint32_t n, int dim, const PointStats* box_
 
 Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, int leaf_size) {
   if (dim != 2 && dim != 3) throw std::runtime_error("dimension must be 2 or 3");
-  if (n > 0x3FFFFFFFu) throw std::runtime_error("search_count exceeds the scene limit of 2^30 points");
+  if (n > (uint32_t)kMaxScenePoints)
+    throw std::runtime_error("search_count exceeds the scene limit of 67,108,864 points");
   if (leaf_size < 1) leaf_size = 1;
   if (leaf_size > 32) leaf_size = 32;
   Scene* sc = new Scene();
@@ -350,14 +426,32 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
     int* last = static_cast<int*>(dev_alloc(sizeof(int) * ni, s));
     int* parent_int = static_cast<int*>(dev_alloc(sizeof(int) * ni, s));
     int* parent_leaf = static_cast<int*>(dev_alloc(sizeof(int) * n, s));
+    int* right_of_split = static_cast<int*>(dev_alloc(sizeof(int) * ni, s));
     unsigned int* arrivals = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * ni, s));
     float4* boxes = static_cast<float4*>(dev_alloc(sizeof(float4) * 2 * (size_t)ni, s));
     RTDL_CUDA_CHECK(cudaMemsetAsync(arrivals, 0, sizeof(unsigned int) * ni, s));
     RTDL_CUDA_CHECK(cudaMemsetAsync(parent_int, 0xFF, sizeof(int) * ni, s));  // root keeps -1
-    k_karras<<<grid_for(ni), kThreads, 0, s>>>(codes, n, child_l, child_r, first, last, parent_int, parent_leaf);
+    k_karras<<<grid_for(ni), kThreads, 0, s>>>(codes, n, child_l, child_r, first, last, parent_int, parent_leaf,
+                                              right_of_split);
     k_refit<<<grid_for(n), kThreads, 0, s>>>(n, sc->pts, child_l, child_r, parent_int, parent_leaf, arrivals, boxes);
-    sc->nodes = static_cast<float4*>(dev_alloc(sizeof(float4) * 4 * (size_t)ni, s));
-    k_pack<<<grid_for(ni), kThreads, 0, s>>>(n, sc->pts, child_l, child_r, first, last, boxes, leaf_size, sc->nodes);
+    RTDL_LAUNCHED(2);
+    Ent E{child_l, child_r, first, last, parent_int, parent_leaf, n};
+    const uint64_t ents = 2ull * n - 1;
+    uint8_t* flags = static_cast<uint8_t*>(dev_alloc(ents, s));
+    uint32_t* leaf_start = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
+    uint64_t* leaves_before = static_cast<uint64_t*>(dev_alloc(sizeof(uint64_t) * (n + 1), s));
+    uint32_t* leaves_before32 = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (n + 1), s));
+    int* ent2pre = static_cast<int*>(dev_alloc(sizeof(int) * ents, s));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(leaf_start, 0, sizeof(uint32_t) * n, s));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(ent2pre, 0xFF, sizeof(int) * ents, s));  // kRopeEnd for entities off the tree
+    k_mark_collapsed<<<grid_for(ents), kThreads, 0, s>>>(E, leaf_size, flags, leaf_start);
+    RTDL_LAUNCHED(1);
+    scan_counts_u64(leaf_start, nullptr, nullptr, n, reinterpret_cast<unsigned long long*>(leaves_before), s);
+    k_narrow_u64<<<grid_for(n + 1), kThreads, 0, s>>>(leaves_before, n + 1, leaves_before32);
+    sc->nodes = static_cast<float4*>(dev_alloc(sizeof(float4) * 2 * ents, s));
+    k_compact<<<grid_for(ents), kThreads, 0, s>>>(E, flags, leaves_before32, sc->pts, boxes, right_of_split, ent2pre,
+                                                  sc->nodes);
+    k_translate_ropes<<<grid_for(ents), kThreads, 0, s>>>(leaves_before32 + n, ent2pre, sc->nodes);
     RTDL_LAUNCHED(3);
     dev_free(child_l, s);
     dev_free(child_r, s);
@@ -367,15 +461,18 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
     dev_free(parent_leaf, s);
     dev_free(arrivals, s);
     dev_free(boxes, s);
+    dev_free(right_of_split, s);
+    dev_free(flags, s);
+    dev_free(leaf_start, s);
+    dev_free(leaves_before, s);
+    dev_free(leaves_before32, s);
+    dev_free(ent2pre, s);
+  } else if (n == 1) {
+    sc->nodes = static_cast<float4*>(dev_alloc(sizeof(float4) * 2, s));
+    k_single_point<<<1, 1, 0, s>>>(sc->pts, sc->nodes);
+    RTDL_LAUNCHED(1);
   }
   dev_free(codes, s);
-  if (n <= (uint32_t)leaf_size) {
-    sc->root_ref = 0;
-    sc->root_cnt = (int)n;
-  } else {
-    sc->root_ref = 0;
-    sc->root_cnt = 0;
-  }
   return sc;
 }
 

@@ -304,56 +304,20 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
     return true;
   };
 
-  if (S.n > 0) {
-    if (S.root_cnt > 0) {
-      visit_leaf(S.root_ref, S.root_cnt);
-    } else {
-      int2 stack[kStackDepth];
-      int sp = 0;
-      int cur = S.root_ref;
-      while (true) {
-        const float4* nd = S.nodes + 4 * (size_t)cur;
-        if (STATS) ++st_nodes;
-        const float4 a = __ldg(nd), b = __ldg(nd + 1), e = __ldg(nd + 2), f = __ldg(nd + 3);
-        float k0 = box_d2(c.qx, c.qy, c.qz, a, b), k1 = box_d2(c.qx, c.qy, c.qz, e, f);
-        int r0 = __float_as_int(a.w), n0 = __float_as_int(b.w);
-        int r1 = __float_as_int(e.w), n1 = __float_as_int(f.w);
-        if (k1 < k0) {
-          const float tk = k0; k0 = k1; k1 = tk;
-          const int tr = r0; r0 = r1; r1 = tr;
-          const int tn = n0; n0 = n1; n1 = tn;
-        }
-        int next = -1;
-        if (box_ok(k0)) {
-          if (n0) visit_leaf(r0, n0);
-          else next = r0;
-        }
-        if (box_ok(k1)) {
-          if (n1) {
-            visit_leaf(r1, n1);
-          } else if (next < 0) {
-            next = r1;
-          } else {
-            if (sp >= kStackDepth) {
-              atomicOr(P.error, 1u);
-              break;
-            }
-            stack[sp++] = make_int2(r1, __float_as_int(k1));
-          }
-        }
-        if (next < 0) {
-          while (sp > 0) {
-            const int2 en = stack[--sp];
-            if (box_ok(__int_as_float(en.y))) {
-              next = en.x;
-              break;
-            }
-          }
-          if (next < 0) break;
-        }
-        cur = next;
+  // stackless depth-first walk over the pre-order records
+  int cur = S.n > 0 ? 0 : kRopeEnd;
+  while (cur != kRopeEnd) {
+    const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+    if (STATS) ++st_nodes;
+    const int hit = __float_as_int(a.w);
+    if (box_ok(box_d2(c.qx, c.qy, c.qz, a, b))) {
+      if (hit >= 0) {
+        ++cur;  // internal node: its left child is the next record
+        continue;
       }
+      visit_leaf(leaf_first(hit), leaf_count(hit));
     }
+    cur = __float_as_int(b.w);
   }
 
   if (STATS) {
@@ -391,7 +355,17 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
 // test their buckets together.  In-radius candidates are appended unsorted to
 // the query's slab (capacity C); the exact in-radius count is kept, so the
 // overflow flag and the row offsets are exact without any per-query list.
-constexpr int kSlab = 128;  // slab capacity (candidates kept per query)
+constexpr int kSlab = 256;      // candidates kept per query
+constexpr int kSlabHead = 64;   // slots kept slot-major (read by the lane-per-query emit)
+
+// Slab layout: slots below kSlabHead are slot-major (slot s of the query at
+// processing rank t at s * nq + t, so a warp of consecutive queries reads one
+// slot with one coalesced request); the remaining slots are query-major after
+// them (read by the warp-per-query emit, one query at a time).
+__host__ __device__ __forceinline__ size_t slab_at(uint32_t c, uint32_t t, uint32_t nq) {
+  return c < (uint32_t)kSlabHead ? (size_t)c * nq + t
+                                 : (size_t)kSlabHead * nq + (size_t)t * (kSlab - kSlabHead) + (c - kSlabHead);
+}
 
 struct CollectParams {
   SceneView S;
@@ -402,9 +376,10 @@ struct CollectParams {
   uint32_t nq;
   uint32_t kmax;
   const DevBands* bands;
-  uint32_t* slab;        // nq * kSlab
+  uint32_t* slab;        // kSlab * nq candidate indices, laid out by slab_at()
+  uint32_t* keys;        // same layout: the candidate's FP32 sort key (bits)
   uint32_t* counts;      // min(count, kmax), query input order
-  uint8_t* ncand;        // min(count, kSlab)
+  uint16_t* ncand;       // min(count, kSlab), by processing rank
   uint8_t* flags;        // bit0: count > kmax, bit1: count > kSlab (generic path), bit2: count > 64
   uint32_t* heavy_list;
   uint32_t* heavy_m;
@@ -413,106 +388,156 @@ struct CollectParams {
   unsigned long long* stats;
 };
 
-template <bool STATS>
-__global__ void __launch_bounds__(256) k_collect(CollectParams P) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.nq) return;
-  const uint32_t qin = P.qorder[t];
-  const float4 q = P.qpts[qin];
-  const DevBands B = *P.bands;
-  const SceneView& S = P.S;
-  const int scene_inexact = *S.inexact;
-  double ex = 0.0, ey = 0.0, ez = 0.0;
-  bool have_exact = false;
-  uint32_t* slab = P.slab + (size_t)qin * kSlab;
-  uint32_t count = 0;
-  unsigned long long st_nodes = 0, st_points = 0, st_band = 0;
+// Per-query state of the collect pass and its accept / finish steps, shared by
+// the per-lane and the per-warp (packet) traversals.
+struct CollectLane {
+  uint32_t t, qin;
+  float4 q;
+  double ex, ey, ez;
+  uint32_t count;
+  unsigned long long st_nodes, st_points, st_band;
+};
 
-  int2 stack[kStackDepth];
-  int sp = 0;
-  int ref = S.root_ref, cnt = S.root_cnt;
-  bool alive = S.n > 0;
-  while (alive) {
-    // internal nodes until this lane holds a leaf bucket
-    while (alive && cnt == 0) {
-      const float4* nd = S.nodes + 4 * (size_t)ref;
-      if (STATS) ++st_nodes;
-      const float4 a = __ldg(nd), b = __ldg(nd + 1), e = __ldg(nd + 2), f = __ldg(nd + 3);
-      const bool h0 = box_d2(q.x, q.y, q.z, a, b) <= B.box_hi2;
-      const bool h1 = box_d2(q.x, q.y, q.z, e, f) <= B.box_hi2;
-      if (h0) {
-        if (h1) {
-          if (sp >= kStackDepth) {
-            atomicOr(&P.small[1], 1u);
-            alive = false;
-            break;
-          }
-          stack[sp++] = make_int2(__float_as_int(e.w), __float_as_int(f.w));
-        }
-        ref = __float_as_int(a.w);
-        cnt = __float_as_int(b.w);
-      } else if (h1) {
-        ref = __float_as_int(e.w);
-        cnt = __float_as_int(f.w);
-      } else if (sp > 0) {
-        --sp;
-        ref = stack[sp].x;
-        cnt = stack[sp].y;
-      } else {
-        alive = false;
-      }
-    }
-    if (!alive) break;
-    if (STATS) st_points += cnt;
-    for (int i = ref; i < ref + cnt; ++i) {
-      const float4 p = __ldg(&S.pts[i]);
-      const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-      const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-      if (d2 > B.hi2) continue;
-      if (d2 >= B.lo2) {
-        if (STATS) ++st_band;
-        if (!have_exact) {
-          const double* r = P.qraw + (size_t)qin * P.qstride;
-          ex = r[1];
-          ey = r[2];
-          ez = P.qstride == 4 ? r[3] : 0.0;
-          have_exact = true;
-        }
-        if (exact_d2_at(ex, ey, ez, S.pts, S.pts64, scene_inexact, (uint32_t)i) > B.r2) continue;
-      }
-      if (count < (uint32_t)kSlab) slab[count] = (uint32_t)i;
-      ++count;
-    }
-    if (sp > 0) {
-      --sp;
-      ref = stack[sp].x;
-      cnt = stack[sp].y;
-    } else {
-      alive = false;
-    }
+// Tests sorted point i against the lane's query and appends it when it is in
+// radius: FP32 decides outside the band, FP64 inside.  The stored key is the
+// FP32 d2 for FP32-exact inputs, else the exact FP64 d2 rounded to FP32.
+template <bool STATS>
+__device__ __forceinline__ void collect_point(const CollectParams& P, const DevBands& B, int scene_inexact,
+                                              CollectLane& L, uint32_t i, const float4& p) {
+  const float dx = p.x - L.q.x, dy = p.y - L.q.y, dz = p.z - L.q.z;
+  float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+  if (d2 > B.hi2) return;
+  if (d2 >= B.lo2 || B.any_inexact) {
+    if (STATS && d2 >= B.lo2) ++L.st_band;
+    const double e2 = exact_d2_at(L.ex, L.ey, L.ez, P.S.pts, P.S.pts64, scene_inexact, i);
+    if (d2 >= B.lo2 && e2 > B.r2) return;
+    if (B.any_inexact) d2 = __double2float_rn(e2);
   }
+  if (L.count < (uint32_t)kSlab) {
+    const size_t at = slab_at(L.count, L.t, P.nq);
+    P.slab[at] = i;
+    P.keys[at] = __float_as_uint(d2);
+  }
+  ++L.count;
+}
+
+template <bool STATS>
+__device__ __forceinline__ void collect_finish(const CollectParams& P, const CollectLane& L) {
   if (STATS) {
-    atomicAdd(&P.stats[kStatNodes], st_nodes);
-    atomicAdd(&P.stats[kStatLeafPoints], st_points);
-    atomicAdd(&P.stats[kStatInRadius], (unsigned long long)count);
-    atomicAdd(&P.stats[kStatBand], st_band);
-    atomicMax(&P.stats[kStatMaxLeafPoints], (unsigned long long)count);
+    atomicAdd(&P.stats[kStatNodes], L.st_nodes);
+    atomicAdd(&P.stats[kStatLeafPoints], L.st_points);
+    atomicAdd(&P.stats[kStatInRadius], (unsigned long long)L.count);
+    atomicAdd(&P.stats[kStatBand], L.st_band);
+    atomicMax(&P.stats[kStatMaxLeafPoints], (unsigned long long)L.count);
   }
-  const uint32_t kmax = P.kmax;
-  P.counts[qin] = count < kmax ? count : kmax;
+  const uint32_t count = L.count, kmax = P.kmax;
+  P.counts[L.qin] = count < kmax ? count : kmax;
   uint8_t fl = count > kmax ? 1 : 0;
   if (count > (uint32_t)kSlab) {
     fl |= 2;
     const unsigned int h = atomicAdd(&P.small[0], 1u);
-    P.heavy_list[h] = qin;
+    P.heavy_list[h] = L.qin;
     P.heavy_m[h] = count;
-    slab[0] = h;  // the generic path's slot for this query
   } else if (count > 64) {
     fl |= 4;
-    P.big_list[atomicAdd(&P.small[2], 1u)] = qin;
+    P.big_list[atomicAdd(&P.small[2], 1u)] = L.t;  // processing rank: the slab column of the query
   }
-  P.ncand[qin] = (uint8_t)(count < (uint32_t)kSlab ? count : (uint32_t)kSlab);
-  P.flags[qin] = fl;
+  P.ncand[L.t] = (uint16_t)(count < (uint32_t)kSlab ? count : (uint32_t)kSlab);
+  P.flags[L.qin] = fl;
+}
+
+__device__ __forceinline__ void collect_init(const CollectParams& P, const DevBands& B, uint32_t t, CollectLane& L) {
+  L.t = t;
+  L.qin = P.qorder[t];
+  L.q = P.qpts[L.qin];
+  const double* r = P.qraw + (size_t)L.qin * P.qstride;
+  L.ex = r[1];
+  L.ey = r[2];
+  L.ez = P.qstride == 4 ? r[3] : 0.0;
+  L.count = 0;
+  L.st_nodes = L.st_points = L.st_band = 0;
+}
+
+// One thread per query, queries in Morton order.  Stackless walk over the
+// rope-linked nodes, while-while style: a lane advances through internal
+// nodes until it stands on an overlapping leaf bucket, then the lanes test
+// their buckets together.
+template <bool STATS>
+__global__ void __launch_bounds__(256) k_collect(CollectParams P) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P.nq) return;
+  const DevBands B = *P.bands;
+  const SceneView& S = P.S;
+  const int scene_inexact = *S.inexact;
+  CollectLane L;
+  collect_init(P, B, t, L);
+  int cur = S.n > 0 ? 0 : kRopeEnd;
+  while (cur != kRopeEnd) {
+    int first = 0, cnt = 0;
+    while (cur != kRopeEnd) {
+      const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+      if (STATS) ++L.st_nodes;
+      const int hit = __float_as_int(a.w);
+      const bool over = box_d2(L.q.x, L.q.y, L.q.z, a, b) <= B.box_hi2;
+      if (over && hit >= 0) {
+        ++cur;  // internal node: its left child is the next record
+        continue;
+      }
+      cur = __float_as_int(b.w);
+      if (over) {
+        first = leaf_first(hit);
+        cnt = leaf_count(hit);
+        break;
+      }
+    }
+    if (STATS) L.st_points += cnt;
+    for (int i = first; i < first + cnt; ++i) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)i, __ldg(&S.pts[i]));
+  }
+  collect_finish<STATS>(P, L);
+}
+
+// One warp per 32 Morton-consecutive queries (packet traversal): the warp
+// walks the rope-linked nodes once, entering a node when any lane's query
+// sphere overlaps it.  Node and point loads are warp-uniform (one request
+// each) and the control flow never diverges; each lane tests leaf points
+// against its own query.
+template <bool STATS>
+__global__ void __launch_bounds__(256) k_collect_packet(CollectParams P) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = t < P.nq;
+  if (!__any_sync(0xffffffffu, valid)) return;  // whole warp past the end
+  const DevBands B = *P.bands;
+  const SceneView& S = P.S;
+  const int scene_inexact = *S.inexact;
+  CollectLane L;
+  if (valid) {
+    collect_init(P, B, t, L);
+  } else {
+    L.q = make_float4(INFINITY, INFINITY, INFINITY, 0.f);  // never overlaps
+    L.count = 0;
+    L.st_nodes = L.st_points = L.st_band = 0;
+  }
+  int cur = S.n > 0 ? 0 : kRopeEnd;
+  while (cur != kRopeEnd) {
+    const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+    if (STATS) ++L.st_nodes;
+    const int hit = __float_as_int(a.w);
+    const bool over = valid && box_d2(L.q.x, L.q.y, L.q.z, a, b) <= B.box_hi2;
+    if (__any_sync(0xffffffffu, over)) {
+      if (hit >= 0) {
+        ++cur;  // internal node: its left child is the next record
+        continue;
+      }
+      const int first = leaf_first(hit), cnt = leaf_count(hit);
+      if (STATS) L.st_points += cnt;
+      for (int i = first; i < first + cnt; ++i) {
+        const float4 p = __ldg(&S.pts[i]);
+        if (over) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)i, p);
+      }
+    }
+    cur = __float_as_int(b.w);
+  }
+  if (valid) collect_finish<STATS>(P, L);
 }
 
 // ---- register sorting network --------------------------------------------
@@ -562,7 +587,7 @@ __device__ __forceinline__ void sort_network(uint32_t (&e)[N]) {
   for (int t = 0; t < OddEvenMergeNet<N>::kSize; ++t) cmpswap(e[net.a[t]], e[net.b[t]]);
 }
 
-// Emitted row writer shared by the lane-per-query emit kernels.
+// Emitted row writer shared by the emit kernels.
 struct RowSink {
   void* rows;
   unsigned long long capacity;
@@ -587,13 +612,16 @@ struct EmitParams {
   const float4* qpts;
   const double* qraw;
   int qstride;
-  const uint32_t* qorder;     // Morton order (all-query emit) or the list of large queries
+  const uint32_t* qorder;     // processing rank -> query input index (Morton order)
+  const uint32_t* work;       // optional: processing ranks to handle (large queries)
   uint32_t nwork;
+  uint32_t nq;                // slab stride
   const uint32_t* qrank;      // query input index -> output rank (identity when ids are sorted)
   const DevBands* bands;
-  const uint32_t* slab;
-  const uint8_t* ncand;
-  const uint8_t* flags;
+  const uint32_t* slab;       // slot-major: slab[s * nq + t]
+  const uint32_t* keys;       // same layout: FP32 sort keys
+  const uint16_t* ncand;      // by processing rank
+  const uint8_t* flags;       // by query input index
   const unsigned long long* offsets;
   uint32_t kmax;
   RowSink sink;
@@ -607,23 +635,10 @@ __device__ __forceinline__ uint32_t pack_key(float d2, uint32_t slot) {
   return (__float_as_uint(d2) & ~((1u << SHIFT) - 1u)) | slot;
 }
 
-// FP32-comparable key of candidate i (exact inputs: FP32 d2; inexact inputs:
-// the exact FP64 d2 rounded to FP32, so the key error stays relative).
-__device__ __forceinline__ float cand_key(const SceneView& S, int any_inexact, int scene_inexact, const float4& q,
-                                          double ex, double ey, double ez, uint32_t i) {
-  if (!any_inexact) {
-    const float4 p = __ldg(&S.pts[i]);
-    const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-    return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-  }
-  return __double2float_rn(exact_d2_at(ex, ey, ez, S.pts, S.pts64, scene_inexact, i));
-}
-
-// After the network: the sorted packed keys go to a per-thread column of
-// shared memory ([slot][thread], conflict free) so the register array is dead
-// before any call; neighbours whose truncated keys differ by at most one unit
-// are re-decided exactly (odd-even transposition restricted to those pairs,
-// bounded by n passes), then the rows are written.
+// After the network the sorted packed keys go to a per-thread column of
+// shared memory ([slot][thread], conflict free), so the register array is
+// dead before any call; neighbours whose truncated keys differ by at most one
+// unit are then re-decided exactly and the rows written.
 template <int N, int SHIFT>
 __device__ __forceinline__ bool store_sorted(const uint32_t (&e)[N], int n, uint32_t* col, int stride) {
   bool amb = false;
@@ -636,9 +651,12 @@ __device__ __forceinline__ bool store_sorted(const uint32_t (&e)[N], int n, uint
   return amb;
 }
 
+// Odd-even transposition passes restricted to ambiguous neighbours, until no
+// swap happens (bounded by n passes).  Pairs whose truncated keys differ by two
+// units or more are in exact order already.
 template <int SHIFT>
-__device__ __noinline__ void exact_fixup(uint32_t* col, int stride, int n, const uint32_t* slab, SceneView S,
-                                         int inexact, double ex, double ey, double ez) {
+__device__ __noinline__ void exact_fixup(uint32_t* col, int stride, int n, const uint32_t* slab, size_t ss,
+                                         SceneView S, int inexact, double ex, double ey, double ez) {
   constexpr uint32_t kMask = (1u << SHIFT) - 1u;
   for (int pass = 0; pass < n; ++pass) {
     bool changed = false;
@@ -646,7 +664,8 @@ __device__ __noinline__ void exact_fixup(uint32_t* col, int stride, int n, const
       for (int i = parity; i + 1 < n; i += 2) {
         const uint32_t a = col[i * stride], b = col[(i + 1) * stride];
         if ((b >> SHIFT) - (a >> SHIFT) > 1u) continue;
-        if (exact_before(ex, ey, ez, S.pts, S.pts64, S.perm, inexact, slab[b & kMask], slab[a & kMask])) {
+        if (exact_before(ex, ey, ez, S.pts, S.pts64, S.perm, inexact, slab[(b & kMask) * ss],
+                         slab[(a & kMask) * ss])) {
           col[i * stride] = b;
           col[(i + 1) * stride] = a;
           changed = true;
@@ -657,31 +676,13 @@ __device__ __noinline__ void exact_fixup(uint32_t* col, int stride, int n, const
   }
 }
 
-// Exact insertion sort of all n candidates by the reference key (slots in
-// col).  Used when the 64/65 boundary of a large query is ambiguous in FP32.
-__device__ __noinline__ void exact_sort_all(uint32_t* col, int stride, int n, const uint32_t* slab, SceneView S,
-                                            int inexact, double ex, double ey, double ez) {
-  for (int i = 0; i < n; ++i) col[i * stride] = (uint32_t)i;
-  for (int i = 1; i < n; ++i) {
-    const uint32_t v = col[i * stride];
-    int j = i;
-    while (j > 0) {
-      const uint32_t u = col[(j - 1) * stride];
-      if (!exact_before(ex, ey, ez, S.pts, S.pts64, S.perm, inexact, slab[v], slab[u])) break;
-      col[j * stride] = u;
-      --j;
-    }
-    col[j * stride] = v;
-  }
-}
-
 template <int SHIFT>
-__device__ __forceinline__ void emit_rows(const uint32_t* col, int stride, int kk, const uint32_t* slab,
+__device__ __forceinline__ void emit_rows(const uint32_t* col, int stride, int kk, const uint32_t* slab, size_t ss,
                                           const SceneView& S, int inexact, double ex, double ey, double ez,
                                           uint32_t qid, unsigned long long base, const RowSink& sink) {
   constexpr uint32_t kMask = (1u << SHIFT) - 1u;
   for (int s = 0; s < kk; ++s) {
-    const uint32_t i = slab[col[s * stride] & kMask];
+    const uint32_t i = slab[(col[s * stride] & kMask) * ss];
     const float4 p = __ldg(&S.pts[i]);
     const double dist = __dsqrt_rn(exact_d2_at(ex, ey, ez, S.pts, S.pts64, inexact, i));
     sink.put(base + s, qid, __float_as_uint(p.w), dist, (uint32_t)s + 1);
@@ -689,27 +690,28 @@ __device__ __forceinline__ void emit_rows(const uint32_t* col, int stride, int k
 }
 
 template <int N>
-__device__ __forceinline__ void emit_one_query(const EmitParams& P, uint32_t qin, int n, int inexact, int any_inexact,
-                                               uint32_t* col, int stride) {
+__device__ __forceinline__ void emit_one_query(const EmitParams& P, uint32_t t, uint32_t qin, int n, int inexact,
+                                               int any_inexact, uint32_t* col, int stride) {
   constexpr int SHIFT = 6;
   const float4 q = P.qpts[qin];
   const double* r = P.qraw + (size_t)qin * P.qstride;
   const double ex = r[1], ey = r[2], ez = P.qstride == 4 ? r[3] : 0.0;
-  const uint32_t* slab = P.slab + (size_t)qin * kSlab;
+  const uint32_t* slab = P.slab + t;
+  const uint32_t* keys = P.keys + t;
+  const size_t ss = P.nq;
   bool amb;
   {
     uint32_t e[N];
 #pragma unroll
     for (int s = 0; s < N; ++s)
-      e[s] = s < n ? pack_key<SHIFT>(cand_key(P.S, any_inexact, inexact, q, ex, ey, ez, slab[s]), (uint32_t)s)
-                   : 0xFFFFFFFFu;
+      e[s] = s < n ? pack_key<SHIFT>(__uint_as_float(keys[s * ss]), (uint32_t)s) : 0xFFFFFFFFu;
     sort_network<N>(e);
     amb = store_sorted<N, SHIFT>(e, n, col, stride);
   }
-  if (amb) exact_fixup<SHIFT>(col, stride, n, slab, P.S, inexact, ex, ey, ez);
+  if (amb) exact_fixup<SHIFT>(col, stride, n, slab, ss, P.S, inexact, ex, ey, ez);
   const int kk = n < (int)P.kmax ? n : (int)P.kmax;
-  emit_rows<SHIFT>(col, stride, kk, slab, P.S, inexact, ex, ey, ez, __float_as_uint(q.w), P.offsets[P.qrank[qin]],
-                   P.sink);
+  emit_rows<SHIFT>(col, stride, kk, slab, ss, P.S, inexact, ex, ey, ez, __float_as_uint(q.w),
+                   P.offsets[P.qrank[qin]], P.sink);
 }
 
 // Lane-per-query emit for queries with at most 64 candidates, in Morton order
@@ -726,81 +728,136 @@ __global__ void __launch_bounds__(128) k_emit_lanes(EmitParams P) {
   const uint8_t fl = valid ? P.flags[qin] : 0;
   if (valid && P.overflow_out) P.overflow_out[qin] = fl & 1;
   const bool mine = valid && (fl & 6) == 0;
-  const int n = mine ? (int)P.ncand[qin] : 0;
+  const int n = mine ? (int)P.ncand[t] : 0;
   const int inexact = *P.S.inexact;
   const int any_inexact = P.bands->any_inexact;
   const unsigned int active = __ballot_sync(0xffffffffu, mine && n > 0);
   if (!(mine && n > 0)) return;
   if (__all_sync(active, n <= 32))
-    emit_one_query<32>(P, qin, n, inexact, any_inexact, col, stride);
+    emit_one_query<32>(P, t, qin, n, inexact, any_inexact, col, stride);
   else
-    emit_one_query<64>(P, qin, n, inexact, any_inexact, col, stride);
+    emit_one_query<64>(P, t, qin, n, inexact, any_inexact, col, stride);
 }
 
-// Lane-per-query emit for queries with 65..128 candidates: the first 64 are
-// sorted and parked in shared memory, the rest sorted in registers, then a
-// bitonic keep-smallest merge yields the 64 nearest in order.  If the best
-// dropped candidate is within one truncated unit of the last kept one, the
-// cut at 64 is not decided by FP32 and all candidates are sorted exactly.
-// Dynamic shared memory: 128 words per thread.
-__global__ void __launch_bounds__(64) k_emit_big(EmitParams P) {
-  constexpr int SHIFT = 7;
-  constexpr int N = 64;
-  extern __shared__ uint32_t emit_smem[];
-  uint32_t* col = emit_smem + threadIdx.x;
-  const int stride = blockDim.x;
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.nwork) return;
+// ---- warp-per-query emit for 65..256 candidates -----------------------------
+// Bitonic sort across the warp: E packed keys per lane in a blocked layout
+// (element i = lane * E + r), exchanges within a lane in registers and across
+// lanes with one shuffle per element.
+template <int E>
+__device__ __forceinline__ void warp_bitonic(uint32_t (&v)[E], int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32 * E; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= E) {
+        const int lj = j / E;
+        const bool lower = (lane & lj) == 0;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          const bool up = ((lane * E + r) & k) == 0;
+          const uint32_t other = __shfl_xor_sync(0xffffffffu, v[r], lj);
+          v[r] = (lower == up) ? min(v[r], other) : max(v[r], other);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          const int pr = r ^ j;
+          if (pr > r) {
+            const bool up = ((lane * E + r) & k) == 0;
+            const uint32_t a = v[r], b = v[pr];
+            v[r] = up ? min(a, b) : max(a, b);
+            v[pr] = up ? max(a, b) : min(a, b);
+          }
+        }
+      }
+    }
+  }
+}
+
+// Single-thread exact fixup over a warp's sorted buffer (same rule as
+// exact_fixup, with slab_at addressing); only when a neighbour pair is
+// ambiguous.
+__device__ __noinline__ void exact_fixup_linear(uint32_t* buf, int n, const uint32_t* slab, uint32_t t, uint32_t nq,
+                                                SceneView S, int inexact, double ex, double ey, double ez) {
+  constexpr int SHIFT = 8;
+  constexpr uint32_t kMask = (1u << SHIFT) - 1u;
+  for (int pass = 0; pass < n; ++pass) {
+    bool changed = false;
+    for (int parity = 0; parity < 2; ++parity) {
+      for (int i = parity; i + 1 < n; i += 2) {
+        const uint32_t a = buf[i], b = buf[i + 1];
+        if ((b >> SHIFT) - (a >> SHIFT) > 1u) continue;
+        if (exact_before(ex, ey, ez, S.pts, S.pts64, S.perm, inexact, slab[slab_at(b & kMask, t, nq)],
+                         slab[slab_at(a & kMask, t, nq)])) {
+          buf[i] = b;
+          buf[i + 1] = a;
+          changed = true;
+        }
+      }
+    }
+    if (!changed) break;
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void emit_warp_query(const EmitParams& P, uint32_t t, int lane, uint32_t* wbuf) {
+  constexpr int SHIFT = 8;  // 256 slots
+  constexpr uint32_t kMask = (1u << SHIFT) - 1u;
   const uint32_t qin = P.qorder[t];
-  const int n = (int)P.ncand[qin];
+  const int n = (int)P.ncand[t];
+  const uint32_t nq = P.nq;
   const int inexact = *P.S.inexact;
-  const int any_inexact = P.bands->any_inexact;
-  const float4 q = P.qpts[qin];
-  const double* r = P.qraw + (size_t)qin * P.qstride;
-  const double ex = r[1], ey = r[2], ez = P.qstride == 4 ? r[3] : 0.0;
-  const uint32_t* slab = P.slab + (size_t)qin * kSlab;
-  bool amb = false, cut_ambiguous = false;
-  {
-    uint32_t e[N];
+  uint32_t v[E];
 #pragma unroll
-    for (int s = 0; s < N; ++s)
-      e[s] = pack_key<SHIFT>(cand_key(P.S, any_inexact, inexact, q, ex, ey, ez, slab[s]), (uint32_t)s);
-    sort_network<N>(e);
-#pragma unroll
-    for (int s = 0; s < N; ++s) col[s * stride] = e[s];
+  for (int r = 0; r < E; ++r) {
+    const int sl = lane * E + r;
+    v[r] = sl < n ? pack_key<SHIFT>(__uint_as_float(P.keys[slab_at(sl, t, nq)]), (uint32_t)sl) : 0xFFFFFFFFu;
   }
-  {
-    uint32_t f[N];
+  warp_bitonic<E>(v, lane);
+  bool amb = false;
 #pragma unroll
-    for (int s = 0; s < N; ++s)
-      f[s] = s + N < n
-                 ? pack_key<SHIFT>(cand_key(P.S, any_inexact, inexact, q, ex, ey, ez, slab[s + N]), (uint32_t)(s + N))
-                 : 0xFFFFFFFFu;
-    sort_network<N>(f);
-    uint32_t g[N];
-    uint32_t dropped = 0xFFFFFFFFu;  // smallest candidate not kept
+  for (int r = 0; r + 1 < E; ++r)
+    amb |= v[r + 1] != 0xFFFFFFFFu && (v[r + 1] >> SHIFT) - (v[r] >> SHIFT) <= 1u;
+  const uint32_t next = __shfl_down_sync(0xffffffffu, v[0], 1);
+  if (lane < 31) amb |= next != 0xFFFFFFFFu && (next >> SHIFT) - (v[E - 1] >> SHIFT) <= 1u;
+  const double* rq = P.qraw + (size_t)qin * P.qstride;
+  const double ex = rq[1], ey = rq[2], ez = P.qstride == 4 ? rq[3] : 0.0;
+  if (__any_sync(0xffffffffu, amb)) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
-      const uint32_t a = col[i * stride], b = f[N - 1 - i];
-      g[i] = min(a, b);  // the 64 smallest, as a bitonic sequence
-      dropped = min(dropped, max(a, b));
-    }
+    for (int r = 0; r < E; ++r) wbuf[lane * E + r] = v[r];
+    __syncwarp();
+    if (lane == 0) exact_fixup_linear(wbuf, n, P.slab, t, nq, P.S, inexact, ex, ey, ez);
+    __syncwarp();
 #pragma unroll
-    for (int k = N / 2; k >= 1; k >>= 1) {
-#pragma unroll
-      for (int i = 0; i < N; ++i)
-        if ((i & k) == 0) cmpswap(g[i], g[i + k]);
-    }
-    cut_ambiguous = (dropped >> SHIFT) - (g[N - 1] >> SHIFT) <= 1u;
-    if (!cut_ambiguous) amb = store_sorted<N, SHIFT>(g, N, col, stride);
+    for (int r = 0; r < E; ++r) v[r] = wbuf[lane * E + r];
+    __syncwarp();
   }
-  if (cut_ambiguous)
-    exact_sort_all(col, stride, n, slab, P.S, inexact, ex, ey, ez);
-  else if (amb)
-    exact_fixup<SHIFT>(col, stride, N, slab, P.S, inexact, ex, ey, ez);
-  const int kk = (int)P.kmax < N ? (int)P.kmax : N;
-  emit_rows<SHIFT>(col, stride, kk, slab, P.S, inexact, ex, ey, ez, __float_as_uint(q.w), P.offsets[P.qrank[qin]],
-                   P.sink);
+  const int kk = n < (int)P.kmax ? n : (int)P.kmax;
+  const uint32_t qid = __float_as_uint(P.qpts[qin].w);
+  const unsigned long long base = P.offsets[P.qrank[qin]];
+#pragma unroll
+  for (int r = 0; r < E; ++r) {
+    const int i = lane * E + r;
+    if (i < kk) {
+      const uint32_t idx = P.slab[slab_at(v[r] & kMask, t, nq)];
+      const float4 p = __ldg(&P.S.pts[idx]);
+      const double dist = __dsqrt_rn(exact_d2_at(ex, ey, ez, P.S.pts, P.S.pts64, inexact, idx));
+      P.sink.put(base + i, qid, __float_as_uint(p.w), dist, (uint32_t)i + 1);
+    }
+  }
+}
+
+// One warp per query with 65..256 candidates (processing ranks in P.work).
+__global__ void __launch_bounds__(128) k_emit_warp(EmitParams P) {
+  __shared__ uint32_t wbuf[4][kSlab];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (j >= P.nwork) return;  // whole warp
+  const uint32_t t = P.work[j];
+  if (P.ncand[t] <= 128)
+    emit_warp_query<4>(P, t, lane, wbuf[wib]);
+  else
+    emit_warp_query<8>(P, t, lane, wbuf[wib]);
 }
 
 __global__ void k_invert(const uint32_t* order, uint32_t n, const unsigned int* identity_flag, uint32_t* inv) {
@@ -914,14 +971,18 @@ __global__ void __launch_bounds__(32)
   const uint32_t P2 = seg_size[h];
   const unsigned int lt_mask = (1u << lane) - 1u;
   uint32_t cnt = 0;
-  int2 stack[kStackDepth];
-  int sp = 0;
-  int ref = S.root_ref, leaf = S.root_cnt;
-  bool alive = S.n > 0;
-  while (alive) {
-    if (leaf > 0) {
+  int cur = S.n > 0 ? 0 : kRopeEnd;
+  while (cur != kRopeEnd) {  // warp-uniform: every lane follows the same nodes
+    const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+    const int hit = __float_as_int(a.w);
+    if (box_d2(c.qx, c.qy, c.qz, a, b) <= B.box_hi2) {
+      if (hit >= 0) {
+        ++cur;  // internal node: its left child is the next record
+        continue;
+      }
+      const int first = leaf_first(hit), leaf = leaf_count(hit);
       bool acc = false;
-      const uint32_t i = (uint32_t)(ref + lane);
+      const uint32_t i = (uint32_t)(first + lane);
       if (lane < leaf) {
         const float4 p = __ldg(&S.pts[i]);
         const float dx = p.x - c.qx, dy = p.y - c.qy, dz = p.z - c.qz;
@@ -942,40 +1003,8 @@ __global__ void __launch_bounds__(32)
         }
       }
       cnt += __popc(m);
-      leaf = 0;
-      if (sp > 0) {
-        --sp;
-        ref = stack[sp].x;
-        leaf = stack[sp].y;
-      } else {
-        alive = false;
-      }
-      continue;
     }
-    const float4* nd = S.nodes + 4 * (size_t)ref;
-    const float4 a = __ldg(nd), b = __ldg(nd + 1), e = __ldg(nd + 2), f = __ldg(nd + 3);
-    const bool h0 = box_d2(c.qx, c.qy, c.qz, a, b) <= B.box_hi2;
-    const bool h1 = box_d2(c.qx, c.qy, c.qz, e, f) <= B.box_hi2;
-    if (h0) {
-      if (h1) {
-        if (sp >= kStackDepth) {
-          atomicOr(error, 1u);
-          break;
-        }
-        stack[sp++] = make_int2(__float_as_int(e.w), __float_as_int(f.w));
-      }
-      ref = __float_as_int(a.w);
-      leaf = __float_as_int(b.w);
-    } else if (h1) {
-      ref = __float_as_int(e.w);
-      leaf = __float_as_int(f.w);
-    } else if (sp > 0) {
-      --sp;
-      ref = stack[sp].x;
-      leaf = stack[sp].y;
-    } else {
-      alive = false;
-    }
+    cur = __float_as_int(b.w);
   }
   for (uint32_t i = cnt + lane; i < P2; i += 32) {
     HeavyEntry en;
@@ -993,11 +1022,10 @@ __device__ __forceinline__ bool heavy_greater(const HeavyEntry& a, const HeavyEn
   return perm[a.sidx] > perm[b.sidx];
 }
 
-__global__ void __launch_bounds__(kHeavyThreads)
-    k_heavy_sort(const unsigned long long* seg_off, const uint32_t* seg_size, HeavyEntry* scratch,
-                 const uint32_t* perm) {
-  HeavyEntry* e = scratch + seg_off[blockIdx.x];
-  const uint32_t P2 = seg_size[blockIdx.x];
+constexpr uint32_t kHeavySmemEntries = 2048;  // 32 KiB of 16-B entries per block
+
+template <typename Ptr>
+__device__ __forceinline__ void bitonic_block(Ptr e, uint32_t P2, const uint32_t* perm) {
   for (uint32_t k = 2; k <= P2; k <<= 1) {
     for (uint32_t j = k >> 1; j > 0; j >>= 1) {
       for (uint32_t i = threadIdx.x; i < P2; i += blockDim.x) {
@@ -1013,6 +1041,24 @@ __global__ void __launch_bounds__(kHeavyThreads)
       }
       __syncthreads();
     }
+  }
+}
+
+// Block-per-query bitonic sort of a segment by (distance, neighbor id, search
+// input index); in shared memory up to 2,048 entries, in global memory above.
+__global__ void __launch_bounds__(kHeavyThreads)
+    k_heavy_sort(const unsigned long long* seg_off, const uint32_t* seg_size, HeavyEntry* scratch,
+                 const uint32_t* perm) {
+  extern __shared__ HeavyEntry heavy_smem[];
+  HeavyEntry* e = scratch + seg_off[blockIdx.x];
+  const uint32_t P2 = seg_size[blockIdx.x];
+  if (P2 <= kHeavySmemEntries) {
+    for (uint32_t i = threadIdx.x; i < P2; i += blockDim.x) heavy_smem[i] = e[i];
+    __syncthreads();
+    bitonic_block(heavy_smem, P2, perm);
+    for (uint32_t i = threadIdx.x; i < P2; i += blockDim.x) e[i] = heavy_smem[i];
+  } else {
+    bitonic_block(e, P2, perm);
   }
 }
 
@@ -1065,8 +1111,9 @@ __global__ void __launch_bounds__(kExpandThreads) k_expand(ExpandParams P) {
     const uint32_t qid = __float_as_uint(P.qpts[qin].w);
     const double* r = P.qraw + (size_t)qin * P.qstride;
     const double ex = r[1], ey = r[2], ez = P.qstride == 4 ? r[3] : 0.0;
-    const uint32_t* src = (fl & 2) ? P.heavy_out + P.heavy_out_off[P.temp[(size_t)qin * P.L]]
-                                   : P.temp + (size_t)qin * P.L;
+    const uint32_t* src = P.work_list ? P.heavy_out + P.heavy_out_off[j]
+                          : (fl & 2) ? P.heavy_out + P.heavy_out_off[P.temp[(size_t)qin * P.L]]
+                                     : P.temp + (size_t)qin * P.L;
     for (uint32_t s = lane; s < cnt; s += 32) {
       const uint32_t sidx = src[s];
       if (sidx >= P.S.n) {  // never expected: a generic-path slot without a candidate
@@ -1320,7 +1367,8 @@ GenericOut run_generic_path(Scene* sc, const QueryPrep& qp, const void* queries_
   else
     k_heavy_gather_bvh<<<H, 32, 0, s>>>(sc->view(), qp.qpts, static_cast<const double*>(queries_dev), qstride,
                                         heavy_list, d_seg_off, d_seg_size, qp.bands, scratch, error);
-  k_heavy_sort<<<H, kHeavyThreads, 0, s>>>(d_seg_off, d_seg_size, scratch, sc->perm);
+  k_heavy_sort<<<H, kHeavyThreads, sizeof(HeavyEntry) * kHeavySmemEntries, s>>>(d_seg_off, d_seg_size, scratch,
+                                                                                sc->perm);
   k_heavy_emit<<<H, kHeavyThreads, 0, s>>>(d_seg_off, g.heavy_out_off, d_out_cnt, scratch, g.heavy_out);
   RTDL_LAUNCHED(3);
   RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors above are read by the copies
@@ -1348,8 +1396,9 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
   RTDL_LAUNCHED(1);
   if (timer) timer->mark("query_prep");
   uint32_t* slab = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (size_t)nq * kSlab, s));
+  uint32_t* keys = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (size_t)nq * kSlab, s));
   uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint8_t* ncand = static_cast<uint8_t*>(dev_alloc(nq, s));
+  uint16_t* ncand = static_cast<uint16_t*>(dev_alloc(sizeof(uint16_t) * nq, s));
   uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq, s));
   uint32_t* heavy_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   uint32_t* heavy_m = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
@@ -1362,6 +1411,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     g.release(s);
     dev_free(qrank, s);
     dev_free(slab, s);
+    dev_free(keys, s);
     dev_free(counts, s);
     dev_free(ncand, s);
     dev_free(flags, s);
@@ -1383,6 +1433,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     C.kmax = kmax;
     C.bands = qp.bands;
     C.slab = slab;
+    C.keys = keys;
     C.counts = counts;
     C.ncand = ncand;
     C.flags = flags;
@@ -1397,10 +1448,19 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       RTDL_CUDA_CHECK(cudaMemsetAsync(C.stats, 0, sizeof(unsigned long long) * kStatCount, s));
     }
     const int threads = tuning().block_threads;
-    if (stats)
-      k_collect<true><<<div_up(nq, threads), threads, 0, s>>>(C);
-    else
-      k_collect<false><<<div_up(nq, threads), threads, 0, s>>>(C);
+    if (timer) timer->mark("setup");
+    const bool packet = tuning().traversal == 0;
+    if (packet) {
+      if (stats)
+        k_collect_packet<true><<<div_up(nq, threads), threads, 0, s>>>(C);
+      else
+        k_collect_packet<false><<<div_up(nq, threads), threads, 0, s>>>(C);
+    } else {
+      if (stats)
+        k_collect<true><<<div_up(nq, threads), threads, 0, s>>>(C);
+      else
+        k_collect<false><<<div_up(nq, threads), threads, 0, s>>>(C);
+    }
     RTDL_LAUNCHED(1);
     if (stats) {
       RTDL_CUDA_CHECK(cudaMemcpyAsync(last_stats().data(), C.stats, sizeof(unsigned long long) * kStatCount,
@@ -1441,10 +1501,13 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     E.qraw = static_cast<const double*>(queries_dev);
     E.qstride = qstride;
     E.qorder = qp.qorder;
+    E.work = nullptr;
     E.nwork = nq;
+    E.nq = nq;
     E.qrank = qrank;
     E.bands = qp.bands;
     E.slab = slab;
+    E.keys = keys;
     E.ncand = ncand;
     E.flags = flags;
     E.offsets = offsets;
@@ -1456,10 +1519,10 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     k_emit_lanes<<<div_up(nq, 128), 128, 128 * 64 * sizeof(uint32_t), s>>>(E);
     RTDL_LAUNCHED(1);
     if (big > 0) {
-      E.qorder = big_list;
+      E.work = big_list;
       E.nwork = big;
       E.overflow_out = nullptr;
-      k_emit_big<<<div_up(big, 64), 64, 64 * kSlab * sizeof(uint32_t), s>>>(E);
+      k_emit_warp<<<div_up((uint64_t)big * 32, 128), 128, 0, s>>>(E);
       RTDL_LAUNCHED(1);
     }
     if (r.heavy > 0) {

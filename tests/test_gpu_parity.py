@@ -250,7 +250,7 @@ def test_lattice_shell_ties_at_the_cut(gpu):
     pts = pts[order]
     s = _cols(pts, ids=(rng.integers(0, 60, len(pts))).astype(np.uint32))  # many duplicate ids
     q = _cols(centres, ids=np.array([7, 3, 5], dtype=np.uint32))
-    # radius^2 = 26: 102 candidates per query (65..128 path); 27: 134 (generic path)
+    # radius^2 = 26: 102 candidates per query, 27: 134 (both on the warp-per-query emit)
     for r2, per_query in ((26.0, 102), (27.0, 134)):
         radius = float(np.nextafter(np.sqrt(r2), np.inf))  # radius * radius >= r2 in FP64
         for k_max in (10, 30, 40, 64, 100):
@@ -263,3 +263,24 @@ def test_lattice_shell_ties_at_the_cut(gpu):
             assert (counts == per_query).all()
             _assert_same_rows(got, exp, False)
             assert np.array_equal(overflow.astype(bool), counts > k_max)
+
+
+def test_lattice_ball_generic_path(gpu):
+    """All integer points with |v|^2 <= 50 around each query (about 1,500
+    candidates, many exactly equal distances): more candidates than the
+    per-query slab holds, so the generic path decides the k_max nearest."""
+    rng = np.random.default_rng(18)
+    r = np.arange(-8, 9)
+    grid = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3)
+    ball = grid[(grid ** 2).sum(1) <= 50].astype(np.float64)
+    centres = np.array([[0.0, 0.0, 0.0], [100.0, 0.0, 0.0]])
+    pts = np.concatenate([c + ball for c in centres])[rng.permutation(2 * len(ball))]
+    s = _cols(pts, ids=rng.integers(0, 200, len(pts)).astype(np.uint32))
+    q = _cols(centres, ids=np.array([1, 0], dtype=np.uint32))
+    radius = float(np.nextafter(np.sqrt(50.0), np.inf))
+    for k_max in (1, 17, 64):
+        v, = [rt.runtime.fixed_radius_neighbors(_pack(q), _pack(s), radius=radius, k_max=k_max)]
+        exp, counts = O.fixed_radius_neighbors(q, s, radius=radius, k_max=k_max, with_counts=True)
+        assert (counts > 256).all()
+        _assert_same_rows(v.to_numpy(), exp, False)
+        v.close()

@@ -201,6 +201,38 @@ RTDL_B200_API int rtdl_b200_scene_directed_hausdorff(
     double* nearest_distance_out, uint32_t* nearest_id_out,
     char* error_out, size_t error_size);
 
+/* Result record of rtdl_b200_scene_directed_hausdorff_noalloc (device memory).
+ * status: 0 = ok, 1 = a coordinate is non-finite or beyond 1e18, 2 = the
+ * traversal stack overflowed. */
+typedef struct RtdlB200Witness {
+  double distance;
+  uint32_t source_id, target_id;
+  uint32_t status, reserved;
+} RtdlB200Witness;
+
+/* Directed Hausdorff on a scene without allocating device memory.  No
+ * counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc while they run the query -- an application whose allocator owns
+ * the whole device heap, code running inside a larger CUDA graph it does not
+ * own, or a real-time loop where an allocation could stall.  Inputs and
+ * outputs are device pointers the caller owns: query_points_dev (RtdlPoint or
+ * RtdlPoint3D records matching the scene's dimension), the optional per-query
+ * nearest_distance_dev / nearest_id_dev arrays (query input order) and
+ * witness_dev.  The work is enqueued on `stream` (NULL = the legacy default
+ * stream) and the call returns without waiting; read witness_dev->status after
+ * the stream has finished.  All scratch comes from one fixed device array of
+ * 8.75 MiB that every GPU loading the library holds until the process exits,
+ * which caps query_count at 262,144; larger counts are rejected with an
+ * error.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call reuses the same array, so calls that overlap on the GPU (on
+ * different streams, or from different threads) race and must be serialized
+ * by the caller.  Results equal rtdl_b200_scene_directed_hausdorff. */
+RTDL_B200_API int rtdl_b200_scene_directed_hausdorff_noalloc(
+    void* scene, const void* query_points_dev, size_t query_count,
+    double* nearest_distance_dev, uint32_t* nearest_id_dev, RtdlB200Witness* witness_dev,
+    void* stream, char* error_out, size_t error_size);
+
 /* Phase timings of the last call on this thread, in milliseconds (device
  * events).  Mirrors rtdl_optix_fixed_radius_neighbors_3d_get_last_phase_timings
  * (src/rtdsl/optix_runtime.py:4916, 5029-5106).  Fills up to `capacity`

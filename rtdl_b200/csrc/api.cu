@@ -563,6 +563,21 @@ int rtdl_b200_scene_directed_hausdorff(void* scene, const void* query_points, si
   }, error_out, error_size);
 }
 
+int rtdl_b200_scene_directed_hausdorff_noalloc(void* scene, const void* query_points_dev, size_t query_count,
+                                               double* nearest_distance_dev, uint32_t* nearest_id_dev,
+                                               RtdlB200Witness* witness_dev, void* stream, char* error_out,
+                                               size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(scene);
+    if (!sc) throw std::runtime_error("scene must not be null");
+    if (!witness_dev) throw std::runtime_error("witness_dev must not be null");
+    if (query_count > (size_t)UINT32_MAX) throw std::runtime_error("query_count exceeds uint32 limit");
+    if (query_count != 0 && !query_points_dev) throw std::runtime_error("query_points_dev must not be null");
+    run_directed_hausdorff_noalloc(sc, query_points_dev, (uint32_t)query_count, nearest_distance_dev, nearest_id_dev,
+                                   witness_dev, static_cast<cudaStream_t>(stream));
+  }, error_out, error_size);
+}
+
 int rtdl_b200_prepare_fixed_radius_neighbors_3d(const RtdlPoint3D* search_points, size_t search_count,
                                                 double max_radius, void** prepared_out, char* error_out,
                                                 size_t error_size) {

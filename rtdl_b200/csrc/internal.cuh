@@ -194,6 +194,11 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
 // candidates.
 std::vector<unsigned long long>& last_stats();
 
+// Allocation-free directed Hausdorff (scratch in a fixed device array);
+// results and status land in witness_dev on stream s.
+void run_directed_hausdorff_noalloc(Scene* sc, const void* queries_dev, uint32_t nq, double* nearest_dist_dev,
+                                    uint32_t* nearest_id_dev, RtdlB200Witness* witness_dev, cudaStream_t s);
+
 inline unsigned int div_up(unsigned long long a, unsigned long long b) { return (unsigned int)((a + b - 1) / b); }
 
 }  // namespace rtdl_b200

@@ -28,6 +28,7 @@
 //     k_max, or k > 64) go to a generic block-per-query path (gather, bitonic
 //     sort in global memory, emit).
 #include <cstdlib>
+#include <mutex>
 
 #include "internal.cuh"
 
@@ -1789,6 +1790,130 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   out.source_id = w.qid;
   out.target_id = w.nid;
   return out;
+}
+
+
+// ---- allocation-free directed Hausdorff ------------------------------------
+// Some callers cannot allocate device memory while they run this query: an
+// application that hands the whole device heap to its own allocator, code
+// running between the capture points of a larger CUDA graph it does not own,
+// or a real-time loop where an allocation could stall.  For them
+// rtdl_b200_scene_directed_hausdorff_noalloc takes every scratch buffer of
+// the nearest pass and of the max-witness reduction from this file-scope
+// device array instead of the stream-ordered allocator.  Every GPU that loads
+// the library holds the array until the process exits.
+namespace {
+
+constexpr uint32_t kNoAllocMaxQueries = 1u << 18;  // 262,144 queries per call
+constexpr unsigned int kNoAllocReduceBlocks = 2 * kSmCount;
+
+constexpr size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+struct NoAllocLayout {  // byte offsets into the scratch array, 256-B aligned
+  static constexpr size_t kStats = 0;
+  static constexpr size_t kBands = align256(kStats + sizeof(PointStats));
+  static constexpr size_t kSmall = align256(kBands + sizeof(DevBands));
+  static constexpr size_t kBest = align256(kSmall + 4 * sizeof(unsigned int));
+  static constexpr size_t kPartial = align256(kBest + sizeof(Witness));
+  static constexpr size_t kQpts = align256(kPartial + kNoAllocReduceBlocks * sizeof(Witness));
+  static constexpr size_t kOrder = align256(kQpts + (size_t)kNoAllocMaxQueries * sizeof(float4));
+  static constexpr size_t kTemp = align256(kOrder + (size_t)kNoAllocMaxQueries * sizeof(uint32_t));
+  static constexpr size_t kCounts = align256(kTemp + (size_t)kNoAllocMaxQueries * sizeof(uint32_t));
+  static constexpr size_t kFlags = align256(kCounts + (size_t)kNoAllocMaxQueries * sizeof(uint32_t));
+  static constexpr size_t kTotal = align256(kFlags + (size_t)kNoAllocMaxQueries);
+};
+
+// 8.75 MiB: scratch for up to kNoAllocMaxQueries queries.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::kTotal];
+
+// Converts the reduced witness into the public record and folds in the
+// input checks, so the call never needs a host round trip.
+__global__ void k_noalloc_finish(const Witness* best, const PointStats* scene_stats, const PointStats* query_stats,
+                                 const unsigned int* error, RtdlB200Witness* out) {
+  if (threadIdx.x != 0) return;
+  RtdlB200Witness w;
+  unsigned long long db = best->dist;
+  w.distance = __longlong_as_double((long long)db);
+  w.source_id = best->qid;
+  w.target_id = best->nid;
+  w.status = (scene_stats->bad || query_stats->bad) ? 1u : ((*error & 1u) ? 2u : 0u);
+  w.reserved = 0u;
+  *out = w;
+}
+
+unsigned char* noalloc_scratch_for_current_device() {
+  static std::mutex m;
+  static std::vector<unsigned char*> ptrs;
+  int dev = 0;
+  RTDL_CUDA_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(m);
+  if ((int)ptrs.size() <= dev) ptrs.resize(dev + 1, nullptr);
+  if (ptrs[dev] == nullptr) {
+    // The symbol name is a host-side stand-in; the device address comes from
+    // the runtime, per device, with that device current.
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      throw std::runtime_error(std::string("cudaGetSymbolAddress of the scratch array failed: ") +
+                               cudaGetErrorString(e));
+    ptrs[dev] = static_cast<unsigned char*>(p);
+  }
+  return ptrs[dev];
+}
+
+}  // namespace
+
+void run_directed_hausdorff_noalloc(Scene* sc, const void* queries_dev, uint32_t nq, double* nearest_dist_dev,
+                                    uint32_t* nearest_id_dev, RtdlB200Witness* witness_dev, cudaStream_t s) {
+  if (nq == 0 || sc->n == 0) throw std::runtime_error("Hausdorff distance requires non-empty point sets");
+  if (nq > kNoAllocMaxQueries)
+    throw std::runtime_error("rtdl_b200_scene_directed_hausdorff_noalloc: query_count exceeds the limit of 262144 "
+                             "queries set by its fixed scratch array");
+  unsigned char* base = noalloc_scratch_for_current_device();
+  PointStats* qst = reinterpret_cast<PointStats*>(base + NoAllocLayout::kStats);
+  DevBands* bands = reinterpret_cast<DevBands*>(base + NoAllocLayout::kBands);
+  unsigned int* small = reinterpret_cast<unsigned int*>(base + NoAllocLayout::kSmall);
+  Witness* best = reinterpret_cast<Witness*>(base + NoAllocLayout::kBest);
+  Witness* partial = reinterpret_cast<Witness*>(base + NoAllocLayout::kPartial);
+  float4* qpts = reinterpret_cast<float4*>(base + NoAllocLayout::kQpts);
+  uint32_t* qorder = reinterpret_cast<uint32_t*>(base + NoAllocLayout::kOrder);
+  uint32_t* temp = reinterpret_cast<uint32_t*>(base + NoAllocLayout::kTemp);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(base + NoAllocLayout::kCounts);
+  uint8_t* flags = reinterpret_cast<uint8_t*>(base + NoAllocLayout::kFlags);
+  // The array keeps the previous call's contents: reset what must start at zero.
+  reset_stats(qst, s);
+  RTDL_CUDA_CHECK(cudaMemsetAsync(small, 0, 4 * sizeof(unsigned int), s));
+  prep_points(queries_dev, nq, sc->dim, qpts, qst, s);
+  k_bands<<<1, 32, 0, s>>>(sc->stats, qst, 0.0, 0, bands);
+  RTDL_LAUNCHED(1);
+  iota_u32(qorder, nq, s);  // input order: no sort, hence no sort scratch
+  Pass1Params P;
+  P.S = sc->view();
+  P.qpts = qpts;
+  P.qraw = static_cast<const double*>(queries_dev);
+  P.qstride = sc->dim == 3 ? 4 : 3;
+  P.qorder = qorder;
+  P.nq = nq;
+  P.kmax = 1;
+  P.L = 1;
+  P.bands = bands;
+  P.temp = temp;
+  P.counts = counts;
+  P.flags = flags;
+  P.heavy_list = nullptr;
+  P.heavy_m = nullptr;
+  P.heavy_count = small;
+  P.error = small + 1;
+  P.stats = nullptr;
+  const int threads = tuning().block_threads;
+  k_pass1<true, false><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
+  RTDL_LAUNCHED(1);
+  const unsigned int blocks = grid_for(nq, 256) < kNoAllocReduceBlocks ? grid_for(nq, 256) : kNoAllocReduceBlocks;
+  k_nearest_reduce<<<blocks, 256, 0, s>>>(sc->view(), qpts, static_cast<const double*>(queries_dev), P.qstride, nq,
+                                          temp, nearest_dist_dev, nearest_id_dev, partial);
+  k_witness_final<<<1, 32, 0, s>>>(partial, (int)blocks, best);
+  k_noalloc_finish<<<1, 32, 0, s>>>(best, sc->stats, qst, small + 1, witness_dev);
+  RTDL_LAUNCHED(3);
 }
 
 }  // namespace rtdl_b200

@@ -201,6 +201,16 @@ RTDL_B200_API int rtdl_b200_scene_directed_hausdorff(
     double* nearest_distance_out, uint32_t* nearest_id_out,
     char* error_out, size_t error_size);
 
+/* Device-resident form of rtdl_b200_scene_directed_hausdorff: the queries and
+ * the optional per-query outputs are device pointers, the work runs on
+ * `stream` (NULL = the scene's stream) and the witness is returned to the
+ * host after the stream finishes. */
+RTDL_B200_API int rtdl_b200_scene_directed_hausdorff_device(
+    void* scene, const void* query_points_dev, size_t query_count,
+    double* nearest_distance_dev, uint32_t* nearest_id_dev,
+    double* distance_out, uint32_t* source_id_out, uint32_t* target_id_out,
+    void* stream, char* error_out, size_t error_size);
+
 /* Result record of rtdl_b200_scene_directed_hausdorff_noalloc (device memory).
  * status: 0 = ok, 1 = a coordinate is non-finite or beyond 1e18, 2 = the
  * traversal stack overflowed. */
@@ -221,7 +231,7 @@ typedef struct RtdlB200Witness {
  * witness_dev.  The work is enqueued on `stream` (NULL = the legacy default
  * stream) and the call returns without waiting; read witness_dev->status after
  * the stream has finished.  All scratch comes from one fixed device array of
- * 8.75 MiB that every GPU loading the library holds until the process exits,
+ * 9.75 MiB that every GPU loading the library holds until the process exits,
  * which caps query_count at 262,144; larger counts are rejected with an
  * error.  The first call on a device looks up that array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.

@@ -95,6 +95,7 @@ SIGNATURES = {
     "rtdl_b200_scene_query": (_i, [_vp, _vp, _sz, _i, _d, _sz, _vpp, _szp, _u8p, _cp, _sz]),
     "rtdl_b200_scene_query_device": (_i, [_vp, _vp, _sz, _i, _d, _sz, _vp, _sz, _szp, _vp, _vp, _cp, _sz]),
     "rtdl_b200_scene_directed_hausdorff": (_i, [_vp, _vp, _sz, _dp, _u32p, _u32p, _dp, _u32p, _cp, _sz]),
+    "rtdl_b200_scene_directed_hausdorff_device": (_i, [_vp, _vp, _sz, _vp, _vp, _dp, _u32p, _u32p, _vp, _cp, _sz]),
     "rtdl_b200_scene_directed_hausdorff_noalloc": (_i, [_vp, _vp, _sz, _vp, _vp, _vp, _vp, _cp, _sz]),
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i, _i]),

@@ -563,6 +563,26 @@ int rtdl_b200_scene_directed_hausdorff(void* scene, const void* query_points, si
   }, error_out, error_size);
 }
 
+int rtdl_b200_scene_directed_hausdorff_device(void* scene, const void* query_points_dev, size_t query_count,
+                                              double* nearest_distance_dev, uint32_t* nearest_id_dev,
+                                              double* distance_out, uint32_t* source_id_out, uint32_t* target_id_out,
+                                              void* stream, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(scene);
+    if (!sc) throw std::runtime_error("scene must not be null");
+    if (query_count > (size_t)UINT32_MAX) throw std::runtime_error("query_count exceeds uint32 limit");
+    if (query_count == 0 || sc->n == 0) throw std::runtime_error("Hausdorff distance requires non-empty point sets");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sc->stream;
+    PhaseTimer timer(s);
+    HausdorffResult h = run_directed_hausdorff(sc, query_points_dev, (uint32_t)query_count, nearest_distance_dev,
+                                               nearest_id_dev, s, &timer);
+    timer.publish();
+    if (distance_out) *distance_out = h.distance;
+    if (source_id_out) *source_id_out = h.source_id;
+    if (target_id_out) *target_id_out = h.target_id;
+  }, error_out, error_size);
+}
+
 int rtdl_b200_scene_directed_hausdorff_noalloc(void* scene, const void* query_points_dev, size_t query_count,
                                                double* nearest_distance_dev, uint32_t* nearest_id_dev,
                                                RtdlB200Witness* witness_dev, void* stream, char* error_out,

@@ -105,6 +105,7 @@ struct Scene {
   uint32_t* perm = nullptr;
   double* pts64 = nullptr;
   float4* nodes = nullptr;
+  uint32_t* codes = nullptr;    // Morton codes of the sorted points (seed nearest searches)
   PointStats* stats = nullptr;  // device copy of the build statistics
   SceneView view() const {
     SceneView v;

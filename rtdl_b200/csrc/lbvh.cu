@@ -472,7 +472,7 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
     k_single_point<<<1, 1, 0, s>>>(sc->pts, sc->nodes);
     RTDL_LAUNCHED(1);
   }
-  dev_free(codes, s);
+  sc->codes = codes;  // kept: nearest searches seed from a window around the query's code
   return sc;
 }
 
@@ -483,6 +483,7 @@ void destroy_scene(Scene* sc) {
   dev_free(sc->perm, s);
   dev_free(sc->pts64, s);
   dev_free(sc->nodes, s);
+  dev_free(sc->codes, s);
   dev_free(sc->stats, s);
   if (sc->own_stream && s) {
     cudaStreamSynchronize(s);

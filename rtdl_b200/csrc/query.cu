@@ -192,6 +192,8 @@ struct Pass1Params {
   unsigned int* heavy_count;
   unsigned int* error;
   unsigned long long* stats;  // kStatCount counters, only with STATS
+  const uint32_t* qcodes;     // KNN: query Morton codes in processing order (seeds the list)
+  const uint32_t* scodes;     // KNN: the scene's sorted Morton codes
 };
 
 // Traversal counters gathered by the STATS instantiation (diagnostics).
@@ -240,6 +242,7 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
   float klast = INFINITY;
   uint32_t ilast = kNone;
   unsigned long long st_nodes = 0, st_points = 0, st_inserts = 0, st_shifts = 0, st_band = 0;
+  int win_lo = 0, win_hi = 0;  // seeded window (already in the list)
 
   auto insert = [&](float key, uint32_t idx) {
     int pos;
@@ -269,6 +272,7 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
   auto visit_leaf = [&](int first, int cnt) {
     if (STATS) st_points += cnt;
     for (int i = first; i < first + cnt; ++i) {
+      if (KNN && i >= win_lo && i < win_hi) continue;
       const float4 p = __ldg(&S.pts[i]);
       const float dx = p.x - c.qx, dy = p.y - c.qy, dz = p.z - c.qz;
       const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
@@ -305,6 +309,29 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
     return true;
   };
 
+  // KNN: seed the list with the scene points around the query's Morton code
+  // (a window in the sorted order), so the walk starts with a tight k-th
+  // bound; the walk skips the window's points.
+  if (KNN && S.n > 0 && P.scodes != nullptr) {
+    const uint32_t code = P.qcodes[t];
+    uint32_t lo = 0, hi = S.n;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(&P.scodes[mid]) < code) lo = mid + 1;
+      else hi = mid;
+    }
+    const int w = L < 8 ? 8 : L;
+    int a = (int)lo - w;
+    if (a < 0) a = 0;
+    int b = a + 2 * w;
+    if (b > (int)S.n) {
+      b = (int)S.n;
+      a = b - 2 * w < 0 ? 0 : b - 2 * w;
+    }
+    visit_leaf(a, b - a);
+    win_lo = a;
+    win_hi = b;
+  }
   // stackless depth-first walk over the pre-order records
   int cur = S.n > 0 ? 0 : kRopeEnd;
   while (cur != kRopeEnd) {
@@ -1271,6 +1298,7 @@ struct QueryPrep {
   float4* qpts = nullptr;
   DevBands* bands = nullptr;
   uint32_t* qorder = nullptr;
+  uint32_t* qcodes = nullptr;  // Morton codes in processing order (qcodes[t] belongs to qorder[t])
   uint32_t* oorder = nullptr;
 };
 
@@ -1285,18 +1313,19 @@ QueryPrep prepare_queries(Scene* sc, const void* queries_dev, uint32_t nq, bool 
   prep_points(queries_dev, nq, sc->dim, qp.qpts, qp.qst, s);
   k_bands<<<1, 32, 0, s>>>(sc->stats, qp.qst, radius, has_radius ? 1 : 0, qp.bands);
   RTDL_LAUNCHED(1);
-  uint32_t* qcodes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  morton_codes(qp.qpts, nq, sc->dim, sc->stats, qcodes, s);
+  qp.qcodes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  morton_codes(qp.qpts, nq, sc->dim, sc->stats, qp.qcodes, s);
   iota_u32(qp.qorder, nq, s);
-  radix_sort_pairs(qcodes, qp.qorder, nq, 0, sc->dim == 3 ? 30 : 32, nullptr, s);
+  radix_sort_pairs(qp.qcodes, qp.qorder, nq, 0, sc->dim == 3 ? 30 : 32, nullptr, s);
   if (want_output_order) {
     qp.oorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-    k_extract_ids<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, qcodes);
+    uint32_t* ids = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+    k_extract_ids<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, ids);
     RTDL_LAUNCHED(1);
     iota_u32(qp.oorder, nq, s);
-    radix_sort_pairs(qcodes, qp.oorder, nq, 0, 32, &qp.bands->ids_sorted, s);
+    radix_sort_pairs(ids, qp.oorder, nq, 0, 32, &qp.bands->ids_sorted, s);
+    dev_free(ids, s);
   }
-  dev_free(qcodes, s);
   return qp;
 }
 
@@ -1305,6 +1334,7 @@ void free_prep(QueryPrep& qp, cudaStream_t s) {
   dev_free(qp.qpts, s);
   dev_free(qp.bands, s);
   dev_free(qp.qorder, s);
+  dev_free(qp.qcodes, s);
   dev_free(qp.oorder, s);
 }
 
@@ -1638,6 +1668,8 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
       const unsigned int blocks = div_up(nq, threads);
       const bool stats = stats_enabled();
       P.stats = nullptr;
+      P.qcodes = qp.qcodes;
+      P.scodes = sc->codes;
       if (stats) {
         P.stats = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * kStatCount, s));
         RTDL_CUDA_CHECK(cudaMemsetAsync(P.stats, 0, sizeof(unsigned long long) * kStatCount, s));
@@ -1755,6 +1787,8 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   P.error = small + 1;
   const int threads = tuning().block_threads;
   P.stats = nullptr;
+  P.qcodes = qp.qcodes;
+  P.scodes = sc->codes;
   k_pass1<true, false><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
   RTDL_LAUNCHED(1);
   if (timer) timer->mark("traverse");
@@ -1820,10 +1854,11 @@ struct NoAllocLayout {  // byte offsets into the scratch array, 256-B aligned
   static constexpr size_t kTemp = align256(kOrder + (size_t)kNoAllocMaxQueries * sizeof(uint32_t));
   static constexpr size_t kCounts = align256(kTemp + (size_t)kNoAllocMaxQueries * sizeof(uint32_t));
   static constexpr size_t kFlags = align256(kCounts + (size_t)kNoAllocMaxQueries * sizeof(uint32_t));
-  static constexpr size_t kTotal = align256(kFlags + (size_t)kNoAllocMaxQueries);
+  static constexpr size_t kCodes = align256(kFlags + (size_t)kNoAllocMaxQueries);
+  static constexpr size_t kTotal = align256(kCodes + (size_t)kNoAllocMaxQueries * sizeof(uint32_t));
 };
 
-// 8.75 MiB: scratch for up to kNoAllocMaxQueries queries.
+// 9.75 MiB: scratch for up to kNoAllocMaxQueries queries.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::kTotal];
 
 // Converts the reduced witness into the public record and folds in the
@@ -1880,6 +1915,7 @@ void run_directed_hausdorff_noalloc(Scene* sc, const void* queries_dev, uint32_t
   uint32_t* temp = reinterpret_cast<uint32_t*>(base + NoAllocLayout::kTemp);
   uint32_t* counts = reinterpret_cast<uint32_t*>(base + NoAllocLayout::kCounts);
   uint8_t* flags = reinterpret_cast<uint8_t*>(base + NoAllocLayout::kFlags);
+  uint32_t* codes = reinterpret_cast<uint32_t*>(base + NoAllocLayout::kCodes);
   // The array keeps the previous call's contents: reset what must start at zero.
   reset_stats(qst, s);
   RTDL_CUDA_CHECK(cudaMemsetAsync(small, 0, 4 * sizeof(unsigned int), s));
@@ -1887,6 +1923,7 @@ void run_directed_hausdorff_noalloc(Scene* sc, const void* queries_dev, uint32_t
   k_bands<<<1, 32, 0, s>>>(sc->stats, qst, 0.0, 0, bands);
   RTDL_LAUNCHED(1);
   iota_u32(qorder, nq, s);  // input order: no sort, hence no sort scratch
+  morton_codes(qpts, nq, sc->dim, sc->stats, codes, s);  // seeds the nearest search (input order)
   Pass1Params P;
   P.S = sc->view();
   P.qpts = qpts;
@@ -1905,6 +1942,8 @@ void run_directed_hausdorff_noalloc(Scene* sc, const void* queries_dev, uint32_t
   P.heavy_count = small;
   P.error = small + 1;
   P.stats = nullptr;
+  P.qcodes = codes;
+  P.scodes = sc->codes;
   const int threads = tuning().block_threads;
   k_pass1<true, false><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
   RTDL_LAUNCHED(1);

@@ -468,6 +468,20 @@ class B200Scene:
         result = {"distance": dist.value, "source_id": int(src.value), "target_id": int(tgt.value), "row_count": n}
         return (result, nd, ni) if with_nearest else result
 
+    def directed_hausdorff_device(self, query_address: int, query_count: int, *, nearest_distance_address=None,
+                                  nearest_id_address=None, stream: int | None = None) -> dict:
+        """Device-resident directed Hausdorff; per-query outputs stay in device memory."""
+        dist = ctypes.c_double()
+        src = ctypes.c_uint32()
+        tgt = ctypes.c_uint32()
+        err = _native.error_buffer()
+        status = self._lib.rtdl_b200_scene_directed_hausdorff_device(
+            self._handle, query_address, int(query_count), nearest_distance_address, nearest_id_address,
+            ctypes.byref(dist), ctypes.byref(src), ctypes.byref(tgt), stream, err, len(err))
+        _native.check_status(status, err)
+        return {"distance": dist.value, "source_id": int(src.value), "target_id": int(tgt.value),
+                "row_count": int(query_count)}
+
     def close(self) -> None:
         if not getattr(self, "_closed", True):
             self._lib.rtdl_b200_scene_destroy(self._handle)

@@ -329,6 +329,7 @@ def run_secondary(args) -> int:
 # ---------------------------------------------------------------------------
 
 def main(argv=None) -> int:
+    global N_PROBE, N_BUILD
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -336,12 +337,15 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--probes", type=int, default=N_PROBE, help="probe points per GPU (profiling a smaller case)")
+    ap.add_argument("--build", type=int, default=N_BUILD, help="build points (profiling a smaller case)")
     ap.add_argument("--workload", choices=("frn", "knn", "hausdorff"), default="frn",
                     help="frn: the headline fixed-radius config; knn: k=16 on the same 3D sets; "
                          "hausdorff: 4,194,304 x 4,194,304 2D directed nearest-distance reduction")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    N_PROBE, N_BUILD = args.probes, args.build
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload != "frn":

@@ -58,6 +58,21 @@ def _env_int(name, default):
         return default
 
 
+def measured_traffic(kernel: str, workload: str, probes: int, build: int):
+    """DRAM bytes (read + write) of one launch of `kernel`, from the committed ncu capture of the same workload.
+
+    None when no capture of exactly this kernel and size is on record.
+    """
+    try:
+        table = json.loads((ROOT / "profiles" / "dram_traffic.json").read_text())
+    except (OSError, ValueError):
+        return None
+    for e in table.get("entries", []):
+        if (e.get("kernel"), e.get("workload"), e.get("probes"), e.get("build")) == (kernel, workload, probes, build):
+            return int(e["read_bytes"]) + int(e["write_bytes"])
+    return None
+
+
 # ---------------------------------------------------------------------------
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
@@ -454,14 +469,19 @@ def main(argv=None) -> int:
     except Exception:
         hbm_peak, peak_note = 6650.0, "fallback"
     R = rows_total
-    # algorithmic bytes (per launch) of the two query kernels
+    # algorithmic bytes (per launch) of the two query phases: the collect kernel reads every probe and build
+    # point once and keeps a 4-byte neighbour index per row plus a count and a flag per probe; the emit
+    # kernels read those indices back and write 16-byte rows plus per-probe offset/count/flags/point.
     traverse_bytes = N_PROBE * 16 + N_BUILD * 16 + R * 4 + N_PROBE * 5
     emit_bytes = R * 4 + R * 16 + N_PROBE * (4 + 1 + 1 + 8 + 32)
     if traverse_ms >= emit_ms:
-        dom, dom_ms, dom_bytes = "k_pass1 (LBVH traversal + FP64 band + per-query list)", traverse_ms, traverse_bytes
+        dom, dom_kernel, dom_ms, dom_bytes = ("k_collect_packet (packet LBVH walk, FP32 test + FP64 band)",
+                                              "k_collect_packet", traverse_ms, traverse_bytes)
     else:
-        dom, dom_ms, dom_bytes = "k_expand (exact FP64 row emission)", emit_ms, emit_bytes
+        dom, dom_kernel, dom_ms, dom_bytes = ("k_emit_lanes + k_emit_warp (exact FP64 sort and row emission)",
+                                              "k_emit_lanes", emit_ms, emit_bytes)
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = measured_traffic(dom_kernel, "clustered_3d_fixed_radius", N_PROBE, N_BUILD)
     phase_bytes = N_PROBE * 16 + N_BUILD * 16 + R * 16 + N_PROBE * 4 + N_PROBE // 8
     phase_achieved = phase_bytes / (query_ms / 1e3) / 1e9
 
@@ -524,8 +544,10 @@ def main(argv=None) -> int:
             "phases_ms": {"build": build_ms, "query_prep": prep_ms, "traverse": traverse_ms, "scan": scan_ms,
                           "emit": emit_ms, "query_total": query_ms},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_note,
-                         "algorithmic_bytes": dom_bytes},
+                         "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_note,
+                         "algorithmic_bytes": dom_bytes,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture of this "
+                                           "launch (profiles/dram_traffic.json)" if traffic else None},
             "phase_roofline": {"phase": "query+emit", "achieved": phase_achieved, "peak": hbm_peak, "unit": "GB/s",
                                "frac": phase_achieved / hbm_peak, "algorithmic_bytes": phase_bytes},
             "e2e": e2e,

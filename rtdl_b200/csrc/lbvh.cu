@@ -43,8 +43,19 @@ inline unsigned int grid_for(uint64_t n, int threads = kThreads) {
   return (unsigned int)(b < cap ? b : cap);
 }
 
+constexpr int kPrepThreads = 256;
+
+// k_prep's grid: enough blocks to fill the SMs a few times over, few enough
+// that the per-block atomics stay cheap.
+inline unsigned int prep_grid(uint64_t n) {
+  uint64_t b = (n + kPrepThreads - 1) / kPrepThreads;
+  if (b < 1) b = 1;
+  const uint64_t cap = (uint64_t)kSmCount * 4;
+  return (unsigned int)(b < cap ? b : cap);
+}
+
 template <int DIM>
-__global__ void k_prep(const double* __restrict__ raw, uint32_t n, float4* __restrict__ out,
+__global__ void __launch_bounds__(kPrepThreads) k_prep(const double* __restrict__ raw, uint32_t n, float4* __restrict__ out,
                        PointStats* __restrict__ st) {
   constexpr int kStride = DIM == 3 ? 4 : 3;  // record size in doubles (id occupies the first slot)
   float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -72,7 +83,9 @@ __global__ void k_prep(const double* __restrict__ raw, uint32_t n, float4* __res
     }
     out[i] = make_float4(f[0], f[1], f[2], __uint_as_float(id));
   }
-  // warp reduction, then one set of atomics per warp
+  // warp reduction, then a block reduction through shared memory, then one set
+  // of atomics per block (same-address atomics from every warp would
+  // serialise in L2)
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -85,7 +98,31 @@ __global__ void k_prep(const double* __restrict__ raw, uint32_t n, float4* __res
     bad |= __shfl_xor_sync(0xffffffffu, bad, o);
     unsorted |= __shfl_xor_sync(0xffffffffu, unsorted, o);
   }
+  __shared__ float s_lo[3][kPrepThreads / 32], s_hi[3][kPrepThreads / 32];
+  __shared__ double s_abs[kPrepThreads / 32];
+  __shared__ unsigned int s_flags[kPrepThreads / 32];
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      s_lo[a][warp] = lo[a];
+      s_hi[a][warp] = hi[a];
+    }
+    s_abs[warp] = max_abs;
+    s_flags[warp] = inexact | (bad << 1) | (unsorted << 2);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int fl = 0;
+    for (int w = 0; w < nwarps; ++w) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = fminf(lo[a], s_lo[a][w]);
+        hi[a] = fmaxf(hi[a], s_hi[a][w]);
+      }
+      max_abs = fmax(max_abs, s_abs[w]);
+      fl |= s_flags[w];
+    }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       if (lo[a] <= hi[a]) {
@@ -94,9 +131,9 @@ __global__ void k_prep(const double* __restrict__ raw, uint32_t n, float4* __res
       }
     }
     atomicMax(&st->max_abs_bits, (unsigned long long)__double_as_longlong(max_abs));
-    if (inexact) atomicOr(&st->inexact, 1u);
-    if (bad) atomicOr(&st->bad, 1u);
-    if (unsorted) atomicOr(&st->ids_unsorted, 1u);
+    if (fl & 1u) atomicOr(&st->inexact, 1u);
+    if (fl & 2u) atomicOr(&st->bad, 1u);
+    if (fl & 4u) atomicOr(&st->ids_unsorted, 1u);
   }
 }
 
@@ -375,9 +412,9 @@ void prep_points(const void* points_dev, uint32_t n, int dim, float4* out, Point
   if (n == 0) return;
   const double* raw = static_cast<const double*>(points_dev);
   if (dim == 3)
-    k_prep<3><<<grid_for(n), kThreads, 0, s>>>(raw, n, out, stats);
+    k_prep<3><<<prep_grid(n), kPrepThreads, 0, s>>>(raw, n, out, stats);
   else
-    k_prep<2><<<grid_for(n), kThreads, 0, s>>>(raw, n, out, stats);
+    k_prep<2><<<prep_grid(n), kPrepThreads, 0, s>>>(raw, n, out, stats);
   RTDL_LAUNCHED(1);
 }
 

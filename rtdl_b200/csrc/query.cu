@@ -378,22 +378,34 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
 }
 
 // ---- fixed-radius collect pass ----------------------------------------------
-// One thread per query in Morton order.  The traversal is a while-while loop:
-// a lane walks internal nodes until it holds a leaf bucket, then all lanes
-// test their buckets together.  In-radius candidates are appended unsorted to
-// the query's slab (capacity C); the exact in-radius count is kept, so the
-// overflow flag and the row offsets are exact without any per-query list.
-constexpr int kSlab = 256;      // candidates kept per query
-constexpr int kSlabHead = 64;   // slots kept slot-major (read by the lane-per-query emit)
+// One thread per query in Morton order.  In-radius candidates are appended
+// unsorted to the query's slab (capacity kSlab) as one 8-byte entry each; the
+// exact in-radius count is kept, so the overflow flag and the row offsets are
+// exact without any per-query list.
+constexpr int kSlab = 256;  // candidates kept per query
 
-// Slab layout: slots below kSlabHead are slot-major (slot s of the query at
-// processing rank t at s * nq + t, so a warp of consecutive queries reads one
-// slot with one coalesced request); the remaining slots are query-major after
-// them (read by the warp-per-query emit, one query at a time).
-__host__ __device__ __forceinline__ size_t slab_at(uint32_t c, uint32_t t, uint32_t nq) {
-  return c < (uint32_t)kSlabHead ? (size_t)c * nq + t
-                                 : (size_t)kSlabHead * nq + (size_t)t * (kSlab - kSlabHead) + (c - kSlabHead);
+// Candidate slab: query-major, kSlab entries for the query at processing rank
+// t starting at t * kSlab.  An entry is (FP32 sort key bits << 32) | sorted
+// point index, so a lane appends one candidate with one 8-byte store and a
+// warp reads a query's candidates with contiguous loads.
+__host__ __device__ __forceinline__ size_t slab_base(uint32_t t) { return (size_t)t * kSlab; }
+
+__device__ __forceinline__ unsigned long long slab_entry(float key, uint32_t i) {
+  return ((unsigned long long)__float_as_uint(key) << 32) | i;
 }
+
+// Per-query record written by the collect pass at the query's processing rank
+// and read by the emit kernels, so they find the query's exact coordinates,
+// id and candidate count with one load.
+struct QueryInfo {
+  double ex, ey, ez;  // exact query coordinates (z = 0 in 2D)
+  uint32_t qid;
+  uint32_t meta;      // candidate count (<= kSlab) and the kQuery* bits
+};
+constexpr uint32_t kQueryCountMask = 0xFFFFu;
+constexpr uint32_t kQueryGeneric = 1u << 16;   // more than kSlab candidates: generic path
+constexpr uint32_t kQueryBig = 1u << 17;       // 65..kSlab candidates: k_emit_big
+constexpr uint32_t kQueryOverflow = 1u << 18;  // more in-radius points than kmax
 
 struct CollectParams {
   SceneView S;
@@ -404,15 +416,15 @@ struct CollectParams {
   uint32_t nq;
   uint32_t kmax;
   const DevBands* bands;
-  uint32_t* slab;        // kSlab * nq candidate indices, laid out by slab_at()
-  uint32_t* keys;        // same layout: the candidate's FP32 sort key (bits)
-  uint32_t* counts;      // min(count, kmax), query input order
-  uint16_t* ncand;       // min(count, kSlab), by processing rank
-  uint8_t* flags;        // bit0: count > kmax, bit1: count > kSlab (generic path), bit2: count > 64
+  unsigned long long* slab;  // kSlab entries per query, see slab_base()
+  uint32_t* counts;          // min(count, kmax), query input order
+  QueryInfo* qinfo;          // by processing rank
+  uint8_t* flags;            // bit0: count > kmax, bit1: count > kSlab (generic path), bit2: count > 64
   uint32_t* heavy_list;
   uint32_t* heavy_m;
-  uint32_t* big_list;
-  unsigned int* small;   // [0] heavy count, [1] error bits, [2] big count
+  uint32_t* big_list;        // processing ranks of the queries with 65..kSlab candidates
+  unsigned int* small;       // [0] generic-path query count, [1] error bits, [2] big_list length
+  uint8_t* overflow_out;     // optional: 1 per query (input order) when count > kmax
   unsigned long long* stats;
 };
 
@@ -423,6 +435,7 @@ struct CollectLane {
   float4 q;
   double ex, ey, ez;
   uint32_t count;
+  unsigned long long* out;  // this query's slab entries
   unsigned long long st_nodes, st_points, st_band;
 };
 
@@ -441,11 +454,7 @@ __device__ __forceinline__ void collect_point(const CollectParams& P, const DevB
     if (d2 >= B.lo2 && e2 > B.r2) return;
     if (B.any_inexact) d2 = __double2float_rn(e2);
   }
-  if (L.count < (uint32_t)kSlab) {
-    const size_t at = slab_at(L.count, L.t, P.nq);
-    P.slab[at] = i;
-    P.keys[at] = __float_as_uint(d2);
-  }
+  if (L.count < (uint32_t)kSlab) L.out[L.count] = slab_entry(d2, i);
   ++L.count;
 }
 
@@ -466,15 +475,23 @@ __device__ __forceinline__ void collect_finish(const CollectParams& P, const Col
     const unsigned int h = atomicAdd(&P.small[0], 1u);
     P.heavy_list[h] = L.qin;
     P.heavy_m[h] = count;
-  } else if (count > 64) {
+  } else if (count > 64u) {
     fl |= 4;
-    P.big_list[atomicAdd(&P.small[2], 1u)] = L.t;  // processing rank: the slab column of the query
+    P.big_list[atomicAdd(&P.small[2], 1u)] = L.t;
   }
-  P.ncand[L.t] = (uint16_t)(count < (uint32_t)kSlab ? count : (uint32_t)kSlab);
+  QueryInfo qi;
+  qi.ex = L.ex;
+  qi.ey = L.ey;
+  qi.ez = L.ez;
+  qi.qid = __float_as_uint(L.q.w);
+  qi.meta = (count < (uint32_t)kSlab ? count : (uint32_t)kSlab) | ((fl & 1) ? kQueryOverflow : 0u) |
+            ((fl & 2) ? kQueryGeneric : 0u) | ((fl & 4) ? kQueryBig : 0u);
+  P.qinfo[L.t] = qi;
   P.flags[L.qin] = fl;
+  if (P.overflow_out) P.overflow_out[L.qin] = fl & 1;
 }
 
-__device__ __forceinline__ void collect_init(const CollectParams& P, const DevBands& B, uint32_t t, CollectLane& L) {
+__device__ __forceinline__ void collect_init(const CollectParams& P, uint32_t t, CollectLane& L) {
   L.t = t;
   L.qin = P.qorder[t];
   L.q = P.qpts[L.qin];
@@ -483,7 +500,26 @@ __device__ __forceinline__ void collect_init(const CollectParams& P, const DevBa
   L.ey = r[2];
   L.ez = P.qstride == 4 ? r[3] : 0.0;
   L.count = 0;
+  L.out = P.slab + slab_base(t);
   L.st_nodes = L.st_points = L.st_band = 0;
+}
+
+// Tests the points of leaf bucket [first, first + cnt) against the lane's
+// query, loading them BATCH at a time so the loads of a batch are in flight
+// together (more registers for more loads in flight).  `test` false: the lane
+// only takes part in the loads.
+template <bool STATS, int BATCH>
+__device__ __forceinline__ void collect_leaf(const CollectParams& P, const DevBands& B, int scene_inexact,
+                                             CollectLane& L, int first, int cnt, bool test) {
+  for (int j0 = 0; j0 < cnt; j0 += BATCH) {
+    float4 p[BATCH];
+#pragma unroll
+    for (int j = 0; j < BATCH; ++j)
+      if (j0 + j < cnt) p[j] = __ldg(&P.S.pts[first + j0 + j]);
+#pragma unroll
+    for (int j = 0; j < BATCH; ++j)
+      if (test && j0 + j < cnt) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)(first + j0 + j), p[j]);
+  }
 }
 
 // One thread per query, queries in Morton order.  Stackless walk over the
@@ -498,7 +534,7 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
   const SceneView& S = P.S;
   const int scene_inexact = *S.inexact;
   CollectLane L;
-  collect_init(P, B, t, L);
+  collect_init(P, t, L);
   int cur = S.n > 0 ? 0 : kRopeEnd;
   while (cur != kRopeEnd) {
     int first = 0, cnt = 0;
@@ -519,7 +555,7 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
       }
     }
     if (STATS) L.st_points += cnt;
-    for (int i = first; i < first + cnt; ++i) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)i, __ldg(&S.pts[i]));
+    collect_leaf<STATS, 1>(P, B, scene_inexact, L, first, cnt, true);
   }
   collect_finish<STATS>(P, L);
 }
@@ -529,7 +565,7 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
 // sphere overlaps it.  Node and point loads are warp-uniform (one request
 // each) and the control flow never diverges; each lane tests leaf points
 // against its own query.
-template <bool STATS>
+template <bool STATS, int BATCH>
 __global__ void __launch_bounds__(256) k_collect_packet(CollectParams P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = t < P.nq;
@@ -539,10 +575,11 @@ __global__ void __launch_bounds__(256) k_collect_packet(CollectParams P) {
   const int scene_inexact = *S.inexact;
   CollectLane L;
   if (valid) {
-    collect_init(P, B, t, L);
+    collect_init(P, t, L);
   } else {
     L.q = make_float4(INFINITY, INFINITY, INFINITY, 0.f);  // never overlaps
     L.count = 0;
+    L.out = nullptr;
     L.st_nodes = L.st_points = L.st_band = 0;
   }
   int cur = S.n > 0 ? 0 : kRopeEnd;
@@ -558,64 +595,15 @@ __global__ void __launch_bounds__(256) k_collect_packet(CollectParams P) {
       }
       const int first = leaf_first(hit), cnt = leaf_count(hit);
       if (STATS) L.st_points += cnt;
-      for (int i = first; i < first + cnt; ++i) {
-        const float4 p = __ldg(&S.pts[i]);
-        if (over) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)i, p);
-      }
+      collect_leaf<STATS, BATCH>(P, B, scene_inexact, L, first, cnt, over);
     }
     cur = __float_as_int(b.w);
   }
   if (valid) collect_finish<STATS>(P, L);
 }
 
-// ---- register sorting network --------------------------------------------
-// Batcher's odd-even merge sort, fully unrolled: every index is a compile-time
-// constant, so the array lives in registers and each compare-exchange is one
-// min and one max.
-__device__ __forceinline__ void cmpswap(uint32_t& a, uint32_t& b) {
-  const uint32_t lo = min(a, b), hi = max(a, b);
-  a = lo;
-  b = hi;
-}
-
-// Batcher's odd-even merge sort network as a compile-time table of
-// compare-exchange pairs (for N = 32: 191 pairs, N = 64: 543).
-template <int N>
-struct OddEvenMergeNet {
-  static constexpr int count() {
-    int c = 0;
-    for (int p = 1; p < N; p <<= 1)
-      for (int k = p; k >= 1; k >>= 1)
-        for (int j = k % p; j + k < N; j += 2 * k)
-          for (int i = 0; i < k; ++i)
-            if (i + j + k < N && (i + j) / (2 * p) == (i + j + k) / (2 * p)) ++c;
-    return c;
-  }
-  static constexpr int kSize = count();
-  unsigned char a[kSize];
-  unsigned char b[kSize];
-  constexpr OddEvenMergeNet() : a(), b() {
-    int c = 0;
-    for (int p = 1; p < N; p <<= 1)
-      for (int k = p; k >= 1; k >>= 1)
-        for (int j = k % p; j + k < N; j += 2 * k)
-          for (int i = 0; i < k; ++i)
-            if (i + j + k < N && (i + j) / (2 * p) == (i + j + k) / (2 * p)) {
-              a[c] = (unsigned char)(i + j);
-              b[c] = (unsigned char)(i + j + k);
-              ++c;
-            }
-  }
-};
-
-template <int N>
-__device__ __forceinline__ void sort_network(uint32_t (&e)[N]) {
-  constexpr OddEvenMergeNet<N> net{};
-#pragma unroll
-  for (int t = 0; t < OddEvenMergeNet<N>::kSize; ++t) cmpswap(e[net.a[t]], e[net.b[t]]);
-}
-
-// Emitted row writer shared by the emit kernels.
+// ---- emit: warp per query -----------------------------------------------------
+// Emitted row writer.
 struct RowSink {
   void* rows;
   unsigned long long capacity;
@@ -637,186 +625,81 @@ struct RowSink {
 
 struct EmitParams {
   SceneView S;
-  const float4* qpts;
-  const double* qraw;
-  int qstride;
-  const uint32_t* qorder;     // processing rank -> query input index (Morton order)
-  const uint32_t* work;       // optional: processing ranks to handle (large queries)
-  uint32_t nwork;
-  uint32_t nq;                // slab stride
-  const uint32_t* qrank;      // query input index -> output rank (identity when ids are sorted)
-  const DevBands* bands;
-  const uint32_t* slab;       // slot-major: slab[s * nq + t]
-  const uint32_t* keys;       // same layout: FP32 sort keys
-  const uint16_t* ncand;      // by processing rank
-  const uint8_t* flags;       // by query input index
-  const unsigned long long* offsets;
+  uint32_t nq;
+  unsigned long long* slab;
+  const QueryInfo* qinfo;     // by processing rank
+  const unsigned long long* poff;  // first row of each query, by processing rank
   uint32_t kmax;
   RowSink sink;
-  uint8_t* overflow_out;
+  uint32_t* fix_list;         // processing ranks queued for k_emit_fixup
+  unsigned int* fix_count;
 };
 
-// Packed element: FP32 d2 key with its low SHIFT mantissa bits replaced by the
-// slab slot.  Keys closer than two truncated units are re-decided exactly.
+// A deferred query's sorted packed keys (at most 64) live in its slab entries
+// 64..95, unused by a query with at most 64 candidates.
+__device__ __forceinline__ uint32_t* deferred_keys(unsigned long long* slab, uint32_t t) {
+  return reinterpret_cast<uint32_t*>(slab + slab_base(t) + 64);
+}
+
+// Packed sort element: the FP32 d2 key with its low SHIFT mantissa bits
+// replaced by the slab slot.  Valid keys are below 0x80000000, so the padding
+// value 0xFFFFFFFF sorts last.  Two elements whose truncated keys differ by two
+// units or more are in exact order (the FP32 keys are within a few ulps of
+// the exact FP64 d2, far less than 2^SHIFT ulps); closer pairs are re-decided
+// exactly.
 template <int SHIFT>
-__device__ __forceinline__ uint32_t pack_key(float d2, uint32_t slot) {
-  return (__float_as_uint(d2) & ~((1u << SHIFT) - 1u)) | slot;
+__device__ __forceinline__ uint32_t pack_key(uint32_t key_bits, uint32_t slot) {
+  return (key_bits & ~((1u << SHIFT) - 1u)) | slot;
 }
 
-// After the network the sorted packed keys go to a per-thread column of
-// shared memory ([slot][thread], conflict free), so the register array is
-// dead before any call; neighbours whose truncated keys differ by at most one
-// unit are then re-decided exactly and the rows written.
-template <int N, int SHIFT>
-__device__ __forceinline__ bool store_sorted(const uint32_t (&e)[N], int n, uint32_t* col, int stride) {
-  bool amb = false;
-#pragma unroll
-  for (int i = 0; i + 1 < N; ++i)
-    if (i + 1 < n) amb |= (e[i + 1] >> SHIFT) - (e[i] >> SHIFT) <= 1u;
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-    if (i < n) col[i * stride] = e[i];
-  return amb;
-}
-
-// Odd-even transposition passes restricted to ambiguous neighbours, until no
-// swap happens (bounded by n passes).  Pairs whose truncated keys differ by two
-// units or more are in exact order already.
-template <int SHIFT>
-__device__ __noinline__ void exact_fixup(uint32_t* col, int stride, int n, const uint32_t* slab, size_t ss,
-                                         SceneView S, int inexact, double ex, double ey, double ez) {
-  constexpr uint32_t kMask = (1u << SHIFT) - 1u;
-  for (int pass = 0; pass < n; ++pass) {
-    bool changed = false;
-    for (int parity = 0; parity < 2; ++parity) {
-      for (int i = parity; i + 1 < n; i += 2) {
-        const uint32_t a = col[i * stride], b = col[(i + 1) * stride];
-        if ((b >> SHIFT) - (a >> SHIFT) > 1u) continue;
-        if (exact_before(ex, ey, ez, S.pts, S.pts64, S.perm, inexact, slab[(b & kMask) * ss],
-                         slab[(a & kMask) * ss])) {
-          col[i * stride] = b;
-          col[(i + 1) * stride] = a;
-          changed = true;
-        }
-      }
-    }
-    if (!changed) break;
-  }
-}
-
-template <int SHIFT>
-__device__ __forceinline__ void emit_rows(const uint32_t* col, int stride, int kk, const uint32_t* slab, size_t ss,
-                                          const SceneView& S, int inexact, double ex, double ey, double ez,
-                                          uint32_t qid, unsigned long long base, const RowSink& sink) {
-  constexpr uint32_t kMask = (1u << SHIFT) - 1u;
-  for (int s = 0; s < kk; ++s) {
-    const uint32_t i = slab[(col[s * stride] & kMask) * ss];
-    const float4 p = __ldg(&S.pts[i]);
-    const double dist = __dsqrt_rn(exact_d2_at(ex, ey, ez, S.pts, S.pts64, inexact, i));
-    sink.put(base + s, qid, __float_as_uint(p.w), dist, (uint32_t)s + 1);
-  }
-}
-
-template <int N>
-__device__ __forceinline__ void emit_one_query(const EmitParams& P, uint32_t t, uint32_t qin, int n, int inexact,
-                                               int any_inexact, uint32_t* col, int stride) {
-  constexpr int SHIFT = 6;
-  const float4 q = P.qpts[qin];
-  const double* r = P.qraw + (size_t)qin * P.qstride;
-  const double ex = r[1], ey = r[2], ez = P.qstride == 4 ? r[3] : 0.0;
-  const uint32_t* slab = P.slab + t;
-  const uint32_t* keys = P.keys + t;
-  const size_t ss = P.nq;
-  bool amb;
-  {
-    uint32_t e[N];
-#pragma unroll
-    for (int s = 0; s < N; ++s)
-      e[s] = s < n ? pack_key<SHIFT>(__uint_as_float(keys[s * ss]), (uint32_t)s) : 0xFFFFFFFFu;
-    sort_network<N>(e);
-    amb = store_sorted<N, SHIFT>(e, n, col, stride);
-  }
-  if (amb) exact_fixup<SHIFT>(col, stride, n, slab, ss, P.S, inexact, ex, ey, ez);
-  const int kk = n < (int)P.kmax ? n : (int)P.kmax;
-  emit_rows<SHIFT>(col, stride, kk, slab, ss, P.S, inexact, ex, ey, ez, __float_as_uint(q.w),
-                   P.offsets[P.qrank[qin]], P.sink);
-}
-
-// Lane-per-query emit for queries with at most 64 candidates, in Morton order
-// so a warp's 32 queries are alike; warps whose queries all have <= 32
-// candidates use the 32-wide network.  Dynamic shared memory: 64 words per
-// thread.
-__global__ void __launch_bounds__(128) k_emit_lanes(EmitParams P) {
-  extern __shared__ uint32_t emit_smem[];
-  uint32_t* col = emit_smem + threadIdx.x;
-  const int stride = blockDim.x;
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = t < P.nwork;
-  const uint32_t qin = valid ? P.qorder[t] : 0u;
-  const uint8_t fl = valid ? P.flags[qin] : 0;
-  if (valid && P.overflow_out) P.overflow_out[qin] = fl & 1;
-  const bool mine = valid && (fl & 6) == 0;
-  const int n = mine ? (int)P.ncand[t] : 0;
-  const int inexact = *P.S.inexact;
-  const int any_inexact = P.bands->any_inexact;
-  const unsigned int active = __ballot_sync(0xffffffffu, mine && n > 0);
-  if (!(mine && n > 0)) return;
-  if (__all_sync(active, n <= 32))
-    emit_one_query<32>(P, t, qin, n, inexact, any_inexact, col, stride);
-  else
-    emit_one_query<64>(P, t, qin, n, inexact, any_inexact, col, stride);
-}
-
-// ---- warp-per-query emit for 65..256 candidates -----------------------------
-// Bitonic sort across the warp: E packed keys per lane in a blocked layout
-// (element i = lane * E + r), exchanges within a lane in registers and across
-// lanes with one shuffle per element.
+// Bitonic sort across the warp of 32 * E packed elements in a striped layout
+// (element i = r * 32 + lane): exchanges at distance >= 32 stay in a lane's
+// registers, shorter ones take one shuffle per register.  Ascending.
 template <int E>
-__device__ __forceinline__ void warp_bitonic(uint32_t (&v)[E], int lane) {
+__device__ __forceinline__ void warp_bitonic_striped(uint32_t (&v)[E], int lane) {
 #pragma unroll
   for (int k = 2; k <= 32 * E; k <<= 1) {
 #pragma unroll
     for (int j = k >> 1; j > 0; j >>= 1) {
-      if (j >= E) {
-        const int lj = j / E;
-        const bool lower = (lane & lj) == 0;
+      if (j >= 32) {
+        const int rj = j >> 5;
 #pragma unroll
         for (int r = 0; r < E; ++r) {
-          const bool up = ((lane * E + r) & k) == 0;
-          const uint32_t other = __shfl_xor_sync(0xffffffffu, v[r], lj);
-          v[r] = (lower == up) ? min(v[r], other) : max(v[r], other);
-        }
-      } else {
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-          const int pr = r ^ j;
+          const int pr = r ^ rj;
           if (pr > r) {
-            const bool up = ((lane * E + r) & k) == 0;
+            const bool up = (((r << 5) | lane) & k) == 0;
             const uint32_t a = v[r], b = v[pr];
             v[r] = up ? min(a, b) : max(a, b);
             v[pr] = up ? max(a, b) : min(a, b);
           }
         }
+      } else {
+        const bool lower = (lane & j) == 0;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          const bool up = (((r << 5) | lane) & k) == 0;
+          const uint32_t other = __shfl_xor_sync(0xffffffffu, v[r], j);
+          v[r] = (lower == up) ? min(v[r], other) : max(v[r], other);
+        }
       }
     }
   }
 }
 
-// Single-thread exact fixup over a warp's sorted buffer (same rule as
-// exact_fixup, with slab_at addressing); only when a neighbour pair is
-// ambiguous.
-__device__ __noinline__ void exact_fixup_linear(uint32_t* buf, int n, const uint32_t* slab, uint32_t t, uint32_t nq,
+// Odd-even transposition over a warp's sorted buffer, one thread, restricted
+// to neighbours whose truncated keys differ by at most one unit, until no swap
+// happens (bounded by n passes).  Runs only when such a pair exists.
+__device__ __noinline__ void exact_fixup_sorted(uint32_t* buf, int n, int shift, const unsigned long long* ent,
                                                 SceneView S, int inexact, double ex, double ey, double ez) {
-  constexpr int SHIFT = 8;
-  constexpr uint32_t kMask = (1u << SHIFT) - 1u;
+  const uint32_t mask = (1u << shift) - 1u;
   for (int pass = 0; pass < n; ++pass) {
     bool changed = false;
     for (int parity = 0; parity < 2; ++parity) {
       for (int i = parity; i + 1 < n; i += 2) {
         const uint32_t a = buf[i], b = buf[i + 1];
-        if ((b >> SHIFT) - (a >> SHIFT) > 1u) continue;
-        if (exact_before(ex, ey, ez, S.pts, S.pts64, S.perm, inexact, slab[slab_at(b & kMask, t, nq)],
-                         slab[slab_at(a & kMask, t, nq)])) {
+        if ((b >> shift) - (a >> shift) > 1u) continue;
+        if (exact_before(ex, ey, ez, S.pts, S.pts64, S.perm, inexact, (uint32_t)ent[b & mask],
+                         (uint32_t)ent[a & mask])) {
           buf[i] = b;
           buf[i + 1] = a;
           changed = true;
@@ -827,65 +710,182 @@ __device__ __noinline__ void exact_fixup_linear(uint32_t* buf, int n, const uint
   }
 }
 
-template <int E>
-__device__ __forceinline__ void emit_warp_query(const EmitParams& P, uint32_t t, int lane, uint32_t* wbuf) {
-  constexpr int SHIFT = 8;  // 256 slots
+// What a warp needs of one query before it sorts: three independent loads
+// (the query's record, its first row and slab entry `lane`), so a query costs
+// one memory round trip before the sort and one (the point gather) after it.
+struct EmitQuery {
+  QueryInfo qi;
+  unsigned long long base;  // first row of the query
+  unsigned long long e0;    // slab entry `lane` (read before the count is known; unused beyond it)
+};
+
+__device__ __forceinline__ void emit_load(const EmitParams& P, uint32_t t, int lane, EmitQuery& q) {
+  q.qi = P.qinfo[t];
+  q.base = P.poff[t];
+  q.e0 = P.slab[slab_base(t) + lane];  // inside the query's kSlab entries whatever its count
+}
+
+// Sorts the query's n <= 32 * E candidates by the reference's key and writes
+// its first min(n, kmax) rows; lane l writes rows l, l + 32, ... so each store
+// instruction covers 32 consecutive rows.  When two neighbours need the exact
+// comparison, DEFER == false re-decides them here through `wbuf` (shared
+// memory); DEFER == true leaves the sorted list in the query's spare slab
+// entries and queues the query for k_emit_fixup, which keeps this kernel free
+// of the exact comparison's call (and of the registers that call needs).
+template <int E, bool DEFER>
+__device__ __forceinline__ void emit_query(const EmitParams& P, uint32_t t, const EmitQuery& q, int n, int lane,
+                                           uint32_t* wbuf) {
+  constexpr int SHIFT = E == 1 ? 5 : E == 2 ? 6 : E == 4 ? 7 : 8;
   constexpr uint32_t kMask = (1u << SHIFT) - 1u;
-  const uint32_t qin = P.qorder[t];
-  const int n = (int)P.ncand[t];
-  const uint32_t nq = P.nq;
-  const int inexact = *P.S.inexact;
-  uint32_t v[E];
+  const unsigned long long* ent = P.slab + slab_base(t);
+  uint32_t v[E], ids[E];
 #pragma unroll
   for (int r = 0; r < E; ++r) {
-    const int sl = lane * E + r;
-    v[r] = sl < n ? pack_key<SHIFT>(__uint_as_float(P.keys[slab_at(sl, t, nq)]), (uint32_t)sl) : 0xFFFFFFFFu;
+    const int s = (r << 5) | lane;
+    if (s < n) {
+      const unsigned long long e = r == 0 ? q.e0 : ent[s];
+      v[r] = pack_key<SHIFT>((uint32_t)(e >> 32), (uint32_t)s);
+      ids[r] = (uint32_t)e;
+    } else {
+      v[r] = 0xFFFFFFFFu;
+      ids[r] = 0u;
+    }
   }
-  warp_bitonic<E>(v, lane);
+  warp_bitonic_striped<E>(v, lane);
+  // ambiguous neighbours: element i and i + 1 within one truncated unit
   bool amb = false;
 #pragma unroll
-  for (int r = 0; r + 1 < E; ++r)
-    amb |= v[r + 1] != 0xFFFFFFFFu && (v[r + 1] >> SHIFT) - (v[r] >> SHIFT) <= 1u;
-  const uint32_t next = __shfl_down_sync(0xffffffffu, v[0], 1);
-  if (lane < 31) amb |= next != 0xFFFFFFFFu && (next >> SHIFT) - (v[E - 1] >> SHIFT) <= 1u;
-  const double* rq = P.qraw + (size_t)qin * P.qstride;
-  const double ex = rq[1], ey = rq[2], ez = P.qstride == 4 ? rq[3] : 0.0;
+  for (int r = 0; r < E; ++r) {
+    uint32_t nx = __shfl_down_sync(0xffffffffu, v[r], 1);
+    const uint32_t wrap = __shfl_sync(0xffffffffu, v[r + 1 < E ? r + 1 : r], 0);
+    if (lane == 31) nx = r + 1 < E ? wrap : 0xFFFFFFFFu;
+    amb |= nx != 0xFFFFFFFFu && (nx >> SHIFT) - (v[r] >> SHIFT) <= 1u;
+  }
+  const double ex = q.qi.ex, ey = q.qi.ey, ez = q.qi.ez;
+  const int inexact = *P.S.inexact;
   if (__any_sync(0xffffffffu, amb)) {
+    if (DEFER) {
+      uint32_t* spare = deferred_keys(P.slab, t);
 #pragma unroll
-    for (int r = 0; r < E; ++r) wbuf[lane * E + r] = v[r];
+      for (int r = 0; r < E; ++r) spare[(r << 5) | lane] = v[r];
+      if (lane == 0) P.fix_list[atomicAdd(P.fix_count, 1u)] = t;
+      return;
+    }
+#pragma unroll
+    for (int r = 0; r < E; ++r) wbuf[(r << 5) | lane] = v[r];
     __syncwarp();
-    if (lane == 0) exact_fixup_linear(wbuf, n, P.slab, t, nq, P.S, inexact, ex, ey, ez);
+    if (lane == 0) exact_fixup_sorted(wbuf, n, SHIFT, ent, P.S, inexact, ex, ey, ez);
     __syncwarp();
 #pragma unroll
-    for (int r = 0; r < E; ++r) v[r] = wbuf[lane * E + r];
+    for (int r = 0; r < E; ++r) v[r] = wbuf[(r << 5) | lane];
     __syncwarp();
   }
   const int kk = n < (int)P.kmax ? n : (int)P.kmax;
-  const uint32_t qid = __float_as_uint(P.qpts[qin].w);
-  const unsigned long long base = P.offsets[P.qrank[qin]];
 #pragma unroll
   for (int r = 0; r < E; ++r) {
-    const int i = lane * E + r;
+    const int i = (r << 5) | lane;
+    const uint32_t slot = v[r] & kMask;
+    uint32_t idx;
+    if (E <= 2) {  // the entry of slot s sits in lane s % 32, register s / 32
+      idx = __shfl_sync(0xffffffffu, ids[0], slot & 31);
+      if (E == 2) {
+        const uint32_t hi = __shfl_sync(0xffffffffu, ids[E - 1], slot & 31);
+        if (slot >= 32) idx = hi;
+      }
+    } else {
+      idx = i < kk ? (uint32_t)ent[slot] : 0u;
+    }
     if (i < kk) {
-      const uint32_t idx = P.slab[slab_at(v[r] & kMask, t, nq)];
       const float4 p = __ldg(&P.S.pts[idx]);
-      const double dist = __dsqrt_rn(exact_d2_at(ex, ey, ez, P.S.pts, P.S.pts64, inexact, idx));
-      P.sink.put(base + i, qid, __float_as_uint(p.w), dist, (uint32_t)i + 1);
+      double sx, sy, sz;
+      if (inexact) {
+        const double* pp = P.S.pts64 + 3ull * idx;
+        sx = pp[0];
+        sy = pp[1];
+        sz = pp[2];
+      } else {
+        sx = p.x;
+        sy = p.y;
+        sz = p.z;
+      }
+      const double dx = __dsub_rn(sx, ex), dy = __dsub_rn(sy, ey), dz = __dsub_rn(sz, ez);
+      const double dist = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+      P.sink.put(q.base + i, q.qi.qid, __float_as_uint(p.w), dist, (uint32_t)i + 1);
     }
   }
 }
 
-// One warp per query with 65..256 candidates (processing ranks in P.work).
-__global__ void __launch_bounds__(128) k_emit_warp(EmitParams P) {
-  __shared__ uint32_t wbuf[4][kSlab];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (j >= P.nwork) return;  // whole warp
-  const uint32_t t = P.work[j];
-  if (P.ncand[t] <= 128)
-    emit_warp_query<4>(P, t, lane, wbuf[wib]);
+// Warp per query in processing (Morton) order for the queries with at most
+// 64 candidates; queries with 65..kSlab candidates are k_emit_big's, those on
+// the generic path get their rows from k_expand.
+constexpr int kEmitThreads = 256;
+
+__global__ void __launch_bounds__(kEmitThreads) k_emit(EmitParams P) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t t64 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (t64 >= P.nq) return;  // whole warp
+  const uint32_t t = (uint32_t)t64;
+  EmitQuery q;
+  emit_load(P, t, lane, q);
+  const uint32_t meta = q.qi.meta;
+  const int n = (int)(meta & kQueryCountMask);
+  if ((meta & (kQueryGeneric | kQueryBig)) || n == 0) return;
+  if (n <= 32)
+    emit_query<1, true>(P, t, q, n, lane, nullptr);
   else
-    emit_warp_query<8>(P, t, lane, wbuf[wib]);
+    emit_query<2, true>(P, t, q, n, lane, nullptr);
+}
+
+// The queries k_emit queued: exact odd-even transposition of the neighbours
+// within one truncated unit, then the rows; one thread per query (they are
+// few), count read on the device so no host round trip is needed.
+__global__ void __launch_bounds__(128) k_emit_fixup(EmitParams P) {
+  const unsigned int m = *P.fix_count;
+  const int inexact = *P.S.inexact;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = P.fix_list[j];
+    const QueryInfo qi = P.qinfo[t];
+    const int n = (int)(qi.meta & kQueryCountMask);
+    const int shift = n <= 32 ? 5 : 6;
+    const uint32_t mask = (1u << shift) - 1u;
+    const unsigned long long* ent = P.slab + slab_base(t);
+    uint32_t* keys = deferred_keys(P.slab, t);
+    exact_fixup_sorted(keys, n, shift, ent, P.S, inexact, qi.ex, qi.ey, qi.ez);
+    const unsigned long long base = P.poff[t];
+    const int kk = n < (int)P.kmax ? n : (int)P.kmax;
+    for (int i = 0; i < kk; ++i) {
+      const uint32_t idx = (uint32_t)ent[keys[i] & mask];
+      const float4 p = __ldg(&P.S.pts[idx]);
+      const double dist = __dsqrt_rn(exact_d2_at(qi.ex, qi.ey, qi.ez, P.S.pts, P.S.pts64, inexact, idx));
+      P.sink.put(base + i, qi.qid, __float_as_uint(p.w), dist, (uint32_t)i + 1);
+    }
+  }
+}
+
+// Row offsets in processing order: poff[t] = offsets[qrank[qorder[t]]].
+__global__ void k_proc_offsets(const uint32_t* qorder, const uint32_t* qrank, const unsigned long long* offsets,
+                               uint32_t nq, unsigned long long* poff) {
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += (uint64_t)gridDim.x * blockDim.x)
+    poff[t] = offsets[qrank[qorder[t]]];
+}
+
+// One warp per query with 65..kSlab candidates (processing ranks in `work`).
+constexpr int kEmitBigThreads = 128;
+
+__global__ void __launch_bounds__(kEmitBigThreads) k_emit_big(EmitParams P, const uint32_t* work, uint32_t nwork) {
+  __shared__ uint32_t wbuf[kEmitBigThreads / 32][kSlab];
+  const int lane = threadIdx.x & 31;
+  const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (j >= nwork) return;  // whole warp
+  const uint32_t t = work[j];
+  EmitQuery q;
+  emit_load(P, t, lane, q);
+  const int n = (int)(q.qi.meta & kQueryCountMask);
+  uint32_t* wb = wbuf[threadIdx.x >> 5];
+  if (n <= 128)
+    emit_query<4, false>(P, t, q, n, lane, wb);
+  else
+    emit_query<8, false>(P, t, q, n, lane, wb);
 }
 
 __global__ void k_invert(const uint32_t* order, uint32_t n, const unsigned int* identity_flag, uint32_t* inv) {
@@ -1255,6 +1255,16 @@ bool stats_enabled() {
   return on;
 }
 
+// Leaf points loaded together by the packet collect pass (1, 2 or 4;
+// RTDL_B200_COLLECT_BATCH, default 1).
+int collect_batch() {
+  static const int b = [] {
+    const char* v = std::getenv("RTDL_B200_COLLECT_BATCH");
+    return v ? std::atoi(v) : 1;
+  }();
+  return b;
+}
+
 }  // namespace
 
 std::vector<unsigned long long>& last_stats() {
@@ -1426,25 +1436,26 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
   k_invert<<<grid_for(nq, 256), 256, 0, s>>>(qp.oorder, nq, &qp.bands->ids_sorted, qrank);
   RTDL_LAUNCHED(1);
   if (timer) timer->mark("query_prep");
-  uint32_t* slab = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (size_t)nq * kSlab, s));
-  uint32_t* keys = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (size_t)nq * kSlab, s));
+  unsigned long long* slab =
+      static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * slab_base(nq), s));
   uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint16_t* ncand = static_cast<uint16_t*>(dev_alloc(sizeof(uint16_t) * nq, s));
+  QueryInfo* qinfo = static_cast<QueryInfo*>(dev_alloc(sizeof(QueryInfo) * nq, s));
   uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq, s));
   uint32_t* heavy_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   uint32_t* heavy_m = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   uint32_t* big_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   unsigned int* small = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * 4, s));
   unsigned long long* offsets = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (nq + 1), s));
+  unsigned long long* poff = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * nq, s));
   RTDL_CUDA_CHECK(cudaMemsetAsync(small, 0, sizeof(unsigned int) * 4, s));
   GenericOut g;
   auto cleanup = [&]() {
     g.release(s);
+    dev_free(poff, s);
     dev_free(qrank, s);
     dev_free(slab, s);
-    dev_free(keys, s);
     dev_free(counts, s);
-    dev_free(ncand, s);
+    dev_free(qinfo, s);
     dev_free(flags, s);
     dev_free(heavy_list, s);
     dev_free(heavy_m, s);
@@ -1464,14 +1475,14 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     C.kmax = kmax;
     C.bands = qp.bands;
     C.slab = slab;
-    C.keys = keys;
     C.counts = counts;
-    C.ncand = ncand;
+    C.qinfo = qinfo;
     C.flags = flags;
     C.heavy_list = heavy_list;
     C.heavy_m = heavy_m;
     C.big_list = big_list;
     C.small = small;
+    C.overflow_out = overflow_dev;
     C.stats = nullptr;
     const bool stats = stats_enabled();
     if (stats) {
@@ -1482,10 +1493,16 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     if (timer) timer->mark("setup");
     const bool packet = tuning().traversal == 0;
     if (packet) {
+      const unsigned int grid = div_up(nq, threads);
+      const int batch = collect_batch();
       if (stats)
-        k_collect_packet<true><<<div_up(nq, threads), threads, 0, s>>>(C);
+        k_collect_packet<true, 1><<<grid, threads, 0, s>>>(C);
+      else if (batch >= 4)
+        k_collect_packet<false, 4><<<grid, threads, 0, s>>>(C);
+      else if (batch == 2)
+        k_collect_packet<false, 2><<<grid, threads, 0, s>>>(C);
       else
-        k_collect_packet<false><<<div_up(nq, threads), threads, 0, s>>>(C);
+        k_collect_packet<false, 1><<<grid, threads, 0, s>>>(C);
     } else {
       if (stats)
         k_collect<true><<<div_up(nq, threads), threads, 0, s>>>(C);
@@ -1526,34 +1543,25 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       rows_capacity = res.rows;
       *rows_alloc = rows_dev;
     }
+    k_proc_offsets<<<grid_for(nq, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, nq, poff);
+    RTDL_LAUNCHED(1);
     EmitParams E;
     E.S = sc->view();
-    E.qpts = qp.qpts;
-    E.qraw = static_cast<const double*>(queries_dev);
-    E.qstride = qstride;
-    E.qorder = qp.qorder;
-    E.work = nullptr;
-    E.nwork = nq;
     E.nq = nq;
-    E.qrank = qrank;
-    E.bands = qp.bands;
     E.slab = slab;
-    E.keys = keys;
-    E.ncand = ncand;
-    E.flags = flags;
-    E.offsets = offsets;
+    E.qinfo = qinfo;
+    E.poff = poff;
     E.kmax = kmax;
     E.sink.rows = rows_dev;
     E.sink.capacity = rows_dev ? rows_capacity : 0;
     E.sink.ranked = predicate == kFrn ? 0 : 1;
-    E.overflow_out = overflow_dev;
-    k_emit_lanes<<<div_up(nq, 128), 128, 128 * 64 * sizeof(uint32_t), s>>>(E);
-    RTDL_LAUNCHED(1);
+    E.fix_list = big_list + big;  // the fixup queue shares big_list's nq slots (big + fixups <= nq)
+    E.fix_count = small + 3;
+    k_emit<<<div_up((uint64_t)nq * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
+    k_emit_fixup<<<kSmCount, 128, 0, s>>>(E);
+    RTDL_LAUNCHED(2);
     if (big > 0) {
-      E.work = big_list;
-      E.nwork = big;
-      E.overflow_out = nullptr;
-      k_emit_warp<<<div_up((uint64_t)big * 32, 128), 128, 0, s>>>(E);
+      k_emit_big<<<div_up((uint64_t)big * 32, kEmitBigThreads), kEmitBigThreads, 0, s>>>(E, big_list, big);
       RTDL_LAUNCHED(1);
     }
     if (r.heavy > 0) {
@@ -1568,7 +1576,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       X.L = kSlab;
       X.counts = counts;
       X.flags = flags;
-      X.temp = slab;
+      X.temp = nullptr;  // unused with a work list
       X.heavy_out = g.heavy_out;
       X.heavy_out_off = g.heavy_out_off;
       X.offsets = offsets;

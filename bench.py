@@ -357,6 +357,9 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", choices=("frn", "knn", "hausdorff"), default="frn",
                     help="frn: the headline fixed-radius config; knn: k=16 on the same 3D sets; "
                          "hausdorff: 4,194,304 x 4,194,304 2D directed nearest-distance reduction")
+    ap.add_argument("--traversal", choices=("packet", "lane", "packet_cube"), default=None,
+                    help="collect-pass traversal (library default when omitted)")
+    ap.add_argument("--leaf-size", type=int, default=None, help="LBVH leaf bucket size (library default when omitted)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -376,6 +379,8 @@ def main(argv=None) -> int:
     local = _env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
     rt.set_device(local)
+    if args.traversal is not None or args.leaf_size is not None:
+        rt.set_tuning(leaf_size=args.leaf_size or 8, traversal=args.traversal or "packet")
     dist = None
     if world > 1:
         import datetime

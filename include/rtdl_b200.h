@@ -263,7 +263,8 @@ RTDL_B200_API int rtdl_b200_get_launch_count(unsigned long long* count_out);
 /* Tuning knobs; the autotuner sets these.  leaf_size: points per LBVH leaf
  * bucket (1..32, applies to scenes built afterwards); block_threads: 64, 128
  * or 256; traversal: 0 = one warp walks the tree for 32 neighbouring queries
- * (packet), 1 = one thread per query.  Returns 0 on success. */
+ * (packet), 1 = one thread per query, 2 = packet with the query's bounding
+ * cube tested at internal nodes.  Returns 0 on success. */
 RTDL_B200_API int rtdl_b200_set_tuning(int leaf_size, int block_threads, int traversal);
 
 #ifdef __cplusplus

@@ -151,7 +151,7 @@ def launch_count() -> int:
 
 
 STAT_NAMES = ("nodes", "leaf_points", "in_radius", "inserts", "shifts", "band_checks", "max_count",
-              "generic_queries", "large_queries")
+              "generic_queries", "large_queries", "leaf_pairs", "emit_fixups")
 
 
 def last_query_stats() -> dict[str, int]:

@@ -123,7 +123,8 @@ struct Scene {
 struct Tuning {
   int leaf_size = 8;
   int block_threads = 128;
-  int traversal = 0;  // fixed-radius collect: 0 = one warp per 32 queries (packet), 1 = one thread per query
+  int traversal = 0;  // fixed-radius collect: 0 = one warp per 32 queries (packet), 1 = one thread per
+                      // query, 2 = packet with cube tests at internal nodes
 };
 Tuning& tuning();
 

@@ -27,6 +27,8 @@
 //               buckets left of it, depth its depth and r the right turns on
 //               its root path; its rope is the right child of the internal
 //               node whose split equals the node's last point.
+#include <cuda/atomic>
+
 #include "internal.cuh"
 
 namespace rtdl_b200 {
@@ -285,24 +287,32 @@ __device__ __forceinline__ void child_box(int c, const float4* __restrict__ pts,
   }
 }
 
-__global__ void k_refit(uint32_t n, const float4* __restrict__ pts, const int* __restrict__ child_l,
-                        const int* __restrict__ child_r, const int* __restrict__ parent_int,
-                        const int* __restrict__ parent_leaf, unsigned int* __restrict__ arrivals, float4* boxes) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    int p = parent_leaf[i];
-    while (p >= 0) {
-      __threadfence();
-      if (atomicAdd(&arrivals[p], 1u) == 0u) break;  // the sibling subtree is not finished yet
-      __threadfence();
-      float4 al, ah, bl, bh;
-      child_box(child_l[p], pts, boxes, al, ah);
-      child_box(child_r[p], pts, boxes, bl, bh);
-      const float4 lo = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.f);
-      const float4 hi = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.f);
-      __stcg(&boxes[2 * p], lo);
-      __stcg(&boxes[2 * p + 1], hi);
-      p = parent_int[p];
-    }
+// One thread per point walks towards the root; at each internal node an
+// acquire-release arrival counter lets the second child to arrive continue
+// (the first stops).  The walking thread carries its subtree's box in
+// registers, so it reads only the sibling's box.
+__global__ void __launch_bounds__(kThreads) k_refit(uint32_t n, const float4* __restrict__ pts,
+                                                   const int* __restrict__ child_l, const int* __restrict__ child_r,
+                                                   const int* __restrict__ parent_int, const int* __restrict__ parent_leaf,
+                                                   unsigned int* __restrict__ arrivals, float4* boxes) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 p0 = pts[i];
+  float4 lo = make_float4(p0.x, p0.y, p0.z, 0.f), hi = lo;
+  int me = (int)i | kLeafFlag;  // child code of the subtree the thread stands on
+  int p = parent_leaf[i];
+  while (p >= 0) {
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> arrived(arrivals[p]);
+    if (arrived.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) break;  // the sibling is not finished yet
+    const int l = child_l[p], r = child_r[p];
+    float4 sl, sh;
+    child_box(l == me ? r : l, pts, boxes, sl, sh);
+    lo = make_float4(fminf(lo.x, sl.x), fminf(lo.y, sl.y), fminf(lo.z, sl.z), 0.f);
+    hi = make_float4(fmaxf(hi.x, sh.x), fmaxf(hi.y, sh.y), fmaxf(hi.z, sh.z), 0.f);
+    __stcg(&boxes[2 * p], lo);
+    __stcg(&boxes[2 * p + 1], hi);
+    me = p;
+    p = parent_int[p];
   }
 }
 
@@ -470,7 +480,8 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
     RTDL_CUDA_CHECK(cudaMemsetAsync(parent_int, 0xFF, sizeof(int) * ni, s));  // root keeps -1
     k_karras<<<grid_for(ni), kThreads, 0, s>>>(codes, n, child_l, child_r, first, last, parent_int, parent_leaf,
                                               right_of_split);
-    k_refit<<<grid_for(n), kThreads, 0, s>>>(n, sc->pts, child_l, child_r, parent_int, parent_leaf, arrivals, boxes);
+    k_refit<<<div_up(n, kThreads), kThreads, 0, s>>>(n, sc->pts, child_l, child_r, parent_int, parent_leaf, arrivals,
+                                                   boxes);
     RTDL_LAUNCHED(2);
     Ent E{child_l, child_r, first, last, parent_int, parent_leaf, n};
     const uint64_t ents = 2ull * n - 1;

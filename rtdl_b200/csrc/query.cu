@@ -198,7 +198,7 @@ struct Pass1Params {
 
 // Traversal counters gathered by the STATS instantiation (diagnostics).
 enum Stat { kStatNodes, kStatLeafPoints, kStatInRadius, kStatInserts, kStatShifts, kStatBand, kStatMaxLeafPoints,
-            kStatGenericQueries, kStatLargeQueries, kStatCount };
+            kStatGenericQueries, kStatLargeQueries, kStatLeafPairs, kStatEmitFixups, kStatCount };
 
 // One thread per query, queries in Morton order so a warp walks neighbouring
 // subtrees.  KNN == false: radius-limited (fixed_radius_neighbors and
@@ -404,7 +404,7 @@ struct QueryInfo {
 };
 constexpr uint32_t kQueryCountMask = 0xFFFFu;
 constexpr uint32_t kQueryGeneric = 1u << 16;   // more than kSlab candidates: generic path
-constexpr uint32_t kQueryBig = 1u << 17;       // 65..kSlab candidates: k_emit_big
+constexpr uint32_t kQueryBig = 1u << 17;       // 65..kSlab candidates: k_emit_list
 constexpr uint32_t kQueryOverflow = 1u << 18;  // more in-radius points than kmax
 
 struct CollectParams {
@@ -422,8 +422,10 @@ struct CollectParams {
   uint8_t* flags;            // bit0: count > kmax, bit1: count > kSlab (generic path), bit2: count > 64
   uint32_t* heavy_list;
   uint32_t* heavy_m;
-  uint32_t* big_list;        // processing ranks of the queries with 65..kSlab candidates
-  unsigned int* small;       // [0] generic-path query count, [1] error bits, [2] big_list length
+  uint32_t* mid_list;        // processing ranks of the queries with 65..128 candidates
+  uint32_t* big_list;        // processing ranks of the queries with 129..kSlab candidates
+  unsigned int* small;       // [0] generic-path query count, [1] error bits, [2] mid_list length,
+                             // [3] big_list length, [4] emit fixup queue length
   uint8_t* overflow_out;     // optional: 1 per query (input order) when count > kmax
   unsigned long long* stats;
 };
@@ -436,7 +438,7 @@ struct CollectLane {
   double ex, ey, ez;
   uint32_t count;
   unsigned long long* out;  // this query's slab entries
-  unsigned long long st_nodes, st_points, st_band;
+  unsigned long long st_nodes, st_points, st_band, st_pairs;
 };
 
 // Tests sorted point i against the lane's query and appends it when it is in
@@ -465,6 +467,7 @@ __device__ __forceinline__ void collect_finish(const CollectParams& P, const Col
     atomicAdd(&P.stats[kStatLeafPoints], L.st_points);
     atomicAdd(&P.stats[kStatInRadius], (unsigned long long)L.count);
     atomicAdd(&P.stats[kStatBand], L.st_band);
+    atomicAdd(&P.stats[kStatLeafPairs], L.st_pairs);
     atomicMax(&P.stats[kStatMaxLeafPoints], (unsigned long long)L.count);
   }
   const uint32_t count = L.count, kmax = P.kmax;
@@ -475,9 +478,12 @@ __device__ __forceinline__ void collect_finish(const CollectParams& P, const Col
     const unsigned int h = atomicAdd(&P.small[0], 1u);
     P.heavy_list[h] = L.qin;
     P.heavy_m[h] = count;
+  } else if (count > 128u) {
+    fl |= 4;
+    P.big_list[atomicAdd(&P.small[3], 1u)] = L.t;
   } else if (count > 64u) {
     fl |= 4;
-    P.big_list[atomicAdd(&P.small[2], 1u)] = L.t;
+    P.mid_list[atomicAdd(&P.small[2], 1u)] = L.t;
   }
   QueryInfo qi;
   qi.ex = L.ex;
@@ -501,24 +507,17 @@ __device__ __forceinline__ void collect_init(const CollectParams& P, uint32_t t,
   L.ez = P.qstride == 4 ? r[3] : 0.0;
   L.count = 0;
   L.out = P.slab + slab_base(t);
-  L.st_nodes = L.st_points = L.st_band = 0;
+  L.st_nodes = L.st_points = L.st_band = L.st_pairs = 0;
 }
 
 // Tests the points of leaf bucket [first, first + cnt) against the lane's
-// query, loading them BATCH at a time so the loads of a batch are in flight
-// together (more registers for more loads in flight).  `test` false: the lane
-// only takes part in the loads.
-template <bool STATS, int BATCH>
+// query.  `test` false: the lane only takes part in the (warp-uniform) loads.
+template <bool STATS>
 __device__ __forceinline__ void collect_leaf(const CollectParams& P, const DevBands& B, int scene_inexact,
                                              CollectLane& L, int first, int cnt, bool test) {
-  for (int j0 = 0; j0 < cnt; j0 += BATCH) {
-    float4 p[BATCH];
-#pragma unroll
-    for (int j = 0; j < BATCH; ++j)
-      if (j0 + j < cnt) p[j] = __ldg(&P.S.pts[first + j0 + j]);
-#pragma unroll
-    for (int j = 0; j < BATCH; ++j)
-      if (test && j0 + j < cnt) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)(first + j0 + j), p[j]);
+  for (int i = first; i < first + cnt; ++i) {
+    const float4 p = __ldg(&P.S.pts[i]);
+    if (test) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)i, p);
   }
 }
 
@@ -554,8 +553,11 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
         break;
       }
     }
-    if (STATS) L.st_points += cnt;
-    collect_leaf<STATS, 1>(P, B, scene_inexact, L, first, cnt, true);
+    if (STATS) {
+      L.st_points += cnt;
+      L.st_pairs += cnt;
+    }
+    collect_leaf<STATS>(P, B, scene_inexact, L, first, cnt, true);
   }
   collect_finish<STATS>(P, L);
 }
@@ -564,9 +566,12 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
 // walks the rope-linked nodes once, entering a node when any lane's query
 // sphere overlaps it.  Node and point loads are warp-uniform (one request
 // each) and the control flow never diverges; each lane tests leaf points
-// against its own query.
-template <bool STATS, int BATCH>
-__global__ void __launch_bounds__(256) k_collect_packet(CollectParams P) {
+// against its own query.  CUBE: internal nodes are tested against the
+// query's bounding cube (six compares against bounds rounded outward; it
+// never rejects a node the sphere test accepts), leaf buckets against the
+// sphere.
+template <bool STATS, bool CUBE, int MIN_BLOCKS>
+__global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParams P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = t < P.nq;
   if (!__any_sync(0xffffffffu, valid)) return;  // whole warp past the end
@@ -580,22 +585,35 @@ __global__ void __launch_bounds__(256) k_collect_packet(CollectParams P) {
     L.q = make_float4(INFINITY, INFINITY, INFINITY, 0.f);  // never overlaps
     L.count = 0;
     L.out = nullptr;
-    L.st_nodes = L.st_points = L.st_band = 0;
+    L.st_nodes = L.st_points = L.st_band = L.st_pairs = 0;
+  }
+  float3 clo, chi;  // query cube, CUBE only
+  if (CUBE) {
+    const float h = sqrtf(B.box_hi2) * (1.0f + 4.0f * kU);  // >= the sphere radius
+    clo = make_float3(__fsub_rd(L.q.x, h), __fsub_rd(L.q.y, h), __fsub_rd(L.q.z, h));
+    chi = make_float3(__fadd_ru(L.q.x, h), __fadd_ru(L.q.y, h), __fadd_ru(L.q.z, h));
   }
   int cur = S.n > 0 ? 0 : kRopeEnd;
   while (cur != kRopeEnd) {
     const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
     if (STATS) ++L.st_nodes;
     const int hit = __float_as_int(a.w);
-    const bool over = valid && box_d2(L.q.x, L.q.y, L.q.z, a, b) <= B.box_hi2;
+    bool over;
+    if (CUBE && hit >= 0)
+      over = valid && a.x <= chi.x && b.x >= clo.x && a.y <= chi.y && b.y >= clo.y && a.z <= chi.z && b.z >= clo.z;
+    else
+      over = valid && box_d2(L.q.x, L.q.y, L.q.z, a, b) <= B.box_hi2;
     if (__any_sync(0xffffffffu, over)) {
       if (hit >= 0) {
         ++cur;  // internal node: its left child is the next record
         continue;
       }
       const int first = leaf_first(hit), cnt = leaf_count(hit);
-      if (STATS) L.st_points += cnt;
-      collect_leaf<STATS, BATCH>(P, B, scene_inexact, L, first, cnt, over);
+      if (STATS) {
+        L.st_points += cnt;
+        if (over) L.st_pairs += cnt;
+      }
+      collect_leaf<STATS>(P, B, scene_inexact, L, first, cnt, over);
     }
     cur = __float_as_int(b.w);
   }
@@ -635,10 +653,11 @@ struct EmitParams {
   unsigned int* fix_count;
 };
 
-// A deferred query's sorted packed keys (at most 64) live in its slab entries
-// 64..95, unused by a query with at most 64 candidates.
-__device__ __forceinline__ uint32_t* deferred_keys(unsigned long long* slab, uint32_t t) {
-  return reinterpret_cast<uint32_t*>(slab + slab_base(t) + 64);
+// A deferred query's sorted packed keys live in slab entries its candidates do
+// not use: from entry 64 for at most 64 candidates, from entry 128 for at most
+// 128 (room for 256 keys).
+__device__ __forceinline__ uint32_t* deferred_keys(unsigned long long* slab, uint32_t t, int n) {
+  return reinterpret_cast<uint32_t*>(slab + slab_base(t) + (n <= 64 ? 64 : 128));
 }
 
 // Packed sort element: the FP32 d2 key with its low SHIFT mantissa bits
@@ -765,7 +784,8 @@ __device__ __forceinline__ void emit_query(const EmitParams& P, uint32_t t, cons
   const int inexact = *P.S.inexact;
   if (__any_sync(0xffffffffu, amb)) {
     if (DEFER) {
-      uint32_t* spare = deferred_keys(P.slab, t);
+      static_assert(!DEFER || E <= 4, "a deferred query needs spare slab entries");
+      uint32_t* spare = deferred_keys(P.slab, t, n);
 #pragma unroll
       for (int r = 0; r < E; ++r) spare[(r << 5) | lane] = v[r];
       if (lane == 0) P.fix_list[atomicAdd(P.fix_count, 1u)] = t;
@@ -816,7 +836,7 @@ __device__ __forceinline__ void emit_query(const EmitParams& P, uint32_t t, cons
 }
 
 // Warp per query in processing (Morton) order for the queries with at most
-// 64 candidates; queries with 65..kSlab candidates are k_emit_big's, those on
+// 64 candidates; queries with 65..kSlab candidates are k_emit_list's, those on
 // the generic path get their rows from k_expand.
 constexpr int kEmitThreads = 256;
 
@@ -836,29 +856,57 @@ __global__ void __launch_bounds__(kEmitThreads) k_emit(EmitParams P) {
     emit_query<2, true>(P, t, q, n, lane, nullptr);
 }
 
-// The queries k_emit queued: exact odd-even transposition of the neighbours
-// within one truncated unit, then the rows; one thread per query (they are
-// few), count read on the device so no host round trip is needed.
-__global__ void __launch_bounds__(128) k_emit_fixup(EmitParams P) {
+// The queries the emit kernels queued, one warp per query: the sorted keys go
+// to shared memory, the warp runs odd-even transposition over them (the
+// pairs of one parity are disjoint, so the lanes take them in parallel)
+// re-deciding neighbours within one truncated unit exactly, until a pass
+// swaps nothing; then it writes the rows.  The queue length is read on the
+// device, so no host round trip is needed.
+constexpr int kFixupThreads = 128;
+
+__global__ void __launch_bounds__(kFixupThreads) k_emit_fixup(EmitParams P) {
+  __shared__ uint32_t sk[kFixupThreads / 32][128];
   const unsigned int m = *P.fix_count;
+  const int lane = threadIdx.x & 31;
+  uint32_t* keys = sk[threadIdx.x >> 5];
   const int inexact = *P.S.inexact;
-  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < m; j += warps) {
     const uint32_t t = P.fix_list[j];
     const QueryInfo qi = P.qinfo[t];
-    const int n = (int)(qi.meta & kQueryCountMask);
-    const int shift = n <= 32 ? 5 : 6;
+    const int n = (int)(qi.meta & kQueryCountMask);  // <= 128 for a deferred query
+    const int shift = n <= 32 ? 5 : n <= 64 ? 6 : 7;
     const uint32_t mask = (1u << shift) - 1u;
     const unsigned long long* ent = P.slab + slab_base(t);
-    uint32_t* keys = deferred_keys(P.slab, t);
-    exact_fixup_sorted(keys, n, shift, ent, P.S, inexact, qi.ex, qi.ey, qi.ez);
+    const uint32_t* src = deferred_keys(P.slab, t, n);
+    for (int i = lane; i < n; i += 32) keys[i] = src[i];
+    __syncwarp();
+    for (int pass = 0; pass < n; ++pass) {
+      bool changed = false;
+      for (int parity = 0; parity < 2; ++parity) {
+        for (int i = parity + 2 * lane; i + 1 < n; i += 64) {
+          const uint32_t a = keys[i], b = keys[i + 1];
+          if ((b >> shift) - (a >> shift) > 1u) continue;
+          if (exact_before(qi.ex, qi.ey, qi.ez, P.S.pts, P.S.pts64, P.S.perm, inexact, (uint32_t)ent[b & mask],
+                           (uint32_t)ent[a & mask])) {
+            keys[i] = b;
+            keys[i + 1] = a;
+            changed = true;
+          }
+        }
+        __syncwarp();
+      }
+      if (!__any_sync(0xffffffffu, changed)) break;
+    }
     const unsigned long long base = P.poff[t];
     const int kk = n < (int)P.kmax ? n : (int)P.kmax;
-    for (int i = 0; i < kk; ++i) {
+    for (int i = lane; i < kk; i += 32) {
       const uint32_t idx = (uint32_t)ent[keys[i] & mask];
       const float4 p = __ldg(&P.S.pts[idx]);
       const double dist = __dsqrt_rn(exact_d2_at(qi.ex, qi.ey, qi.ez, P.S.pts, P.S.pts64, inexact, idx));
       P.sink.put(base + i, qi.qid, __float_as_uint(p.w), dist, (uint32_t)i + 1);
     }
+    __syncwarp();
   }
 }
 
@@ -869,11 +917,14 @@ __global__ void k_proc_offsets(const uint32_t* qorder, const uint32_t* qrank, co
     poff[t] = offsets[qrank[qorder[t]]];
 }
 
-// One warp per query with 65..kSlab candidates (processing ranks in `work`).
-constexpr int kEmitBigThreads = 128;
+// One warp per query of a work list (processing ranks): E = 4 for 65..128
+// candidates (exact fixups deferred to k_emit_fixup), E = 8 for 129..kSlab
+// (fixups in place through shared memory).
+constexpr int kEmitListThreads = 128;
 
-__global__ void __launch_bounds__(kEmitBigThreads) k_emit_big(EmitParams P, const uint32_t* work, uint32_t nwork) {
-  __shared__ uint32_t wbuf[kEmitBigThreads / 32][kSlab];
+template <int E, bool DEFER>
+__global__ void __launch_bounds__(kEmitListThreads) k_emit_list(EmitParams P, const uint32_t* work, uint32_t nwork) {
+  __shared__ uint32_t wbuf[DEFER ? 1 : kEmitListThreads / 32][DEFER ? 1 : 32 * E];
   const int lane = threadIdx.x & 31;
   const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (j >= nwork) return;  // whole warp
@@ -881,11 +932,7 @@ __global__ void __launch_bounds__(kEmitBigThreads) k_emit_big(EmitParams P, cons
   EmitQuery q;
   emit_load(P, t, lane, q);
   const int n = (int)(q.qi.meta & kQueryCountMask);
-  uint32_t* wb = wbuf[threadIdx.x >> 5];
-  if (n <= 128)
-    emit_query<4, false>(P, t, q, n, lane, wb);
-  else
-    emit_query<8, false>(P, t, q, n, lane, wb);
+  emit_query<E, DEFER>(P, t, q, n, lane, DEFER ? nullptr : wbuf[threadIdx.x >> 5]);
 }
 
 __global__ void k_invert(const uint32_t* order, uint32_t n, const unsigned int* identity_flag, uint32_t* inv) {
@@ -1255,15 +1302,7 @@ bool stats_enabled() {
   return on;
 }
 
-// Leaf points loaded together by the packet collect pass (1, 2 or 4;
-// RTDL_B200_COLLECT_BATCH, default 1).
-int collect_batch() {
-  static const int b = [] {
-    const char* v = std::getenv("RTDL_B200_COLLECT_BATCH");
-    return v ? std::atoi(v) : 1;
-  }();
-  return b;
-}
+
 
 }  // namespace
 
@@ -1276,11 +1315,13 @@ namespace {
 
 struct Readback {
   unsigned long long rows;
-  unsigned int heavy;  // these three are copied together from the `small` device counters
+  unsigned int heavy;  // these four are copied together from the `small` device counters
   unsigned int error;
+  unsigned int mid;
   unsigned int big;
   unsigned int scene_bad;
   unsigned int query_bad;
+  unsigned int fixups;
   unsigned int pad;
 };
 
@@ -1443,11 +1484,13 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
   uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq, s));
   uint32_t* heavy_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   uint32_t* heavy_m = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  uint32_t* mid_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   uint32_t* big_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  unsigned int* small = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * 4, s));
+  uint32_t* fix_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  unsigned int* small = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * 8, s));
   unsigned long long* offsets = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (nq + 1), s));
   unsigned long long* poff = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * nq, s));
-  RTDL_CUDA_CHECK(cudaMemsetAsync(small, 0, sizeof(unsigned int) * 4, s));
+  RTDL_CUDA_CHECK(cudaMemsetAsync(small, 0, sizeof(unsigned int) * 8, s));
   GenericOut g;
   auto cleanup = [&]() {
     g.release(s);
@@ -1459,7 +1502,9 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     dev_free(flags, s);
     dev_free(heavy_list, s);
     dev_free(heavy_m, s);
+    dev_free(mid_list, s);
     dev_free(big_list, s);
+    dev_free(fix_list, s);
     dev_free(small, s);
     dev_free(offsets, s);
     free_prep(qp, s);
@@ -1480,6 +1525,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     C.flags = flags;
     C.heavy_list = heavy_list;
     C.heavy_m = heavy_m;
+    C.mid_list = mid_list;
     C.big_list = big_list;
     C.small = small;
     C.overflow_out = overflow_dev;
@@ -1491,18 +1537,17 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     }
     const int threads = tuning().block_threads;
     if (timer) timer->mark("setup");
-    const bool packet = tuning().traversal == 0;
+    const bool packet = tuning().traversal != 1;
     if (packet) {
       const unsigned int grid = div_up(nq, threads);
-      const int batch = collect_batch();
+      const bool cube = tuning().traversal == 2;
+      // occupancy bounds chosen so neither variant spills (32 and 40 registers)
       if (stats)
-        k_collect_packet<true, 1><<<grid, threads, 0, s>>>(C);
-      else if (batch >= 4)
-        k_collect_packet<false, 4><<<grid, threads, 0, s>>>(C);
-      else if (batch == 2)
-        k_collect_packet<false, 2><<<grid, threads, 0, s>>>(C);
+        cube ? k_collect_packet<true, true, 1><<<grid, threads, 0, s>>>(C)
+             : k_collect_packet<true, false, 1><<<grid, threads, 0, s>>>(C);
       else
-        k_collect_packet<false, 1><<<grid, threads, 0, s>>>(C);
+        cube ? k_collect_packet<false, true, 6><<<grid, threads, 0, s>>>(C)
+             : k_collect_packet<false, false, 7><<<grid, threads, 0, s>>>(C);
     } else {
       if (stats)
         k_collect<true><<<div_up(nq, threads), threads, 0, s>>>(C);
@@ -1520,7 +1565,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     if (timer) timer->mark("scan");
     Readback* rb = pinned_readback();
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 3, cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, s));
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1528,10 +1573,9 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     check_readback(r);
     res.rows = r.rows;
     res.heavy = r.heavy;
-    const uint32_t big = r.big;
     if (stats) {
       last_stats()[kStatGenericQueries] = r.heavy;
-      last_stats()[kStatLargeQueries] = r.big;
+      last_stats()[kStatLargeQueries] = r.mid + r.big;
     }
     if (r.heavy > 0) {
       g = run_generic_path(sc, qp, queries_dev, qstride, r.heavy, heavy_list, heavy_m, kmax, false, small + 1, s);
@@ -1555,15 +1599,22 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     E.sink.rows = rows_dev;
     E.sink.capacity = rows_dev ? rows_capacity : 0;
     E.sink.ranked = predicate == kFrn ? 0 : 1;
-    E.fix_list = big_list + big;  // the fixup queue shares big_list's nq slots (big + fixups <= nq)
-    E.fix_count = small + 3;
+    E.fix_list = fix_list;
+    E.fix_count = small + 4;
     k_emit<<<div_up((uint64_t)nq * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
-    k_emit_fixup<<<kSmCount, 128, 0, s>>>(E);
-    RTDL_LAUNCHED(2);
-    if (big > 0) {
-      k_emit_big<<<div_up((uint64_t)big * 32, kEmitBigThreads), kEmitBigThreads, 0, s>>>(E, big_list, big);
+    RTDL_LAUNCHED(1);
+    if (r.mid > 0) {
+      k_emit_list<4, true><<<div_up((uint64_t)r.mid * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, mid_list,
+                                                                                                    r.mid);
       RTDL_LAUNCHED(1);
     }
+    if (r.big > 0) {
+      k_emit_list<8, false><<<div_up((uint64_t)r.big * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, big_list,
+                                                                                                     r.big);
+      RTDL_LAUNCHED(1);
+    }
+    k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
+    RTDL_LAUNCHED(1);
     if (r.heavy > 0) {
       ExpandParams X;
       X.S = sc->view();
@@ -1592,7 +1643,9 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     }
     if (timer) timer->mark("emit");
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
     if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
   } catch (...) {
     cudaStreamSynchronize(s);

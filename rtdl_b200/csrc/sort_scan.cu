@@ -7,8 +7,11 @@
 // single-block pass over the tile sums, then a downsweep.  Deterministic and
 // free of inter-block waits.
 // Radix sort: 8-bit digits; per pass a tile histogram kernel, a scan of the
-// (digit, tile) histogram and a scatter kernel that ranks keys stably inside
-// the tile with __match_any_sync and per-warp digit counters.
+// (digit, tile) histogram and a scatter kernel.  The scatter gives each warp a
+// contiguous run of the tile: the warp counts its digits (__match_any_sync,
+// one shared-memory add per digit group), one block-wide scan over
+// (digit, warp) turns the counts into bases, and the warp then places its
+// keys in order, so a tile costs two barriers and the sort stays stable.
 #include "internal.cuh"
 
 namespace rtdl_b200 {
@@ -20,7 +23,7 @@ constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
+constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kSortWarps = kSortThreads / 32;
 
@@ -167,49 +170,77 @@ __global__ void k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n, int 
   hist[(uint64_t)t * num_tiles + blockIdx.x] = h[t];
 }
 
-__global__ void k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-                                uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
-                                int shift, const uint32_t* __restrict__ hist_scanned, uint32_t num_tiles,
-                                const unsigned int* skip) {
+__global__ void __launch_bounds__(kSortThreads)
+    k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n, int shift,
+                    const uint32_t* __restrict__ hist_scanned, uint32_t num_tiles, const unsigned int* skip) {
   if (skip != nullptr && *skip) return;
-  __shared__ unsigned int base_off[256];
-  __shared__ unsigned int warp_cnt[kSortWarps][256];
-  __shared__ unsigned int run[256];
+  __shared__ unsigned int wcnt[kSortWarps][256];  // a warp's digit counts, then its tile-local digit bases
+  __shared__ unsigned int dbase[256];             // tile-local start of each digit
+  __shared__ unsigned int gbase[256];             // global start of each digit for this tile
+  __shared__ unsigned int total;
+  __shared__ uint32_t skeys[kSortTile], svals[kSortTile];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  base_off[t] = hist_scanned[(uint64_t)t * num_tiles + blockIdx.x];
-  run[t] = 0;
-  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
   const unsigned int lt_mask = (1u << lane) - 1u;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) wcnt[w][t] = 0;
+  __syncthreads();
+  // the warp's run of the tile: kSortItems rounds of 32 consecutive keys
+  const uint64_t tile0 = (uint64_t)blockIdx.x * kSortTile;
+  const uint64_t base = tile0 + (uint64_t)warp * (kSortItems * 32);
+  uint32_t key[kSortItems];
+#pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
-#pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) warp_cnt[w][t] = 0;
-    __syncthreads();
-    const uint64_t idx = base + (uint64_t)i * kSortThreads + t;
+    const uint64_t idx = base + (uint64_t)i * 32 + lane;
     const bool valid = idx < n;
-    const uint32_t key = valid ? keys_in[idx] : 0u;
-    const uint32_t d = (key >> shift) & 255u;
-    const unsigned int vmask = __ballot_sync(0xffffffffu, valid);
-    const unsigned int peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u) & vmask;
-    const unsigned int rank = __popc(peers & lt_mask);
-    if (valid && rank == 0) warp_cnt[warp][d] = __popc(peers);
-    __syncthreads();
-    {
-      unsigned int r = run[t];
+    key[i] = valid ? keys_in[idx] : 0u;
+    const uint32_t d = (key[i] >> shift) & 255u;
+    const unsigned int peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u) & __ballot_sync(0xffffffffu, valid);
+    if (valid && (peers & lt_mask) == 0) wcnt[warp][d] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // thread t owns digit t: offsets of the warps within the digit, then the
+  // digit's tile-local start (scan over digits) and its global start
+  unsigned int r = 0;
 #pragma unroll
-      for (int w = 0; w < kSortWarps; ++w) {
-        unsigned int c = warp_cnt[w][t];
-        warp_cnt[w][t] = r;
-        r += c;
-      }
-      run[t] = r;
-    }
-    __syncthreads();
+  for (int w = 0; w < kSortWarps; ++w) {
+    const unsigned int c = wcnt[w][t];
+    wcnt[w][t] = r;
+    r += c;
+  }
+  const unsigned int db = block_exclusive_scan<unsigned int>(r, &total);
+  dbase[t] = db;
+  gbase[t] = hist_scanned[(uint64_t)t * num_tiles + blockIdx.x];
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) wcnt[w][t] += db;
+  __syncthreads();
+  // place the keys in the tile's digit order in shared memory (stable)
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const uint64_t idx = base + (uint64_t)i * 32 + lane;
+    const bool valid = idx < n;
+    const uint32_t d = (key[i] >> shift) & 255u;
+    const unsigned int peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u) & __ballot_sync(0xffffffffu, valid);
     if (valid) {
-      const unsigned int pos = base_off[d] + warp_cnt[warp][d] + rank;
-      keys_out[pos] = key;
-      vals_out[pos] = vals_in[idx];
+      const unsigned int pos = wcnt[warp][d] + __popc(peers & lt_mask);
+      skeys[pos] = key[i];
+      svals[pos] = vals_in[idx];
     }
-    __syncthreads();
+    __syncwarp();
+    if (valid && (peers & lt_mask) == 0) wcnt[warp][d] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // write out: consecutive threads take consecutive keys of a digit's run,
+  // so the global stores are contiguous
+  const unsigned int tile_n = (unsigned int)(n - tile0 < (uint64_t)kSortTile ? n - tile0 : (uint64_t)kSortTile);
+  for (unsigned int j = t; j < tile_n; j += kSortThreads) {
+    const uint32_t k = skeys[j];
+    const uint32_t d = (k >> shift) & 255u;
+    const unsigned int pos = gbase[d] + (j - dbase[d]);
+    keys_out[pos] = k;
+    vals_out[pos] = svals[j];
   }
 }
 

@@ -211,6 +211,51 @@ RTDL_B200_API int rtdl_b200_scene_directed_hausdorff_device(
     double* distance_out, uint32_t* source_id_out, uint32_t* target_id_out,
     void* stream, char* error_out, size_t error_size);
 
+/* ---- problem batches -------------------------------------------------------
+ * Many independent fixed-radius problems of uneven sizes answered together:
+ * one LBVH build over all problems' points (the sort key carries the problem
+ * id, so every problem is a subtree of its own) and one collect / emit launch
+ * sequence over all queries, each warp walking its problem's subtree.  No
+ * reference counterpart: the reference runs one call per problem
+ * (rtdl_optix_api.cpp:4076-4150); its batched form only splits one query set
+ * into chunks (rtdl_optix_workloads.cpp:14380-14409). */
+
+/* Builds the batch.  points: the problems' RtdlPoint / RtdlPoint3D records back
+ * to back, problem p at [point_offsets[p], point_offsets[p + 1]) (host array
+ * of problems + 1 entries, starting at 0); points_on_device says whether
+ * `points` is a device pointer.  At most 67,108,864 points in all.  The
+ * handle is released with rtdl_b200_batch_destroy. */
+RTDL_B200_API int rtdl_b200_batch_create(
+    const void* points, const unsigned long long* point_offsets, uint32_t problems,
+    int dimension, int points_on_device, void* stream, void** batch_out,
+    char* error_out, size_t error_size);
+
+RTDL_B200_API void rtdl_b200_batch_destroy(void* batch);
+
+/* fixed_radius_neighbors for every problem: problem p's queries are
+ * [query_offsets[p], query_offsets[p + 1]) of query_points (host records),
+ * with radius[p] and k_max[p] (1..64).  Rows come back problem by problem,
+ * each problem's exactly as rtdl_b200_run_fixed_radius_neighbors[_3d] returns
+ * them for that problem alone; row_offsets_out (problems + 1 entries) receives
+ * each problem's first row and the total.  *rows_out is released with
+ * rtdl_b200_free_rows.  overflow_out (optional, one byte per query) is 1 where
+ * a query had more than k_max points in radius. */
+RTDL_B200_API int rtdl_b200_batch_fixed_radius_neighbors(
+    void* batch, const void* query_points, const unsigned long long* query_offsets,
+    const double* radius, const uint32_t* k_max,
+    RtdlFixedRadiusNeighborRow** rows_out, unsigned long long* row_offsets_out,
+    uint8_t* overflow_out, char* error_out, size_t error_size);
+
+/* Device-resident form: query records and rows are device pointers, rows are
+ * written up to rows_capacity (row_offsets_out still reports every problem's
+ * full count, so a first call with capacity 0 sizes the buffer); the work runs
+ * on `stream` (NULL = the batch's stream). */
+RTDL_B200_API int rtdl_b200_batch_fixed_radius_neighbors_device(
+    void* batch, const void* query_points_dev, const unsigned long long* query_offsets,
+    const double* radius, const uint32_t* k_max, void* rows_dev, size_t rows_capacity,
+    unsigned long long* row_offsets_out, uint8_t* overflow_dev, void* stream,
+    char* error_out, size_t error_size);
+
 /* Result record of rtdl_b200_scene_directed_hausdorff_noalloc (device memory).
  * status: 0 = ok, 1 = a coordinate is non-finite or beyond 1e18, 2 = the
  * traversal stack overflowed. */

@@ -97,6 +97,12 @@ SIGNATURES = {
     "rtdl_b200_scene_directed_hausdorff": (_i, [_vp, _vp, _sz, _dp, _u32p, _u32p, _dp, _u32p, _cp, _sz]),
     "rtdl_b200_scene_directed_hausdorff_device": (_i, [_vp, _vp, _sz, _vp, _vp, _dp, _u32p, _u32p, _vp, _cp, _sz]),
     "rtdl_b200_scene_directed_hausdorff_noalloc": (_i, [_vp, _vp, _sz, _vp, _vp, _vp, _vp, _cp, _sz]),
+    # batch arrays (offsets, radius, k_max, row offsets) are passed as addresses of numpy buffers
+    "rtdl_b200_batch_create": (_i, [_vp, _vp, ctypes.c_uint32, _i, _i, _vp, _vpp, _cp, _sz]),
+    "rtdl_b200_batch_destroy": (None, [_vp]),
+    "rtdl_b200_batch_fixed_radius_neighbors": (_i, [_vp, _vp, _vp, _vp, _vp, _vpp, _vp, _vp, _cp, _sz]),
+    "rtdl_b200_batch_fixed_radius_neighbors_device": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp,
+                                                           _cp, _sz]),
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i, _i]),
     "rtdl_b200_get_launch_count": (_i, [ctypes.POINTER(ctypes.c_ulonglong)]),

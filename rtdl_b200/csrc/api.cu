@@ -524,6 +524,118 @@ int rtdl_b200_scene_query_device(void* scene, const void* query_points_dev, size
   }, error_out, error_size);
 }
 
+int rtdl_b200_batch_create(const void* points, const unsigned long long* point_offsets, uint32_t problems,
+                           int dimension, int points_on_device, void* stream, void** batch_out, char* error_out,
+                           size_t error_size) {
+  return guarded([&]() {
+    if (!batch_out) throw std::runtime_error("batch_out must not be null");
+    *batch_out = nullptr;
+    if (dimension != 2 && dimension != 3) throw std::runtime_error("dimension must be 2 or 3");
+    if (problems == 0) throw std::runtime_error("a problem batch needs at least one problem");
+    if (!point_offsets) throw std::runtime_error("point_offsets must not be null");
+    const unsigned long long count = point_offsets[problems];
+    if (!points && count != 0) throw std::runtime_error("points pointer must not be null when count is nonzero");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : library_stream();
+    int dev = 0;
+    RTDL_CUDA_CHECK(cudaGetDevice(&dev));
+    ensure_pool_configured(dev);
+    const void* d_points = points;
+    void* owned = nullptr;
+    Scene* sc = nullptr;
+    try {
+      if (!points_on_device && count) {
+        owned = upload(points, record_size(dimension) * count, s);
+        d_points = owned;
+      }
+      sc = build_scene_batch(d_points, point_offsets, problems, dimension, s, tuning().leaf_size);
+      unsigned int bad = 0;
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      if (bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+    } catch (...) {
+      destroy_scene(sc);
+      dev_free(owned, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(owned, s);
+    *batch_out = sc;
+  }, error_out, error_size);
+}
+
+void rtdl_b200_batch_destroy(void* batch) { rtdl_b200_scene_destroy(batch); }
+
+int rtdl_b200_batch_fixed_radius_neighbors(void* batch, const void* query_points,
+                                           const unsigned long long* query_offsets, const double* radius,
+                                           const uint32_t* k_max, RtdlFixedRadiusNeighborRow** rows_out,
+                                           unsigned long long* row_offsets_out, uint8_t* overflow_out,
+                                           char* error_out, size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(batch);
+    if (!sc || sc->problems == 0) throw std::runtime_error("batch must be a problem batch handle");
+    if (!query_offsets || !radius || !k_max || !rows_out || !row_offsets_out)
+      throw std::runtime_error("query_offsets, radius, k_max, rows_out and row_offsets_out must not be null");
+    *rows_out = nullptr;
+    const unsigned long long nq = query_offsets[sc->problems];
+    if (!query_points && nq != 0) throw std::runtime_error("query_points pointer must not be null when queries exist");
+    BatchSpec bs;
+    bs.problems = sc->problems;
+    bs.qoff = query_offsets;
+    bs.radius = radius;
+    bs.kmax = k_max;
+    bs.row_offsets = row_offsets_out;
+    cudaStream_t s = sc->stream;
+    PhaseTimer timer(s);
+    timer.mark("begin");
+    void* d_query = nq ? upload(query_points, record_size(sc->dim) * nq, s) : nullptr;
+    uint8_t* d_overflow = (overflow_out && nq) ? static_cast<uint8_t*>(dev_alloc(nq, s)) : nullptr;
+    if (d_overflow) RTDL_CUDA_CHECK(cudaMemsetAsync(d_overflow, 0, nq, s));
+    timer.mark("upload");
+    void* d_rows = nullptr;
+    try {
+      QueryResult r = run_query_batch(sc, d_query, bs, nullptr, 0, &d_rows, d_overflow, s, &timer);
+      if (d_overflow) RTDL_CUDA_CHECK(cudaMemcpyAsync(overflow_out, d_overflow, nq, cudaMemcpyDeviceToHost, s));
+      void* host = download_rows(d_rows, sizeof(RtdlFixedRadiusNeighborRow) * r.rows, s);
+      timer.mark("download");
+      timer.publish();
+      *rows_out = static_cast<RtdlFixedRadiusNeighborRow*>(host);
+    } catch (...) {
+      dev_free(d_rows, s);
+      dev_free(d_query, s);
+      dev_free(d_overflow, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(d_rows, s);
+    dev_free(d_query, s);
+    dev_free(d_overflow, s);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_batch_fixed_radius_neighbors_device(void* batch, const void* query_points_dev,
+                                                  const unsigned long long* query_offsets, const double* radius,
+                                                  const uint32_t* k_max, void* rows_dev, size_t rows_capacity,
+                                                  unsigned long long* row_offsets_out, uint8_t* overflow_dev,
+                                                  void* stream, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(batch);
+    if (!sc || sc->problems == 0) throw std::runtime_error("batch must be a problem batch handle");
+    if (!query_offsets || !radius || !k_max || !row_offsets_out)
+      throw std::runtime_error("query_offsets, radius, k_max and row_offsets_out must not be null");
+    BatchSpec bs;
+    bs.problems = sc->problems;
+    bs.qoff = query_offsets;
+    bs.radius = radius;
+    bs.kmax = k_max;
+    bs.row_offsets = row_offsets_out;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sc->stream;
+    PhaseTimer timer(s);
+    run_query_batch(sc, query_points_dev, bs, rows_dev, rows_capacity, nullptr, overflow_dev, s, &timer);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    timer.publish();
+  }, error_out, error_size);
+}
+
 int rtdl_b200_scene_directed_hausdorff(void* scene, const void* query_points, size_t query_count,
                                        double* distance_out, uint32_t* source_id_out, uint32_t* target_id_out,
                                        double* nearest_distance_out, uint32_t* nearest_id_out, char* error_out,

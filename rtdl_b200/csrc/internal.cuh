@@ -91,6 +91,7 @@ struct SceneView {
   const float4* nodes;    // 2 float4 per node, collapsed tree in pre-order
   uint32_t n;
   const unsigned int* inexact;  // device flag: scene coordinates are not all FP32-exact
+  const int* prob_root;   // problem batch: pre-order index of each problem's subtree (nullptr: one problem)
 };
 
 struct Scene {
@@ -107,6 +108,16 @@ struct Scene {
   float4* nodes = nullptr;
   uint32_t* codes = nullptr;    // Morton codes of the sorted points (seed nearest searches)
   PointStats* stats = nullptr;  // device copy of the build statistics
+  // A batch of independent problems (problems > 0) is built as one tree: the
+  // sort key is (problem << code_bits) | Morton code in the problem's own box,
+  // so every problem is one subtree; prob_root holds its pre-order index
+  // (kRopeEnd for a problem without points) and the subtree ends at that
+  // node's rope.
+  uint32_t problems = 0;
+  int code_bits = 0;
+  PointStats* prob_stats = nullptr;  // device, per problem: the box of its Morton codes
+  int* prob_root = nullptr;          // device, per problem
+  std::vector<unsigned long long> prob_offsets;  // host, problems + 1: input offsets of each problem's points
   SceneView view() const {
     SceneView v;
     v.pts = pts;
@@ -115,6 +126,7 @@ struct Scene {
     v.nodes = nodes;
     v.n = n;
     v.inexact = stats ? &stats->inexact : nullptr;
+    v.prob_root = prob_root;
     return v;
   }
 };
@@ -158,6 +170,21 @@ void iota_u32(uint32_t* out, uint32_t n, cudaStream_t s);
 // ---- scene build (lbvh.cu) -------------------------------------------------
 // `points` is a device AoS of RtdlPoint (dim 2) or RtdlPoint3D (dim 3).
 Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, int leaf_size);
+// Problem batch: points_dev holds the problems' points back to back, problem
+// p at [offsets[p], offsets[p + 1]) (host array of problems + 1 entries).
+Scene* build_scene_batch(const void* points_dev, const unsigned long long* offsets, uint32_t problems, int dim,
+                         cudaStream_t s, int leaf_size);
+// Bits of the problem id in a batch's sort keys, and the Morton bits below it.
+int batch_problem_bits(uint32_t problems);
+int batch_code_bits(uint32_t problems, int dim);
+// Per-point problem ids and per-problem boxes for points laid out by offsets_dev
+// (problems + 1 entries), then composite codes (p << code_bits) | Morton.
+void batch_problem_ids(const unsigned long long* offsets_dev, uint32_t problems, uint32_t n, uint32_t* pid,
+                       cudaStream_t s);
+void batch_boxes(const float4* pts, const uint32_t* pid, uint32_t n, PointStats* prob_stats, uint32_t problems,
+                 cudaStream_t s);
+void batch_codes(const float4* pts, const uint32_t* pid, uint32_t n, int dim, const PointStats* prob_stats,
+                 int code_bits, uint32_t* codes, cudaStream_t s);
 void destroy_scene(Scene* sc);
 // Converts AoS points to float4 (w = id bits) and accumulates statistics.
 void prep_points(const void* points_dev, uint32_t n, int dim, float4* out, PointStats* stats, cudaStream_t s);
@@ -173,6 +200,21 @@ struct QueryResult {
   unsigned long long rows = 0;   // total rows
   unsigned int heavy = 0;        // queries resolved by the generic path
 };
+
+// fixed_radius_neighbors over a batch of problems (see build_scene_batch):
+// problem p's queries are [qoff[p], qoff[p + 1]) of the query records, with
+// its own radius and kmax; rows come out problem by problem, each problem's
+// in the order a single query would give.
+struct BatchSpec {
+  uint32_t problems = 0;
+  const unsigned long long* qoff = nullptr;  // host, problems + 1
+  const double* radius = nullptr;            // host, problems
+  const uint32_t* kmax = nullptr;            // host, problems (1..64)
+  unsigned long long* row_offsets = nullptr; // host out, problems + 1: first row of each problem, then the total
+};
+QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec& bs, void* rows_dev,
+                            size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
+                            PhaseTimer* timer);
 
 // Runs a neighbor query on a scene.  All buffers are device buffers; rows are
 // written as RtdlFixedRadiusNeighborRow (kFrn) or RtdlKnnNeighborRow.  When

@@ -336,17 +336,31 @@ struct Ent {
   }
 };
 
+__device__ __forceinline__ uint32_t problem_of(uint32_t code, int code_bits) {
+  return code_bits >= 32 ? 0u : code >> code_bits;
+}
+
+// True when entity e's points belong to more than one problem of a batch
+// (codes == nullptr: a single problem).
+__device__ __forceinline__ bool spans_problems(const Ent& E, int e, const uint32_t* codes, int code_bits) {
+  return codes != nullptr && problem_of(codes[E.lo(e)], code_bits) != problem_of(codes[E.hi(e)], code_bits);
+}
+
 // Marks the nodes of the collapsed tree (flag bit 0) and its leaf buckets
-// (bit 1); a bucket sets leaf_start at its first point.
-__global__ void k_mark_collapsed(Ent E, int leaf_size, uint8_t* __restrict__ flags, uint32_t* __restrict__ leaf_start) {
+// (bit 1); a bucket sets leaf_start at its first point.  In a problem batch a
+// node whose points span problems is never a bucket, so each problem keeps a
+// subtree of its own.
+__global__ void k_mark_collapsed(Ent E, int leaf_size, const uint32_t* codes, int code_bits,
+                                 uint8_t* __restrict__ flags, uint32_t* __restrict__ leaf_start) {
   const int total = 2 * (int)E.n - 1;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
     const int par = e == 0 ? -1 : E.parent(e);
-    const bool in = e == 0 || (par >= 0 && E.hi(par) - E.lo(par) + 1 > leaf_size);
+    const bool in = e == 0 || (par >= 0 && (E.hi(par) - E.lo(par) + 1 > leaf_size ||
+                                            spans_problems(E, par, codes, code_bits)));
     uint8_t f = 0;
     if (in) {
       f = 1;
-      if (E.is_point(e) || E.hi(e) - E.lo(e) + 1 <= leaf_size) {
+      if (E.is_point(e) || (E.hi(e) - E.lo(e) + 1 <= leaf_size && !spans_problems(E, e, codes, code_bits))) {
         f |= 2;
         leaf_start[E.lo(e)] = 1u;
       }
@@ -399,6 +413,112 @@ __global__ void k_translate_ropes(const uint32_t* __restrict__ leaves_total, con
   }
 }
 
+// Problem batch: the subtree root of each problem is the collapsed-tree node
+// whose points lie in one problem while its parent's span several (or the
+// root itself).
+__global__ void k_batch_roots(Ent E, const uint8_t* __restrict__ flags, const uint32_t* __restrict__ codes,
+                              int code_bits, const int* __restrict__ ent2pre, int* __restrict__ prob_root) {
+  const int total = 2 * (int)E.n - 1;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    if (!(flags[e] & 1) || spans_problems(E, e, codes, code_bits)) continue;
+    if (e != 0 && !spans_problems(E, E.parent(e), codes, code_bits)) continue;
+    prob_root[problem_of(codes[E.lo(e)], code_bits)] = ent2pre[e];
+  }
+}
+
+__global__ void k_batch_single_root(const uint32_t* __restrict__ codes, int code_bits, int* __restrict__ prob_root) {
+  prob_root[problem_of(codes[0], code_bits)] = 0;
+}
+
+// Problem id of every point: one block per problem fills its range.
+__global__ void k_batch_ids(const unsigned long long* __restrict__ offsets, uint32_t* __restrict__ pid) {
+  const uint32_t p = blockIdx.x;
+  const unsigned long long a = offsets[p], b = offsets[p + 1];
+  for (unsigned long long i = a + threadIdx.x; i < b; i += blockDim.x) pid[i] = p;
+}
+
+// Per-problem boxes: a warp whose points share one problem reduces first and
+// issues one set of atomics; mixed warps fall back to per-lane atomics.
+__global__ void k_batch_boxes(const float4* __restrict__ pts, const uint32_t* __restrict__ pid, uint32_t n,
+                              PointStats* __restrict__ st) {
+  const int lane = threadIdx.x & 31;
+  for (uint64_t i0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull; i0 < n;
+       i0 += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = i0 + lane;
+    const bool valid = i < n;
+    const uint32_t p = valid ? pid[i] : 0xFFFFFFFFu;
+    const float4 q = valid ? pts[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float lo[3] = {valid ? q.x : INFINITY, valid ? q.y : INFINITY, valid ? q.z : INFINITY};
+    float hi[3] = {valid ? q.x : -INFINITY, valid ? q.y : -INFINITY, valid ? q.z : -INFINITY};
+    const uint32_t p0 = __shfl_sync(0xffffffffu, p, 0);
+    if (__all_sync(0xffffffffu, p == p0 || !valid)) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+          hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+      }
+      if (lane == 0 && p0 != 0xFFFFFFFFu) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          atomicMin(&st[p0].lo[a], float_to_ordered(lo[a]));
+          atomicMax(&st[p0].hi[a], float_to_ordered(hi[a]));
+        }
+      }
+    } else if (valid) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        atomicMin(&st[p].lo[a], float_to_ordered(lo[a]));
+        atomicMax(&st[p].hi[a], float_to_ordered(hi[a]));
+      }
+    }
+  }
+}
+
+__global__ void k_reset_stats_n(PointStats* st, uint32_t m) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    for (int a = 0; a < 3; ++a) {
+      st[i].lo[a] = 0xFFFFFFFFu;
+      st[i].hi[a] = 0u;
+    }
+    st[i].max_abs_bits = 0ull;
+    st[i].inexact = 0u;
+    st[i].bad = 0u;
+    st[i].ids_unsorted = 0u;
+    st[i].pad = 0u;
+  }
+}
+
+// Composite sort keys (problem << code_bits) | Morton code of the point in its
+// problem's box, code_bits / dim bits per axis.
+__global__ void k_batch_codes(const float4* __restrict__ pts, const uint32_t* __restrict__ pid, uint32_t n, int dim,
+                              const PointStats* __restrict__ st, int code_bits, uint32_t* __restrict__ codes) {
+  const int bpa = code_bits / dim;
+  const float cells = (float)((1u << bpa) - 1u);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = pid[i];
+    const float4 q = pts[i];
+    const float c[3] = {q.x, q.y, q.z};
+    uint32_t m[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const unsigned int ol = st[p].lo[a], oh = st[p].hi[a];
+      const float l = ol == 0xFFFFFFFFu ? 0.f : ordered_to_float(ol);
+      const float h = ol == 0xFFFFFFFFu ? 0.f : ordered_to_float(oh);
+      const float ext = h - l;
+      const float scale = (ext > 0.f && isfinite(ext)) ? cells / ext : 0.f;
+      float t = (c[a] - l) * scale;
+      t = fminf(fmaxf(t, 0.f), cells);
+      m[a] = (uint32_t)t;
+    }
+    const uint32_t mort = dim == 3 ? (spread10(m[0]) << 2) | (spread10(m[1]) << 1) | spread10(m[2])
+                                   : (spread16(m[0]) << 1) | spread16(m[1]);
+    codes[i] = (code_bits < 32 ? (p << code_bits) : 0u) | mort;
+  }
+}
+
 __global__ void k_narrow_u64(const uint64_t* __restrict__ in, uint64_t n, uint32_t* __restrict__ out) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     out[i] = (uint32_t)in[i];
@@ -434,12 +554,51 @@ void morton_codes(const float4* pts, uint32_t n, int dim, const PointStats* box_
   RTDL_LAUNCHED(1);
 }
 
-Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, int leaf_size) {
+int batch_problem_bits(uint32_t problems) {
+  int b = 0;
+  while (b < 32 && (1ull << b) < (unsigned long long)problems) ++b;
+  return b;
+}
+
+int batch_code_bits(uint32_t problems, int dim) {
+  int bits = 32 - batch_problem_bits(problems);
+  if (bits > (dim == 3 ? 30 : 32)) bits = dim == 3 ? 30 : 32;
+  return bits - bits % dim;
+}
+
+void batch_problem_ids(const unsigned long long* offsets_dev, uint32_t problems, uint32_t n, uint32_t* pid,
+                       cudaStream_t s) {
+  if (n == 0 || problems == 0) return;
+  k_batch_ids<<<problems, 256, 0, s>>>(offsets_dev, pid);
+  RTDL_LAUNCHED(1);
+}
+
+void batch_boxes(const float4* pts, const uint32_t* pid, uint32_t n, PointStats* prob_stats, uint32_t problems,
+                 cudaStream_t s) {
+  k_reset_stats_n<<<div_up(problems, 256), 256, 0, s>>>(prob_stats, problems);
+  RTDL_LAUNCHED(1);
+  if (n == 0) return;
+  k_batch_boxes<<<grid_for(n), kThreads, 0, s>>>(pts, pid, n, prob_stats);
+  RTDL_LAUNCHED(1);
+}
+
+void batch_codes(const float4* pts, const uint32_t* pid, uint32_t n, int dim, const PointStats* prob_stats,
+                 int code_bits, uint32_t* codes, cudaStream_t s) {
+  if (n == 0) return;
+  k_batch_codes<<<grid_for(n), kThreads, 0, s>>>(pts, pid, n, dim, prob_stats, code_bits, codes);
+  RTDL_LAUNCHED(1);
+}
+
+namespace {
+
+Scene* build_scene_impl(const void* points_dev, uint32_t n, int dim, cudaStream_t s, int leaf_size,
+                        const unsigned long long* offsets, uint32_t problems) {
   if (dim != 2 && dim != 3) throw std::runtime_error("dimension must be 2 or 3");
   if (n > (uint32_t)kMaxScenePoints)
     throw std::runtime_error("search_count exceeds the scene limit of 67,108,864 points");
   if (leaf_size < 1) leaf_size = 1;
   if (leaf_size > 32) leaf_size = 32;
+  const bool batch = offsets != nullptr;
   Scene* sc = new Scene();
   sc->dim = dim;
   sc->n = n;
@@ -448,15 +607,39 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
   RTDL_CUDA_CHECK(cudaGetDevice(&sc->device));
   sc->stats = static_cast<PointStats*>(dev_alloc(sizeof(PointStats), s));
   reset_stats(sc->stats, s);
-  if (n == 0) return sc;
+  if (batch) {
+    sc->problems = problems;
+    sc->code_bits = batch_code_bits(problems, dim);
+    sc->prob_offsets.assign(offsets, offsets + problems + 1);
+    sc->prob_stats = static_cast<PointStats*>(dev_alloc(sizeof(PointStats) * problems, s));
+    sc->prob_root = static_cast<int*>(dev_alloc(sizeof(int) * problems, s));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(sc->prob_root, 0xFF, sizeof(int) * problems, s));  // kRopeEnd: no points
+  }
+  if (n == 0) {
+    if (batch) batch_boxes(nullptr, nullptr, 0, sc->prob_stats, problems, s);
+    return sc;
+  }
   const double* raw = static_cast<const double*>(points_dev);
   float4* pts_in = static_cast<float4*>(dev_alloc(sizeof(float4) * n, s));
   prep_points(points_dev, n, dim, pts_in, sc->stats, s);
   uint32_t* codes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
-  morton_codes(pts_in, n, dim, sc->stats, codes, s);
+  if (batch) {
+    unsigned long long* d_off =
+        static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (problems + 1), s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(d_off, sc->prob_offsets.data(), sizeof(unsigned long long) * (problems + 1),
+                                    cudaMemcpyHostToDevice, s));
+    uint32_t* pid = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
+    batch_problem_ids(d_off, problems, n, pid, s);
+    batch_boxes(pts_in, pid, n, sc->prob_stats, problems, s);
+    batch_codes(pts_in, pid, n, dim, sc->prob_stats, sc->code_bits, codes, s);
+    dev_free(pid, s);
+    dev_free(d_off, s);
+  } else {
+    morton_codes(pts_in, n, dim, sc->stats, codes, s);
+  }
   sc->perm = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
   iota_u32(sc->perm, n, s);
-  radix_sort_pairs(codes, sc->perm, n, 0, dim == 3 ? 30 : 32, nullptr, s);
+  radix_sort_pairs(codes, sc->perm, n, 0, batch ? 32 : (dim == 3 ? 30 : 32), nullptr, s);
   sc->pts = static_cast<float4*>(dev_alloc(sizeof(float4) * n, s));
   sc->pts64 = static_cast<double*>(dev_alloc(sizeof(double) * 3 * (size_t)n, s));
   if (dim == 3)
@@ -492,7 +675,8 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
     int* ent2pre = static_cast<int*>(dev_alloc(sizeof(int) * ents, s));
     RTDL_CUDA_CHECK(cudaMemsetAsync(leaf_start, 0, sizeof(uint32_t) * n, s));
     RTDL_CUDA_CHECK(cudaMemsetAsync(ent2pre, 0xFF, sizeof(int) * ents, s));  // kRopeEnd for entities off the tree
-    k_mark_collapsed<<<grid_for(ents), kThreads, 0, s>>>(E, leaf_size, flags, leaf_start);
+    k_mark_collapsed<<<grid_for(ents), kThreads, 0, s>>>(E, leaf_size, batch ? codes : nullptr, sc->code_bits,
+                                                         flags, leaf_start);
     RTDL_LAUNCHED(1);
     scan_counts_u64(leaf_start, nullptr, nullptr, n, reinterpret_cast<unsigned long long*>(leaves_before), s);
     k_narrow_u64<<<grid_for(n + 1), kThreads, 0, s>>>(leaves_before, n + 1, leaves_before32);
@@ -501,6 +685,10 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
                                                   sc->nodes);
     k_translate_ropes<<<grid_for(ents), kThreads, 0, s>>>(leaves_before32 + n, ent2pre, sc->nodes);
     RTDL_LAUNCHED(3);
+    if (batch) {
+      k_batch_roots<<<grid_for(ents), kThreads, 0, s>>>(E, flags, codes, sc->code_bits, ent2pre, sc->prob_root);
+      RTDL_LAUNCHED(1);
+    }
     dev_free(child_l, s);
     dev_free(child_r, s);
     dev_free(first, s);
@@ -519,9 +707,32 @@ Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, 
     sc->nodes = static_cast<float4*>(dev_alloc(sizeof(float4) * 2, s));
     k_single_point<<<1, 1, 0, s>>>(sc->pts, sc->nodes);
     RTDL_LAUNCHED(1);
+    if (batch) {
+      k_batch_single_root<<<1, 1, 0, s>>>(codes, sc->code_bits, sc->prob_root);
+      RTDL_LAUNCHED(1);
+    }
   }
   sc->codes = codes;  // kept: nearest searches seed from a window around the query's code
   return sc;
+}
+
+}  // namespace
+
+Scene* build_scene(const void* points_dev, uint32_t n, int dim, cudaStream_t s, int leaf_size) {
+  return build_scene_impl(points_dev, n, dim, s, leaf_size, nullptr, 0);
+}
+
+Scene* build_scene_batch(const void* points_dev, const unsigned long long* offsets, uint32_t problems, int dim,
+                         cudaStream_t s, int leaf_size) {
+  if (problems == 0) throw std::runtime_error("a problem batch needs at least one problem");
+  for (uint32_t p = 0; p < problems; ++p)
+    if (offsets[p + 1] < offsets[p]) throw std::runtime_error("problem offsets must be non-decreasing");
+  if (offsets[0] != 0) throw std::runtime_error("problem offsets must start at 0");
+  if (offsets[problems] > (unsigned long long)kMaxScenePoints)
+    throw std::runtime_error("a problem batch holds at most 67,108,864 search points");
+  if (batch_problem_bits(problems) > 26)
+    throw std::runtime_error("a problem batch holds at most 67,108,864 problems");
+  return build_scene_impl(points_dev, (uint32_t)offsets[problems], dim, s, leaf_size, offsets, problems);
 }
 
 void destroy_scene(Scene* sc) {
@@ -533,6 +744,8 @@ void destroy_scene(Scene* sc) {
   dev_free(sc->nodes, s);
   dev_free(sc->codes, s);
   dev_free(sc->stats, s);
+  dev_free(sc->prob_stats, s);
+  dev_free(sc->prob_root, s);
   if (sc->own_stream && s) {
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);

@@ -53,9 +53,7 @@ struct DevBands {
 //   |d_fp32 - d| <= 3u*d + 3.5u*M (u = 2^-24, M = max |coordinate|; the M
 //   term is absent when every coordinate is FP32-exact).
 // The bands below are wider: relative 1e-5 and absolute 8u*M.
-__global__ void k_bands(const PointStats* scene, const PointStats* queries, double radius, int has_radius,
-                        DevBands* out) {
-  if (threadIdx.x != 0) return;
+__device__ DevBands make_bands(const PointStats* scene, const PointStats* queries, double radius, int has_radius) {
   const double M = fmax(__longlong_as_double((long long)scene->max_abs_bits),
                         __longlong_as_double((long long)queries->max_abs_bits));
   const bool inexact = scene->inexact || queries->inexact;
@@ -83,7 +81,23 @@ __global__ void k_bands(const PointStats* scene, const PointStats* queries, doub
     b.box_hi2 = INFINITY;
     b.r2 = INFINITY;
   }
-  *out = b;
+  return b;
+}
+
+__global__ void k_bands(const PointStats* scene, const PointStats* queries, double radius, int has_radius,
+                        DevBands* out) {
+  if (threadIdx.x == 0) *out = make_bands(scene, queries, radius, has_radius);
+}
+
+// Problem batch: bands per problem (the statistics are the whole batch's, which
+// only widens the bands); ids_sorted from the batch's per-problem check.
+__global__ void k_bands_batch(const PointStats* scene, const PointStats* queries, const double* radius, uint32_t m,
+                              const unsigned int* ids_sorted, DevBands* out) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x) {
+    DevBands b = make_bands(scene, queries, radius[p], 1);
+    b.ids_sorted = *ids_sorted;
+    out[p] = b;
+  }
 }
 
 struct Ctx {
@@ -400,22 +414,26 @@ __device__ __forceinline__ unsigned long long slab_entry(float key, uint32_t i) 
 struct QueryInfo {
   double ex, ey, ez;  // exact query coordinates (z = 0 in 2D)
   uint32_t qid;
-  uint32_t meta;      // candidate count (<= kSlab) and the kQuery* bits
+  uint32_t meta;      // candidate count (<= kSlab), the kQuery* bits and the query's kmax (<= 64)
 };
 constexpr uint32_t kQueryCountMask = 0xFFFFu;
 constexpr uint32_t kQueryGeneric = 1u << 16;   // more than kSlab candidates: generic path
 constexpr uint32_t kQueryBig = 1u << 17;       // 65..kSlab candidates: k_emit_list
 constexpr uint32_t kQueryOverflow = 1u << 18;  // more in-radius points than kmax
+constexpr int kQueryKmaxShift = 19;            // bits 19..25: kmax
+__device__ __forceinline__ int query_kmax(uint32_t meta) { return (int)((meta >> kQueryKmaxShift) & 127u); }
 
 struct CollectParams {
   SceneView S;
   const float4* qpts;
   const double* qraw;
   int qstride;
-  const uint32_t* qorder;
-  uint32_t nq;
+  const uint32_t* qorder;    // processing rank -> query input index (kNone: padding of a problem batch)
+  uint32_t nq;               // processing ranks (a batch pads every problem to whole warps)
   uint32_t kmax;
-  const DevBands* bands;
+  const DevBands* bands;     // one per problem (one in all for a single problem)
+  const uint32_t* warp_prob; // problem batch: the problem of each warp of processing ranks (nullptr: single)
+  const uint32_t* prob_kmax; // problem batch: kmax per problem
   unsigned long long* slab;  // kSlab entries per query, see slab_base()
   uint32_t* counts;          // min(count, kmax), query input order
   QueryInfo* qinfo;          // by processing rank
@@ -461,7 +479,7 @@ __device__ __forceinline__ void collect_point(const CollectParams& P, const DevB
 }
 
 template <bool STATS>
-__device__ __forceinline__ void collect_finish(const CollectParams& P, const CollectLane& L) {
+__device__ __forceinline__ void collect_finish(const CollectParams& P, const CollectLane& L, uint32_t kmax) {
   if (STATS) {
     atomicAdd(&P.stats[kStatNodes], L.st_nodes);
     atomicAdd(&P.stats[kStatLeafPoints], L.st_points);
@@ -470,7 +488,7 @@ __device__ __forceinline__ void collect_finish(const CollectParams& P, const Col
     atomicAdd(&P.stats[kStatLeafPairs], L.st_pairs);
     atomicMax(&P.stats[kStatMaxLeafPoints], (unsigned long long)L.count);
   }
-  const uint32_t count = L.count, kmax = P.kmax;
+  const uint32_t count = L.count;
   P.counts[L.qin] = count < kmax ? count : kmax;
   uint8_t fl = count > kmax ? 1 : 0;
   if (count > (uint32_t)kSlab) {
@@ -491,7 +509,7 @@ __device__ __forceinline__ void collect_finish(const CollectParams& P, const Col
   qi.ez = L.ez;
   qi.qid = __float_as_uint(L.q.w);
   qi.meta = (count < (uint32_t)kSlab ? count : (uint32_t)kSlab) | ((fl & 1) ? kQueryOverflow : 0u) |
-            ((fl & 2) ? kQueryGeneric : 0u) | ((fl & 4) ? kQueryBig : 0u);
+            ((fl & 2) ? kQueryGeneric : 0u) | ((fl & 4) ? kQueryBig : 0u) | (kmax << kQueryKmaxShift);
   P.qinfo[L.t] = qi;
   P.flags[L.qin] = fl;
   if (P.overflow_out) P.overflow_out[L.qin] = fl & 1;
@@ -559,7 +577,7 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
     }
     collect_leaf<STATS>(P, B, scene_inexact, L, first, cnt, true);
   }
-  collect_finish<STATS>(P, L);
+  collect_finish<STATS>(P, L, P.kmax);
 }
 
 // One warp per 32 Morton-consecutive queries (packet traversal): the warp
@@ -573,9 +591,13 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
 template <bool STATS, bool CUBE, int MIN_BLOCKS>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParams P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = t < P.nq;
-  if (!__any_sync(0xffffffffu, valid)) return;  // whole warp past the end
-  const DevBands B = *P.bands;
+  if (!__any_sync(0xffffffffu, t < P.nq)) return;  // whole warp past the end
+  // a problem batch pads every problem to whole warps, so a warp has one problem
+  const uint32_t prob = P.warp_prob ? P.warp_prob[t >> 5] : 0u;
+  const bool valid = t < P.nq && (P.warp_prob == nullptr || P.qorder[t] != kNone);
+  if (!valid && t < P.nq) P.qinfo[t] = QueryInfo{0.0, 0.0, 0.0, 0u, 0u};  // padding: nothing to emit
+  const DevBands B = P.bands[prob];
+  const uint32_t kmax = P.prob_kmax ? P.prob_kmax[prob] : P.kmax;
   const SceneView& S = P.S;
   const int scene_inexact = *S.inexact;
   CollectLane L;
@@ -593,8 +615,13 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParam
     clo = make_float3(__fsub_rd(L.q.x, h), __fsub_rd(L.q.y, h), __fsub_rd(L.q.z, h));
     chi = make_float3(__fadd_ru(L.q.x, h), __fadd_ru(L.q.y, h), __fadd_ru(L.q.z, h));
   }
-  int cur = S.n > 0 ? 0 : kRopeEnd;
-  while (cur != kRopeEnd) {
+  // the walk covers the problem's subtree: from its root to the root's rope
+  int cur = S.n > 0 ? 0 : kRopeEnd, end = kRopeEnd;
+  if (S.prob_root) {
+    cur = S.prob_root[prob];
+    if (cur != kRopeEnd) end = __float_as_int(__ldg(&S.nodes[2 * cur + 1]).w);
+  }
+  while (cur != end) {
     const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
     if (STATS) ++L.st_nodes;
     const int hit = __float_as_int(a.w);
@@ -617,7 +644,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParam
     }
     cur = __float_as_int(b.w);
   }
-  if (valid) collect_finish<STATS>(P, L);
+  if (valid) collect_finish<STATS>(P, L, kmax);
 }
 
 // ---- emit: warp per query -----------------------------------------------------
@@ -647,7 +674,6 @@ struct EmitParams {
   unsigned long long* slab;
   const QueryInfo* qinfo;     // by processing rank
   const unsigned long long* poff;  // first row of each query, by processing rank
-  uint32_t kmax;
   RowSink sink;
   uint32_t* fix_list;         // processing ranks queued for k_emit_fixup
   unsigned int* fix_count;
@@ -783,24 +809,26 @@ __device__ __forceinline__ void emit_query(const EmitParams& P, uint32_t t, cons
   const double ex = q.qi.ex, ey = q.qi.ey, ez = q.qi.ez;
   const int inexact = *P.S.inexact;
   if (__any_sync(0xffffffffu, amb)) {
-    if (DEFER) {
-      static_assert(!DEFER || E <= 4, "a deferred query needs spare slab entries");
+    if constexpr (DEFER) {
+      static_assert(E <= 4, "a deferred query needs spare slab entries");
       uint32_t* spare = deferred_keys(P.slab, t, n);
 #pragma unroll
       for (int r = 0; r < E; ++r) spare[(r << 5) | lane] = v[r];
       if (lane == 0) P.fix_list[atomicAdd(P.fix_count, 1u)] = t;
       return;
+    } else {
+#pragma unroll
+      for (int r = 0; r < E; ++r) wbuf[(r << 5) | lane] = v[r];
+      __syncwarp();
+      if (lane == 0) exact_fixup_sorted(wbuf, n, SHIFT, ent, P.S, inexact, ex, ey, ez);
+      __syncwarp();
+#pragma unroll
+      for (int r = 0; r < E; ++r) v[r] = wbuf[(r << 5) | lane];
+      __syncwarp();
     }
-#pragma unroll
-    for (int r = 0; r < E; ++r) wbuf[(r << 5) | lane] = v[r];
-    __syncwarp();
-    if (lane == 0) exact_fixup_sorted(wbuf, n, SHIFT, ent, P.S, inexact, ex, ey, ez);
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < E; ++r) v[r] = wbuf[(r << 5) | lane];
-    __syncwarp();
   }
-  const int kk = n < (int)P.kmax ? n : (int)P.kmax;
+  const int kmax = query_kmax(q.qi.meta);
+  const int kk = n < kmax ? n : kmax;
 #pragma unroll
   for (int r = 0; r < E; ++r) {
     const int i = (r << 5) | lane;
@@ -899,7 +927,8 @@ __global__ void __launch_bounds__(kFixupThreads) k_emit_fixup(EmitParams P) {
       if (!__any_sync(0xffffffffu, changed)) break;
     }
     const unsigned long long base = P.poff[t];
-    const int kk = n < (int)P.kmax ? n : (int)P.kmax;
+    const int kmax = query_kmax(qi.meta);
+    const int kk = n < kmax ? n : kmax;
     for (int i = lane; i < kk; i += 32) {
       const uint32_t idx = (uint32_t)ent[keys[i] & mask];
       const float4 p = __ldg(&P.S.pts[idx]);
@@ -913,8 +942,10 @@ __global__ void __launch_bounds__(kFixupThreads) k_emit_fixup(EmitParams P) {
 // Row offsets in processing order: poff[t] = offsets[qrank[qorder[t]]].
 __global__ void k_proc_offsets(const uint32_t* qorder, const uint32_t* qrank, const unsigned long long* offsets,
                                uint32_t nq, unsigned long long* poff) {
-  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += (uint64_t)gridDim.x * blockDim.x)
-    poff[t] = offsets[qrank[qorder[t]]];
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t qin = qorder[t];
+    poff[t] = qin == kNone ? 0ull : offsets[qrank[qin]];
+  }
 }
 
 // One warp per query of a work list (processing ranks): E = 4 for 65..128
@@ -933,6 +964,38 @@ __global__ void __launch_bounds__(kEmitListThreads) k_emit_list(EmitParams P, co
   emit_load(P, t, lane, q);
   const int n = (int)(q.qi.meta & kQueryCountMask);
   emit_query<E, DEFER>(P, t, q, n, lane, DEFER ? nullptr : wbuf[threadIdx.x >> 5]);
+}
+
+// Problem batch: *flag stays nonzero while every problem's query ids ascend.
+__global__ void k_batch_ids_sorted(const float4* qpts, const uint32_t* qprob, uint32_t n, unsigned int* flag) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    if (qprob[i] == qprob[i - 1] && __float_as_uint(qpts[i].w) < __float_as_uint(qpts[i - 1].w)) *flag = 0u;
+}
+
+// Problem batch: one block per problem copies its sorted queries to the padded
+// processing order (kNone fills the last warp) and records each warp's problem.
+__global__ void k_batch_pad(const unsigned long long* qoff, const unsigned long long* pstart, const uint32_t* sorted,
+                            uint32_t* qorder, uint32_t* warp_prob) {
+  const uint32_t p = blockIdx.x;
+  const unsigned long long a = qoff[p], nqp = qoff[p + 1] - a, base = pstart[p], padded = pstart[p + 1] - base;
+  for (unsigned long long j = threadIdx.x; j < padded; j += blockDim.x) {
+    qorder[base + j] = j < nqp ? sorted[a + j] : kNone;
+    if ((j & 31) == 0) warp_prob[(base + j) >> 5] = p;
+  }
+}
+
+// keys[j] = src[order[j]] (skipped when *skip is nonzero).
+__global__ void k_gather_u32(const uint32_t* src, const uint32_t* order, uint32_t n, const unsigned int* skip,
+                             uint32_t* keys) {
+  if (*skip) return;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+    keys[j] = src[order[j]];
+}
+
+// out[p] = offsets[qoff[p]]: the first row of each problem (and the total).
+__global__ void k_problem_rows(const unsigned long long* offsets, const unsigned long long* qoff, uint32_t m,
+                               unsigned long long* out) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p <= m; p += gridDim.x * blockDim.x) out[p] = offsets[qoff[p]];
 }
 
 __global__ void k_invert(const uint32_t* order, uint32_t n, const unsigned int* identity_flag, uint32_t* inv) {
@@ -1036,18 +1099,23 @@ __global__ void __launch_bounds__(kHeavyThreads)
 __global__ void __launch_bounds__(32)
     k_heavy_gather_bvh(SceneView S, const float4* qpts, const double* qraw, int qstride, const uint32_t* heavy_list,
                        const unsigned long long* seg_off, const uint32_t* seg_size, const DevBands* bands,
-                       HeavyEntry* scratch, unsigned int* error) {
+                       const uint32_t* qprob, HeavyEntry* scratch, unsigned int* error) {
   const int lane = threadIdx.x;
   const uint32_t h = blockIdx.x;
   const uint32_t qin = heavy_list[h];
-  const DevBands B = *bands;
+  const uint32_t prob = qprob ? qprob[qin] : 0u;
+  const DevBands B = bands[prob];
   const Ctx c = make_ctx(S, qpts, qraw, qstride, qin, B);
   HeavyEntry* seg = scratch + seg_off[h];
   const uint32_t P2 = seg_size[h];
   const unsigned int lt_mask = (1u << lane) - 1u;
   uint32_t cnt = 0;
-  int cur = S.n > 0 ? 0 : kRopeEnd;
-  while (cur != kRopeEnd) {  // warp-uniform: every lane follows the same nodes
+  int cur = S.n > 0 ? 0 : kRopeEnd, end = kRopeEnd;
+  if (S.prob_root) {  // problem batch: the query's problem subtree only
+    cur = S.prob_root[prob];
+    if (cur != kRopeEnd) end = __float_as_int(__ldg(&S.nodes[2 * cur + 1]).w);
+  }
+  while (cur != end) {  // warp-uniform: every lane follows the same nodes
     const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
     const int hit = __float_as_int(a.w);
     if (box_d2(c.qx, c.qy, c.qz, a, b) <= B.box_hi2) {
@@ -1347,11 +1415,21 @@ inline uint32_t next_pow2(uint32_t v) {
 struct QueryPrep {
   PointStats* qst = nullptr;
   float4* qpts = nullptr;
-  DevBands* bands = nullptr;
-  uint32_t* qorder = nullptr;
-  uint32_t* qcodes = nullptr;  // Morton codes in processing order (qcodes[t] belongs to qorder[t])
+  DevBands* bands = nullptr;   // one, or one per problem of a batch
+  uint32_t* qorder = nullptr;  // processing rank -> input index (a batch pads problems to whole warps: kNone)
+  uint32_t* qcodes = nullptr;  // Morton codes in processing order (qcodes[t] belongs to qorder[t]); single only
   uint32_t* oorder = nullptr;
+  uint32_t nproc = 0;          // processing ranks
+  const unsigned int* order_identity = nullptr;  // device flag: output order == input order
+  // problem batch only
+  uint32_t* qprob = nullptr;      // problem of each query (input order)
+  uint32_t* warp_prob = nullptr;  // problem of each warp of processing ranks
+  uint32_t* prob_kmax = nullptr;
+  unsigned int* sorted_flag = nullptr;
+  unsigned long long* qoff = nullptr;  // device copy of the query offsets
 };
+
+
 
 QueryPrep prepare_queries(Scene* sc, const void* queries_dev, uint32_t nq, bool has_radius, double radius,
                           bool want_output_order, cudaStream_t s) {
@@ -1364,6 +1442,8 @@ QueryPrep prepare_queries(Scene* sc, const void* queries_dev, uint32_t nq, bool 
   prep_points(queries_dev, nq, sc->dim, qp.qpts, qp.qst, s);
   k_bands<<<1, 32, 0, s>>>(sc->stats, qp.qst, radius, has_radius ? 1 : 0, qp.bands);
   RTDL_LAUNCHED(1);
+  qp.nproc = nq;
+  qp.order_identity = &qp.bands->ids_sorted;
   qp.qcodes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   morton_codes(qp.qpts, nq, sc->dim, sc->stats, qp.qcodes, s);
   iota_u32(qp.qorder, nq, s);
@@ -1380,6 +1460,70 @@ QueryPrep prepare_queries(Scene* sc, const void* queries_dev, uint32_t nq, bool 
   return qp;
 }
 
+// A problem batch's query preparation: per-query problem ids, per-problem
+// bands and kmax, composite (problem, Morton) sort, processing order padded
+// so each warp holds queries of one problem, and the output order (problem,
+// then query id, stable).
+QueryPrep prepare_queries_batch(Scene* sc, const void* queries_dev, uint32_t nq, const BatchSpec& bs,
+                                cudaStream_t s) {
+  const uint32_t P = bs.problems;
+  QueryPrep qp;
+  std::vector<unsigned long long> pstart(P + 1, 0);
+  for (uint32_t p = 0; p < P; ++p) pstart[p + 1] = pstart[p] + (bs.qoff[p + 1] - bs.qoff[p] + 31) / 32 * 32;
+  if (pstart[P] > 0xFFFFFFFFull - 32) throw std::runtime_error("problem batch has too many queries");
+  qp.nproc = (uint32_t)pstart[P];
+  qp.qst = static_cast<PointStats*>(dev_alloc(sizeof(PointStats), s));
+  qp.qpts = static_cast<float4*>(dev_alloc(sizeof(float4) * (nq ? nq : 1), s));
+  qp.bands = static_cast<DevBands*>(dev_alloc(sizeof(DevBands) * P, s));
+  qp.qorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (qp.nproc ? qp.nproc : 1), s));
+  qp.qprob = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (nq ? nq : 1), s));
+  qp.warp_prob = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (qp.nproc / 32 + 1), s));
+  qp.prob_kmax = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * P, s));
+  qp.sorted_flag = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int), s));
+  qp.qoff = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (P + 1), s));
+  qp.order_identity = qp.sorted_flag;
+  unsigned long long* d_pstart = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (P + 1), s));
+  double* d_radius = static_cast<double*>(dev_alloc(sizeof(double) * P, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(qp.qoff, bs.qoff, sizeof(unsigned long long) * (P + 1), cudaMemcpyHostToDevice, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(d_pstart, pstart.data(), sizeof(unsigned long long) * (P + 1),
+                                  cudaMemcpyHostToDevice, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(d_radius, bs.radius, sizeof(double) * P, cudaMemcpyHostToDevice, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(qp.prob_kmax, bs.kmax, sizeof(uint32_t) * P, cudaMemcpyHostToDevice, s));
+  RTDL_CUDA_CHECK(cudaMemsetAsync(qp.sorted_flag, 0xFF, sizeof(unsigned int), s));  // nonzero: sorted
+  reset_stats(qp.qst, s);
+  prep_points(queries_dev, nq, sc->dim, qp.qpts, qp.qst, s);
+  batch_problem_ids(qp.qoff, P, nq, qp.qprob, s);
+  if (nq > 1) {
+    k_batch_ids_sorted<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, qp.qprob, nq, qp.sorted_flag);
+    RTDL_LAUNCHED(1);
+  }
+  k_bands_batch<<<div_up(P, 128), 128, 0, s>>>(sc->stats, qp.qst, d_radius, P, qp.sorted_flag, qp.bands);
+  RTDL_LAUNCHED(1);
+  // processing order: composite (problem, Morton in the problem's box) sort, padded per problem
+  uint32_t* codes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (nq ? nq : 1), s));
+  uint32_t* sorted = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (nq ? nq : 1), s));
+  batch_codes(qp.qpts, qp.qprob, nq, sc->dim, sc->prob_stats, sc->code_bits, codes, s);
+  iota_u32(sorted, nq, s);
+  radix_sort_pairs(codes, sorted, nq, 0, 32, nullptr, s);
+  k_batch_pad<<<P, 256, 0, s>>>(qp.qoff, d_pstart, sorted, qp.qorder, qp.warp_prob);
+  RTDL_LAUNCHED(1);
+  // output order: by query id, then (stable) by problem; skipped when every
+  // problem's ids are already ascending
+  qp.oorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (nq ? nq : 1), s));
+  iota_u32(qp.oorder, nq, s);
+  k_extract_ids<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, codes);
+  RTDL_LAUNCHED(1);
+  radix_sort_pairs(codes, qp.oorder, nq, 0, 32, qp.sorted_flag, s);
+  k_gather_u32<<<grid_for(nq, 256), 256, 0, s>>>(qp.qprob, qp.oorder, nq, qp.sorted_flag, codes);
+  RTDL_LAUNCHED(1);
+  radix_sort_pairs(codes, qp.oorder, nq, 0, batch_problem_bits(P), qp.sorted_flag, s);
+  dev_free(codes, s);
+  dev_free(sorted, s);
+  dev_free(d_pstart, s);
+  dev_free(d_radius, s);
+  return qp;
+}
+
 void free_prep(QueryPrep& qp, cudaStream_t s) {
   dev_free(qp.qst, s);
   dev_free(qp.qpts, s);
@@ -1387,6 +1531,11 @@ void free_prep(QueryPrep& qp, cudaStream_t s) {
   dev_free(qp.qorder, s);
   dev_free(qp.qcodes, s);
   dev_free(qp.oorder, s);
+  dev_free(qp.qprob, s);
+  dev_free(qp.warp_prob, s);
+  dev_free(qp.prob_kmax, s);
+  dev_free(qp.sorted_flag, s);
+  dev_free(qp.qoff, s);
 }
 
 }  // namespace
@@ -1448,7 +1597,7 @@ GenericOut run_generic_path(Scene* sc, const QueryPrep& qp, const void* queries_
                                                heavy_list, d_seg_off, d_seg_size, 1, qp.bands, scratch, error);
   else
     k_heavy_gather_bvh<<<H, 32, 0, s>>>(sc->view(), qp.qpts, static_cast<const double*>(queries_dev), qstride,
-                                        heavy_list, d_seg_off, d_seg_size, qp.bands, scratch, error);
+                                        heavy_list, d_seg_off, d_seg_size, qp.bands, qp.qprob, scratch, error);
   k_heavy_sort<<<H, kHeavyThreads, sizeof(HeavyEntry) * kHeavySmemEntries, s>>>(d_seg_off, d_seg_size, scratch,
                                                                                 sc->perm);
   k_heavy_emit<<<H, kHeavyThreads, 0, s>>>(d_seg_off, g.heavy_out_off, d_out_cnt, scratch, g.heavy_out);
@@ -1469,31 +1618,41 @@ void check_readback(const Readback& r) {
 // fixed_radius_neighbors / bounded_knn_rows: collect, scan, emit.
 QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius,
                              uint32_t kmax, void* rows_dev, size_t rows_capacity, void** rows_alloc,
-                             uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer) {
+                             uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer, const BatchSpec* bs = nullptr) {
   QueryResult res;
   const int qstride = sc->dim == 3 ? 4 : 3;
-  QueryPrep qp = prepare_queries(sc, queries_dev, nq, true, radius, true, s);
-  uint32_t* qrank = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  k_invert<<<grid_for(nq, 256), 256, 0, s>>>(qp.oorder, nq, &qp.bands->ids_sorted, qrank);
+  if (bs) {  // the largest kmax bounds the generic path's output
+    kmax = 1;
+    for (uint32_t p = 0; p < bs->problems; ++p) kmax = bs->kmax[p] > kmax ? bs->kmax[p] : kmax;
+  }
+  QueryPrep qp = bs ? prepare_queries_batch(sc, queries_dev, nq, *bs, s)
+                    : prepare_queries(sc, queries_dev, nq, true, radius, true, s);
+  const uint32_t np = qp.nproc;  // processing ranks
+  const size_t nq1 = nq ? nq : 1, np1 = np ? np : 1;
+  uint32_t* qrank = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
+  k_invert<<<grid_for(nq, 256), 256, 0, s>>>(qp.oorder, nq, qp.order_identity, qrank);
   RTDL_LAUNCHED(1);
   if (timer) timer->mark("query_prep");
   unsigned long long* slab =
-      static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * slab_base(nq), s));
-  uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  QueryInfo* qinfo = static_cast<QueryInfo*>(dev_alloc(sizeof(QueryInfo) * nq, s));
-  uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq, s));
-  uint32_t* heavy_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* heavy_m = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* mid_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* big_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* fix_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+      static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * slab_base((uint32_t)np1), s));
+  uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
+  QueryInfo* qinfo = static_cast<QueryInfo*>(dev_alloc(sizeof(QueryInfo) * np1, s));
+  uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq1, s));
+  uint32_t* heavy_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
+  uint32_t* heavy_m = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
+  uint32_t* mid_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * np1, s));
+  uint32_t* big_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * np1, s));
+  uint32_t* fix_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * np1, s));
   unsigned int* small = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * 8, s));
   unsigned long long* offsets = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (nq + 1), s));
-  unsigned long long* poff = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * nq, s));
+  unsigned long long* poff = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * np1, s));
+  unsigned long long* prob_rows =
+      bs ? static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (bs->problems + 1), s)) : nullptr;
   RTDL_CUDA_CHECK(cudaMemsetAsync(small, 0, sizeof(unsigned int) * 8, s));
   GenericOut g;
   auto cleanup = [&]() {
     g.release(s);
+    dev_free(prob_rows, s);
     dev_free(poff, s);
     dev_free(qrank, s);
     dev_free(slab, s);
@@ -1516,9 +1675,11 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     C.qraw = static_cast<const double*>(queries_dev);
     C.qstride = qstride;
     C.qorder = qp.qorder;
-    C.nq = nq;
+    C.nq = np;
     C.kmax = kmax;
     C.bands = qp.bands;
+    C.warp_prob = qp.warp_prob;
+    C.prob_kmax = qp.prob_kmax;
     C.slab = slab;
     C.counts = counts;
     C.qinfo = qinfo;
@@ -1537,9 +1698,9 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     }
     const int threads = tuning().block_threads;
     if (timer) timer->mark("setup");
-    const bool packet = tuning().traversal != 1;
+    const bool packet = tuning().traversal != 1 || bs != nullptr;  // a problem batch walks in packets
     if (packet) {
-      const unsigned int grid = div_up(nq, threads);
+      const unsigned int grid = div_up(np, threads);
       const bool cube = tuning().traversal == 2;
       // occupancy bounds chosen so neither variant spills (32 and 40 registers)
       if (stats)
@@ -1561,7 +1722,13 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       dev_free(C.stats, s);
     }
     if (timer) timer->mark("traverse");
-    scan_counts_u64(counts, qp.oorder, &qp.bands->ids_sorted, nq, offsets, s);
+    scan_counts_u64(counts, qp.oorder, qp.order_identity, nq, offsets, s);
+    if (bs) {
+      k_problem_rows<<<div_up(bs->problems + 1, 256), 256, 0, s>>>(offsets, qp.qoff, bs->problems, prob_rows);
+      RTDL_LAUNCHED(1);
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(bs->row_offsets, prob_rows, sizeof(unsigned long long) * (bs->problems + 1),
+                                      cudaMemcpyDeviceToHost, s));
+    }
     if (timer) timer->mark("scan");
     Readback* rb = pinned_readback();
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -1587,21 +1754,20 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       rows_capacity = res.rows;
       *rows_alloc = rows_dev;
     }
-    k_proc_offsets<<<grid_for(nq, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, nq, poff);
+    k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, np, poff);
     RTDL_LAUNCHED(1);
     EmitParams E;
     E.S = sc->view();
-    E.nq = nq;
+    E.nq = np;
     E.slab = slab;
     E.qinfo = qinfo;
     E.poff = poff;
-    E.kmax = kmax;
     E.sink.rows = rows_dev;
     E.sink.capacity = rows_dev ? rows_capacity : 0;
     E.sink.ranked = predicate == kFrn ? 0 : 1;
     E.fix_list = fix_list;
     E.fix_count = small + 4;
-    k_emit<<<div_up((uint64_t)nq * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
+    k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
     RTDL_LAUNCHED(1);
     if (r.mid > 0) {
       k_emit_list<4, true><<<div_up((uint64_t)r.mid * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, mid_list,
@@ -1658,11 +1824,33 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
 
 }  // namespace
 
+QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec& bs, void* rows_dev,
+                            size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
+                            PhaseTimer* timer) {
+  if (rows_alloc) *rows_alloc = nullptr;
+  if (sc->problems != bs.problems) throw std::runtime_error("query batch and scene batch differ in problem count");
+  if (bs.qoff[0] != 0) throw std::runtime_error("query offsets must start at 0");
+  for (uint32_t p = 0; p < bs.problems; ++p) {
+    if (bs.qoff[p + 1] < bs.qoff[p]) throw std::runtime_error("query offsets must be non-decreasing");
+    if (!(bs.radius[p] >= 0.0)) throw std::runtime_error("radius must be non-negative");
+    if (bs.kmax[p] < 1 || bs.kmax[p] > 64) throw std::runtime_error("a problem batch takes k_max in [1, 64]");
+  }
+  const unsigned long long nq = bs.qoff[bs.problems];
+  if (nq > 0xFFFFFFFFull) throw std::runtime_error("query_count exceeds uint32 limit");
+  if (nq == 0 || sc->n == 0) {
+    for (uint32_t p = 0; p <= bs.problems; ++p) bs.row_offsets[p] = 0;
+    return QueryResult{};
+  }
+  return run_radius_query(sc, queries_dev, (uint32_t)nq, kFrn, 0.0, 0, rows_dev, rows_capacity, rows_alloc,
+                          overflow_dev, s, timer, &bs);
+}
+
 QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius, uint32_t limit,
                       void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
                       PhaseTimer* timer) {
   QueryResult res;
   if (rows_alloc) *rows_alloc = nullptr;
+  if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
   const bool knn = predicate == kKnn;
   const int qstride = sc->dim == 3 ? 4 : 3;
   if (nq == 0) return res;
@@ -1819,6 +2007,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
 
 HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint32_t nq, double* nearest_dist_dev,
                                        uint32_t* nearest_id_dev, cudaStream_t s, PhaseTimer* timer) {
+  if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
   if (nq == 0 || sc->n == 0) throw std::runtime_error("Hausdorff distance requires non-empty point sets");
   const int qstride = sc->dim == 3 ? 4 : 3;
   if (timer) timer->mark("start");
@@ -1961,6 +2150,7 @@ unsigned char* noalloc_scratch_for_current_device() {
 
 void run_directed_hausdorff_noalloc(Scene* sc, const void* queries_dev, uint32_t nq, double* nearest_dist_dev,
                                     uint32_t* nearest_id_dev, RtdlB200Witness* witness_dev, cudaStream_t s) {
+  if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
   if (nq == 0 || sc->n == 0) throw std::runtime_error("Hausdorff distance requires non-empty point sets");
   if (nq > kNoAllocMaxQueries)
     throw std::runtime_error("rtdl_b200_scene_directed_hausdorff_noalloc: query_count exceeds the limit of 262144 "

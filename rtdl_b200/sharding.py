@@ -33,11 +33,17 @@ def shard_queries(query_records: np.ndarray, world: int, rank: int) -> np.ndarra
 
 
 def merge_rows(per_rank_rows: list[np.ndarray]) -> np.ndarray:
-    """Concatenates rank results in rank order (already globally ordered)."""
+    """Concatenates rank results in rank order (already globally ordered), keeping
+    the ABI row layout (np.concatenate would drop a structured dtype's padding)."""
     nonempty = [r for r in per_rank_rows if len(r)]
     if not nonempty:
         return per_rank_rows[0][:0] if per_rank_rows else np.zeros(0)
-    return np.concatenate(nonempty)
+    out = np.empty(sum(len(r) for r in nonempty), dtype=nonempty[0].dtype)
+    i = 0
+    for r in nonempty:
+        out[i: i + len(r)] = r
+        i += len(r)
+    return out
 
 
 def merge_directed_hausdorff(per_rank: list[dict]) -> dict:

@@ -514,6 +514,92 @@ def run_batch(args) -> int:
     return 0
 
 
+def serve_trace(seconds: float, rate: float, scenes: dict, pools: dict, seed: int = 6):
+    """Poisson arrivals: (arrival_s, scene, op, queries, radius, limit); probes per request log-uniform
+    [100, 1M] taken from the scene's probe pool; op uniform over fixed_radius_neighbors (k_max 64, radius for
+    ~32 neighbours at the scene's density) and knn_rows with k in {1, 8, 32}."""
+    from rtdl_b200.serve import FRN, KNN
+
+    rng = np.random.default_rng(seed)
+    names = sorted(scenes)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            return out
+        name = names[rng.integers(len(names))]
+        pool = pools[name]
+        n = min(len(pool), int(np.exp(rng.uniform(np.log(100), np.log(1 << 20)))))
+        a = int(rng.integers(0, len(pool) - n + 1))
+        q = pool[a: a + n]
+        op = int(rng.integers(4))
+        if op == 0:
+            out.append((t, name, FRN, q, RADIUS * ((1 << 20) / scenes[name]) ** (1.0 / 3.0), 64))
+        else:
+            out.append((t, name, KNN, q, 0.0, (1, 8, 32)[op - 1]))
+
+
+def run_serve(args) -> int:
+    """Served loop: resident scenes, Poisson arrivals, continuous batching, p50/p99 against the plain
+    per-call path on the same trace."""
+    import torch
+
+    import rtdl_b200 as rt
+    from rtdl_b200 import _native, workloads
+    from rtdl_b200.serve import B200Server, replay, run_plain, same_rows
+
+    torch.cuda.set_device(0)
+    rt.set_device(0)
+    rng = np.random.default_rng(6)
+    c = np.random.default_rng(0).random((64, 3))
+    sizes = np.exp(rng.uniform(np.log(100_000), np.log(8_000_000), args.scenes)).astype(np.int64)
+    points = {f"scene{i:02d}": workloads.records(workloads._mixture(np.random.default_rng(100 + i), int(n), c))
+              for i, n in enumerate(sizes)}
+    pools = {name: workloads.records(workloads._mixture(np.random.default_rng(200 + i), 1 << 20, c))
+             for i, name in enumerate(points)}
+    trace = serve_trace(args.serve_seconds, args.rate, {k: len(v) for k, v in points.items()}, pools)
+    with B200Server(memory_budget=120 << 30, streams=4) as server:
+        for name, p in points.items():
+            server.add_scene(name, p)
+        replay(server, trace[: min(len(trace), 32)], keep=set())  # warm-up: allocator pools, pinned buffers
+        server.completed.clear()
+        sample = set(np.random.default_rng(3).choice(len(trace), min(24, len(trace)), replace=False).tolist())
+        sampler = ClockSampler(0)
+        sampler.start()
+        launches0 = _native.launch_count()
+        reqs = replay(server, trace, keep=sample)  # rows of the sampled requests are kept for the check
+        launches = _native.launch_count() - launches0
+        clocks = sampler.stop()
+        served = server.stats()
+        failed = [r.error for r in reqs if r.error]
+        equal = True
+        for i in sorted(sample):  # exactness: the sampled requests against the plain call alone
+            r = reqs[i]
+            view = server.scenes[r.scene].query(r.queries, predicate=r.op, radius=r.radius, limit=r.limit)
+            equal &= same_rows(r.rows, view.to_numpy())
+            view.close()
+        plain = run_plain(server.scenes, reqs, [t[0] for t in trace])
+    line = {
+        "metric": f"served neighbor rows/s with continuous batching ({args.scenes} resident 3D scenes, "
+                  "Poisson arrivals)",
+        "value": served.get("rows_per_s"), "unit": "rows/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": served.get("seconds", 0) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 traversal + f64 band recheck and distances", "data": "synthetic",
+        "config": {"workload": f"{args.scenes} scenes, sizes log-uniform [100k, 8M] (clustered mixture), "
+                               f"{args.rate:.0f} req/s Poisson for {args.serve_seconds} s (seed 6), probes per "
+                               "request log-uniform [100, 1M], op uniform over FRN (k_max 64) and KNN k in "
+                               "{1, 8, 32}, 120 GB budget, 4 streams",
+                   "requests": len(trace), "scene_points": int(sizes.sum()),
+                   "timing": "host wall clock per request (arrival to rows in pinned host memory)"},
+        "served": served, "plain_per_call": plain,
+        "throughput_vs_plain": (served["rows_per_s"] / plain["rows_per_s"]) if served.get("rows_per_s") else None,
+        "exactness": {"requests_checked": len(sample), "rows_equal_to_plain_call": equal, "failed": len(failed)},
+        "e2e": None, "cpu_baseline": None, "roofline": None, "clocks": clocks, "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main(argv=None) -> int:
     global N_PROBE, N_BUILD
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -525,11 +611,15 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--probes", type=int, default=N_PROBE, help="probe points per GPU (profiling a smaller case)")
     ap.add_argument("--build", type=int, default=N_BUILD, help="build points (profiling a smaller case)")
-    ap.add_argument("--workload", choices=("frn", "knn", "hausdorff", "batch"), default="frn",
+    ap.add_argument("--workload", choices=("frn", "knn", "hausdorff", "batch", "serve"), default="frn",
                     help="frn: the headline fixed-radius config; knn: k=16 on the same 3D sets; "
                          "hausdorff: 4,194,304 x 4,194,304 2D directed nearest-distance reduction; "
-                         "batch: 2,048 uneven fixed-radius problems, batched vs one call per problem")
+                         "batch: 2,048 uneven fixed-radius problems, batched vs one call per problem; "
+                         "serve: request loop over resident scenes vs the plain per-call path")
     ap.add_argument("--problems", type=int, default=2048, help="problems of the batch workload")
+    ap.add_argument("--scenes", type=int, default=16, help="resident scenes of the serve workload")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve workload arrivals per second")
+    ap.add_argument("--serve-seconds", type=float, default=1.0, help="serve workload trace length")
     ap.add_argument("--traversal", choices=("packet", "lane", "packet_cube"), default=None,
                     help="collect-pass traversal (library default when omitted)")
     ap.add_argument("--leaf-size", type=int, default=None, help="LBVH leaf bucket size (library default when omitted)")
@@ -541,6 +631,8 @@ def main(argv=None) -> int:
         return run_reference_arm(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     if args.workload != "frn":
         return run_secondary(args)
 

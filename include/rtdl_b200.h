@@ -256,6 +256,21 @@ RTDL_B200_API int rtdl_b200_batch_fixed_radius_neighbors_device(
     unsigned long long* row_offsets_out, uint8_t* overflow_dev, void* stream,
     char* error_out, size_t error_size);
 
+/* Several fixed_radius_neighbors requests against one resident scene (from
+ * rtdl_b200_scene_create) answered by one launch sequence: request r's
+ * queries are [query_offsets[r], query_offsets[r + 1]) of query_points_dev,
+ * with radius[r] and k_max[r] (1..64).  Rows come out request by request,
+ * each request's exactly as rtdl_b200_scene_query_device returns them for
+ * that request alone; row_offsets_out (requests + 1 entries) receives each
+ * request's first row and the total.  The served request loop batches with
+ * it.  No reference counterpart (the reference serves one query set per
+ * call, rtdl_optix_api.cpp:4152-4435). */
+RTDL_B200_API int rtdl_b200_scene_fixed_radius_neighbors_multi_device(
+    void* scene, const void* query_points_dev, const unsigned long long* query_offsets, uint32_t requests,
+    const double* radius, const uint32_t* k_max, void* rows_dev, size_t rows_capacity,
+    unsigned long long* row_offsets_out, uint8_t* overflow_dev, void* stream,
+    char* error_out, size_t error_size);
+
 /* Result record of rtdl_b200_scene_directed_hausdorff_noalloc (device memory).
  * status: 0 = ok, 1 = a coordinate is non-finite or beyond 1e18, 2 = the
  * traversal stack overflowed. */

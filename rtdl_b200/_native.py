@@ -103,6 +103,8 @@ SIGNATURES = {
     "rtdl_b200_batch_fixed_radius_neighbors": (_i, [_vp, _vp, _vp, _vp, _vp, _vpp, _vp, _vp, _cp, _sz]),
     "rtdl_b200_batch_fixed_radius_neighbors_device": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp,
                                                            _cp, _sz]),
+    "rtdl_b200_scene_fixed_radius_neighbors_multi_device": (_i, [_vp, _vp, _vp, ctypes.c_uint32, _vp, _vp, _vp, _sz,
+                                                                  _vp, _vp, _vp, _cp, _sz]),
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i, _i]),
     "rtdl_b200_get_launch_count": (_i, [ctypes.POINTER(ctypes.c_ulonglong)]),

@@ -636,6 +636,33 @@ int rtdl_b200_batch_fixed_radius_neighbors_device(void* batch, const void* query
   }, error_out, error_size);
 }
 
+int rtdl_b200_scene_fixed_radius_neighbors_multi_device(void* scene, const void* query_points_dev,
+                                                        const unsigned long long* query_offsets, uint32_t requests,
+                                                        const double* radius, const uint32_t* k_max, void* rows_dev,
+                                                        size_t rows_capacity, unsigned long long* row_offsets_out,
+                                                        uint8_t* overflow_dev, void* stream, char* error_out,
+                                                        size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(scene);
+    if (!sc) throw std::runtime_error("scene must not be null");
+    if (sc->problems != 0) throw std::runtime_error("a problem batch is queried with the batch entry points");
+    if (requests == 0) throw std::runtime_error("requests must be positive");
+    if (!query_offsets || !radius || !k_max || !row_offsets_out)
+      throw std::runtime_error("query_offsets, radius, k_max and row_offsets_out must not be null");
+    BatchSpec bs;
+    bs.problems = requests;
+    bs.qoff = query_offsets;
+    bs.radius = radius;
+    bs.kmax = k_max;
+    bs.row_offsets = row_offsets_out;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sc->stream;
+    PhaseTimer timer(s);
+    run_query_batch(sc, query_points_dev, bs, rows_dev, rows_capacity, nullptr, overflow_dev, s, &timer);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    timer.publish();
+  }, error_out, error_size);
+}
+
 int rtdl_b200_scene_directed_hausdorff(void* scene, const void* query_points, size_t query_count,
                                        double* distance_out, uint32_t* source_id_out, uint32_t* target_id_out,
                                        double* nearest_distance_out, uint32_t* nearest_id_out, char* error_out,

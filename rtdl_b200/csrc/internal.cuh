@@ -184,7 +184,7 @@ void batch_problem_ids(const unsigned long long* offsets_dev, uint32_t problems,
 void batch_boxes(const float4* pts, const uint32_t* pid, uint32_t n, PointStats* prob_stats, uint32_t problems,
                  cudaStream_t s);
 void batch_codes(const float4* pts, const uint32_t* pid, uint32_t n, int dim, const PointStats* prob_stats,
-                 int code_bits, uint32_t* codes, cudaStream_t s);
+                 int stats_stride, int code_bits, uint32_t* codes, cudaStream_t s);
 void destroy_scene(Scene* sc);
 // Converts AoS points to float4 (w = id bits) and accumulates statistics.
 void prep_points(const void* points_dev, uint32_t n, int dim, float4* out, PointStats* stats, cudaStream_t s);
@@ -204,7 +204,9 @@ struct QueryResult {
 // fixed_radius_neighbors over a batch of problems (see build_scene_batch):
 // problem p's queries are [qoff[p], qoff[p + 1]) of the query records, with
 // its own radius and kmax; rows come out problem by problem, each problem's
-// in the order a single query would give.
+// in the order a single query would give.  On a plain scene every problem
+// searches the whole scene: several requests against one resident scene
+// answered by one launch sequence.
 struct BatchSpec {
   uint32_t problems = 0;
   const unsigned long long* qoff = nullptr;  // host, problems + 1

@@ -494,17 +494,19 @@ __global__ void k_reset_stats_n(PointStats* st, uint32_t m) {
 // Composite sort keys (problem << code_bits) | Morton code of the point in its
 // problem's box, code_bits / dim bits per axis.
 __global__ void k_batch_codes(const float4* __restrict__ pts, const uint32_t* __restrict__ pid, uint32_t n, int dim,
-                              const PointStats* __restrict__ st, int code_bits, uint32_t* __restrict__ codes) {
+                              const PointStats* __restrict__ st, int stats_stride, int code_bits,
+                              uint32_t* __restrict__ codes) {
   const int bpa = code_bits / dim;
   const float cells = (float)((1u << bpa) - 1u);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t p = pid[i];
+    const PointStats& box = st[(size_t)p * stats_stride];
     const float4 q = pts[i];
     const float c[3] = {q.x, q.y, q.z};
     uint32_t m[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const unsigned int ol = st[p].lo[a], oh = st[p].hi[a];
+      const unsigned int ol = box.lo[a], oh = box.hi[a];
       const float l = ol == 0xFFFFFFFFu ? 0.f : ordered_to_float(ol);
       const float h = ol == 0xFFFFFFFFu ? 0.f : ordered_to_float(oh);
       const float ext = h - l;
@@ -583,9 +585,9 @@ void batch_boxes(const float4* pts, const uint32_t* pid, uint32_t n, PointStats*
 }
 
 void batch_codes(const float4* pts, const uint32_t* pid, uint32_t n, int dim, const PointStats* prob_stats,
-                 int code_bits, uint32_t* codes, cudaStream_t s) {
+                 int stats_stride, int code_bits, uint32_t* codes, cudaStream_t s) {
   if (n == 0) return;
-  k_batch_codes<<<grid_for(n), kThreads, 0, s>>>(pts, pid, n, dim, prob_stats, code_bits, codes);
+  k_batch_codes<<<grid_for(n), kThreads, 0, s>>>(pts, pid, n, dim, prob_stats, stats_stride, code_bits, codes);
   RTDL_LAUNCHED(1);
 }
 
@@ -631,7 +633,7 @@ Scene* build_scene_impl(const void* points_dev, uint32_t n, int dim, cudaStream_
     uint32_t* pid = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
     batch_problem_ids(d_off, problems, n, pid, s);
     batch_boxes(pts_in, pid, n, sc->prob_stats, problems, s);
-    batch_codes(pts_in, pid, n, dim, sc->prob_stats, sc->code_bits, codes, s);
+    batch_codes(pts_in, pid, n, dim, sc->prob_stats, 1, sc->code_bits, codes, s);
     dev_free(pid, s);
     dev_free(d_off, s);
   } else {

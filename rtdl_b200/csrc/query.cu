@@ -966,6 +966,10 @@ __global__ void __launch_bounds__(kEmitListThreads) k_emit_list(EmitParams P, co
   emit_query<E, DEFER>(P, t, q, n, lane, DEFER ? nullptr : wbuf[threadIdx.x >> 5]);
 }
 
+__global__ void k_fill_i32(int* out, uint32_t n, int v) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = v;
+}
+
 // Problem batch: *flag stays nonzero while every problem's query ids ascend.
 __global__ void k_batch_ids_sorted(const float4* qpts, const uint32_t* qprob, uint32_t n, unsigned int* flag) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -1427,6 +1431,8 @@ struct QueryPrep {
   uint32_t* prob_kmax = nullptr;
   unsigned int* sorted_flag = nullptr;
   unsigned long long* qoff = nullptr;  // device copy of the query offsets
+  int* shared_roots = nullptr;         // requests against one plain scene: every problem's root is the scene's
+  SceneView view{};                    // the scene as the traversal kernels see it
 };
 
 
@@ -1444,6 +1450,7 @@ QueryPrep prepare_queries(Scene* sc, const void* queries_dev, uint32_t nq, bool 
   RTDL_LAUNCHED(1);
   qp.nproc = nq;
   qp.order_identity = &qp.bands->ids_sorted;
+  qp.view = sc->view();
   qp.qcodes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   morton_codes(qp.qpts, nq, sc->dim, sc->stats, qp.qcodes, s);
   iota_u32(qp.qorder, nq, s);
@@ -1468,6 +1475,14 @@ QueryPrep prepare_queries_batch(Scene* sc, const void* queries_dev, uint32_t nq,
                                 cudaStream_t s) {
   const uint32_t P = bs.problems;
   QueryPrep qp;
+  const bool shared = sc->problems == 0;  // several requests against one plain scene
+  qp.view = sc->view();
+  if (shared) {
+    qp.shared_roots = static_cast<int*>(dev_alloc(sizeof(int) * P, s));
+    k_fill_i32<<<div_up(P, 256), 256, 0, s>>>(qp.shared_roots, P, sc->n > 0 ? 0 : kRopeEnd);
+    RTDL_LAUNCHED(1);
+    qp.view.prob_root = qp.shared_roots;
+  }
   std::vector<unsigned long long> pstart(P + 1, 0);
   for (uint32_t p = 0; p < P; ++p) pstart[p + 1] = pstart[p] + (bs.qoff[p + 1] - bs.qoff[p] + 31) / 32 * 32;
   if (pstart[P] > 0xFFFFFFFFull - 32) throw std::runtime_error("problem batch has too many queries");
@@ -1502,7 +1517,10 @@ QueryPrep prepare_queries_batch(Scene* sc, const void* queries_dev, uint32_t nq,
   // processing order: composite (problem, Morton in the problem's box) sort, padded per problem
   uint32_t* codes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (nq ? nq : 1), s));
   uint32_t* sorted = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (nq ? nq : 1), s));
-  batch_codes(qp.qpts, qp.qprob, nq, sc->dim, sc->prob_stats, sc->code_bits, codes, s);
+  if (shared)
+    batch_codes(qp.qpts, qp.qprob, nq, sc->dim, sc->stats, 0, batch_code_bits(P, sc->dim), codes, s);
+  else
+    batch_codes(qp.qpts, qp.qprob, nq, sc->dim, sc->prob_stats, 1, sc->code_bits, codes, s);
   iota_u32(sorted, nq, s);
   radix_sort_pairs(codes, sorted, nq, 0, 32, nullptr, s);
   k_batch_pad<<<P, 256, 0, s>>>(qp.qoff, d_pstart, sorted, qp.qorder, qp.warp_prob);
@@ -1536,6 +1554,7 @@ void free_prep(QueryPrep& qp, cudaStream_t s) {
   dev_free(qp.prob_kmax, s);
   dev_free(qp.sorted_flag, s);
   dev_free(qp.qoff, s);
+  dev_free(qp.shared_roots, s);
 }
 
 }  // namespace
@@ -1596,7 +1615,7 @@ GenericOut run_generic_path(Scene* sc, const QueryPrep& qp, const void* queries_
     k_heavy_gather<<<H, kHeavyThreads, 0, s>>>(sc->view(), qp.qpts, static_cast<const double*>(queries_dev), qstride,
                                                heavy_list, d_seg_off, d_seg_size, 1, qp.bands, scratch, error);
   else
-    k_heavy_gather_bvh<<<H, 32, 0, s>>>(sc->view(), qp.qpts, static_cast<const double*>(queries_dev), qstride,
+    k_heavy_gather_bvh<<<H, 32, 0, s>>>(qp.view, qp.qpts, static_cast<const double*>(queries_dev), qstride,
                                         heavy_list, d_seg_off, d_seg_size, qp.bands, qp.qprob, scratch, error);
   k_heavy_sort<<<H, kHeavyThreads, sizeof(HeavyEntry) * kHeavySmemEntries, s>>>(d_seg_off, d_seg_size, scratch,
                                                                                 sc->perm);
@@ -1670,7 +1689,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
   };
   try {
     CollectParams C;
-    C.S = sc->view();
+    C.S = qp.view;
     C.qpts = qp.qpts;
     C.qraw = static_cast<const double*>(queries_dev);
     C.qstride = qstride;
@@ -1828,7 +1847,8 @@ QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec&
                             size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
                             PhaseTimer* timer) {
   if (rows_alloc) *rows_alloc = nullptr;
-  if (sc->problems != bs.problems) throw std::runtime_error("query batch and scene batch differ in problem count");
+  if (sc->problems != 0 && sc->problems != bs.problems)
+    throw std::runtime_error("query batch and scene batch differ in problem count");
   if (bs.qoff[0] != 0) throw std::runtime_error("query offsets must start at 0");
   for (uint32_t p = 0; p < bs.problems; ++p) {
     if (bs.qoff[p + 1] < bs.qoff[p]) throw std::runtime_error("query offsets must be non-decreasing");

@@ -184,7 +184,11 @@ class B200RowView:
 
     def to_numpy(self, copy: bool = True) -> np.ndarray:
         a = self._array()
-        return a.copy() if copy else a
+        if not copy:
+            return a
+        out = np.empty(len(a), dtype=self.row_dtype)  # a byte copy: padding stays as the library wrote it
+        out.view(np.uint8)[:] = a.view(np.uint8)
+        return out
 
     def close(self) -> None:
         if not self._closed:
@@ -448,6 +452,24 @@ class B200Scene:
             rows_address, int(rows_capacity), ctypes.byref(count), overflow_address, stream, err, len(err))
         _native.check_status(status, err)
         return count.value
+
+    def fixed_radius_neighbors_multi_device(self, query_address: int, query_offsets, *, radius, k_max,
+                                            rows_address: int | None, rows_capacity: int,
+                                            overflow_address: int | None = None,
+                                            stream: int | None = None) -> np.ndarray:
+        """Several fixed_radius_neighbors requests (query ranges given by query_offsets, one radius and
+        k_max each) in one launch sequence; returns row_offsets (requests + 1 entries)."""
+        qoff = np.ascontiguousarray(np.asarray(query_offsets, dtype=np.uint64))
+        m = len(qoff) - 1
+        r = np.ascontiguousarray(np.broadcast_to(np.asarray(radius, dtype=np.float64), (m,)))
+        k = np.ascontiguousarray(np.broadcast_to(np.asarray(k_max, dtype=np.uint32), (m,)))
+        row_offsets = np.zeros(m + 1, dtype=np.uint64)
+        err = _native.error_buffer()
+        status = self._lib.rtdl_b200_scene_fixed_radius_neighbors_multi_device(
+            self._handle, query_address, qoff.ctypes.data, m, r.ctypes.data, k.ctypes.data, rows_address,
+            int(rows_capacity), row_offsets.ctypes.data, overflow_address, stream, err, len(err))
+        _native.check_status(status, err)
+        return row_offsets
 
     def directed_hausdorff(self, query_points, *, with_nearest: bool = False):
         if self._closed:

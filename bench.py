@@ -600,6 +600,85 @@ def run_serve(args) -> int:
     return 0
 
 
+def run_summary(args) -> int:
+    """The reference's own published GPU benchmark: ranked-summary aggregate of fixed_radius_neighbors
+    (r = 0.02, k_max = 50) on its three 262,144-point RTNN sets (queries = search points, float32 inputs,
+    prepared scene and resident queries), regenerated with its generator; medians beside its RTX A5000
+    medians, aggregates checked against its published values."""
+    import torch
+
+    import rtdl_b200 as rt
+    from rtdl_b200 import _native, workloads
+
+    torch.cuda.set_device(0)
+    rt.set_device(0)
+    golden = json.loads((ROOT / "tests" / "golden" / "rtnn_ranked_summary_262144.json").read_text())
+    radius, k_max = golden["radius"], golden["k_max"]
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    results, total_ms, launches = {}, 0.0, 0
+    sampler = ClockSampler(0)
+    sampler.start()
+    for dist_name, g in golden["distributions"].items():
+        pts = workloads.rtnn_points(dist_name, g["point_count"], g["seed"])
+        for c in ("x", "y", "z"):
+            pts[c] = pts[c].astype(np.float32).astype(np.float64)
+        d_pts = torch.from_numpy(pts.view(np.uint8).copy()).to(dev)
+        scene = rt.B200Scene(None, dimension=3, stream=sh, device_points=(d_pts.data_ptr(), len(pts)))
+        try:
+            for _ in range(args.warmup):
+                agg = scene.ranked_summaries_device(d_pts.data_ptr(), len(pts), radius=radius, k_max=k_max, stream=sh)
+            torch.cuda.synchronize()
+            l0 = _native.launch_count()
+            ms = []
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                    a = torch.cuda.Event(enable_timing=True)
+                    b = torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                agg = scene.ranked_summaries_device(d_pts.data_ptr(), len(pts), radius=radius, k_max=k_max, stream=sh)
+                with torch.cuda.stream(stream):
+                    b.record(stream)
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+            launches += _native.launch_count() - l0
+            phases = _native.last_phase_timings()
+        finally:
+            scene.close()
+        exp = g["exact_aggregate"]
+        med = float(np.median(ms))
+        total_ms += med
+        results[dist_name] = {
+            "median_ms": med, "runs_ms": ms, "phases_ms": phases,
+            "published_reference_median_ms": g["reference_median_s"] * 1e3,
+            "published_reference_gpu": golden.get("gpu") or "RTX A5000",
+            "published_cupy_grid_median_ms": g["cupy_grid_median_s"] * 1e3,
+            "speedup_vs_published_reference": g["reference_median_s"] * 1e3 / med,
+            "aggregate": agg,
+            "counts_and_checksums_equal_published": all(agg[f] == exp[f] for f in (
+                "bounded_neighbor_count", "nearest_id_checksum", "kth_id_checksum")),
+            "sum_distance_rel_diff_vs_published": abs(agg["sum_distance"] - exp["sum_distance"]) / exp["sum_distance"],
+        }
+    clocks = sampler.stop()
+    line = {
+        "metric": "ranked-summary aggregate time, 262,144 x 262,144 3D RTNN sets (uniform + clustered + shell), "
+                  "r=0.02, k_max=50",
+        "value": total_ms, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 traversal + f64 band recheck and distances", "data": "synthetic (reference generator)",
+        "config": {"workload": "the reference's published ranked-summary benchmark: prepared scene, resident "
+                               "queries (= search points), float32 inputs; step = query prep + traversal + "
+                               "emit + summaries + aggregate", "l2": "flushed between steps (512 MiB write)"},
+        "distributions": results, "e2e": None, "cpu_baseline": None, "roofline": None, "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main(argv=None) -> int:
     global N_PROBE, N_BUILD
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -611,11 +690,12 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--probes", type=int, default=N_PROBE, help="probe points per GPU (profiling a smaller case)")
     ap.add_argument("--build", type=int, default=N_BUILD, help="build points (profiling a smaller case)")
-    ap.add_argument("--workload", choices=("frn", "knn", "hausdorff", "batch", "serve"), default="frn",
+    ap.add_argument("--workload", choices=("frn", "knn", "hausdorff", "batch", "serve", "summary"), default="frn",
                     help="frn: the headline fixed-radius config; knn: k=16 on the same 3D sets; "
                          "hausdorff: 4,194,304 x 4,194,304 2D directed nearest-distance reduction; "
                          "batch: 2,048 uneven fixed-radius problems, batched vs one call per problem; "
-                         "serve: request loop over resident scenes vs the plain per-call path")
+                         "serve: request loop over resident scenes vs the plain per-call path; "
+                         "summary: the reference's published ranked-summary benchmark")
     ap.add_argument("--problems", type=int, default=2048, help="problems of the batch workload")
     ap.add_argument("--scenes", type=int, default=16, help="resident scenes of the serve workload")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve workload arrivals per second")
@@ -633,6 +713,8 @@ def main(argv=None) -> int:
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "summary":
+        return run_summary(args)
     if args.workload != "frn":
         return run_secondary(args)
 

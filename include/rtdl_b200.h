@@ -65,6 +65,29 @@ typedef struct RtdlKnnNeighborRow {
   uint32_t neighbor_rank;
 } RtdlKnnNeighborRow;
 
+/* Per-query ranked summary and its aggregate over a query set: same layouts
+ * as src/native/optix/rtdl_optix_prelude.h:300-316
+ * (RtdlFixedRadiusRankedNeighborSummary, 40 B) and :318-329
+ * (RtdlFixedRadiusRankedNeighborAggregate, 40 B).  A query without
+ * neighbours in radius has count 0, ids 0xFFFFFFFF and distances 0. */
+typedef struct RtdlFixedRadiusRankedNeighborSummary {
+  uint32_t query_id;
+  uint32_t neighbor_count;       /* min(in-radius count, k_max) */
+  uint32_t nearest_neighbor_id;  /* first row of the query's fixed_radius_neighbors rows */
+  uint32_t kth_neighbor_id;      /* last row */
+  double nearest_distance;
+  double kth_distance;
+  double sum_distance;           /* the rows' distances added in row order */
+} RtdlFixedRadiusRankedNeighborSummary;
+
+typedef struct RtdlFixedRadiusRankedNeighborAggregate {
+  size_t query_count;
+  size_t bounded_neighbor_count;  /* sum of neighbor_count */
+  uint64_t nearest_id_checksum;   /* sum of nearest_neighbor_id (mod 2^64) */
+  uint64_t kth_id_checksum;       /* sum of kth_neighbor_id (mod 2^64) */
+  double sum_distance;            /* sum of sum_distance (fixed reduction order, run to run identical) */
+} RtdlFixedRadiusRankedNeighborAggregate;
+
 /* Version triple (the reference exports rtdl_optix_get_version,
  * rtdl_optix_api.cpp:1-7). */
 RTDL_B200_API int rtdl_b200_get_version(int* major, int* minor, int* patch);
@@ -269,6 +292,36 @@ RTDL_B200_API int rtdl_b200_scene_fixed_radius_neighbors_multi_device(
     void* scene, const void* query_points_dev, const unsigned long long* query_offsets, uint32_t requests,
     const double* radius, const uint32_t* k_max, void* rows_dev, size_t rows_capacity,
     unsigned long long* row_offsets_out, uint8_t* overflow_dev, void* stream,
+    char* error_out, size_t error_size);
+
+/* ---- ranked summaries --------------------------------------------------------
+ * fixed_radius_neighbors reduced per query to the reference's ranked summary
+ * (neighbour count, first and last row, sum of the row distances) and to the
+ * aggregate over the query set, without returning rows.  k_max <= 64. */
+
+/* Replaces rtdl_optix_run_prepared_ranked_fixed_radius_neighbor_summaries_3d
+ * (rtdl_optix_api.cpp:4218-4231): one summary per query, in query order;
+ * *rows_out is released with rtdl_b200_free_rows. */
+RTDL_B200_API int rtdl_b200_run_prepared_ranked_fixed_radius_neighbor_summaries_3d(
+    void* prepared, const RtdlPoint3D* query_points, size_t query_count, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborSummary** rows_out, size_t* row_count_out,
+    char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_aggregate_prepared_ranked_fixed_radius_neighbor_summaries_3d
+ * (rtdl_optix_api.cpp:4251-4266). */
+RTDL_B200_API int rtdl_b200_aggregate_prepared_ranked_fixed_radius_neighbor_summaries_3d(
+    void* prepared, const RtdlPoint3D* query_points, size_t query_count, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, char* error_out, size_t error_size);
+
+/* Device-resident form on any scene (2D or 3D): query records on the device,
+ * optional per-query summaries written to summaries_dev (query order), the
+ * aggregate returned to the host after `stream` (NULL = the scene's stream)
+ * finishes.  Against an empty scene nothing is written to summaries_dev and
+ * the aggregate is zero apart from query_count. */
+RTDL_B200_API int rtdl_b200_scene_ranked_summaries_device(
+    void* scene, const void* query_points_dev, size_t query_count, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
+    RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, void* stream,
     char* error_out, size_t error_size);
 
 /* Result record of rtdl_b200_scene_directed_hausdorff_noalloc (device memory).

@@ -127,6 +127,59 @@ def fixed_radius_neighbors(query, search, *, radius, k_max, threads=1, ranked=Fa
     return _call_rows(query, search, 0, radius, k_max, ranked, threads, with_counts)
 
 
+SUMMARY_DTYPE = np.dtype(
+    {
+        "names": ["query_id", "neighbor_count", "nearest_neighbor_id", "kth_neighbor_id", "nearest_distance",
+                  "kth_distance", "sum_distance"],
+        "formats": ["<u4", "<u4", "<u4", "<u4", "<f8", "<f8", "<f8"],
+        "offsets": [0, 4, 8, 12, 16, 24, 32],
+        "itemsize": 40,
+    }
+)
+
+
+def ranked_summaries(query, search, *, radius, k_max, threads=1):
+    """Per-query ranked summaries (query input order) and their aggregate, restated from the FRN rows.
+
+    Semantics of the reference's exact summary kernel (``src/native/optix/rtdl_optix_core.cpp:5215-5296``:
+    the k_max nearest by (distance, id), first and last of them, their distances added in rank order)
+    and of its aggregate (``:5377-5431``: sums of the counts, of the first and last ids, of the distance
+    sums).  The rows are the oracle's fixed_radius_neighbors rows, so rank order is (distance, id).  The
+    per-query sum is a left-to-right sequential sum (``np.cumsum``); the aggregate's distance sum adds the
+    per-query sums in query order.
+    """
+    rows, counts = fixed_radius_neighbors(query, search, radius=radius, k_max=k_max, threads=threads,
+                                          with_counts=True)
+    n = len(counts)
+    qid = np.asarray(query["id"], dtype=np.uint32)
+    kept = np.minimum(counts.astype(np.int64), int(k_max))
+    order = np.argsort(qid, kind="stable")  # rows are grouped by query id, stable in input order
+    starts = np.zeros(n + 1, dtype=np.int64)
+    starts[1:] = np.cumsum(kept[order])
+    out = np.zeros(n, dtype=SUMMARY_DTYPE)
+    out["query_id"] = qid
+    out["nearest_neighbor_id"] = 0xFFFFFFFF
+    out["kth_neighbor_id"] = 0xFFFFFFFF
+    for j, i in enumerate(order):
+        a, b = starts[j], starts[j + 1]
+        out[i]["neighbor_count"] = b - a
+        if b > a:
+            seg = rows[a:b]
+            out[i]["nearest_neighbor_id"] = seg["neighbor_id"][0]
+            out[i]["kth_neighbor_id"] = seg["neighbor_id"][-1]
+            out[i]["nearest_distance"] = seg["distance"][0]
+            out[i]["kth_distance"] = seg["distance"][-1]
+            out[i]["sum_distance"] = np.cumsum(seg["distance"])[-1]
+    agg = {
+        "query_count": n,
+        "bounded_neighbor_count": int(kept.sum()),
+        "nearest_id_checksum": int(out["nearest_neighbor_id"].astype(np.uint64).sum()) % (1 << 64),
+        "kth_id_checksum": int(out["kth_neighbor_id"].astype(np.uint64).sum()) % (1 << 64),
+        "sum_distance": float(np.cumsum(out["sum_distance"])[-1]) if n else 0.0,
+    }
+    return out, agg
+
+
 def knn_rows(query, search, *, k, threads=1):
     """KNN rows (``reference.py:379-403``)."""
     return _call_rows(query, search, 1, 0.0, k, True, threads, False)

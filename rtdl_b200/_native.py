@@ -62,6 +62,34 @@ class RtdlB200Witness(ctypes.Structure):
     ]
 
 
+class RtdlFixedRadiusRankedNeighborSummary(ctypes.Structure):
+    """Per-query ranked summary -- rtdl_optix_prelude.h:300-316 (40 B)."""
+
+    _fields_ = [
+        ("query_id", ctypes.c_uint32),
+        ("neighbor_count", ctypes.c_uint32),
+        ("nearest_neighbor_id", ctypes.c_uint32),
+        ("kth_neighbor_id", ctypes.c_uint32),
+        ("nearest_distance", ctypes.c_double),
+        ("kth_distance", ctypes.c_double),
+        ("sum_distance", ctypes.c_double),
+    ]
+
+
+class RtdlFixedRadiusRankedNeighborAggregate(ctypes.Structure):
+    """Aggregate of the summaries -- rtdl_optix_prelude.h:318-329 (40 B)."""
+
+    _fields_ = [
+        ("query_count", ctypes.c_size_t),
+        ("bounded_neighbor_count", ctypes.c_size_t),
+        ("nearest_id_checksum", ctypes.c_uint64),
+        ("kth_id_checksum", ctypes.c_uint64),
+        ("sum_distance", ctypes.c_double),
+    ]
+
+
+assert ctypes.sizeof(RtdlFixedRadiusRankedNeighborSummary) == 40
+assert ctypes.sizeof(RtdlFixedRadiusRankedNeighborAggregate) == 40
 assert ctypes.sizeof(RtdlPoint) == 24 and ctypes.sizeof(RtdlPoint3D) == 32
 assert ctypes.sizeof(RtdlFixedRadiusNeighborRow) == 16 and ctypes.sizeof(RtdlKnnNeighborRow) == 24
 
@@ -105,6 +133,11 @@ SIGNATURES = {
                                                            _cp, _sz]),
     "rtdl_b200_scene_fixed_radius_neighbors_multi_device": (_i, [_vp, _vp, _vp, ctypes.c_uint32, _vp, _vp, _vp, _sz,
                                                                   _vp, _vp, _vp, _cp, _sz]),
+    "rtdl_b200_run_prepared_ranked_fixed_radius_neighbor_summaries_3d": (_i, [_vp, _vp, _sz, _d, _sz, _vpp, _szp,
+                                                                               _cp, _sz]),
+    "rtdl_b200_aggregate_prepared_ranked_fixed_radius_neighbor_summaries_3d": (_i, [_vp, _vp, _sz, _d, _sz, _vp, _cp,
+                                                                                     _sz]),
+    "rtdl_b200_scene_ranked_summaries_device": (_i, [_vp, _vp, _sz, _d, _sz, _vp, _vp, _vp, _cp, _sz]),
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i, _i]),
     "rtdl_b200_get_launch_count": (_i, [ctypes.POINTER(ctypes.c_ulonglong)]),
@@ -159,7 +192,7 @@ def launch_count() -> int:
 
 
 STAT_NAMES = ("nodes", "leaf_points", "in_radius", "inserts", "shifts", "band_checks", "max_count",
-              "generic_queries", "large_queries", "leaf_pairs", "emit_fixups")
+              "generic_queries", "large_queries", "leaf_pairs", "emit_fixups", "refined_queries")
 
 
 def last_query_stats() -> dict[str, int]:

@@ -784,4 +784,105 @@ int rtdl_b200_run_prepared_fixed_radius_neighbors_3d(void* prepared, const RtdlP
 
 void rtdl_b200_destroy_prepared_fixed_radius_neighbors_3d(void* prepared) { rtdl_b200_scene_destroy(prepared); }
 
+namespace {
+// Shared checks of the prepared ranked-summary calls (messages as
+// rtdl_optix_workloads.cpp:15011-15022).
+Scene* prepared_summary_scene(void* prepared, double radius, size_t query_count, size_t k_max) {
+  Scene* sc = static_cast<Scene*>(prepared);
+  if (!sc) throw std::runtime_error("prepared OptiX fixed-radius-neighbor 3D handle must not be null");
+  if (sc->dim != 3) throw std::runtime_error("prepared scene is not 3D");
+  if (radius < 0.0) throw std::runtime_error("fixed_radius_neighbors_3d radius must be non-negative");
+  if (radius > sc->max_radius + 1.0e-7)
+    throw std::runtime_error("fixed_radius_neighbors_3d radius exceeds prepared max_radius");
+  if (query_count > (size_t)UINT32_MAX) throw std::runtime_error("fixed_radius_neighbors_3d query_count exceeds uint32 limit");
+  if (k_max == 0) throw std::runtime_error("fixed_radius_neighbors_3d k_max must be positive");
+  if (k_max > 64)
+    throw std::runtime_error("prepared ranked fixed_radius_neighbors_3d aggregate currently supports k_max <= 64");
+  return sc;
+}
+}  // namespace
+
+int rtdl_b200_run_prepared_ranked_fixed_radius_neighbor_summaries_3d(
+    void* prepared, const RtdlPoint3D* query_points, size_t query_count, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborSummary** rows_out, size_t* row_count_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    Scene* sc = prepared_summary_scene(prepared, radius, query_count, k_max);
+    if (query_count == 0 || sc->n == 0) return;
+    if (!query_points) throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    cudaStream_t s = sc->stream;
+    PhaseTimer timer(s);
+    timer.mark("begin");
+    void* d_query = upload(query_points, sizeof(RtdlPoint3D) * query_count, s);
+    RtdlFixedRadiusRankedNeighborSummary* d_sum = nullptr;
+    try {
+      d_sum = static_cast<RtdlFixedRadiusRankedNeighborSummary*>(
+          dev_alloc(sizeof(RtdlFixedRadiusRankedNeighborSummary) * query_count, s));
+      timer.mark("upload");
+      RtdlFixedRadiusRankedNeighborAggregate agg;
+      run_ranked_summaries(sc, d_query, (uint32_t)query_count, radius, (uint32_t)k_max, d_sum, &agg, s, &timer);
+      void* host = download_rows(d_sum, sizeof(RtdlFixedRadiusRankedNeighborSummary) * query_count, s);
+      timer.mark("download");
+      timer.publish();
+      *rows_out = static_cast<RtdlFixedRadiusRankedNeighborSummary*>(host);
+      *row_count_out = query_count;
+    } catch (...) {
+      dev_free(d_sum, s);
+      dev_free(d_query, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(d_sum, s);
+    dev_free(d_query, s);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_aggregate_prepared_ranked_fixed_radius_neighbor_summaries_3d(
+    void* prepared, const RtdlPoint3D* query_points, size_t query_count, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!aggregate_out) throw std::runtime_error("aggregate_out must not be null");
+    *aggregate_out = RtdlFixedRadiusRankedNeighborAggregate{query_count, 0u, 0u, 0u, 0.0};
+    Scene* sc = prepared_summary_scene(prepared, radius, query_count, k_max);
+    if (query_count == 0 || sc->n == 0) return;
+    if (!query_points) throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    cudaStream_t s = sc->stream;
+    PhaseTimer timer(s);
+    timer.mark("begin");
+    void* d_query = upload(query_points, sizeof(RtdlPoint3D) * query_count, s);
+    try {
+      timer.mark("upload");
+      run_ranked_summaries(sc, d_query, (uint32_t)query_count, radius, (uint32_t)k_max, nullptr, aggregate_out, s,
+                           &timer);
+      timer.publish();
+    } catch (...) {
+      dev_free(d_query, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(d_query, s);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_scene_ranked_summaries_device(void* scene, const void* query_points_dev, size_t query_count,
+                                            double radius, size_t k_max,
+                                            RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
+                                            RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, void* stream,
+                                            char* error_out, size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(scene);
+    if (!sc) throw std::runtime_error("scene must not be null");
+    if (!aggregate_out) throw std::runtime_error("aggregate_out must not be null");
+    validate_common(radius, k_max, query_count, sc->n, true, "fixed_radius_neighbors", "k_max");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sc->stream;
+    PhaseTimer timer(s);
+    run_ranked_summaries(sc, query_points_dev, (uint32_t)query_count, radius, (uint32_t)k_max, summaries_dev,
+                         aggregate_out, s, &timer);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    timer.publish();
+  }, error_out, error_size);
+}
+
 }  // extern "C"

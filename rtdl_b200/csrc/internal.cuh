@@ -214,6 +214,13 @@ struct BatchSpec {
   const uint32_t* kmax = nullptr;            // host, problems (1..64)
   unsigned long long* row_offsets = nullptr; // host out, problems + 1: first row of each problem, then the total
 };
+// fixed_radius_neighbors reduced to per-query ranked summaries (query input
+// order, device, optional) and their aggregate (host), without row output to
+// the caller.
+QueryResult run_ranked_summaries(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t kmax,
+                                 RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
+                                 RtdlFixedRadiusRankedNeighborAggregate* aggregate_host, cudaStream_t s,
+                                 PhaseTimer* timer);
 QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec& bs, void* rows_dev,
                             size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
                             PhaseTimer* timer);

@@ -212,7 +212,7 @@ struct Pass1Params {
 
 // Traversal counters gathered by the STATS instantiation (diagnostics).
 enum Stat { kStatNodes, kStatLeafPoints, kStatInRadius, kStatInserts, kStatShifts, kStatBand, kStatMaxLeafPoints,
-            kStatGenericQueries, kStatLargeQueries, kStatLeafPairs, kStatEmitFixups, kStatCount };
+            kStatGenericQueries, kStatLargeQueries, kStatLeafPairs, kStatEmitFixups, kStatRefined, kStatCount };
 
 // One thread per query, queries in Morton order so a warp walks neighbouring
 // subtrees.  KNN == false: radius-limited (fixed_radius_neighbors and
@@ -440,6 +440,7 @@ struct CollectParams {
   uint8_t* flags;            // bit0: count > kmax, bit1: count > kSlab (generic path), bit2: count > 64
   uint32_t* heavy_list;
   uint32_t* heavy_m;
+  uint32_t* heavy_t;         // processing rank of each heavy_list entry (optional)
   uint32_t* mid_list;        // processing ranks of the queries with 65..128 candidates
   uint32_t* big_list;        // processing ranks of the queries with 129..kSlab candidates
   unsigned int* small;       // [0] generic-path query count, [1] error bits, [2] mid_list length,
@@ -496,6 +497,7 @@ __device__ __forceinline__ void collect_finish(const CollectParams& P, const Col
     const unsigned int h = atomicAdd(&P.small[0], 1u);
     P.heavy_list[h] = L.qin;
     P.heavy_m[h] = count;
+    if (P.heavy_t) P.heavy_t[h] = L.t;
   } else if (count > 128u) {
     fl |= 4;
     P.big_list[atomicAdd(&P.small[3], 1u)] = L.t;
@@ -587,17 +589,19 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
 // against its own query.  CUBE: internal nodes are tested against the
 // query's bounding cube (six compares against bounds rounded outward; it
 // never rejects a node the sphere test accepts), leaf buckets against the
-// sphere.
-template <bool STATS, bool CUBE, int MIN_BLOCKS>
+// sphere.  BATCH: several problems (a problem batch, or several requests on
+// one scene): each warp walks its problem's subtree with its problem's bands
+// and kmax; kept out of the single-problem instantiation, whose registers it
+// would cost.
+template <bool STATS, bool CUBE, bool BATCH, int MIN_BLOCKS>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParams P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!__any_sync(0xffffffffu, t < P.nq)) return;  // whole warp past the end
   // a problem batch pads every problem to whole warps, so a warp has one problem
-  const uint32_t prob = P.warp_prob ? P.warp_prob[t >> 5] : 0u;
-  const bool valid = t < P.nq && (P.warp_prob == nullptr || P.qorder[t] != kNone);
-  if (!valid && t < P.nq) P.qinfo[t] = QueryInfo{0.0, 0.0, 0.0, 0u, 0u};  // padding: nothing to emit
+  const uint32_t prob = BATCH ? P.warp_prob[t >> 5] : 0u;
+  const bool valid = t < P.nq && (!BATCH || P.qorder[t] != kNone);
+  if (BATCH && !valid && t < P.nq) P.qinfo[t] = QueryInfo{0.0, 0.0, 0.0, 0u, 0u};  // padding: nothing to emit
   const DevBands B = P.bands[prob];
-  const uint32_t kmax = P.prob_kmax ? P.prob_kmax[prob] : P.kmax;
   const SceneView& S = P.S;
   const int scene_inexact = *S.inexact;
   CollectLane L;
@@ -617,7 +621,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParam
   }
   // the walk covers the problem's subtree: from its root to the root's rope
   int cur = S.n > 0 ? 0 : kRopeEnd, end = kRopeEnd;
-  if (S.prob_root) {
+  if (BATCH) {
     cur = S.prob_root[prob];
     if (cur != kRopeEnd) end = __float_as_int(__ldg(&S.nodes[2 * cur + 1]).w);
   }
@@ -644,7 +648,175 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParam
     }
     cur = __float_as_int(b.w);
   }
-  if (valid) collect_finish<STATS>(P, L, kmax);
+  if (valid) collect_finish<STATS>(P, L, BATCH ? P.prob_kmax[prob] : P.kmax);
+}
+
+// ---- heavy queries: radius refinement -------------------------------------------
+// A query with more than kSlab points in radius needs only its kmax (<= 64)
+// nearest.  If at least kmax points lie within a smaller radius r', those kmax
+// nearest are all among them, so the query is collected again at r' and then
+// sorted and emitted like any other query (its rows and counts still refer to
+// the original radius: the kmax nearest within r).  r' is chosen from the
+// in-radius count (cube-root scaling towards ~2 kmax points) inside a bracket
+// [lo, hi] that every pass narrows; queries still unresolved after a few
+// passes (for instance many points at one distance) take the generic path.
+
+// The bands of DevBands recomputed for another radius (same formulas; the
+// FP32 e_abs is rounded up, which only widens them).
+__device__ __forceinline__ DevBands bands_at_radius(const DevBands& base, double radius) {
+  DevBands b = base;
+  const double rho = (double)base.rho, e_abs = (double)base.e_abs;
+  const double r_hi = radius * (1.0 + rho) + e_abs + 1.0e-18;
+  const double r_lo = radius * (1.0 - rho) - e_abs;
+  float hi2 = __double2float_ru(r_hi * r_hi);
+  if (hi2 < b.floor2) hi2 = b.floor2;
+  b.hi2 = hi2;
+  b.lo2 = r_lo > 0.0 ? __double2float_rd(r_lo * r_lo) : 0.0f;
+  b.box_hi2 = __double2float_ru((double)hi2 * (1.0 + 1.0e-6));
+  b.r2 = radius * radius;
+  return b;
+}
+
+struct RefineParams {
+  CollectParams C;         // scene, queries, processing order, bands, slab
+  const uint32_t* qprob;   // problem of each query (input order); nullptr: one problem
+  const uint32_t* work;    // processing ranks to collect again
+  const double* rad;       // their radii
+  uint32_t nwork;
+  uint32_t* cnt;           // out: in-radius count at rad (all of them, not only the kSlab stored)
+};
+
+// One thread per work item, warp-packet walks: the lanes of a warp that share
+// a subtree root walk it together (a problem batch can mix roots in a warp).
+__global__ void __launch_bounds__(256) k_collect_refine(RefineParams R) {
+  const CollectParams& P = R.C;
+  const SceneView& S = P.S;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = j < R.nwork;
+  if (!__any_sync(0xffffffffu, valid)) return;
+  const int scene_inexact = *S.inexact;
+  CollectLane L;
+  uint32_t prob = 0;
+  DevBands LB = P.bands[0];
+  int root = kRopeEnd, end = kRopeEnd;
+  if (valid) {
+    collect_init(P, R.work[j], L);
+    prob = R.qprob ? R.qprob[L.qin] : 0u;
+    LB = bands_at_radius(P.bands[prob], R.rad[j]);
+    root = S.prob_root ? S.prob_root[prob] : (S.n > 0 ? 0 : kRopeEnd);
+    if (root != kRopeEnd) end = __float_as_int(__ldg(&S.nodes[2 * root + 1]).w);
+  } else {
+    L.q = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+    L.count = 0;
+    L.out = nullptr;
+  }
+  bool todo = valid && root != kRopeEnd;
+  while (true) {
+    const unsigned int pending = __ballot_sync(0xffffffffu, todo);
+    if (!pending) break;
+    const int leader = __ffs(pending) - 1;
+    const int r0 = __shfl_sync(0xffffffffu, root, leader), e0 = __shfl_sync(0xffffffffu, end, leader);
+    const bool mine = todo && root == r0;
+    int cur = r0;
+    while (cur != e0) {
+      const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+      const int hit = __float_as_int(a.w);
+      const bool over = mine && box_d2(L.q.x, L.q.y, L.q.z, a, b) <= LB.box_hi2;
+      if (__any_sync(0xffffffffu, over)) {
+        if (hit >= 0) {
+          ++cur;
+          continue;
+        }
+        collect_leaf<false>(P, LB, scene_inexact, L, leaf_first(hit), leaf_count(hit), over);
+      }
+      cur = __float_as_int(b.w);
+    }
+    todo = todo && !mine;
+  }
+  if (valid) R.cnt[j] = L.count;
+}
+
+struct RefineUpdate {
+  const uint32_t* qorder;
+  const uint32_t* qprob;      // nullptr: one problem
+  const uint32_t* prob_kmax;  // nullptr: kmax below
+  uint32_t kmax;
+  QueryInfo* qinfo;
+  uint8_t* flags;
+  uint32_t* mid_list;
+  uint32_t* big_list;
+  unsigned int* small;        // [2] mid_list length, [3] big_list length
+  // this pass
+  const uint32_t* work;
+  const double* rad;
+  const double* lo;
+  const double* hi;
+  const uint32_t* full;       // in-radius count at the original radius
+  const uint32_t* cnt;
+  uint32_t nwork;
+  // next pass (or, on the last pass, the generic path's list)
+  uint32_t* next_work;
+  double* next_rad;
+  double* next_lo;
+  double* next_hi;
+  uint32_t* next_full;
+  unsigned int* next_count;
+  uint32_t* generic_qin;      // last pass: unresolved queries (input index) and their full counts
+  uint32_t* generic_m;
+  int last;
+};
+
+__global__ void k_refine_update(RefineUpdate U) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= U.nwork) return;
+  const uint32_t t = U.work[j], qin = U.qorder[t], c = U.cnt[j];
+  const uint32_t kmax = U.prob_kmax ? U.prob_kmax[U.qprob ? U.qprob[qin] : 0u] : U.kmax;
+  if (c >= kmax && c <= (uint32_t)kSlab) {  // resolved: the slab holds every point within rad
+    uint8_t fl = (uint8_t)((U.flags[qin] & ~6u) | (c > 64u ? 4u : 0u));
+    U.flags[qin] = fl;
+    U.qinfo[t].meta = c | ((fl & 1) ? kQueryOverflow : 0u) | (c > 64u ? kQueryBig : 0u) | (kmax << kQueryKmaxShift);
+    if (c > 128u)
+      U.big_list[atomicAdd(&U.small[3], 1u)] = t;
+    else if (c > 64u)
+      U.mid_list[atomicAdd(&U.small[2], 1u)] = t;
+    return;
+  }
+  if (U.last) {
+    const unsigned int k = atomicAdd(U.next_count, 1u);
+    U.generic_qin[k] = qin;
+    U.generic_m[k] = U.full[j];
+    return;
+  }
+  const double r = U.rad[j];
+  double l = U.lo[j], h = U.hi[j];
+  if (c < kmax) l = r; else h = r;
+  double est = r * cbrt(2.0 * kmax / (double)(c > 0u ? c : 1u));
+  if (!(est > l && est < h)) est = 0.5 * (l + h);
+  const unsigned int k = atomicAdd(U.next_count, 1u);
+  U.next_work[k] = t;
+  U.next_rad[k] = est;
+  U.next_lo[k] = l;
+  U.next_hi[k] = h;
+  U.next_full[k] = U.full[j];
+}
+
+// The first refinement pass's work: the collect pass's heavy queries (listed
+// by input index with their full counts), radius scaled from the full count.
+__global__ void k_refine_init(const uint32_t* heavy_qin, const uint32_t* heavy_m, const uint32_t* heavy_t,
+                              uint32_t H, const uint32_t* qprob, const double* prob_radius, double radius,
+                              const uint32_t* prob_kmax, uint32_t kmax, uint32_t* work, double* rad, double* lo,
+                              double* hi, uint32_t* full) {
+  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= H) return;
+  const uint32_t qin = heavy_qin[h], p = qprob ? qprob[qin] : 0u;
+  const double r = prob_radius ? prob_radius[p] : radius;
+  const uint32_t k = prob_kmax ? prob_kmax[p] : kmax;
+  const uint32_t m = heavy_m[h];
+  work[h] = heavy_t[h];
+  rad[h] = r * cbrt(2.0 * k / (double)m);
+  lo[h] = 0.0;
+  hi[h] = r;
+  full[h] = m;
 }
 
 // ---- emit: warp per query -----------------------------------------------------
@@ -936,6 +1108,102 @@ __global__ void __launch_bounds__(kFixupThreads) k_emit_fixup(EmitParams P) {
       P.sink.put(base + i, qi.qid, __float_as_uint(p.w), dist, (uint32_t)i + 1);
     }
     __syncwarp();
+  }
+}
+
+// ---- ranked summaries ----------------------------------------------------------
+// One warp per query in output order reads the query's rows (contiguous) and
+// reduces them to the reference's ranked summary: count, first and last row,
+// and the distances added one by one in row order (so the sum is the one a
+// sequential loop over the rows gives).  Each block also writes its queries'
+// partial aggregate (in warp order), which k_summary_final reduces in block
+// order: the aggregate is the same on every run.
+struct SummaryPartial {
+  unsigned long long count, nearest, kth;
+  double sum;
+};
+
+struct SummarySpec {
+  RtdlFixedRadiusRankedNeighborSummary* summaries_dev;  // per query, input order (optional)
+  RtdlFixedRadiusRankedNeighborAggregate* aggregate_host;
+};
+
+
+constexpr int kSummaryThreads = 256;
+
+__global__ void __launch_bounds__(kSummaryThreads)
+    k_summarize(const RtdlFixedRadiusNeighborRow* rows, const unsigned long long* offsets, const uint32_t* oorder,
+                const unsigned int* identity, const float4* qpts, uint32_t nq,
+                RtdlFixedRadiusRankedNeighborSummary* summaries, SummaryPartial* partial) {
+  __shared__ SummaryPartial wsum[kSummaryThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  SummaryPartial mine{0ull, 0ull, 0ull, 0.0};
+  if (j < nq) {  // warp-uniform
+    const uint32_t qin = *identity ? (uint32_t)j : oorder[j];
+    const unsigned long long a = offsets[j], b = offsets[j + 1];
+    const int cnt = (int)(b - a);  // at most 64
+    double d0 = 0.0, d1 = 0.0;
+    if (lane < cnt) d0 = rows[a + lane].distance;
+    if (lane + 32 < cnt) d1 = rows[a + 32 + lane].distance;
+    double sum = 0.0;
+    for (int i = 0; i < cnt; ++i) sum += __shfl_sync(0xffffffffu, i < 32 ? d0 : d1, i & 31);
+    RtdlFixedRadiusRankedNeighborSummary sm;
+    sm.query_id = __float_as_uint(qpts[qin].w);
+    sm.neighbor_count = (uint32_t)cnt;
+    sm.nearest_neighbor_id = cnt ? rows[a].neighbor_id : 0xFFFFFFFFu;
+    sm.kth_neighbor_id = cnt ? rows[b - 1].neighbor_id : 0xFFFFFFFFu;
+    sm.nearest_distance = cnt ? rows[a].distance : 0.0;
+    sm.kth_distance = cnt ? rows[b - 1].distance : 0.0;
+    sm.sum_distance = sum;
+    if (lane == 0) {
+      if (summaries) summaries[qin] = sm;
+      mine = SummaryPartial{(unsigned long long)cnt, sm.nearest_neighbor_id, sm.kth_neighbor_id, sum};
+    }
+  }
+  if (lane == 0) wsum[warp] = mine;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    SummaryPartial acc{0ull, 0ull, 0ull, 0.0};
+    for (int w = 0; w < kSummaryThreads / 32; ++w) {
+      acc.count += wsum[w].count;
+      acc.nearest += wsum[w].nearest;
+      acc.kth += wsum[w].kth;
+      acc.sum += wsum[w].sum;
+    }
+    partial[blockIdx.x] = acc;
+  }
+}
+
+// One block: thread t adds partials t, t + blockDim, ... in order, then a
+// fixed tree over the threads.
+__global__ void __launch_bounds__(1024) k_summary_final(const SummaryPartial* partial, uint32_t m, uint32_t nq,
+                                                        RtdlFixedRadiusRankedNeighborAggregate* out) {
+  __shared__ SummaryPartial sp[1024];
+  SummaryPartial acc{0ull, 0ull, 0ull, 0.0};
+  for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+    acc.count += partial[i].count;
+    acc.nearest += partial[i].nearest;
+    acc.kth += partial[i].kth;
+    acc.sum += partial[i].sum;
+  }
+  sp[threadIdx.x] = acc;
+  __syncthreads();
+  for (unsigned int stride = blockDim.x >> 1; stride > 0; stride >>= 1) {
+    if (threadIdx.x < stride) {
+      sp[threadIdx.x].count += sp[threadIdx.x + stride].count;
+      sp[threadIdx.x].nearest += sp[threadIdx.x + stride].nearest;
+      sp[threadIdx.x].kth += sp[threadIdx.x + stride].kth;
+      sp[threadIdx.x].sum += sp[threadIdx.x + stride].sum;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out->query_count = nq;
+    out->bounded_neighbor_count = sp[0].count;
+    out->nearest_id_checksum = sp[0].nearest;
+    out->kth_id_checksum = sp[0].kth;
+    out->sum_distance = sp[0].sum;
   }
 }
 
@@ -1394,7 +1662,7 @@ struct Readback {
   unsigned int scene_bad;
   unsigned int query_bad;
   unsigned int fixups;
-  unsigned int pad;
+  unsigned int refine_left;  // heavy queries still unresolved after a refinement pass
 };
 
 Readback* pinned_readback() {
@@ -1431,6 +1699,7 @@ struct QueryPrep {
   uint32_t* prob_kmax = nullptr;
   unsigned int* sorted_flag = nullptr;
   unsigned long long* qoff = nullptr;  // device copy of the query offsets
+  double* prob_radius = nullptr;       // radius of each problem
   int* shared_roots = nullptr;         // requests against one plain scene: every problem's root is the scene's
   SceneView view{};                    // the scene as the traversal kernels see it
 };
@@ -1498,7 +1767,8 @@ QueryPrep prepare_queries_batch(Scene* sc, const void* queries_dev, uint32_t nq,
   qp.qoff = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (P + 1), s));
   qp.order_identity = qp.sorted_flag;
   unsigned long long* d_pstart = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (P + 1), s));
-  double* d_radius = static_cast<double*>(dev_alloc(sizeof(double) * P, s));
+  qp.prob_radius = static_cast<double*>(dev_alloc(sizeof(double) * P, s));
+  double* d_radius = qp.prob_radius;
   RTDL_CUDA_CHECK(cudaMemcpyAsync(qp.qoff, bs.qoff, sizeof(unsigned long long) * (P + 1), cudaMemcpyHostToDevice, s));
   RTDL_CUDA_CHECK(cudaMemcpyAsync(d_pstart, pstart.data(), sizeof(unsigned long long) * (P + 1),
                                   cudaMemcpyHostToDevice, s));
@@ -1538,7 +1808,6 @@ QueryPrep prepare_queries_batch(Scene* sc, const void* queries_dev, uint32_t nq,
   dev_free(codes, s);
   dev_free(sorted, s);
   dev_free(d_pstart, s);
-  dev_free(d_radius, s);
   return qp;
 }
 
@@ -1555,6 +1824,7 @@ void free_prep(QueryPrep& qp, cudaStream_t s) {
   dev_free(qp.sorted_flag, s);
   dev_free(qp.qoff, s);
   dev_free(qp.shared_roots, s);
+  dev_free(qp.prob_radius, s);
 }
 
 }  // namespace
@@ -1629,6 +1899,103 @@ GenericOut run_generic_path(Scene* sc, const QueryPrep& qp, const void* queries_
   return g;
 }
 
+// Host side of the radius refinement (see k_collect_refine): up to kRefinePasses
+// passes over the unresolved heavy queries, each followed by an update that
+// resolves queries or narrows their radius; after the last pass the
+// unresolved ones are listed for the generic path.
+constexpr int kRefinePasses = 6;
+
+struct RefineOut {
+  uint32_t generic = 0, mid = 0, big = 0;
+  const uint32_t* generic_qin = nullptr;
+  const uint32_t* generic_m = nullptr;
+  std::vector<void*> buffers;  // released by the caller once the rows are out
+};
+
+RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radius, uint32_t kmax, uint32_t H,
+                       const uint32_t* heavy_list, const uint32_t* heavy_m, const uint32_t* heavy_t,
+                       QueryInfo* qinfo, uint8_t* flags, uint32_t* mid_list, uint32_t* big_list, unsigned int* small,
+                       cudaStream_t s) {
+  RefineOut out;
+  auto alloc = [&](size_t bytes) {
+    void* p = dev_alloc(bytes ? bytes : 1, s);
+    out.buffers.push_back(p);
+    return p;
+  };
+  uint32_t* work[2];
+  double *rad[2], *lo[2], *hi[2];
+  uint32_t* full[2];
+  for (int b = 0; b < 2; ++b) {
+    work[b] = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
+    rad[b] = static_cast<double*>(alloc(sizeof(double) * H));
+    lo[b] = static_cast<double*>(alloc(sizeof(double) * H));
+    hi[b] = static_cast<double*>(alloc(sizeof(double) * H));
+    full[b] = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
+  }
+  uint32_t* cnt = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
+  uint32_t* gen_qin = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
+  uint32_t* gen_m = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
+  unsigned int* next_count = static_cast<unsigned int*>(alloc(sizeof(unsigned int)));
+  k_refine_init<<<div_up(H, 256), 256, 0, s>>>(heavy_list, heavy_m, heavy_t, H, qp.qprob, qp.prob_radius, radius,
+                                               qp.prob_kmax, kmax, work[0], rad[0], lo[0], hi[0], full[0]);
+  RTDL_LAUNCHED(1);
+  Readback* rb = pinned_readback();
+  uint32_t n = H;
+  int cur = 0;
+  for (int pass = 0; pass < kRefinePasses && n > 0; ++pass) {
+    const bool last = pass == kRefinePasses - 1;
+    RefineParams R;
+    R.C = C;
+    R.qprob = qp.qprob;
+    R.work = work[cur];
+    R.rad = rad[cur];
+    R.nwork = n;
+    R.cnt = cnt;
+    k_collect_refine<<<div_up(n, 256), 256, 0, s>>>(R);
+    RTDL_CUDA_CHECK(cudaMemsetAsync(next_count, 0, sizeof(unsigned int), s));
+    RefineUpdate U;
+    U.qorder = qp.qorder;
+    U.qprob = qp.qprob;
+    U.prob_kmax = qp.prob_kmax;
+    U.kmax = kmax;
+    U.qinfo = qinfo;
+    U.flags = flags;
+    U.mid_list = mid_list;
+    U.big_list = big_list;
+    U.small = small;
+    U.work = work[cur];
+    U.rad = rad[cur];
+    U.lo = lo[cur];
+    U.hi = hi[cur];
+    U.full = full[cur];
+    U.cnt = cnt;
+    U.nwork = n;
+    U.next_work = work[cur ^ 1];
+    U.next_rad = rad[cur ^ 1];
+    U.next_lo = lo[cur ^ 1];
+    U.next_hi = hi[cur ^ 1];
+    U.next_full = full[cur ^ 1];
+    U.next_count = next_count;
+    U.generic_qin = gen_qin;
+    U.generic_m = gen_m;
+    U.last = last ? 1 : 0;
+    k_refine_update<<<div_up(n, 256), 256, 0, s>>>(U);
+    RTDL_LAUNCHED(2);
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->refine_left, next_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    n = rb->refine_left;
+    if (last) out.generic = n;
+    cur ^= 1;
+  }
+  out.generic_qin = gen_qin;
+  out.generic_m = gen_m;
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->mid, small + 2, sizeof(unsigned int) * 2, cudaMemcpyDeviceToHost, s));
+  RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+  out.mid = rb->mid;
+  out.big = rb->big;
+  return out;
+}
+
 void check_readback(const Readback& r) {
   if (r.scene_bad || r.query_bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
   if (r.error & 1u) throw std::runtime_error("BVH traversal stack overflow");
@@ -1637,8 +2004,11 @@ void check_readback(const Readback& r) {
 // fixed_radius_neighbors / bounded_knn_rows: collect, scan, emit.
 QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius,
                              uint32_t kmax, void* rows_dev, size_t rows_capacity, void** rows_alloc,
-                             uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer, const BatchSpec* bs = nullptr) {
+                             uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer, const BatchSpec* bs = nullptr,
+                             const SummarySpec* ss = nullptr) {
   QueryResult res;
+  void* summary_rows = nullptr;  // ranked summaries: the rows stay internal
+  if (ss) rows_alloc = &summary_rows;
   const int qstride = sc->dim == 3 ? 4 : 3;
   if (bs) {  // the largest kmax bounds the generic path's output
     kmax = 1;
@@ -1659,6 +2029,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
   uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq1, s));
   uint32_t* heavy_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
   uint32_t* heavy_m = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
+  uint32_t* heavy_t = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
   uint32_t* mid_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * np1, s));
   uint32_t* big_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * np1, s));
   uint32_t* fix_list = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * np1, s));
@@ -1669,8 +2040,10 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       bs ? static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (bs->problems + 1), s)) : nullptr;
   RTDL_CUDA_CHECK(cudaMemsetAsync(small, 0, sizeof(unsigned int) * 8, s));
   GenericOut g;
+  std::vector<void*> refine_bufs;
   auto cleanup = [&]() {
     g.release(s);
+    for (void* p : refine_bufs) dev_free(p, s);
     dev_free(prob_rows, s);
     dev_free(poff, s);
     dev_free(qrank, s);
@@ -1680,6 +2053,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     dev_free(flags, s);
     dev_free(heavy_list, s);
     dev_free(heavy_m, s);
+    dev_free(heavy_t, s);
     dev_free(mid_list, s);
     dev_free(big_list, s);
     dev_free(fix_list, s);
@@ -1705,6 +2079,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     C.flags = flags;
     C.heavy_list = heavy_list;
     C.heavy_m = heavy_m;
+    C.heavy_t = heavy_t;
     C.mid_list = mid_list;
     C.big_list = big_list;
     C.small = small;
@@ -1722,12 +2097,14 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       const unsigned int grid = div_up(np, threads);
       const bool cube = tuning().traversal == 2;
       // occupancy bounds chosen so neither variant spills (32 and 40 registers)
-      if (stats)
-        cube ? k_collect_packet<true, true, 1><<<grid, threads, 0, s>>>(C)
-             : k_collect_packet<true, false, 1><<<grid, threads, 0, s>>>(C);
+      if (bs)  // several problems (traversal counters are not gathered here)
+        k_collect_packet<false, false, true, 5><<<grid, threads, 0, s>>>(C);
+      else if (stats)
+        cube ? k_collect_packet<true, true, false, 1><<<grid, threads, 0, s>>>(C)
+             : k_collect_packet<true, false, false, 1><<<grid, threads, 0, s>>>(C);
       else
-        cube ? k_collect_packet<false, true, 6><<<grid, threads, 0, s>>>(C)
-             : k_collect_packet<false, false, 7><<<grid, threads, 0, s>>>(C);
+        cube ? k_collect_packet<false, true, false, 6><<<grid, threads, 0, s>>>(C)
+             : k_collect_packet<false, false, false, 7><<<grid, threads, 0, s>>>(C);
     } else {
       if (stats)
         k_collect<true><<<div_up(nq, threads), threads, 0, s>>>(C);
@@ -1758,13 +2135,29 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     const Readback r = *rb;
     check_readback(r);
     res.rows = r.rows;
-    res.heavy = r.heavy;
-    if (stats) {
-      last_stats()[kStatGenericQueries] = r.heavy;
-      last_stats()[kStatLargeQueries] = r.mid + r.big;
-    }
+    uint32_t mid = r.mid, big = r.big, generic = r.heavy;
+    const uint32_t* generic_list = heavy_list;
+    const uint32_t* generic_m = heavy_m;
     if (r.heavy > 0) {
-      g = run_generic_path(sc, qp, queries_dev, qstride, r.heavy, heavy_list, heavy_m, kmax, false, small + 1, s);
+      // queries with more than kSlab points in radius: collect again at smaller radii
+      RefineOut ro = refine_heavy(C, qp, radius, kmax, r.heavy, heavy_list, heavy_m, heavy_t, qinfo, flags, mid_list,
+                                  big_list, small, s);
+      refine_bufs = ro.buffers;
+      generic = ro.generic;
+      generic_list = ro.generic_qin;
+      generic_m = ro.generic_m;
+      mid = ro.mid;
+      big = ro.big;
+      if (timer) timer->mark("refine");
+    }
+    res.heavy = generic;
+    if (stats) {
+      last_stats()[kStatGenericQueries] = generic;
+      last_stats()[kStatLargeQueries] = mid + big;
+      last_stats()[kStatRefined] = r.heavy - generic;
+    }
+    if (generic > 0) {
+      g = run_generic_path(sc, qp, queries_dev, qstride, generic, generic_list, generic_m, kmax, false, small + 1, s);
       if (timer) timer->mark("generic_path");
     }
     if (rows_alloc != nullptr) {
@@ -1788,19 +2181,19 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     E.fix_count = small + 4;
     k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
     RTDL_LAUNCHED(1);
-    if (r.mid > 0) {
-      k_emit_list<4, true><<<div_up((uint64_t)r.mid * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, mid_list,
-                                                                                                    r.mid);
+    if (mid > 0) {
+      k_emit_list<4, true><<<div_up((uint64_t)mid * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, mid_list,
+                                                                                                  mid);
       RTDL_LAUNCHED(1);
     }
-    if (r.big > 0) {
-      k_emit_list<8, false><<<div_up((uint64_t)r.big * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, big_list,
-                                                                                                     r.big);
+    if (big > 0) {
+      k_emit_list<8, false><<<div_up((uint64_t)big * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, big_list,
+                                                                                                   big);
       RTDL_LAUNCHED(1);
     }
     k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
     RTDL_LAUNCHED(1);
-    if (r.heavy > 0) {
+    if (generic > 0) {
       ExpandParams X;
       X.S = sc->view();
       X.qpts = qp.qpts;
@@ -1808,7 +2201,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       X.qstride = qstride;
       X.oorder = qp.oorder;
       X.bands = qp.bands;
-      X.nq = r.heavy;
+      X.nq = generic;
       X.L = kSlab;
       X.counts = counts;
       X.flags = flags;
@@ -1821,9 +2214,9 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       X.ranked = predicate == kFrn ? 0 : 1;
       X.overflow_out = nullptr;
       X.error = small + 1;
-      X.work_list = heavy_list;
+      X.work_list = generic_list;
       X.qrank = qrank;
-      k_expand<<<grid_for((uint64_t)r.heavy * 32, kExpandThreads), kExpandThreads, 0, s>>>(X);
+      k_expand<<<grid_for((uint64_t)generic * 32, kExpandThreads), kExpandThreads, 0, s>>>(X);
       RTDL_LAUNCHED(1);
     }
     if (timer) timer->mark("emit");
@@ -1832,16 +2225,52 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
     if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
     if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
+    if (ss) {
+      const uint32_t blocks = div_up((uint64_t)nq * 32, kSummaryThreads);
+      SummaryPartial* partial = static_cast<SummaryPartial*>(dev_alloc(sizeof(SummaryPartial) * blocks, s));
+      RtdlFixedRadiusRankedNeighborAggregate* agg = static_cast<RtdlFixedRadiusRankedNeighborAggregate*>(
+          dev_alloc(sizeof(RtdlFixedRadiusRankedNeighborAggregate), s));
+      k_summarize<<<blocks, kSummaryThreads, 0, s>>>(static_cast<const RtdlFixedRadiusNeighborRow*>(summary_rows),
+                                                    offsets, qp.oorder, qp.order_identity, qp.qpts, nq,
+                                                    ss->summaries_dev, partial);
+      k_summary_final<<<1, 1024, 0, s>>>(partial, blocks, nq, agg);
+      RTDL_LAUNCHED(2);
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(ss->aggregate_host, agg, sizeof(*agg), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      dev_free(partial, s);
+      dev_free(agg, s);
+      if (timer) timer->mark("summarize");
+    }
   } catch (...) {
     cudaStreamSynchronize(s);
+    dev_free(summary_rows, s);
     cleanup();
     throw;
   }
+  dev_free(summary_rows, s);
   cleanup();
   return res;
 }
 
 }  // namespace
+
+QueryResult run_ranked_summaries(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t kmax,
+                                 RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
+                                 RtdlFixedRadiusRankedNeighborAggregate* aggregate_host, cudaStream_t s,
+                                 PhaseTimer* timer) {
+  if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
+  if (kmax < 1 || kmax > 64)
+    throw std::runtime_error("prepared ranked fixed_radius_neighbors_3d aggregate currently supports k_max <= 64");
+  *aggregate_host = RtdlFixedRadiusRankedNeighborAggregate{nq, 0u, 0u, 0u, 0.0};
+  if (nq == 0) return QueryResult{};
+  // an empty search set gives no summaries and a zero aggregate, as the
+  // reference's wrappers do (optix_runtime.py:2555-2572, 2644-2651)
+  if (sc->n == 0) return QueryResult{};
+  if (timer) timer->mark("start");
+  SummarySpec ss{summaries_dev, aggregate_host};
+  return run_radius_query(sc, queries_dev, nq, kFrn, radius, kmax, nullptr, 0, nullptr, nullptr, s, timer, nullptr,
+                          &ss);
+}
 
 QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec& bs, void* rows_dev,
                             size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,

@@ -38,6 +38,16 @@ POINT3D_DTYPE = np.dtype(
 FRN_ROW_DTYPE = np.dtype(
     {"names": ["query_id", "neighbor_id", "distance"], "formats": ["<u4", "<u4", "<f8"], "offsets": [0, 4, 8], "itemsize": 16}
 )
+SUMMARY_DTYPE = np.dtype(
+    {
+        "names": ["query_id", "neighbor_count", "nearest_neighbor_id", "kth_neighbor_id", "nearest_distance",
+                  "kth_distance", "sum_distance"],
+        "formats": ["<u4", "<u4", "<u4", "<u4", "<f8", "<f8", "<f8"],
+        "offsets": [0, 4, 8, 12, 16, 24, 32],
+        "itemsize": 40,
+    }
+)
+AGGREGATE_FIELDS = ("query_count", "bounded_neighbor_count", "nearest_id_checksum", "kth_id_checksum", "sum_distance")
 KNN_ROW_DTYPE = np.dtype(
     {
         "names": ["query_id", "neighbor_id", "distance", "neighbor_rank"],
@@ -471,6 +481,18 @@ class B200Scene:
         _native.check_status(status, err)
         return row_offsets
 
+    def ranked_summaries_device(self, query_address: int, query_count: int, *, radius: float, k_max: int,
+                                summaries_address: int | None = None, stream: int | None = None) -> dict:
+        """fixed_radius_neighbors reduced to per-query ranked summaries (written to summaries_address,
+        SUMMARY_DTYPE, query order, when given) and their aggregate, which is returned."""
+        agg = _native.RtdlFixedRadiusRankedNeighborAggregate()
+        err = _native.error_buffer()
+        status = self._lib.rtdl_b200_scene_ranked_summaries_device(
+            self._handle, query_address, int(query_count), float(radius), int(k_max), summaries_address,
+            ctypes.byref(agg), stream, err, len(err))
+        _native.check_status(status, err)
+        return {f: (float(getattr(agg, f)) if f == "sum_distance" else int(getattr(agg, f))) for f in AGGREGATE_FIELDS}
+
     def directed_hausdorff(self, query_points, *, with_nearest: bool = False):
         if self._closed:
             raise RuntimeError("scene is closed")
@@ -584,6 +606,62 @@ class PreparedB200FixedRadiusNeighbors3D:
             return view.to_dict_rows()
         finally:
             view.close()
+
+    def _summary_checks(self, query_points, radius: float, k_max: int, what: str):
+        if self._closed:
+            raise RuntimeError("prepared b200 fixed-radius-neighbor 3D handle is closed")
+        if radius < 0:
+            raise ValueError("radius must be non-negative")
+        if radius > self._max_radius:
+            raise ValueError("radius must be less than or equal to prepared max_radius")
+        if k_max <= 0:
+            raise ValueError("k_max must be positive")
+        if k_max > 64:
+            raise ValueError(f"PreparedB200FixedRadiusNeighbors3D.{what} currently supports k_max <= 64")
+        addr, n, dim, keep = _pack_any(query_points, 3)
+        if dim != 3:
+            raise ValueError(f"PreparedB200FixedRadiusNeighbors3D.{what} requires 3-D points")
+        return addr, n, keep
+
+    def run_ranked_summary_raw(self, query_points, *, radius: float, k_max: int) -> B200RowView:
+        """One ranked summary per query (``optix_runtime.py:2541-2609``)."""
+        addr, n, keep = self._summary_checks(query_points, radius, k_max, "run_ranked_summary_raw")
+        if n == 0 or self._count == 0:
+            return B200RowView(0, 0, SUMMARY_DTYPE, SUMMARY_DTYPE.names)
+        lib = _native.load_library()
+        rows = ctypes.c_void_p()
+        count = ctypes.c_size_t()
+        err = _native.error_buffer()
+        status = lib.rtdl_b200_run_prepared_ranked_fixed_radius_neighbor_summaries_3d(
+            self._handle, addr, n, float(radius), int(k_max), ctypes.byref(rows), ctypes.byref(count), err, len(err))
+        del keep
+        _native.check_status(status, err)
+        return B200RowView(rows.value or 0, count.value, SUMMARY_DTYPE, SUMMARY_DTYPE.names)
+
+    def run_ranked_summary(self, query_points, *, radius: float, k_max: int) -> tuple:
+        view = self.run_ranked_summary_raw(query_points, radius=radius, k_max=k_max)
+        try:
+            return view.to_dict_rows()
+        finally:
+            view.close()
+
+    def aggregate_ranked_summary(self, query_points, *, radius: float, k_max: int,
+                                 precision: str = "float64") -> dict:
+        """The aggregate over all queries (``optix_runtime.py:2618-2687``); the distances are exact
+        FP64 whatever ``precision`` names."""
+        if precision not in {"float64", "float32"}:
+            raise ValueError("precision must be 'float64' or 'float32'")
+        addr, n, keep = self._summary_checks(query_points, radius, k_max, "aggregate_ranked_summary")
+        if n == 0 or self._count == 0:
+            return {"query_count": int(n), "bounded_neighbor_count": 0, "nearest_id_checksum": 0,
+                    "kth_id_checksum": 0, "sum_distance": 0.0}
+        agg = _native.RtdlFixedRadiusRankedNeighborAggregate()
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_aggregate_prepared_ranked_fixed_radius_neighbor_summaries_3d(
+            self._handle, addr, n, float(radius), int(k_max), ctypes.byref(agg), err, len(err))
+        del keep
+        _native.check_status(status, err)
+        return {f: (float(getattr(agg, f)) if f == "sum_distance" else int(getattr(agg, f))) for f in AGGREGATE_FIELDS}
 
     def close(self) -> None:
         if not self._closed:

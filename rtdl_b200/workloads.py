@@ -84,3 +84,50 @@ def batched_problems(count: int = 2048, seed: int = 5, lo: int = 1024, hi: int =
         radius = (mean * volume / (nb * 4.0 / 3.0 * np.pi)) ** (1.0 / 3.0)
         out.append((records(probe), records(build), float(radius), 64))
     return out
+
+
+def rtnn_points(distribution: str, n: int = 262_144, seed: int | None = None) -> np.ndarray:
+    """The reference's RTNN-style 3D point sets, regenerated point for point.
+
+    Restates the generator of the reference's published ranked-summary runs
+    (``scripts/goal2348_rtnn_v2_2_external_runner.py:19-103``): Python's
+    ``random.Random(seed)``; ``uniform``: x, y, z = three ``random()`` draws;
+    ``clustered``: 8 centres drawn first (each axis ``uniform(0.12, 0.88)``),
+    point i takes centre i mod 8 and each axis ``gauss(centre, 0.035)`` clamped
+    to [0, 1]; ``shell``: the same 8 centre draws, then per point an angle
+    ``random() * 2 pi``, ``z = uniform(-1, 1)`` and a shell radius
+    ``gauss(0.34, 0.025)`` clamped to [0, 0.49] around (0.5, 0.5, 0.5).  Every
+    coordinate passes through the 9-decimal text form the reference writes
+    (``"%.9f"``) and reads back.  Ids are the point indices.  Default seeds are
+    those of the published runs: 2800, 2801, 2802.
+    """
+    import math
+    import random
+
+    seeds = {"uniform": 2800, "clustered": 2801, "shell": 2802}
+    if distribution not in seeds:
+        raise ValueError("distribution must be uniform, clustered or shell")
+    rng = random.Random(seeds[distribution] if seed is None else seed)
+    xyz = np.empty((n, 3), dtype=np.float64)
+    if distribution == "uniform":
+        for i in range(n):
+            xyz[i, 0] = rng.random()
+            xyz[i, 1] = rng.random()
+            xyz[i, 2] = rng.random()
+    else:
+        centres = [tuple(rng.uniform(0.12, 0.88) for _ in range(3)) for _ in range(8)]
+        for i in range(n):
+            if distribution == "clustered":
+                c = centres[i % 8]
+                for a in range(3):
+                    xyz[i, a] = min(1.0, max(0.0, rng.gauss(c[a], 0.035)))
+            else:
+                theta = rng.random() * 6.283185307179586
+                z = rng.uniform(-1.0, 1.0)
+                radial = math.sqrt(max(0.0, 1.0 - z * z))
+                r = min(0.49, max(0.0, rng.gauss(0.34, 0.025)))
+                xyz[i, 0] = 0.5 + r * radial * math.cos(theta)
+                xyz[i, 1] = 0.5 + r * radial * math.sin(theta)
+                xyz[i, 2] = 0.5 + r * z
+    xyz = np.array([float(f"{v:.9f}") for v in xyz.ravel()], dtype=np.float64).reshape(n, 3)
+    return records(xyz)

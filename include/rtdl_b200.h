@@ -324,6 +324,48 @@ RTDL_B200_API int rtdl_b200_scene_ranked_summaries_device(
     RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, void* stream,
     char* error_out, size_t error_size);
 
+/* ---- prepared query sets -------------------------------------------------------
+ * A query set prepared once (uploaded, converted, ordered) for repeated
+ * fixed-radius calls against resident scenes.  Handles are released with
+ * rtdl_b200_queries_destroy. */
+RTDL_B200_API int rtdl_b200_queries_create(
+    const void* points, size_t count, int dimension, int points_on_device, void* stream,
+    void** queries_out, char* error_out, size_t error_size);
+
+RTDL_B200_API void rtdl_b200_queries_destroy(void* queries);
+
+/* Replaces rtdl_optix_prepare_fixed_radius_query_points_3d
+ * (rtdl_optix_api.cpp:4233-4249) and its destroy (:4437). */
+RTDL_B200_API int rtdl_b200_prepare_fixed_radius_query_points_3d(
+    const RtdlPoint3D* query_points, size_t query_count, void** prepared_queries_out,
+    char* error_out, size_t error_size);
+
+RTDL_B200_API void rtdl_b200_destroy_prepared_fixed_radius_query_points_3d(void* prepared_queries);
+
+/* Replaces rtdl_optix_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d_f32
+ * (rtdl_optix_api.cpp:4284-4299); the _f32 name computes the same exact
+ * aggregate. */
+RTDL_B200_API int rtdl_b200_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d(
+    void* prepared, void* prepared_queries, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, char* error_out, size_t error_size);
+
+RTDL_B200_API int rtdl_b200_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d_f32(
+    void* prepared, void* prepared_queries, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, char* error_out, size_t error_size);
+
+/* Ranked summaries and fixed_radius_neighbors rows (k_max <= 64) of a
+ * prepared query set against a resident scene, device-resident outputs, on
+ * `stream` (NULL = the scene's stream). */
+RTDL_B200_API int rtdl_b200_scene_ranked_summaries_prepared_device(
+    void* scene, void* queries, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
+    RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, void* stream,
+    char* error_out, size_t error_size);
+
+RTDL_B200_API int rtdl_b200_scene_query_prepared_device(
+    void* scene, void* queries, double radius, size_t k_max, void* rows_dev, size_t rows_capacity,
+    size_t* row_count_out, uint8_t* overflow_dev, void* stream, char* error_out, size_t error_size);
+
 /* Result record of rtdl_b200_scene_directed_hausdorff_noalloc (device memory).
  * status: 0 = ok, 1 = a coordinate is non-finite or beyond 1e18, 2 = the
  * traversal stack overflowed. */

@@ -36,10 +36,12 @@ from .dsl import (  # noqa: F401
 )
 from .execution import ExecutionPolicy, ExecutionResult, register_with_rtdsl, run  # noqa: F401
 from .runtime import (  # noqa: F401
+    B200Queries,
     B200RowView,
     B200Scene,
     PackedPoints,
     PreparedB200FixedRadiusNeighbors3D,
+    PreparedB200FixedRadiusQueryPoints3D,
     directed_hausdorff,
     hausdorff_distance,
     pack_points,

@@ -138,6 +138,16 @@ SIGNATURES = {
     "rtdl_b200_aggregate_prepared_ranked_fixed_radius_neighbor_summaries_3d": (_i, [_vp, _vp, _sz, _d, _sz, _vp, _cp,
                                                                                      _sz]),
     "rtdl_b200_scene_ranked_summaries_device": (_i, [_vp, _vp, _sz, _d, _sz, _vp, _vp, _vp, _cp, _sz]),
+    "rtdl_b200_queries_create": (_i, [_vp, _sz, _i, _i, _vp, _vpp, _cp, _sz]),
+    "rtdl_b200_queries_destroy": (None, [_vp]),
+    "rtdl_b200_prepare_fixed_radius_query_points_3d": (_i, [_vp, _sz, _vpp, _cp, _sz]),
+    "rtdl_b200_destroy_prepared_fixed_radius_query_points_3d": (None, [_vp]),
+    "rtdl_b200_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d": (_i, [_vp, _vp, _d, _sz, _vp,
+                                                                                           _cp, _sz]),
+    "rtdl_b200_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d_f32": (_i, [_vp, _vp, _d, _sz, _vp,
+                                                                                               _cp, _sz]),
+    "rtdl_b200_scene_ranked_summaries_prepared_device": (_i, [_vp, _vp, _d, _sz, _vp, _vp, _vp, _cp, _sz]),
+    "rtdl_b200_scene_query_prepared_device": (_i, [_vp, _vp, _d, _sz, _vp, _sz, _szp, _vp, _vp, _cp, _sz]),
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i, _i]),
     "rtdl_b200_get_launch_count": (_i, [ctypes.POINTER(ctypes.c_ulonglong)]),

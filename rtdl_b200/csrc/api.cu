@@ -866,6 +866,119 @@ int rtdl_b200_aggregate_prepared_ranked_fixed_radius_neighbor_summaries_3d(
   }, error_out, error_size);
 }
 
+int rtdl_b200_queries_create(const void* points, size_t count, int dimension, int points_on_device, void* stream,
+                             void** queries_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!queries_out) throw std::runtime_error("queries_out must not be null");
+    *queries_out = nullptr;
+    if (dimension != 2 && dimension != 3) throw std::runtime_error("dimension must be 2 or 3");
+    if (!points && count != 0) throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    if (count > (size_t)UINT32_MAX) throw std::runtime_error("query_count exceeds uint32 limit");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : library_stream();
+    int dev = 0;
+    RTDL_CUDA_CHECK(cudaGetDevice(&dev));
+    ensure_pool_configured(dev);
+    const size_t bytes = record_size(dimension) * count;
+    void* owned = dev_alloc(bytes ? bytes : 1, s);
+    if (bytes)
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(owned, points, bytes, points_on_device ? cudaMemcpyDeviceToDevice
+                                                                            : cudaMemcpyHostToDevice, s));
+    PreparedQueries* pq = nullptr;
+    try {
+      pq = prepare_query_set(owned, (uint32_t)count, dimension, s);
+      unsigned int bad = 0;
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &pq->qst->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      if (bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+    } catch (...) {
+      if (pq) destroy_query_set(pq); else dev_free(owned, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    *queries_out = pq;
+  }, error_out, error_size);
+}
+
+void rtdl_b200_queries_destroy(void* queries) {
+  PreparedQueries* pq = static_cast<PreparedQueries*>(queries);
+  if (!pq) return;
+  cudaStream_t s = pq->stream;
+  destroy_query_set(pq);
+  if (s) cudaStreamSynchronize(s);
+}
+
+int rtdl_b200_prepare_fixed_radius_query_points_3d(const RtdlPoint3D* query_points, size_t query_count,
+                                                   void** prepared_queries_out, char* error_out, size_t error_size) {
+  return rtdl_b200_queries_create(query_points, query_count, 3, 0, nullptr, prepared_queries_out, error_out,
+                                  error_size);
+}
+
+void rtdl_b200_destroy_prepared_fixed_radius_query_points_3d(void* prepared_queries) {
+  rtdl_b200_queries_destroy(prepared_queries);
+}
+
+int rtdl_b200_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d(
+    void* prepared, void* prepared_queries, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!aggregate_out) throw std::runtime_error("aggregate_out must not be null");
+    PreparedQueries* pq = static_cast<PreparedQueries*>(prepared_queries);
+    if (!pq) throw std::runtime_error("prepared fixed-radius query handle must not be null");
+    *aggregate_out = RtdlFixedRadiusRankedNeighborAggregate{pq->n, 0u, 0u, 0u, 0.0};
+    Scene* sc = prepared_summary_scene(prepared, radius, pq->n, k_max);
+    if (pq->dim != 3) throw std::runtime_error("prepared queries are not 3D");
+    cudaStream_t s = sc->stream;
+    PhaseTimer timer(s);
+    run_ranked_summaries(sc, nullptr, pq->n, radius, (uint32_t)k_max, nullptr, aggregate_out, s, &timer, pq);
+    timer.publish();
+  }, error_out, error_size);
+}
+
+int rtdl_b200_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d_f32(
+    void* prepared, void* prepared_queries, double radius, size_t k_max,
+    RtdlFixedRadiusRankedNeighborAggregate* aggregate_out, char* error_out, size_t error_size) {
+  return rtdl_b200_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d(
+      prepared, prepared_queries, radius, k_max, aggregate_out, error_out, error_size);
+}
+
+int rtdl_b200_scene_ranked_summaries_prepared_device(void* scene, void* queries, double radius, size_t k_max,
+                                                     RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
+                                                     RtdlFixedRadiusRankedNeighborAggregate* aggregate_out,
+                                                     void* stream, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(scene);
+    PreparedQueries* pq = static_cast<PreparedQueries*>(queries);
+    if (!sc || !pq) throw std::runtime_error("scene and queries must not be null");
+    if (!aggregate_out) throw std::runtime_error("aggregate_out must not be null");
+    validate_common(radius, k_max, pq->n, sc->n, true, "fixed_radius_neighbors", "k_max");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sc->stream;
+    PhaseTimer timer(s);
+    run_ranked_summaries(sc, nullptr, pq->n, radius, (uint32_t)k_max, summaries_dev, aggregate_out, s, &timer, pq);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    timer.publish();
+  }, error_out, error_size);
+}
+
+int rtdl_b200_scene_query_prepared_device(void* scene, void* queries, double radius, size_t k_max, void* rows_dev,
+                                          size_t rows_capacity, size_t* row_count_out, uint8_t* overflow_dev,
+                                          void* stream, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    Scene* sc = static_cast<Scene*>(scene);
+    PreparedQueries* pq = static_cast<PreparedQueries*>(queries);
+    if (!sc || !pq) throw std::runtime_error("scene and queries must not be null");
+    if (!row_count_out) throw std::runtime_error("row_count_out must not be null");
+    validate_common(radius, k_max, pq->n, sc->n, true, "fixed_radius_neighbors", "k_max");
+    *row_count_out = 0;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sc->stream;
+    PhaseTimer timer(s);
+    QueryResult r = run_query_prepared(sc, pq, radius, (uint32_t)k_max, rows_dev, rows_capacity, overflow_dev, s,
+                                       &timer);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    timer.publish();
+    *row_count_out = (size_t)r.rows;
+  }, error_out, error_size);
+}
+
 int rtdl_b200_scene_ranked_summaries_device(void* scene, const void* query_points_dev, size_t query_count,
                                             double radius, size_t k_max,
                                             RtdlFixedRadiusRankedNeighborSummary* summaries_dev,

@@ -214,13 +214,34 @@ struct BatchSpec {
   const uint32_t* kmax = nullptr;            // host, problems (1..64)
   unsigned long long* row_offsets = nullptr; // host out, problems + 1: first row of each problem, then the total
 };
+// A query set prepared once for repeated fixed-radius calls: device records,
+// FP32 points, Morton processing order (in the set's own box) and output
+// order, so a call only computes its bands.
+struct PreparedQueries {
+  int dim = 3;
+  int device = 0;
+  uint32_t n = 0;
+  cudaStream_t stream = nullptr;
+  void* raw = nullptr;            // device copy of the records (owned)
+  PointStats* qst = nullptr;
+  float4* qpts = nullptr;
+  uint32_t* qorder = nullptr;     // processing rank -> input index
+  uint32_t* oorder = nullptr;     // output rank -> input index
+  uint32_t* qrank = nullptr;      // input index -> output rank
+  unsigned int* identity = nullptr;  // device flag: ids ascend (output order == input order)
+};
+PreparedQueries* prepare_query_set(const void* records_dev, uint32_t n, int dim, cudaStream_t s);
+void destroy_query_set(PreparedQueries* pq);
+QueryResult run_query_prepared(Scene* sc, const PreparedQueries* pq, double radius, uint32_t kmax, void* rows_dev,
+                               size_t rows_capacity, uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer);
+
 // fixed_radius_neighbors reduced to per-query ranked summaries (query input
 // order, device, optional) and their aggregate (host), without row output to
 // the caller.
 QueryResult run_ranked_summaries(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t kmax,
                                  RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
                                  RtdlFixedRadiusRankedNeighborAggregate* aggregate_host, cudaStream_t s,
-                                 PhaseTimer* timer);
+                                 PhaseTimer* timer, const PreparedQueries* pq = nullptr);
 QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec& bs, void* rows_dev,
                             size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
                             PhaseTimer* timer);

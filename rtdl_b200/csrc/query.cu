@@ -1702,7 +1702,26 @@ struct QueryPrep {
   double* prob_radius = nullptr;       // radius of each problem
   int* shared_roots = nullptr;         // requests against one plain scene: every problem's root is the scene's
   SceneView view{};                    // the scene as the traversal kernels see it
+  const PreparedQueries* borrowed = nullptr;  // set: the query-side buffers belong to a prepared query set
 };
+
+// The call-side view of a prepared query set: its buffers are borrowed, only
+// the bands (scene and query statistics, this radius) are computed.
+QueryPrep borrow_prepared(Scene* sc, const PreparedQueries* pq, double radius, cudaStream_t s) {
+  QueryPrep qp;
+  qp.borrowed = pq;
+  qp.qst = pq->qst;
+  qp.qpts = pq->qpts;
+  qp.qorder = pq->qorder;
+  qp.oorder = pq->oorder;
+  qp.nproc = pq->n;
+  qp.order_identity = pq->identity;
+  qp.view = sc->view();
+  qp.bands = static_cast<DevBands*>(dev_alloc(sizeof(DevBands), s));
+  k_bands<<<1, 32, 0, s>>>(sc->stats, pq->qst, radius, 1, qp.bands);
+  RTDL_LAUNCHED(1);
+  return qp;
+}
 
 
 
@@ -1812,6 +1831,10 @@ QueryPrep prepare_queries_batch(Scene* sc, const void* queries_dev, uint32_t nq,
 }
 
 void free_prep(QueryPrep& qp, cudaStream_t s) {
+  if (qp.borrowed) {
+    dev_free(qp.bands, s);
+    return;
+  }
   dev_free(qp.qst, s);
   dev_free(qp.qpts, s);
   dev_free(qp.bands, s);
@@ -2005,22 +2028,26 @@ void check_readback(const Readback& r) {
 QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius,
                              uint32_t kmax, void* rows_dev, size_t rows_capacity, void** rows_alloc,
                              uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer, const BatchSpec* bs = nullptr,
-                             const SummarySpec* ss = nullptr) {
+                             const SummarySpec* ss = nullptr, const PreparedQueries* pq = nullptr) {
   QueryResult res;
   void* summary_rows = nullptr;  // ranked summaries: the rows stay internal
   if (ss) rows_alloc = &summary_rows;
+  if (pq) queries_dev = pq->raw;
   const int qstride = sc->dim == 3 ? 4 : 3;
   if (bs) {  // the largest kmax bounds the generic path's output
     kmax = 1;
     for (uint32_t p = 0; p < bs->problems; ++p) kmax = bs->kmax[p] > kmax ? bs->kmax[p] : kmax;
   }
-  QueryPrep qp = bs ? prepare_queries_batch(sc, queries_dev, nq, *bs, s)
-                    : prepare_queries(sc, queries_dev, nq, true, radius, true, s);
+  QueryPrep qp = pq   ? borrow_prepared(sc, pq, radius, s)
+                 : bs ? prepare_queries_batch(sc, queries_dev, nq, *bs, s)
+                      : prepare_queries(sc, queries_dev, nq, true, radius, true, s);
   const uint32_t np = qp.nproc;  // processing ranks
   const size_t nq1 = nq ? nq : 1, np1 = np ? np : 1;
-  uint32_t* qrank = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
-  k_invert<<<grid_for(nq, 256), 256, 0, s>>>(qp.oorder, nq, qp.order_identity, qrank);
-  RTDL_LAUNCHED(1);
+  uint32_t* qrank = pq ? pq->qrank : static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
+  if (!pq) {
+    k_invert<<<grid_for(nq, 256), 256, 0, s>>>(qp.oorder, nq, qp.order_identity, qrank);
+    RTDL_LAUNCHED(1);
+  }
   if (timer) timer->mark("query_prep");
   unsigned long long* slab =
       static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * slab_base((uint32_t)np1), s));
@@ -2046,7 +2073,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     for (void* p : refine_bufs) dev_free(p, s);
     dev_free(prob_rows, s);
     dev_free(poff, s);
-    dev_free(qrank, s);
+    if (!pq) dev_free(qrank, s);
     dev_free(slab, s);
     dev_free(counts, s);
     dev_free(qinfo, s);
@@ -2257,7 +2284,11 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
 QueryResult run_ranked_summaries(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t kmax,
                                  RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
                                  RtdlFixedRadiusRankedNeighborAggregate* aggregate_host, cudaStream_t s,
-                                 PhaseTimer* timer) {
+                                 PhaseTimer* timer, const PreparedQueries* pq) {
+  if (pq) {
+    if (pq->dim != sc->dim) throw std::runtime_error("prepared queries and scene differ in dimension");
+    nq = pq->n;
+  }
   if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
   if (kmax < 1 || kmax > 64)
     throw std::runtime_error("prepared ranked fixed_radius_neighbors_3d aggregate currently supports k_max <= 64");
@@ -2269,7 +2300,79 @@ QueryResult run_ranked_summaries(Scene* sc, const void* queries_dev, uint32_t nq
   if (timer) timer->mark("start");
   SummarySpec ss{summaries_dev, aggregate_host};
   return run_radius_query(sc, queries_dev, nq, kFrn, radius, kmax, nullptr, 0, nullptr, nullptr, s, timer, nullptr,
-                          &ss);
+                          &ss, pq);
+}
+
+QueryResult run_query_prepared(Scene* sc, const PreparedQueries* pq, double radius, uint32_t kmax, void* rows_dev,
+                               size_t rows_capacity, uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer) {
+  if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
+  if (pq->dim != sc->dim) throw std::runtime_error("prepared queries and scene differ in dimension");
+  if (kmax < 1 || kmax > (uint32_t)kMaxList) throw std::runtime_error("prepared queries take k_max in [1, 64]");
+  if (pq->n == 0) return QueryResult{};
+  if (sc->n == 0) {
+    if (overflow_dev) RTDL_CUDA_CHECK(cudaMemsetAsync(overflow_dev, 0, pq->n, s));
+    return QueryResult{};
+  }
+  if (timer) timer->mark("start");
+  return run_radius_query(sc, pq->raw, pq->n, kFrn, radius, kmax, rows_dev, rows_capacity, nullptr, overflow_dev, s,
+                          timer, nullptr, nullptr, pq);
+}
+
+namespace {
+__global__ void k_identity_flag(const PointStats* qst, unsigned int* identity) {
+  if (threadIdx.x == 0) *identity = qst->ids_unsorted ? 0u : 1u;
+}
+}  // namespace
+
+PreparedQueries* prepare_query_set(const void* records_dev, uint32_t n, int dim, cudaStream_t s) {
+  PreparedQueries* pq = new PreparedQueries();
+  pq->dim = dim;
+  pq->n = n;
+  pq->stream = s;
+  RTDL_CUDA_CHECK(cudaGetDevice(&pq->device));
+  const size_t n1 = n ? n : 1;
+  try {
+    pq->raw = const_cast<void*>(records_dev);
+    pq->qst = static_cast<PointStats*>(dev_alloc(sizeof(PointStats), s));
+    pq->qpts = static_cast<float4*>(dev_alloc(sizeof(float4) * n1, s));
+    pq->qorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n1, s));
+    pq->oorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n1, s));
+    pq->qrank = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n1, s));
+    pq->identity = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int), s));
+    reset_stats(pq->qst, s);
+    prep_points(records_dev, n, dim, pq->qpts, pq->qst, s);
+    k_identity_flag<<<1, 32, 0, s>>>(pq->qst, pq->identity);
+    RTDL_LAUNCHED(1);
+    uint32_t* codes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n1, s));
+    morton_codes(pq->qpts, n, dim, pq->qst, codes, s);  // the set's own box: the order only groups neighbours
+    iota_u32(pq->qorder, n, s);
+    radix_sort_pairs(codes, pq->qorder, n, 0, dim == 3 ? 30 : 32, nullptr, s);
+    k_extract_ids<<<grid_for(n, 256), 256, 0, s>>>(pq->qpts, n, codes);
+    RTDL_LAUNCHED(1);
+    iota_u32(pq->oorder, n, s);
+    radix_sort_pairs(codes, pq->oorder, n, 0, 32, pq->identity, s);
+    k_invert<<<grid_for(n, 256), 256, 0, s>>>(pq->oorder, n, pq->identity, pq->qrank);
+    RTDL_LAUNCHED(1);
+    dev_free(codes, s);
+  } catch (...) {
+    pq->raw = nullptr;
+    destroy_query_set(pq);
+    throw;
+  }
+  return pq;
+}
+
+void destroy_query_set(PreparedQueries* pq) {
+  if (!pq) return;
+  cudaStream_t s = pq->stream;
+  dev_free(pq->raw, s);
+  dev_free(pq->qst, s);
+  dev_free(pq->qpts, s);
+  dev_free(pq->qorder, s);
+  dev_free(pq->oorder, s);
+  dev_free(pq->qrank, s);
+  dev_free(pq->identity, s);
+  delete pq;
 }
 
 QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec& bs, void* rows_dev,

@@ -493,6 +493,29 @@ class B200Scene:
         _native.check_status(status, err)
         return {f: (float(getattr(agg, f)) if f == "sum_distance" else int(getattr(agg, f))) for f in AGGREGATE_FIELDS}
 
+    def ranked_summaries_prepared(self, queries: B200Queries, *, radius: float, k_max: int,
+                                  summaries_address: int | None = None, stream: int | None = None) -> dict:
+        """ranked_summaries_device for a prepared query set."""
+        agg = _native.RtdlFixedRadiusRankedNeighborAggregate()
+        err = _native.error_buffer()
+        status = self._lib.rtdl_b200_scene_ranked_summaries_prepared_device(
+            self._handle, queries.handle, float(radius), int(k_max), summaries_address, ctypes.byref(agg), stream,
+            err, len(err))
+        _native.check_status(status, err)
+        return {f: (float(getattr(agg, f)) if f == "sum_distance" else int(getattr(agg, f))) for f in AGGREGATE_FIELDS}
+
+    def query_prepared_device(self, queries: B200Queries, *, radius: float, k_max: int, rows_address: int | None,
+                              rows_capacity: int, overflow_address: int | None = None,
+                              stream: int | None = None) -> int:
+        """fixed_radius_neighbors rows (k_max <= 64) of a prepared query set; returns the total row count."""
+        count = ctypes.c_size_t()
+        err = _native.error_buffer()
+        status = self._lib.rtdl_b200_scene_query_prepared_device(
+            self._handle, queries.handle, float(radius), int(k_max), rows_address, int(rows_capacity),
+            ctypes.byref(count), overflow_address, stream, err, len(err))
+        _native.check_status(status, err)
+        return count.value
+
     def directed_hausdorff(self, query_points, *, with_nearest: bool = False):
         if self._closed:
             raise RuntimeError("scene is closed")
@@ -542,6 +565,68 @@ class B200Scene:
             self.close()
         except Exception:
             pass
+
+
+class B200Queries:
+    """A query set prepared once on the device (records, FP32 points, processing and output order) for
+    repeated fixed-radius calls against resident scenes (``rtdl_b200_queries_create``)."""
+
+    def __init__(self, query_points=None, *, dimension: int | None = None, stream: int | None = None,
+                 device_points: tuple[int, int] | None = None):
+        lib = _native.load_library()
+        self._lib = lib
+        self._handle = ctypes.c_void_p()
+        self._closed = False
+        err = _native.error_buffer()
+        if device_points is not None:
+            address, count = device_points
+            if dimension not in (2, 3):
+                raise ValueError("device_points needs an explicit dimension")
+            self.dimension, self.count = dimension, int(count)
+            status = lib.rtdl_b200_queries_create(address, self.count, dimension, 1, stream,
+                                                  ctypes.byref(self._handle), err, len(err))
+        else:
+            addr, n, dim, keep = _pack_any(query_points, dimension)
+            self.dimension, self.count = dim, n
+            status = lib.rtdl_b200_queries_create(addr, n, dim, 0, stream, ctypes.byref(self._handle), err, len(err))
+            del keep
+        _native.check_status(status, err)
+
+    @property
+    def handle(self) -> int:
+        return self._handle.value or 0
+
+    @property
+    def closed(self) -> bool:
+        return self._closed
+
+    def close(self) -> None:
+        if not self._closed:
+            self._lib.rtdl_b200_queries_destroy(self._handle)
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PreparedB200FixedRadiusQueryPoints3D(B200Queries):
+    """Prepared 3-D query points; mirrors ``PreparedOptixFixedRadiusQueryPoints3D``
+    (``optix_runtime.py:1843-1910``)."""
+
+    def __init__(self, query_points):
+        addr, n, dim, keep = _pack_any(query_points, 3)
+        if dim != 3:
+            raise ValueError("prepare_b200_fixed_radius_query_points_3d requires 3-D points")
+        super().__init__(query_points, dimension=3)
 
 
 class PreparedB200FixedRadiusNeighbors3D:
@@ -644,6 +729,35 @@ class PreparedB200FixedRadiusNeighbors3D:
             return view.to_dict_rows()
         finally:
             view.close()
+
+    def aggregate_ranked_summary_prepared_queries(self, prepared_queries: B200Queries, *, radius: float, k_max: int,
+                                                  precision: str = "float32") -> dict:
+        """Aggregate over a prepared query set (``optix_runtime.py:2689-2750``); exact FP64 distances
+        whatever ``precision`` names."""
+        if prepared_queries.closed:
+            raise RuntimeError("prepared b200 fixed-radius query handle is closed")
+        if precision not in {"float64", "float32"}:
+            raise ValueError("precision must be 'float64' or 'float32'")
+        if self._closed:
+            raise RuntimeError("prepared b200 fixed-radius-neighbor 3D handle is closed")
+        if radius < 0:
+            raise ValueError("radius must be non-negative")
+        if radius > self._max_radius:
+            raise ValueError("radius must be less than or equal to prepared max_radius")
+        if k_max <= 0:
+            raise ValueError("k_max must be positive")
+        if k_max > 64:
+            raise ValueError("PreparedB200FixedRadiusNeighbors3D.aggregate_ranked_summary_prepared_queries "
+                             "currently supports k_max <= 64")
+        if prepared_queries.count == 0 or self._count == 0:
+            return {"query_count": int(prepared_queries.count), "bounded_neighbor_count": 0,
+                    "nearest_id_checksum": 0, "kth_id_checksum": 0, "sum_distance": 0.0}
+        agg = _native.RtdlFixedRadiusRankedNeighborAggregate()
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d(
+            self._handle, prepared_queries.handle, float(radius), int(k_max), ctypes.byref(agg), err, len(err))
+        _native.check_status(status, err)
+        return {f: (float(getattr(agg, f)) if f == "sum_distance" else int(getattr(agg, f))) for f in AGGREGATE_FIELDS}
 
     def aggregate_ranked_summary(self, query_points, *, radius: float, k_max: int,
                                  precision: str = "float64") -> dict:

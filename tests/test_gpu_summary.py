@@ -119,3 +119,41 @@ def test_rtnn_aggregates_reproduce_published_values(gpu, distribution):
     assert agg["nearest_id_checksum"] == pub["nearest_id_checksum"]
     assert abs(agg["kth_id_checksum"] - pub["kth_id_checksum"]) <= 1e-5 * pub["kth_id_checksum"]
     assert agg["sum_distance"] == pytest.approx(pub["sum_distance"], rel=1e-8)
+
+
+def test_prepared_queries_equal_plain_calls(gpu):
+    import torch
+
+    from rtdl_b200.runtime import FRN_ROW_DTYPE, PreparedB200FixedRadiusQueryPoints3D
+
+    probe, build = workloads.clustered_3d(80_000, 30_000)
+    # ids out of order: the prepared set must keep the reference's output order
+    probe["id"] = np.random.default_rng(3).permutation(len(probe)).astype(np.uint32) * 7
+    radius = 0.006
+    prep = PreparedB200FixedRadiusNeighbors3D(build, max_radius=radius)
+    pq = PreparedB200FixedRadiusQueryPoints3D(probe)
+    try:
+        a1 = prep.aggregate_ranked_summary_prepared_queries(pq, radius=radius, k_max=50)
+        a2 = prep.aggregate_ranked_summary(probe, radius=radius, k_max=50)
+        assert a1 == a2
+    finally:
+        pq.close()
+        prep.close()
+    with rt.B200Scene(rt.pack_points(records=build)) as scene, rt.B200Queries(probe) as q:
+        n = scene.query_prepared_device(q, radius=radius, k_max=40, rows_address=None, rows_capacity=0)
+        rows = torch.empty(max(n, 1) * 16, dtype=torch.uint8, device="cuda")
+        assert scene.query_prepared_device(q, radius=radius, k_max=40, rows_address=rows.data_ptr(),
+                                           rows_capacity=n) == n
+        torch.cuda.synchronize()
+        got = np.frombuffer(rows.cpu().numpy().tobytes(), dtype=FRN_ROW_DTYPE)[:n]
+        view = scene.query(probe, predicate="fixed_radius_neighbors", radius=radius, limit=40)
+        exp = view.to_numpy()
+        view.close()
+        assert np.array_equal(got.view(np.uint8), exp.view(np.uint8))
+        d_s = torch.empty(len(probe) * 40, dtype=torch.uint8, device="cuda")
+        agg = scene.ranked_summaries_prepared(q, radius=radius, k_max=40, summaries_address=d_s.data_ptr())
+        torch.cuda.synchronize()
+        got_s = np.frombuffer(d_s.cpu().numpy().tobytes(), dtype=SUMMARY_DTYPE)
+    exp_s, exp_agg = O.ranked_summaries(probe, build, radius=radius, k_max=40, threads=8)
+    _same_summaries(got_s, exp_s)
+    assert agg["kth_id_checksum"] == exp_agg["kth_id_checksum"]

@@ -387,6 +387,16 @@ def run_batch(args) -> int:
     d_probe = torch.from_numpy(concat_records(probes).view(np.uint8)).to(dev)
     del probs
     chunks = _plan_chunks(nb, nq, 32 << 20, 8 << 20)
+    # autotune (leaf size and block size; batches always walk in warp packets) on the median-size problem
+    from dataclasses import asdict
+
+    from rtdl_b200.autotune import Autotuner
+
+    med = int(np.argsort(nb * nq)[len(nb) // 2])
+    tuner = Autotuner(repeats=2, traversals=("packet",))
+    tune_key, tune_cfg = tuner.tune(d_build.data_ptr() + 32 * int(boff[med]), int(nb[med]),
+                                    d_probe.data_ptr() + 32 * int(qoff[med]), int(nq[med]), dimension=3,
+                                    radius=float(radius[med]), k_max=int(kmax[med]), stream=sh)
 
     def batch_step(rows_buf, cap, sizes_out=None):
         total = 0
@@ -503,6 +513,7 @@ def run_batch(args) -> int:
         "plain_per_call": {"value": rows_total / (plain_ms[0] / 1e3), "unit": "rows/s", "ms": plain_ms[0],
                            "launches": "one scene build + one query per problem"},
         "speedup_vs_plain": plain_ms[0] / ms_step,
+        "autotune": {"shape_class": tune_key, "config": asdict(tune_cfg), "candidates_ms": tuner.cache[tune_key]["ms"]},
         "roofline": {"bound": "hbm", "kernel": "whole batched step (build + collect + emit)",
                      "achieved": alg / (ms_step / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                      "frac": alg / (ms_step / 1e3) / 1e9 / hbm_peak, "traffic": None, "algorithmic_bytes": alg},

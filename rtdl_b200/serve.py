@@ -119,6 +119,13 @@ class B200Server:
         self._work: list[collections.deque] = [collections.deque() for _ in range(streams)]
         self._work_cv = [threading.Condition() for _ in range(streams)]
         self._streams = [torch.cuda.Stream(device=device) for _ in range(streams)]
+        # per-worker pinned staging buffers, page-locked once here for the largest group the scheduler
+        # forms (page-locking while requests wait would stall them), grown only if a group needs more
+        self._pinned: list[dict] = [{} for _ in range(streams)]
+        rows_bytes = max(max_batch_probes * 64 * 16, (1 << 20) * 32 * 24)
+        for pool in self._pinned:
+            self._staging(pool, "queries", max_batch_probes * 32)
+            self._staging(pool, "rows", rows_bytes)
         self._threads: list[threading.Thread] = []
         self._running = False
         self._next_id = 0
@@ -253,7 +260,7 @@ class B200Server:
                     return
                 group, nbytes = self._work[w].popleft()
             try:
-                self._run_group(group, stream)
+                self._run_group(group, stream, self._pinned[w])
             except Exception as exc:  # reported per request; the loop keeps serving
                 for r in group:
                     r.error = str(exc)
@@ -271,7 +278,15 @@ class B200Server:
                     self._free_workers.append(w)
                     self._cv.notify_all()
 
-    def _run_group(self, group: list[Request], stream) -> None:
+    def _staging(self, pool: dict, name: str, nbytes: int):
+        """A pinned host buffer of at least nbytes, kept per worker."""
+        buf = pool.get(name)
+        if buf is None or buf.numel() < nbytes:
+            buf = self._torch.empty(max(nbytes, 1 << 20), dtype=self._torch.uint8, pin_memory=True)
+            pool[name] = buf
+        return buf
+
+    def _run_group(self, group: list[Request], stream, pool: dict) -> None:
         torch = self._torch
         scene = self.scenes[group[0].scene]
         rec = 32 if scene.dimension == 3 else 24
@@ -279,7 +294,7 @@ class B200Server:
         qoff = np.zeros(len(group) + 1, dtype=np.uint64)
         qoff[1:] = np.cumsum(counts)
         nq = int(qoff[-1])
-        host_q = torch.empty(max(nq * rec, 1), dtype=torch.uint8, pin_memory=True)
+        host_q = self._staging(pool, "queries", max(nq * rec, 1))[: max(nq * rec, 1)]
         hq = host_q.numpy()
         for r, a in zip(group, qoff[:-1]):
             hq[int(a) * rec: (int(a) + len(r.queries)) * rec] = r.queries.view(np.uint8)
@@ -302,7 +317,7 @@ class B200Server:
                                            stream=stream.cuda_stream)
                 offs = np.array([0, total], dtype=np.uint64)
                 dtype, row = KNN_ROW_DTYPE, 24
-            host_rows = torch.empty(max(total * row, 1), dtype=torch.uint8, pin_memory=True)
+            host_rows = self._staging(pool, "rows", max(total * row, 1))[: max(total * row, 1)]
             if total:
                 host_rows[: total * row].copy_(d_rows[: total * row], non_blocking=True)
             stream.synchronize()

@@ -190,3 +190,14 @@ def test_register_with_reference_dispatch(monkeypatch):
     rows = rtdsl.run(k, {"query_points": (), "search_points": ()}, execution=rtdsl.ExecutionPolicy(backend="cpu_python_reference")).rows
     assert rows == ()
     sys.modules.pop("rtdsl", None)
+
+
+def test_autotune_shape_classes_and_cache(tmp_path):
+    from rtdl_b200.autotune import Autotuner, Config, shape_class
+
+    assert shape_class(3, 1 << 20, 1 << 20, 31.0) == "d3-b20-q20-m5"
+    assert shape_class(2, 1000, 0, 0.0) == "d2-b10-q0-m0"
+    t = Autotuner(tmp_path / "c.json")
+    t._store("d3-b20-q20-m5", Config(16, "lane", 256), {"16/lane/256": 1.0})
+    assert Autotuner(tmp_path / "c.json").lookup("d3-b20-q20-m5") == Config(16, "lane", 256)
+    assert t.lookup("missing") is None

@@ -686,9 +686,71 @@ struct RefineParams {
   uint32_t* cnt;           // out: in-radius count at rad (all of them, not only the kSlab stored)
 };
 
-// One thread per work item, warp-packet walks: the lanes of a warp that share
-// a subtree root walk it together (a problem batch can mix roots in a warp).
+// One warp per work item: the warp walks the query's subtree once (node
+// tests warp-uniform) and its lanes test a leaf bucket's points together,
+// appending accepted points with a ballot prefix.  The accept rule is
+// collect_point's (FP32 outside the band, FP64 inside).  Heavy queries are few
+// and scattered, so a packet of 32 of them would walk the union of 32 regions.
 __global__ void __launch_bounds__(256) k_collect_refine(RefineParams R) {
+  const CollectParams& P = R.C;
+  const SceneView& S = P.S;
+  const int lane = threadIdx.x & 31;
+  const uint32_t j = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (j >= R.nwork) return;  // whole warp
+  const int scene_inexact = *S.inexact;
+  const uint32_t t = R.work[j], qin = P.qorder[t];
+  const uint32_t prob = R.qprob ? R.qprob[qin] : 0u;
+  const DevBands LB = bands_at_radius(P.bands[prob], R.rad[j]);
+  const float4 q = P.qpts[qin];
+  const double* rq = P.qraw + (size_t)qin * P.qstride;
+  const double ex = rq[1], ey = rq[2], ez = P.qstride == 4 ? rq[3] : 0.0;
+  unsigned long long* out = P.slab + slab_base(t);
+  int cur = S.n > 0 ? 0 : kRopeEnd, end = kRopeEnd;
+  if (S.prob_root) {
+    cur = S.prob_root[prob];
+    if (cur != kRopeEnd) end = __float_as_int(__ldg(&S.nodes[2 * cur + 1]).w);
+  }
+  const unsigned int lt = (1u << lane) - 1u;
+  uint32_t count = 0;
+  while (cur != end) {
+    const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+    const int hit = __float_as_int(a.w);
+    if (box_d2(q.x, q.y, q.z, a, b) <= LB.box_hi2) {
+      if (hit >= 0) {
+        ++cur;
+        continue;
+      }
+      const int first = leaf_first(hit), cnt = leaf_count(hit);
+      bool acc = false;
+      float key = 0.f;
+      const uint32_t i = (uint32_t)(first + lane);
+      if (lane < cnt) {
+        const float4 p = __ldg(&S.pts[i]);
+        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+        key = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        acc = key <= LB.hi2;
+        if (acc && (key >= LB.lo2 || LB.any_inexact)) {
+          const double e2 = exact_d2_at(ex, ey, ez, S.pts, S.pts64, scene_inexact, i);
+          if (key >= LB.lo2 && e2 > LB.r2) acc = false;
+          if (LB.any_inexact) key = __double2float_rn(e2);
+        }
+      }
+      const unsigned int m = __ballot_sync(0xffffffffu, acc);
+      if (acc) {
+        const uint32_t pos = count + __popc(m & lt);
+        if (pos < (uint32_t)kSlab) out[pos] = slab_entry(key, i);
+      }
+      count += __popc(m);
+    }
+    cur = __float_as_int(b.w);
+  }
+  if (lane == 0) R.cnt[j] = count;
+}
+
+// One thread per work item, warp-packet walks (the form for many heavy
+// queries, which then cluster in space): the lanes of a warp that share a
+// subtree root walk it together (a problem batch can mix roots in a warp).
+__global__ void __launch_bounds__(256) k_collect_refine_packet(RefineParams R) {
   const CollectParams& P = R.C;
   const SceneView& S = P.S;
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1974,7 +2036,10 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     R.rad = rad[cur];
     R.nwork = n;
     R.cnt = cnt;
-    k_collect_refine<<<div_up(n, 256), 256, 0, s>>>(R);
+    if (n >= qp.nproc / 8)  // many heavy queries: they cluster, a packet of them walks one region
+      k_collect_refine_packet<<<div_up(n, 256), 256, 0, s>>>(R);
+    else
+      k_collect_refine<<<div_up((uint64_t)n * 32, 256), 256, 0, s>>>(R);
     RTDL_CUDA_CHECK(cudaMemsetAsync(next_count, 0, sizeof(unsigned int), s));
     RefineUpdate U;
     U.qorder = qp.qorder;

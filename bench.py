@@ -611,6 +611,52 @@ def run_serve(args) -> int:
     return 0
 
 
+def _time_summary_graph(pts, radius, k_max, flush, args):
+    """The same request through the captured batch graph (prepared scene + prepared queries): device
+    time of a replay (CUDA events on the graph's stream, L2 flushed before each) and the host time of
+    replay() (launch, aggregate read back, status check)."""
+    import torch
+
+    import rtdl_b200 as rt
+
+    prep = rt.PreparedB200FixedRadiusNeighbors3D(pts, max_radius=radius)
+    pq = rt.PreparedB200FixedRadiusQueryPoints3D(pts)
+    graph = prep.prepare_ranked_summary_prepared_queries_batch_graph(pq, [{"radius": radius, "k_max": k_max}])
+    try:
+        for _ in range(args.warmup):
+            graph.replay()
+        _, _, _, _, gs = graph.launch_device_partials()
+        ext = torch.cuda.ExternalStream(gs)
+        torch.cuda.synchronize()
+        dev_ms = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(ext):
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(ext)
+            graph.launch_device_partials()
+            with torch.cuda.stream(ext):
+                b.record(ext)
+            b.synchronize()
+            dev_ms.append(a.elapsed_time(b))
+        wall_ms = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(ext):
+                flush.zero_()
+            ext.synchronize()
+            t0 = time.perf_counter()
+            (res,) = graph.replay()
+            wall_ms.append((time.perf_counter() - t0) * 1e3)
+        agg = {f: res[f] for f in ("query_count", "bounded_neighbor_count", "nearest_id_checksum",
+                                   "kth_id_checksum", "sum_distance")}
+        return dev_ms, wall_ms, agg
+    finally:
+        graph.close()
+        pq.close()
+        prep.close()
+
+
 def run_summary(args) -> int:
     """The reference's own published GPU benchmark: ranked-summary aggregate of fixed_radius_neighbors
     (r = 0.02, k_max = 50) on its three 262,144-point RTNN sets (queries = search points, float32 inputs,
@@ -666,6 +712,8 @@ def run_summary(args) -> int:
             ms_device, agg_device = timed(lambda: scene.ranked_summaries_device(
                 d_pts.data_ptr(), len(pts), radius=radius, k_max=k_max, stream=sh))
             assert agg_device == agg
+            graph_ms, graph_wall_ms, agg_graph = _time_summary_graph(pts, radius, k_max, flush, args)
+            assert all(agg_graph[f] == agg[f] for f in agg), (agg_graph, agg)
         finally:
             queries.close()
             scene.close()
@@ -675,6 +723,8 @@ def run_summary(args) -> int:
         results[dist_name] = {
             "median_ms": med, "runs_ms": ms, "phases_ms": phases,
             "unprepared_queries_median_ms": float(np.median(ms_device)),
+            "graph_replay_median_ms": float(np.median(graph_ms)),
+            "graph_replay_host_median_ms": float(np.median(graph_wall_ms)),
             "published_reference_median_ms": g["reference_median_s"] * 1e3,
             "published_reference_gpu": golden.get("gpu") or "RTX A5000",
             "published_cupy_grid_median_ms": g["cupy_grid_median_s"] * 1e3,

@@ -366,6 +366,51 @@ RTDL_B200_API int rtdl_b200_scene_query_prepared_device(
     void* scene, void* queries, double radius, size_t k_max, void* rows_dev, size_t rows_capacity,
     size_t* row_count_out, uint8_t* overflow_dev, void* stream, char* error_out, size_t error_size);
 
+/* ---- captured batch graph of prepared-query aggregates -----------------------
+ * Replace the batch-graph entry points of rtdl_optix_api.cpp:4323-4396
+ * (prepare / replay / launch-with-device-partials / update / destroy).
+ * One CUDA graph holds, for each (radius, k_max) request in order, the whole
+ * fixed-radius path over the prepared query set (collect, device-driven
+ * heavy-query refinement, emit into an internal row buffer, ranked summary,
+ * aggregate); all buffers are allocated at prepare.  The graph runs on its own
+ * stream.  update re-captures it with new requests (same request_count).
+ * The aggregates are the exact ones of
+ * rtdl_b200_aggregate_prepared_query_ranked_fixed_radius_neighbor_summaries_3d.
+ * Requests: radius in [0, max_radius], 1 <= k_max <= 64; both handles
+ * non-empty.  No query-count cap beyond device memory (nq x 2 KiB of slab plus
+ * nq x k_max rows). */
+RTDL_B200_API int rtdl_b200_prepare_fixed_radius_ranked_summary_aggregate_batch_graph_3d(
+    void* prepared, void* prepared_queries, const double* radii, const size_t* k_values, size_t request_count,
+    void** graph_out, char* error_out, size_t error_size);
+
+/* Replays the graph and writes request_count aggregates.  A request whose
+ * heavy queries the refinement passes left unresolved is recomputed by the
+ * plain call (its generic path) before this returns. */
+RTDL_B200_API int rtdl_b200_replay_fixed_radius_ranked_summary_aggregate_batch_graph_3d(
+    void* graph, RtdlFixedRadiusRankedNeighborAggregate* aggregates_out, char* error_out, size_t error_size);
+
+/* Enqueues a replay and returns without waiting: the partials are one
+ * RtdlFixedRadiusRankedNeighborAggregate per request in device memory
+ * (query_block_count = 1), valid once the returned stream reaches this point.
+ * A request whose device status word (below) is nonzero has no valid partial:
+ * replay computes it. */
+RTDL_B200_API int rtdl_b200_launch_fixed_radius_ranked_summary_aggregate_batch_graph_device_partials_3d(
+    void* graph, uint64_t* partials_device_ptr_out, size_t* partial_count_out, size_t* request_count_out,
+    size_t* query_block_count_out, uint64_t* cuda_stream_ptr_out, char* error_out, size_t error_size);
+
+/* No counterpart in the reference: the device address of the per-request
+ * status words of the last replay (0 = the partial is valid; bit 0 traversal
+ * stack overflow; bit 1 heavy queries left for the generic path) and how many
+ * requests replay has recomputed by the plain call so far. */
+RTDL_B200_API int rtdl_b200_fixed_radius_ranked_summary_aggregate_batch_graph_status_device_3d(
+    void* graph, uint64_t* status_device_ptr_out, uint64_t* fallback_count_out, char* error_out, size_t error_size);
+
+RTDL_B200_API int rtdl_b200_update_fixed_radius_ranked_summary_aggregate_batch_graph_3d(
+    void* graph, const double* radii, const size_t* k_values, size_t request_count, char* error_out,
+    size_t error_size);
+
+RTDL_B200_API void rtdl_b200_destroy_fixed_radius_ranked_summary_aggregate_batch_graph_3d(void* graph);
+
 /* Result record of rtdl_b200_scene_directed_hausdorff_noalloc (device memory).
  * status: 0 = ok, 1 = a coordinate is non-finite or beyond 1e18, 2 = the
  * traversal stack overflowed. */

@@ -42,6 +42,7 @@ from .runtime import (  # noqa: F401
     PackedPoints,
     PreparedB200FixedRadiusNeighbors3D,
     PreparedB200FixedRadiusQueryPoints3D,
+    PreparedB200FixedRadiusRankedSummaryAggregateBatchGraph3D,
     directed_hausdorff,
     hausdorff_distance,
     pack_points,

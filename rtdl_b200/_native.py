@@ -148,6 +148,16 @@ SIGNATURES = {
                                                                                                _cp, _sz]),
     "rtdl_b200_scene_ranked_summaries_prepared_device": (_i, [_vp, _vp, _d, _sz, _vp, _vp, _vp, _cp, _sz]),
     "rtdl_b200_scene_query_prepared_device": (_i, [_vp, _vp, _d, _sz, _vp, _sz, _szp, _vp, _vp, _cp, _sz]),
+    "rtdl_b200_prepare_fixed_radius_ranked_summary_aggregate_batch_graph_3d": (
+        _i, [_vp, _vp, _dp, ctypes.POINTER(_sz), _sz, _vpp, _cp, _sz]),
+    "rtdl_b200_replay_fixed_radius_ranked_summary_aggregate_batch_graph_3d": (_i, [_vp, _vp, _cp, _sz]),
+    "rtdl_b200_launch_fixed_radius_ranked_summary_aggregate_batch_graph_device_partials_3d": (
+        _i, [_vp, ctypes.POINTER(ctypes.c_uint64), _szp, _szp, _szp, ctypes.POINTER(ctypes.c_uint64), _cp, _sz]),
+    "rtdl_b200_fixed_radius_ranked_summary_aggregate_batch_graph_status_device_3d": (
+        _i, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), _cp, _sz]),
+    "rtdl_b200_update_fixed_radius_ranked_summary_aggregate_batch_graph_3d": (
+        _i, [_vp, _dp, ctypes.POINTER(_sz), _sz, _cp, _sz]),
+    "rtdl_b200_destroy_fixed_radius_ranked_summary_aggregate_batch_graph_3d": (None, [_vp]),
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i, _i]),
     "rtdl_b200_get_launch_count": (_i, [ctypes.POINTER(ctypes.c_ulonglong)]),

@@ -26,6 +26,7 @@ std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 
 void count_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+unsigned long long launches_counted() { return g_launches.load(std::memory_order_relaxed); }
 
 Tuning& tuning() {
   static Tuning t;
@@ -957,6 +958,90 @@ int rtdl_b200_scene_ranked_summaries_prepared_device(void* scene, void* queries,
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
     timer.publish();
   }, error_out, error_size);
+}
+
+namespace {
+std::vector<uint32_t> graph_k_values(const size_t* k_values, size_t request_count) {
+  if (request_count > (size_t)UINT32_MAX)
+    throw std::runtime_error("fixed_radius_neighbors_3d graph request_count exceeds uint32 limit");
+  if (!k_values && request_count) throw std::runtime_error("k_values pointer must not be null when request_count is nonzero");
+  std::vector<uint32_t> k(request_count);
+  for (size_t r = 0; r < request_count; ++r) {
+    if (k_values[r] > 64)
+      throw std::runtime_error("prepared ranked fixed_radius_neighbors_3d aggregate currently supports k_max <= 64");
+    k[r] = (uint32_t)k_values[r];
+  }
+  return k;
+}
+}  // namespace
+
+int rtdl_b200_prepare_fixed_radius_ranked_summary_aggregate_batch_graph_3d(
+    void* prepared, void* prepared_queries, const double* radii, const size_t* k_values, size_t request_count,
+    void** graph_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!graph_out) throw std::runtime_error("graph_out must not be null");
+    *graph_out = nullptr;
+    if (!radii && request_count) throw std::runtime_error("radii pointer must not be null when request_count is nonzero");
+    const std::vector<uint32_t> k = graph_k_values(k_values, request_count);
+    Scene* sc = static_cast<Scene*>(prepared);
+    if (sc && sc->dim != 3) throw std::runtime_error("prepared scene is not 3D");
+    *graph_out = summary_graph_create(sc, static_cast<PreparedQueries*>(prepared_queries), radii, k.data(),
+                                      (uint32_t)request_count);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_update_fixed_radius_ranked_summary_aggregate_batch_graph_3d(
+    void* graph, const double* radii, const size_t* k_values, size_t request_count, char* error_out,
+    size_t error_size) {
+  return guarded([&]() {
+    if (!radii && request_count) throw std::runtime_error("radii pointer must not be null when request_count is nonzero");
+    const std::vector<uint32_t> k = graph_k_values(k_values, request_count);
+    summary_graph_update(static_cast<SummaryGraph*>(graph), radii, k.data(), (uint32_t)request_count);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_replay_fixed_radius_ranked_summary_aggregate_batch_graph_3d(
+    void* graph, RtdlFixedRadiusRankedNeighborAggregate* aggregates_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    SummaryGraph* g = static_cast<SummaryGraph*>(graph);
+    if (!g) throw std::runtime_error("prepared fixed_radius_neighbors_3d graph handle must not be null");
+    summary_graph_replay(g, aggregates_out);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_launch_fixed_radius_ranked_summary_aggregate_batch_graph_device_partials_3d(
+    void* graph, uint64_t* partials_device_ptr_out, size_t* partial_count_out, size_t* request_count_out,
+    size_t* query_block_count_out, uint64_t* cuda_stream_ptr_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    SummaryGraph* g = static_cast<SummaryGraph*>(graph);
+    if (!g) throw std::runtime_error("prepared fixed_radius_neighbors_3d graph handle must not be null");
+    if (!partials_device_ptr_out) throw std::runtime_error("partials_device_ptr_out must not be null");
+    if (!partial_count_out) throw std::runtime_error("partial_count_out must not be null");
+    if (!request_count_out) throw std::runtime_error("request_count_out must not be null");
+    if (!query_block_count_out) throw std::runtime_error("query_block_count_out must not be null");
+    if (!cuda_stream_ptr_out) throw std::runtime_error("cuda_stream_ptr_out must not be null");
+    summary_graph_launch(g);
+    const uint32_t R = summary_graph_requests(g);
+    *partials_device_ptr_out = reinterpret_cast<uint64_t>(summary_graph_device_aggregates(g));
+    *partial_count_out = R;
+    *request_count_out = R;
+    *query_block_count_out = 1;
+    *cuda_stream_ptr_out = reinterpret_cast<uint64_t>(summary_graph_stream(g));
+  }, error_out, error_size);
+}
+
+int rtdl_b200_fixed_radius_ranked_summary_aggregate_batch_graph_status_device_3d(
+    void* graph, uint64_t* status_device_ptr_out, uint64_t* fallback_count_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    SummaryGraph* g = static_cast<SummaryGraph*>(graph);
+    if (!g) throw std::runtime_error("prepared fixed_radius_neighbors_3d graph handle must not be null");
+    if (status_device_ptr_out) *status_device_ptr_out = reinterpret_cast<uint64_t>(summary_graph_device_status(g));
+    if (fallback_count_out) *fallback_count_out = summary_graph_fallbacks(g);
+  }, error_out, error_size);
+}
+
+void rtdl_b200_destroy_fixed_radius_ranked_summary_aggregate_batch_graph_3d(void* graph) {
+  summary_graph_destroy(static_cast<SummaryGraph*>(graph));
 }
 
 int rtdl_b200_scene_query_prepared_device(void* scene, void* queries, double radius, size_t k_max, void* rows_dev,

@@ -24,6 +24,7 @@ namespace rtdl_b200 {
 // Counts kernel launches made by this library (reported by
 // rtdl_b200_get_launch_count) and checks the launch status.
 void count_launches(int n);
+unsigned long long launches_counted();
 #define RTDL_LAUNCHED(n)                              \
   do {                                                \
     ::rtdl_b200::count_launches(n);                   \
@@ -160,6 +161,11 @@ void ensure_pool_configured(int device);
 // when *identity_flag != 0) into out[0..n] (u64); out[n] is the total.
 void scan_counts_u64(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag,
                      uint32_t n, unsigned long long* out, cudaStream_t s);
+// The same with a caller-owned workspace of scan_workspace_bytes(n) bytes (no
+// allocation: usable inside stream capture).
+size_t scan_workspace_bytes(uint32_t n);
+void scan_counts_u64_ws(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag, uint32_t n,
+                        unsigned long long* out, void* workspace, cudaStream_t s);
 // Stable LSD radix sort of (key, value) pairs over bits [begin_bit, end_bit),
 // 8 bits per pass.  The result is left in keys/vals.  When *skip_flag != 0
 // (device memory) every pass returns immediately and the input stays in place.
@@ -242,6 +248,29 @@ QueryResult run_ranked_summaries(Scene* sc, const void* queries_dev, uint32_t nq
                                  RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
                                  RtdlFixedRadiusRankedNeighborAggregate* aggregate_host, cudaStream_t s,
                                  PhaseTimer* timer, const PreparedQueries* pq = nullptr);
+// Ranked-summary aggregates of several (radius, k_max) requests over one
+// prepared query set and one plain scene, captured once as a CUDA graph over
+// buffers allocated at creation (worst-case sizes) and replayed on the graph's
+// own stream.  The captured path is the fixed-radius path without host reads:
+// list lengths and refinement counts stay on the device and every pass is
+// launched.  A request whose heavy queries do not resolve in the refinement
+// passes (the plain call takes its generic path for them) is marked in the
+// status words and recomputed by the plain call at replay.
+struct SummaryGraph;
+SummaryGraph* summary_graph_create(Scene* sc, const PreparedQueries* pq, const double* radii, const uint32_t* kmax,
+                                   uint32_t requests);
+void summary_graph_update(SummaryGraph* g, const double* radii, const uint32_t* kmax, uint32_t requests);
+// Enqueues one replay on the graph's stream (nothing is read back).
+void summary_graph_launch(SummaryGraph* g);
+// Replays, reads the aggregates back, recomputes marked requests by the plain call.
+void summary_graph_replay(SummaryGraph* g, RtdlFixedRadiusRankedNeighborAggregate* out);
+const RtdlFixedRadiusRankedNeighborAggregate* summary_graph_device_aggregates(const SummaryGraph* g);
+const unsigned int* summary_graph_device_status(const SummaryGraph* g);
+cudaStream_t summary_graph_stream(const SummaryGraph* g);
+uint32_t summary_graph_requests(const SummaryGraph* g);
+uint64_t summary_graph_fallbacks(const SummaryGraph* g);
+void summary_graph_destroy(SummaryGraph* g);
+
 QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec& bs, void* rows_dev,
                             size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
                             PhaseTimer* timer);

@@ -684,20 +684,27 @@ struct RefineParams {
   const double* rad;       // their radii
   uint32_t nwork;
   uint32_t* cnt;           // out: in-radius count at rad (all of them, not only the kSlab stored)
+  // device-driven form (captured graphs): the count is read from *nwork_dev, the
+  // packet kernel runs when it is >= packet_min and the warp kernel otherwise,
+  // and both stride over the work with whatever grid they were given
+  const unsigned int* nwork_dev;
+  uint32_t packet_min;
 };
+
+__device__ __forceinline__ uint32_t refine_count(const RefineParams& R, bool packet_kernel) {
+  if (!R.nwork_dev) return R.nwork;
+  const uint32_t n = *R.nwork_dev;
+  return (n >= R.packet_min) == packet_kernel ? n : 0u;
+}
 
 // One warp per work item: the warp walks the query's subtree once (node
 // tests warp-uniform) and its lanes test a leaf bucket's points together,
 // appending accepted points with a ballot prefix.  The accept rule is
 // collect_point's (FP32 outside the band, FP64 inside).  Heavy queries are few
 // and scattered, so a packet of 32 of them would walk the union of 32 regions.
-__global__ void __launch_bounds__(256) k_collect_refine(RefineParams R) {
+__device__ __forceinline__ void collect_refine_warp(const RefineParams& R, uint32_t j, int lane, int scene_inexact) {
   const CollectParams& P = R.C;
   const SceneView& S = P.S;
-  const int lane = threadIdx.x & 31;
-  const uint32_t j = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (j >= R.nwork) return;  // whole warp
-  const int scene_inexact = *S.inexact;
   const uint32_t t = R.work[j], qin = P.qorder[t];
   const uint32_t prob = R.qprob ? R.qprob[qin] : 0u;
   const DevBands LB = bands_at_radius(P.bands[prob], R.rad[j]);
@@ -747,16 +754,22 @@ __global__ void __launch_bounds__(256) k_collect_refine(RefineParams R) {
   if (lane == 0) R.cnt[j] = count;
 }
 
+__global__ void __launch_bounds__(256) k_collect_refine(RefineParams R) {
+  const uint32_t n = refine_count(R, false);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t j = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (j >= n) return;  // whole warp
+  const int scene_inexact = *R.C.S.inexact;
+  for (; j < n; j += warps) collect_refine_warp(R, j, threadIdx.x & 31, scene_inexact);
+}
+
 // One thread per work item, warp-packet walks (the form for many heavy
 // queries, which then cluster in space): the lanes of a warp that share a
 // subtree root walk it together (a problem batch can mix roots in a warp).
-__global__ void __launch_bounds__(256) k_collect_refine_packet(RefineParams R) {
+__device__ __forceinline__ void collect_refine_packet(const RefineParams& R, uint32_t j, bool valid,
+                                                      int scene_inexact) {
   const CollectParams& P = R.C;
   const SceneView& S = P.S;
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = j < R.nwork;
-  if (!__any_sync(0xffffffffu, valid)) return;
-  const int scene_inexact = *S.inexact;
   CollectLane L;
   uint32_t prob = 0;
   DevBands LB = P.bands[0];
@@ -798,6 +811,18 @@ __global__ void __launch_bounds__(256) k_collect_refine_packet(RefineParams R) {
   if (valid) R.cnt[j] = L.count;
 }
 
+__global__ void __launch_bounds__(256) k_collect_refine_packet(RefineParams R) {
+  const uint32_t n = refine_count(R, true);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;  // warp-uniform
+  if (base >= n) return;  // whole warp
+  const int scene_inexact = *R.C.S.inexact;
+  for (; base < n; base += stride) {
+    const uint32_t j = base + (threadIdx.x & 31);
+    collect_refine_packet(R, j, j < n, scene_inexact);
+  }
+}
+
 struct RefineUpdate {
   const uint32_t* qorder;
   const uint32_t* qprob;      // nullptr: one problem
@@ -826,11 +851,10 @@ struct RefineUpdate {
   uint32_t* generic_qin;      // last pass: unresolved queries (input index) and their full counts
   uint32_t* generic_m;
   int last;
+  const unsigned int* nwork_dev;  // non-null: the count is read here (captured graphs)
 };
 
-__global__ void k_refine_update(RefineUpdate U) {
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= U.nwork) return;
+__device__ __forceinline__ void refine_update_one(const RefineUpdate& U, uint32_t j) {
   const uint32_t t = U.work[j], qin = U.qorder[t], c = U.cnt[j];
   const uint32_t kmax = U.prob_kmax ? U.prob_kmax[U.qprob ? U.qprob[qin] : 0u] : U.kmax;
   if (c >= kmax && c <= (uint32_t)kSlab) {  // resolved: the slab holds every point within rad
@@ -862,23 +886,30 @@ __global__ void k_refine_update(RefineUpdate U) {
   U.next_full[k] = U.full[j];
 }
 
+__global__ void k_refine_update(RefineUpdate U) {
+  const uint32_t n = U.nwork_dev ? *U.nwork_dev : U.nwork;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    refine_update_one(U, j);
+}
+
 // The first refinement pass's work: the collect pass's heavy queries (listed
 // by input index with their full counts), radius scaled from the full count.
 __global__ void k_refine_init(const uint32_t* heavy_qin, const uint32_t* heavy_m, const uint32_t* heavy_t,
                               uint32_t H, const uint32_t* qprob, const double* prob_radius, double radius,
                               const uint32_t* prob_kmax, uint32_t kmax, uint32_t* work, double* rad, double* lo,
-                              double* hi, uint32_t* full) {
-  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= H) return;
-  const uint32_t qin = heavy_qin[h], p = qprob ? qprob[qin] : 0u;
-  const double r = prob_radius ? prob_radius[p] : radius;
-  const uint32_t k = prob_kmax ? prob_kmax[p] : kmax;
-  const uint32_t m = heavy_m[h];
-  work[h] = heavy_t[h];
-  rad[h] = r * cbrt(2.0 * k / (double)m);
-  lo[h] = 0.0;
-  hi[h] = r;
-  full[h] = m;
+                              double* hi, uint32_t* full, const unsigned int* H_dev) {
+  if (H_dev) H = *H_dev;  // captured graphs: the collect pass's heavy count
+  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < H; h += gridDim.x * blockDim.x) {
+    const uint32_t qin = heavy_qin[h], p = qprob ? qprob[qin] : 0u;
+    const double r = prob_radius ? prob_radius[p] : radius;
+    const uint32_t k = prob_kmax ? prob_kmax[p] : kmax;
+    const uint32_t m = heavy_m[h];
+    work[h] = heavy_t[h];
+    rad[h] = r * cbrt(2.0 * k / (double)m);
+    lo[h] = 0.0;
+    hi[h] = r;
+    full[h] = m;
+  }
 }
 
 // ---- emit: warp per query -----------------------------------------------------
@@ -1284,16 +1315,21 @@ __global__ void k_proc_offsets(const uint32_t* qorder, const uint32_t* qrank, co
 constexpr int kEmitListThreads = 128;
 
 template <int E, bool DEFER>
-__global__ void __launch_bounds__(kEmitListThreads) k_emit_list(EmitParams P, const uint32_t* work, uint32_t nwork) {
+// nwork_dev non-null (captured graphs): the list length is read there and the
+// warps stride over the list.
+__global__ void __launch_bounds__(kEmitListThreads)
+    k_emit_list(EmitParams P, const uint32_t* work, uint32_t nwork, const unsigned int* nwork_dev) {
   __shared__ uint32_t wbuf[DEFER ? 1 : kEmitListThreads / 32][DEFER ? 1 : 32 * E];
   const int lane = threadIdx.x & 31;
-  const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (j >= nwork) return;  // whole warp
-  const uint32_t t = work[j];
-  EmitQuery q;
-  emit_load(P, t, lane, q);
-  const int n = (int)(q.qi.meta & kQueryCountMask);
-  emit_query<E, DEFER>(P, t, q, n, lane, DEFER ? nullptr : wbuf[threadIdx.x >> 5]);
+  if (nwork_dev) nwork = *nwork_dev;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nwork; j += warps) {  // whole warps
+    const uint32_t t = work[j];
+    EmitQuery q;
+    emit_load(P, t, lane, q);
+    const int n = (int)(q.qi.meta & kQueryCountMask);
+    emit_query<E, DEFER>(P, t, q, n, lane, DEFER ? nullptr : wbuf[threadIdx.x >> 5]);
+  }
 }
 
 __global__ void k_fill_i32(int* out, uint32_t n, int v) {
@@ -2022,7 +2058,8 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
   uint32_t* gen_m = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
   unsigned int* next_count = static_cast<unsigned int*>(alloc(sizeof(unsigned int)));
   k_refine_init<<<div_up(H, 256), 256, 0, s>>>(heavy_list, heavy_m, heavy_t, H, qp.qprob, qp.prob_radius, radius,
-                                               qp.prob_kmax, kmax, work[0], rad[0], lo[0], hi[0], full[0]);
+                                               qp.prob_kmax, kmax, work[0], rad[0], lo[0], hi[0], full[0],
+                                               nullptr);
   RTDL_LAUNCHED(1);
   Readback* rb = pinned_readback();
   uint32_t n = H;
@@ -2036,6 +2073,8 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     R.rad = rad[cur];
     R.nwork = n;
     R.cnt = cnt;
+    R.nwork_dev = nullptr;
+    R.packet_min = 0;
     if (n >= qp.nproc / 8)  // many heavy queries: they cluster, a packet of them walks one region
       k_collect_refine_packet<<<div_up(n, 256), 256, 0, s>>>(R);
     else
@@ -2058,6 +2097,7 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     U.full = full[cur];
     U.cnt = cnt;
     U.nwork = n;
+    U.nwork_dev = nullptr;
     U.next_work = work[cur ^ 1];
     U.next_rad = rad[cur ^ 1];
     U.next_lo = lo[cur ^ 1];
@@ -2082,6 +2122,31 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
   out.mid = rb->mid;
   out.big = rb->big;
   return out;
+}
+
+// The collect pass, by the tuning's traversal (a problem batch walks in packets).
+void launch_collect(const CollectParams& C, uint32_t np, uint32_t nq, bool batch, bool stats, cudaStream_t s) {
+  const int threads = tuning().block_threads;
+  const bool packet = tuning().traversal != 1 || batch;
+  if (packet) {
+    const unsigned int grid = div_up(np, threads);
+    const bool cube = tuning().traversal == 2;
+    // occupancy bounds chosen so neither variant spills (32 and 40 registers)
+    if (batch)  // several problems (traversal counters are not gathered here)
+      k_collect_packet<false, false, true, 5><<<grid, threads, 0, s>>>(C);
+    else if (stats)
+      cube ? k_collect_packet<true, true, false, 1><<<grid, threads, 0, s>>>(C)
+           : k_collect_packet<true, false, false, 1><<<grid, threads, 0, s>>>(C);
+    else
+      cube ? k_collect_packet<false, true, false, 6><<<grid, threads, 0, s>>>(C)
+           : k_collect_packet<false, false, false, 7><<<grid, threads, 0, s>>>(C);
+  } else {
+    if (stats)
+      k_collect<true><<<div_up(nq, threads), threads, 0, s>>>(C);
+    else
+      k_collect<false><<<div_up(nq, threads), threads, 0, s>>>(C);
+  }
+  RTDL_LAUNCHED(1);
 }
 
 void check_readback(const Readback& r) {
@@ -2182,28 +2247,8 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       C.stats = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * kStatCount, s));
       RTDL_CUDA_CHECK(cudaMemsetAsync(C.stats, 0, sizeof(unsigned long long) * kStatCount, s));
     }
-    const int threads = tuning().block_threads;
     if (timer) timer->mark("setup");
-    const bool packet = tuning().traversal != 1 || bs != nullptr;  // a problem batch walks in packets
-    if (packet) {
-      const unsigned int grid = div_up(np, threads);
-      const bool cube = tuning().traversal == 2;
-      // occupancy bounds chosen so neither variant spills (32 and 40 registers)
-      if (bs)  // several problems (traversal counters are not gathered here)
-        k_collect_packet<false, false, true, 5><<<grid, threads, 0, s>>>(C);
-      else if (stats)
-        cube ? k_collect_packet<true, true, false, 1><<<grid, threads, 0, s>>>(C)
-             : k_collect_packet<true, false, false, 1><<<grid, threads, 0, s>>>(C);
-      else
-        cube ? k_collect_packet<false, true, false, 6><<<grid, threads, 0, s>>>(C)
-             : k_collect_packet<false, false, false, 7><<<grid, threads, 0, s>>>(C);
-    } else {
-      if (stats)
-        k_collect<true><<<div_up(nq, threads), threads, 0, s>>>(C);
-      else
-        k_collect<false><<<div_up(nq, threads), threads, 0, s>>>(C);
-    }
-    RTDL_LAUNCHED(1);
+    launch_collect(C, np, nq, bs != nullptr, stats, s);
     if (stats) {
       RTDL_CUDA_CHECK(cudaMemcpyAsync(last_stats().data(), C.stats, sizeof(unsigned long long) * kStatCount,
                                       cudaMemcpyDeviceToHost, s));
@@ -2275,12 +2320,12 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     RTDL_LAUNCHED(1);
     if (mid > 0) {
       k_emit_list<4, true><<<div_up((uint64_t)mid * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, mid_list,
-                                                                                                  mid);
+                                                                                                  mid, nullptr);
       RTDL_LAUNCHED(1);
     }
     if (big > 0) {
       k_emit_list<8, false><<<div_up((uint64_t)big * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, big_list,
-                                                                                                   big);
+                                                                                                   big, nullptr);
       RTDL_LAUNCHED(1);
     }
     k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
@@ -2381,6 +2426,378 @@ QueryResult run_query_prepared(Scene* sc, const PreparedQueries* pq, double radi
   if (timer) timer->mark("start");
   return run_radius_query(sc, pq->raw, pq->n, kFrn, radius, kmax, rows_dev, rows_capacity, nullptr, overflow_dev, s,
                           timer, nullptr, nullptr, pq);
+}
+
+// ---- captured summary graphs ------------------------------------------------
+namespace {
+
+constexpr unsigned int kGraphStatusOverflow = 1u;  // traversal stack overflow (the plain call raises it)
+constexpr unsigned int kGraphStatusGeneric = 2u;   // heavy queries left for the generic path
+
+__global__ void k_graph_status(const unsigned int* small, const unsigned int* pass_count, uint32_t requests,
+                               unsigned int* status) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < requests; r += gridDim.x * blockDim.x)
+    status[r] = ((small[8 * (size_t)r + 1] & 1u) ? kGraphStatusOverflow : 0u) |
+                (pass_count[(size_t)r * kRefinePasses + kRefinePasses - 1] ? kGraphStatusGeneric : 0u);
+}
+
+constexpr unsigned int kGraphStrideBlocks = kSmCount * 8;  // grid of the kernels that stride over device counts
+
+}  // namespace
+
+struct SummaryGraph {
+  Scene* sc = nullptr;
+  const PreparedQueries* pq = nullptr;
+  cudaStream_t stream = nullptr;
+  uint32_t R = 0, nq = 0, kcap = 0;  // requests, queries, row capacity per query
+  std::vector<double> radius;
+  std::vector<uint32_t> kmax;
+  std::vector<void*> buffers;  // device, released at destroy
+  DevBands* bands = nullptr;   // one per request
+  unsigned long long* slab = nullptr;
+  uint32_t* counts = nullptr;
+  QueryInfo* qinfo = nullptr;
+  uint8_t* flags = nullptr;
+  uint32_t *heavy_list = nullptr, *heavy_m = nullptr, *heavy_t = nullptr;
+  uint32_t *mid_list = nullptr, *big_list = nullptr, *fix_list = nullptr;
+  unsigned int* small = nullptr;       // 8 counters per request (CollectParams::small)
+  unsigned int* pass_count = nullptr;  // kRefinePasses per request: work left after each pass
+  unsigned long long *offsets = nullptr, *poff = nullptr;
+  void* scan_ws = nullptr;
+  void* rows = nullptr;  // nq * kcap rows
+  uint32_t* work[2] = {nullptr, nullptr};
+  double *rad[2] = {nullptr, nullptr}, *lo[2] = {nullptr, nullptr}, *hi[2] = {nullptr, nullptr};
+  uint32_t* full[2] = {nullptr, nullptr};
+  uint32_t *cnt = nullptr, *gen_qin = nullptr, *gen_m = nullptr;
+  SummaryPartial* partial = nullptr;
+  uint32_t summary_blocks = 0;
+  RtdlFixedRadiusRankedNeighborAggregate* agg = nullptr;  // one per request
+  unsigned int* status = nullptr;                         // one per request
+  RtdlFixedRadiusRankedNeighborAggregate* agg_host = nullptr;  // pinned
+  unsigned int* status_host = nullptr;                          // pinned
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int kernels = 0;  // kernel nodes per replay
+  uint64_t fallbacks = 0;
+};
+
+namespace {
+
+void graph_check_requests(const Scene* sc, const double* radii, const uint32_t* kmax, uint32_t requests) {
+  if (requests == 0) throw std::runtime_error("fixed_radius_neighbors_3d graph request_count must be positive");
+  if (!radii || !kmax) throw std::runtime_error("radii and k_values must not be null");
+  for (uint32_t r = 0; r < requests; ++r) {
+    if (!(radii[r] >= 0.0)) throw std::runtime_error("fixed_radius_neighbors_3d radius must be non-negative");
+    if (radii[r] > sc->max_radius + 1.0e-7)
+      throw std::runtime_error("fixed_radius_neighbors_3d radius exceeds prepared max_radius");
+    if (kmax[r] == 0) throw std::runtime_error("fixed_radius_neighbors_3d k_max must be positive");
+    if (kmax[r] > 64)
+      throw std::runtime_error("prepared ranked fixed_radius_neighbors_3d aggregate currently supports k_max <= 64");
+  }
+}
+
+// One request's kernels, device-driven (no host reads, no allocation).
+void graph_enqueue_request(SummaryGraph* g, uint32_t r, cudaStream_t s) {
+  Scene* sc = g->sc;
+  const PreparedQueries* pq = g->pq;
+  const uint32_t nq = g->nq, np = nq;
+  const double radius = g->radius[r];
+  const uint32_t kmax = g->kmax[r];
+  unsigned int* small = g->small + 8 * (size_t)r;
+  unsigned int* pc = g->pass_count + (size_t)r * kRefinePasses;
+  k_bands<<<1, 32, 0, s>>>(sc->stats, pq->qst, radius, 1, g->bands + r);
+  RTDL_LAUNCHED(1);
+  CollectParams C;
+  C.S = sc->view();
+  C.qpts = pq->qpts;
+  C.qraw = static_cast<const double*>(pq->raw);
+  C.qstride = sc->dim == 3 ? 4 : 3;
+  C.qorder = pq->qorder;
+  C.nq = np;
+  C.kmax = kmax;
+  C.bands = g->bands + r;
+  C.warp_prob = nullptr;
+  C.prob_kmax = nullptr;
+  C.slab = g->slab;
+  C.counts = g->counts;
+  C.qinfo = g->qinfo;
+  C.flags = g->flags;
+  C.heavy_list = g->heavy_list;
+  C.heavy_m = g->heavy_m;
+  C.heavy_t = g->heavy_t;
+  C.mid_list = g->mid_list;
+  C.big_list = g->big_list;
+  C.small = small;
+  C.overflow_out = nullptr;
+  C.stats = nullptr;
+  launch_collect(C, np, nq, false, false, s);
+  scan_counts_u64_ws(g->counts, pq->oorder, pq->identity, nq, g->offsets, g->scan_ws, s);
+  // heavy queries: every refinement pass is launched; each reads its work count
+  k_refine_init<<<kSmCount * 4, 256, 0, s>>>(g->heavy_list, g->heavy_m, g->heavy_t, 0, nullptr, nullptr, radius,
+                                             nullptr, kmax, g->work[0], g->rad[0], g->lo[0], g->hi[0], g->full[0],
+                                             small);
+  RTDL_LAUNCHED(1);
+  int cur = 0;
+  for (int pass = 0; pass < kRefinePasses; ++pass) {
+    const unsigned int* n_dev = pass == 0 ? small : pc + pass - 1;
+    RefineParams R;
+    R.C = C;
+    R.qprob = nullptr;
+    R.work = g->work[cur];
+    R.rad = g->rad[cur];
+    R.nwork = 0;
+    R.cnt = g->cnt;
+    R.nwork_dev = n_dev;
+    R.packet_min = np / 8;  // the plain call's choice between the two forms
+    k_collect_refine_packet<<<kGraphStrideBlocks, 256, 0, s>>>(R);
+    k_collect_refine<<<kGraphStrideBlocks, 256, 0, s>>>(R);
+    RefineUpdate U;
+    U.qorder = pq->qorder;
+    U.qprob = nullptr;
+    U.prob_kmax = nullptr;
+    U.kmax = kmax;
+    U.qinfo = g->qinfo;
+    U.flags = g->flags;
+    U.mid_list = g->mid_list;
+    U.big_list = g->big_list;
+    U.small = small;
+    U.work = g->work[cur];
+    U.rad = g->rad[cur];
+    U.lo = g->lo[cur];
+    U.hi = g->hi[cur];
+    U.full = g->full[cur];
+    U.cnt = g->cnt;
+    U.nwork = 0;
+    U.next_work = g->work[cur ^ 1];
+    U.next_rad = g->rad[cur ^ 1];
+    U.next_lo = g->lo[cur ^ 1];
+    U.next_hi = g->hi[cur ^ 1];
+    U.next_full = g->full[cur ^ 1];
+    U.next_count = pc + pass;
+    U.generic_qin = g->gen_qin;
+    U.generic_m = g->gen_m;
+    U.last = pass == kRefinePasses - 1 ? 1 : 0;
+    U.nwork_dev = n_dev;
+    k_refine_update<<<kSmCount * 4, 256, 0, s>>>(U);
+    RTDL_LAUNCHED(3);
+    cur ^= 1;
+  }
+  k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(pq->qorder, pq->qrank, g->offsets, np, g->poff);
+  RTDL_LAUNCHED(1);
+  EmitParams E;
+  E.S = sc->view();
+  E.nq = np;
+  E.slab = g->slab;
+  E.qinfo = g->qinfo;
+  E.poff = g->poff;
+  E.sink.rows = g->rows;
+  E.sink.capacity = (unsigned long long)nq * g->kcap;
+  E.sink.ranked = 0;
+  E.fix_list = g->fix_list;
+  E.fix_count = small + 4;
+  k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
+  k_emit_list<4, true><<<kGraphStrideBlocks, kEmitListThreads, 0, s>>>(E, g->mid_list, 0, small + 2);
+  k_emit_list<8, false><<<kGraphStrideBlocks, kEmitListThreads, 0, s>>>(E, g->big_list, 0, small + 3);
+  k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
+  k_summarize<<<g->summary_blocks, kSummaryThreads, 0, s>>>(static_cast<const RtdlFixedRadiusNeighborRow*>(g->rows),
+                                                            g->offsets, pq->oorder, pq->identity, pq->qpts, nq,
+                                                            nullptr, g->partial);
+  k_summary_final<<<1, 1024, 0, s>>>(g->partial, g->summary_blocks, nq, g->agg + r);
+  RTDL_LAUNCHED(6);
+}
+
+void graph_release(SummaryGraph* g) {
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  g->exec = nullptr;
+  g->graph = nullptr;
+}
+
+void graph_capture(SummaryGraph* g) {
+  graph_release(g);
+  cudaStream_t s = g->stream;
+  const unsigned long long before = launches_counted();
+  RTDL_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  try {
+    RTDL_CUDA_CHECK(cudaMemsetAsync(g->small, 0, sizeof(unsigned int) * 8 * (size_t)g->R, s));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(g->pass_count, 0, sizeof(unsigned int) * kRefinePasses * (size_t)g->R, s));
+    for (uint32_t r = 0; r < g->R; ++r) graph_enqueue_request(g, r, s);
+    k_graph_status<<<div_up(g->R, 256), 256, 0, s>>>(g->small, g->pass_count, g->R, g->status);
+    RTDL_LAUNCHED(1);
+  } catch (...) {
+    cudaGraph_t partial = nullptr;
+    cudaStreamEndCapture(s, &partial);
+    if (partial) cudaGraphDestroy(partial);
+    cudaGetLastError();
+    count_launches(-(int)(launches_counted() - before));
+    throw;
+  }
+  // captured kernels are counted when a replay launches them
+  count_launches(-(int)(launches_counted() - before));
+  RTDL_CUDA_CHECK(cudaStreamEndCapture(s, &g->graph));
+  RTDL_CUDA_CHECK(cudaGraphInstantiate(&g->exec, g->graph, 0));
+  size_t n = 0;
+  RTDL_CUDA_CHECK(cudaGraphGetNodes(g->graph, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  RTDL_CUDA_CHECK(cudaGraphGetNodes(g->graph, nodes.data(), &n));
+  g->kernels = 0;
+  for (size_t i = 0; i < n; ++i) {
+    cudaGraphNodeType t;
+    RTDL_CUDA_CHECK(cudaGraphNodeGetType(nodes[i], &t));
+    if (t == cudaGraphNodeTypeKernel) ++g->kernels;
+  }
+}
+
+void graph_set_requests(SummaryGraph* g, const double* radii, const uint32_t* kmax, uint32_t requests) {
+  g->radius.assign(radii, radii + requests);
+  g->kmax.assign(kmax, kmax + requests);
+}
+
+// Row buffer for the largest k_max of the requests (grown by an update, never shrunk).
+void graph_size_rows(SummaryGraph* g) {
+  uint32_t k = 1;
+  for (uint32_t v : g->kmax) k = v > k ? v : k;
+  if (g->rows && k <= g->kcap) return;
+  dev_free(g->rows, g->stream);
+  g->rows = nullptr;
+  g->kcap = 0;
+  g->rows = dev_alloc(sizeof(RtdlFixedRadiusNeighborRow) * (size_t)g->nq * k, g->stream);
+  g->kcap = k;
+}
+
+}  // namespace
+
+SummaryGraph* summary_graph_create(Scene* sc, const PreparedQueries* pq, const double* radii, const uint32_t* kmax,
+                                   uint32_t requests) {
+  if (!sc) throw std::runtime_error("prepared OptiX fixed-radius-neighbor 3D handle must not be null");
+  if (!pq) throw std::runtime_error("prepared fixed-radius query handle must not be null");
+  if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
+  if (pq->dim != sc->dim) throw std::runtime_error("prepared queries and scene differ in dimension");
+  graph_check_requests(sc, radii, kmax, requests);
+  if (pq->n == 0 || sc->n == 0)
+    throw std::runtime_error("fixed_radius_neighbors_3d graph requires non-empty prepared search and query handles");
+  SummaryGraph* g = new SummaryGraph();
+  g->sc = sc;
+  g->pq = pq;
+  g->R = requests;
+  g->nq = pq->n;
+  graph_set_requests(g, radii, kmax, requests);
+  try {
+    RTDL_CUDA_CHECK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    cudaStream_t s = g->stream;
+    // the scene and the prepared queries were built on their own streams
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(sc->stream));
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(pq->stream));
+    unsigned int bad[2] = {0, 0};
+    RTDL_CUDA_CHECK(cudaMemcpy(&bad[0], &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+    RTDL_CUDA_CHECK(cudaMemcpy(&bad[1], &pq->qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+    if (bad[0] || bad[1]) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+    auto alloc = [&](size_t bytes) {
+      void* p = dev_alloc(bytes ? bytes : 1, s);
+      g->buffers.push_back(p);
+      return p;
+    };
+    const size_t n = g->nq, R = g->R;
+    g->bands = static_cast<DevBands*>(alloc(sizeof(DevBands) * R));
+    g->slab = static_cast<unsigned long long*>(alloc(sizeof(unsigned long long) * slab_base(g->nq)));
+    g->counts = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->qinfo = static_cast<QueryInfo*>(alloc(sizeof(QueryInfo) * n));
+    g->flags = static_cast<uint8_t*>(alloc(n));
+    g->heavy_list = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->heavy_m = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->heavy_t = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->mid_list = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->big_list = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->fix_list = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->small = static_cast<unsigned int*>(alloc(sizeof(unsigned int) * 8 * R));
+    g->pass_count = static_cast<unsigned int*>(alloc(sizeof(unsigned int) * kRefinePasses * R));
+    g->offsets = static_cast<unsigned long long*>(alloc(sizeof(unsigned long long) * (n + 1)));
+    g->poff = static_cast<unsigned long long*>(alloc(sizeof(unsigned long long) * n));
+    g->scan_ws = alloc(scan_workspace_bytes(g->nq));
+    graph_size_rows(g);
+    for (int b = 0; b < 2; ++b) {
+      g->work[b] = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+      g->rad[b] = static_cast<double*>(alloc(sizeof(double) * n));
+      g->lo[b] = static_cast<double*>(alloc(sizeof(double) * n));
+      g->hi[b] = static_cast<double*>(alloc(sizeof(double) * n));
+      g->full[b] = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    }
+    g->cnt = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->gen_qin = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->gen_m = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->summary_blocks = div_up((uint64_t)n * 32, kSummaryThreads);
+    g->partial = static_cast<SummaryPartial*>(alloc(sizeof(SummaryPartial) * g->summary_blocks));
+    g->agg = static_cast<RtdlFixedRadiusRankedNeighborAggregate*>(
+        alloc(sizeof(RtdlFixedRadiusRankedNeighborAggregate) * R));
+    g->status = static_cast<unsigned int*>(alloc(sizeof(unsigned int) * R));
+    RTDL_CUDA_CHECK(cudaMallocHost(&g->agg_host, sizeof(RtdlFixedRadiusRankedNeighborAggregate) * R));
+    RTDL_CUDA_CHECK(cudaMallocHost(&g->status_host, sizeof(unsigned int) * R));
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // allocations ready before capture
+    graph_capture(g);
+  } catch (...) {
+    summary_graph_destroy(g);
+    throw;
+  }
+  return g;
+}
+
+void summary_graph_update(SummaryGraph* g, const double* radii, const uint32_t* kmax, uint32_t requests) {
+  if (!g) throw std::runtime_error("prepared fixed_radius_neighbors_3d graph handle must not be null");
+  if (requests != g->R)
+    throw std::runtime_error("fixed_radius_neighbors_3d graph request update requires unchanged request_count");
+  graph_check_requests(g->sc, radii, kmax, requests);
+  RTDL_CUDA_CHECK(cudaStreamSynchronize(g->stream));  // no replay in flight while the graph is replaced
+  graph_set_requests(g, radii, kmax, requests);
+  graph_size_rows(g);
+  RTDL_CUDA_CHECK(cudaStreamSynchronize(g->stream));
+  graph_capture(g);
+}
+
+void summary_graph_launch(SummaryGraph* g) {
+  if (!g || !g->exec) throw std::runtime_error("prepared fixed_radius_neighbors_3d graph handle must not be null");
+  RTDL_CUDA_CHECK(cudaGraphLaunch(g->exec, g->stream));
+  count_launches(g->kernels);
+}
+
+void summary_graph_replay(SummaryGraph* g, RtdlFixedRadiusRankedNeighborAggregate* out) {
+  if (!out) throw std::runtime_error("aggregates_out must not be null");
+  summary_graph_launch(g);
+  cudaStream_t s = g->stream;
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(g->agg_host, g->agg, sizeof(RtdlFixedRadiusRankedNeighborAggregate) * g->R,
+                                  cudaMemcpyDeviceToHost, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(g->status_host, g->status, sizeof(unsigned int) * g->R, cudaMemcpyDeviceToHost, s));
+  RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+  for (uint32_t r = 0; r < g->R; ++r) {
+    if (g->status_host[r] & kGraphStatusOverflow) throw std::runtime_error("BVH traversal stack overflow");
+    if (g->status_host[r] & kGraphStatusGeneric) {
+      // the plain call, with its generic path for the queries refinement left
+      run_ranked_summaries(g->sc, nullptr, g->nq, g->radius[r], g->kmax[r], nullptr, &out[r], s, nullptr, g->pq);
+      ++g->fallbacks;
+    } else {
+      out[r] = g->agg_host[r];
+    }
+  }
+}
+
+const RtdlFixedRadiusRankedNeighborAggregate* summary_graph_device_aggregates(const SummaryGraph* g) { return g->agg; }
+const unsigned int* summary_graph_device_status(const SummaryGraph* g) { return g->status; }
+cudaStream_t summary_graph_stream(const SummaryGraph* g) { return g->stream; }
+uint32_t summary_graph_requests(const SummaryGraph* g) { return g->R; }
+uint64_t summary_graph_fallbacks(const SummaryGraph* g) { return g->fallbacks; }
+
+void summary_graph_destroy(SummaryGraph* g) {
+  if (!g) return;
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  graph_release(g);
+  for (void* p : g->buffers) dev_free(p, g->stream);
+  dev_free(g->rows, g->stream);
+  if (g->stream) {
+    cudaStreamSynchronize(g->stream);
+    cudaStreamDestroy(g->stream);
+  }
+  if (g->agg_host) cudaFreeHost(g->agg_host);
+  if (g->status_host) cudaFreeHost(g->status_host);
+  delete g;
 }
 
 namespace {

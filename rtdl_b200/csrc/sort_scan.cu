@@ -142,15 +142,15 @@ __global__ void k_scan_down(const uint32_t* counts, const uint32_t* order, const
 
 template <typename Out>
 void scan_impl(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag, uint32_t n,
-               Out* out, cudaStream_t s) {
+               Out* out, Out* workspace, cudaStream_t s) {
   uint32_t tiles = div_up(n, kScanTile);
   if (tiles == 0) tiles = 1;
-  Out* sums = static_cast<Out*>(dev_alloc(sizeof(Out) * tiles, s));
+  Out* sums = workspace ? workspace : static_cast<Out*>(dev_alloc(sizeof(Out) * tiles, s));
   k_scan_reduce<Out><<<tiles, kScanThreads, 0, s>>>(counts, order, identity_flag, n, sums);
   k_scan_tile_sums<Out><<<1, 1024, 0, s>>>(sums, tiles, out + n);
   k_scan_down<Out><<<tiles, kScanThreads, 0, s>>>(counts, order, identity_flag, n, sums, out);
   RTDL_LAUNCHED(3);
-  dev_free(sums, s);
+  if (!workspace) dev_free(sums, s);
 }
 
 __global__ void k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift, uint32_t* hist,
@@ -253,7 +253,17 @@ __global__ void k_iota(uint32_t* out, uint32_t n) {
 
 void scan_counts_u64(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag, uint32_t n,
                      unsigned long long* out, cudaStream_t s) {
-  scan_impl<unsigned long long>(counts, order, identity_flag, n, out, s);
+  scan_impl<unsigned long long>(counts, order, identity_flag, n, out, nullptr, s);
+}
+
+size_t scan_workspace_bytes(uint32_t n) {
+  const uint32_t tiles = div_up(n, kScanTile);
+  return sizeof(unsigned long long) * (tiles ? tiles : 1);
+}
+
+void scan_counts_u64_ws(const uint32_t* counts, const uint32_t* order, const unsigned int* identity_flag, uint32_t n,
+                        unsigned long long* out, void* workspace, cudaStream_t s) {
+  scan_impl<unsigned long long>(counts, order, identity_flag, n, out, static_cast<unsigned long long*>(workspace), s);
 }
 
 void iota_u32(uint32_t* out, uint32_t n, cudaStream_t s) {

@@ -777,11 +777,252 @@ class PreparedB200FixedRadiusNeighbors3D:
         _native.check_status(status, err)
         return {f: (float(getattr(agg, f)) if f == "sum_distance" else int(getattr(agg, f))) for f in AGGREGATE_FIELDS}
 
+    def prepare_ranked_summary_prepared_queries_batch_graph(
+            self, prepared_queries: B200Queries, requests, *,
+            precision: str = "float32") -> "PreparedB200FixedRadiusRankedSummaryAggregateBatchGraph3D":
+        """A captured CUDA graph of ranked-summary aggregates for several (radius, k_max)
+        requests over one prepared query set (``optix_runtime.py:2838-2856``)."""
+        if self._closed:
+            raise RuntimeError("prepared b200 fixed-radius-neighbor 3D handle is closed")
+        if prepared_queries.closed:
+            raise RuntimeError("prepared b200 fixed-radius query handle is closed")
+        return PreparedB200FixedRadiusRankedSummaryAggregateBatchGraph3D(self, prepared_queries, requests,
+                                                                          precision=precision)
+
     def close(self) -> None:
         if not self._closed:
             if self._handle.value:
                 _native.load_library().rtdl_b200_destroy_prepared_fixed_radius_neighbors_3d(self._handle)
             self._closed = True
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _normalize_graph_requests(owner: PreparedB200FixedRadiusNeighbors3D, requests) -> tuple:
+    """Request checks of the reference's graph (``optix_runtime.py:2292-2312``)."""
+    normalized = tuple(dict(r) for r in requests)
+    if not normalized:
+        raise ValueError("prepared fixed-radius aggregate graph requires at least one request")
+    out = []
+    for r in normalized:
+        radius = float(r["radius"])
+        k_max = int(r["k_max"])
+        if radius < 0:
+            raise ValueError("radius must be non-negative")
+        if radius > owner.max_radius:
+            raise ValueError("radius must be less than or equal to prepared max_radius")
+        if k_max <= 0:
+            raise ValueError("k_max must be positive")
+        if k_max > 64:
+            raise ValueError("PreparedB200FixedRadiusNeighbors3D prepared query aggregate graph currently supports "
+                             "k_max <= 64")
+        out.append({"radius": radius, "k_max": k_max})
+    return tuple(out)
+
+
+class _DeviceArray:
+    """A raw device buffer exposed through ``__cuda_array_interface__`` (read by torch.as_tensor)."""
+
+    def __init__(self, address: int, nbytes: int, stream: int):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (address, False),
+                                         "version": 3, "stream": stream or None}
+
+
+class PreparedB200FixedRadiusRankedSummaryAggregateBatchGraph3D:
+    """Captured CUDA graph of prepared-query ranked-summary aggregates; mirrors
+    ``PreparedOptixFixedRadiusRankedSummaryAggregateBatchGraph3D`` (``optix_runtime.py:1912-2289``).
+
+    The graph holds the whole fixed-radius path of every request (collect, refinement of heavy
+    queries, emit, summary, aggregate) over buffers allocated once, and runs on its own stream.
+    The aggregates are exact (FP64 distances) whatever ``precision`` names; requests whose heavy
+    queries the captured refinement leaves unresolved are recomputed by the plain call."""
+
+    def __init__(self, owner: PreparedB200FixedRadiusNeighbors3D, prepared_queries: B200Queries, requests, *,
+                 precision: str = "float32"):
+        if precision not in {"float32", "float64"}:
+            raise ValueError("precision must be 'float32' or 'float64'")
+        if owner.closed:
+            raise RuntimeError("prepared b200 fixed-radius-neighbor 3D handle is closed")
+        if prepared_queries.closed:
+            raise RuntimeError("prepared b200 fixed-radius query handle is closed")
+        self._owner = owner
+        self._prepared_queries = prepared_queries
+        self._requests = _normalize_graph_requests(owner, requests)
+        self._precision = precision
+        self._handle = ctypes.c_void_p()
+        self._closed = False
+        self._request_buffer_update_count = 0
+        self._empty = prepared_queries.count == 0 or owner._count == 0
+        if self._empty:
+            return
+        self._call("rtdl_b200_prepare_fixed_radius_ranked_summary_aggregate_batch_graph_3d", owner._handle,
+                   prepared_queries.handle, *self._request_arrays(self._requests), ctypes.byref(self._handle))
+
+    @staticmethod
+    def _request_arrays(requests):
+        n = len(requests)
+        radii = (ctypes.c_double * n)(*[r["radius"] for r in requests])
+        k_values = (ctypes.c_size_t * n)(*[r["k_max"] for r in requests])
+        return radii, k_values, ctypes.c_size_t(n)
+
+    @staticmethod
+    def _call(name, *args):
+        err = _native.error_buffer()
+        status = getattr(_native.load_library(), name)(*args, err, len(err))
+        _native.check_status(status, err)
+
+    def _check_open(self):
+        if self._closed:
+            raise RuntimeError("prepared fixed-radius aggregate graph handle is closed")
+        if self._owner.closed:
+            raise RuntimeError("prepared b200 fixed-radius-neighbor 3D handle is closed")
+        if self._prepared_queries.closed:
+            raise RuntimeError("prepared b200 fixed-radius query handle is closed")
+
+    @property
+    def closed(self) -> bool:
+        return self._closed
+
+    @property
+    def request_buffer_update_count(self) -> int:
+        return self._request_buffer_update_count
+
+    @property
+    def fallback_count(self) -> int:
+        """Requests recomputed by the plain call so far (heavy queries the refinement left)."""
+        if self._empty:
+            return 0
+        fb = ctypes.c_uint64()
+        self._call("rtdl_b200_fixed_radius_ranked_summary_aggregate_batch_graph_status_device_3d", self._handle,
+                   None, ctypes.byref(fb))
+        return int(fb.value)
+
+    def _result(self, index: int, agg: dict, **extra) -> dict:
+        out = {
+            "query_count": int(agg["query_count"]),
+            "bounded_neighbor_count": int(agg["bounded_neighbor_count"]),
+            "nearest_id_checksum": int(agg["nearest_id_checksum"]),
+            "kth_id_checksum": int(agg["kth_id_checksum"]),
+            "sum_distance": float(agg["sum_distance"]),
+            "precision": self._precision,
+            "query_resident": True,
+            "request_index": index,
+            "radius": float(self._requests[index]["radius"]),
+            "k_max": int(self._requests[index]["k_max"]),
+            "cuda_graph_replay": True,
+            "request_buffer_update_count": self._request_buffer_update_count,
+        }
+        out.update(extra)
+        return out
+
+    def _empty_results(self, **extra) -> tuple:
+        zero = {"query_count": int(self._prepared_queries.count), "bounded_neighbor_count": 0,
+                "nearest_id_checksum": 0, "kth_id_checksum": 0, "sum_distance": 0.0}
+        return tuple(self._result(i, zero, **extra) for i in range(len(self._requests)))
+
+    def update_requests(self, requests) -> None:
+        """New (radius, k_max) requests, same count; the graph is captured again."""
+        self._check_open()
+        normalized = _normalize_graph_requests(self._owner, requests)
+        if len(normalized) != len(self._requests):
+            raise ValueError("prepared fixed-radius aggregate graph request updates must keep request_count unchanged")
+        if not self._empty:
+            self._call("rtdl_b200_update_fixed_radius_ranked_summary_aggregate_batch_graph_3d", self._handle,
+                       *self._request_arrays(normalized))
+        self._requests = normalized
+        self._request_buffer_update_count += 1
+
+    def replay(self) -> tuple:
+        self._check_open()
+        if self._empty:
+            return self._empty_results()
+        aggs = (_native.RtdlFixedRadiusRankedNeighborAggregate * len(self._requests))()
+        self._call("rtdl_b200_replay_fixed_radius_ranked_summary_aggregate_batch_graph_3d", self._handle, aggs)
+        return tuple(self._result(i, {f: getattr(a, f) for f in AGGREGATE_FIELDS}) for i, a in enumerate(aggs))
+
+    def launch_device_partials(self) -> tuple[int, int, int, int, int]:
+        """Enqueues one replay without waiting; returns (partials device address, partial count,
+        request count, query blocks per request, the graph's CUDA stream handle)."""
+        self._check_open()
+        if self._empty:
+            raise RuntimeError("an empty prepared handle has no graph to launch")
+        ptr, count, reqs, blocks, stream = (ctypes.c_uint64(), ctypes.c_size_t(), ctypes.c_size_t(),
+                                            ctypes.c_size_t(), ctypes.c_uint64())
+        self._call("rtdl_b200_launch_fixed_radius_ranked_summary_aggregate_batch_graph_device_partials_3d",
+                   self._handle, ctypes.byref(ptr), ctypes.byref(count), ctypes.byref(reqs), ctypes.byref(blocks),
+                   ctypes.byref(stream))
+        n_req, n_blk = int(reqs.value), int(blocks.value)
+        if n_req != len(self._requests) or int(count.value) != n_req * n_blk:
+            raise RuntimeError("native fixed-radius graph returned inconsistent partial counts")
+        return int(ptr.value), int(count.value), n_req, n_blk, int(stream.value)
+
+    def replay_same_stream_device_partials_summary(self) -> dict:
+        """Enqueues a replay and reduces the device partials with a torch consumer on the graph's
+        stream (no host read between the graph and the consumer); the reference's CuPy consumer
+        (``optix_runtime.py:2098-2270``) in torch.  Requests whose status word is nonzero are then
+        recomputed by the plain aggregate call."""
+        import torch
+
+        self._check_open()
+        if self._empty:
+            return {"aggregates": self._empty_results(same_stream_partner_reduced=False),
+                    "metadata": {"backend": "b200", "empty_graph_path": True,
+                                 "same_stream_partner_consumer_executed": False}}
+        ptr, count, n_req, n_blk, stream = self.launch_device_partials()
+        status_ptr = ctypes.c_uint64()
+        self._call("rtdl_b200_fixed_radius_ranked_summary_aggregate_batch_graph_status_device_3d", self._handle,
+                   ctypes.byref(status_ptr), None)
+        ext = torch.cuda.ExternalStream(stream)
+        with torch.cuda.stream(ext):
+            raw = torch.as_tensor(_DeviceArray(ptr, count * 40, stream), device="cuda")
+            words = raw.view(torch.int64).view(n_req, n_blk, 5)
+            ints = words[:, :, :4].sum(dim=1)
+            sums = words[:, :, 4].view(torch.float64).sum(dim=1)
+            status = torch.as_tensor(_DeviceArray(int(status_ptr.value), n_req * 4, stream),
+                                     device="cuda").view(torch.int32).clone()
+            ints_h, sums_h, status_h = ints.cpu(), sums.cpu(), status.cpu()  # waits on the graph's stream
+        aggregates = []
+        recomputed = 0
+        for i in range(n_req):
+            if int(status_h[i]) != 0:
+                agg = self._owner.aggregate_ranked_summary_prepared_queries(
+                    self._prepared_queries, radius=self._requests[i]["radius"], k_max=self._requests[i]["k_max"])
+                recomputed += 1
+            else:
+                agg = dict(zip(AGGREGATE_FIELDS[:4], (int(v) for v in ints_h[i].tolist())))
+                agg["sum_distance"] = float(sums_h[i])
+            aggregates.append(self._result(i, agg, same_stream_partner_reduced=int(status_h[i]) == 0))
+        return {"aggregates": tuple(aggregates),
+                "metadata": {"backend": "b200", "native_symbol":
+                             "rtdl_b200_launch_fixed_radius_ranked_summary_aggregate_batch_graph_device_partials_3d",
+                             "producer_consumer_stream_ordering": "same_cuda_stream",
+                             "producer_host_synchronization_used": False,
+                             "bounded_partner_consumer": "torch",
+                             "partial_row_size_bytes": 40, "partial_count": count,
+                             "request_count": n_req, "query_block_count": n_blk,
+                             "requests_recomputed_by_plain_call": recomputed}}
+
+    # the reference's name for the same-stream consumer (its consumer is CuPy, this one is torch)
+    replay_same_stream_device_partials_summary_cupy = replay_same_stream_device_partials_summary
+
+    def close(self) -> None:
+        if self._closed:
+            return
+        handle = self._handle
+        self._handle = ctypes.c_void_p()
+        self._closed = True
+        if handle.value:
+            _native.load_library().rtdl_b200_destroy_fixed_radius_ranked_summary_aggregate_batch_graph_3d(handle)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def __del__(self):
         try:

@@ -115,6 +115,20 @@ RTDL_B200_API int rtdl_b200_run_fixed_radius_neighbors_3d(
     RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out,
     char* error_out, size_t error_size);
 
+/* No counterpart in the reference: the plain per-call form with device
+ * buffers (records already in HBM).  Builds the scene of search_points_dev and
+ * writes the fixed_radius_neighbors rows of query_points_dev (the
+ * RtdlPoint / RtdlPoint3D layout of `dimension`) into rows_dev, like
+ * rtdl_b200_run_fixed_radius_neighbors[_3d] (rows in the reference's order);
+ * rows_dev NULL only counts.  overflow_dev (optional, one byte per query) is
+ * 1 where the in-radius count exceeds k_max.  With k_max <= 64 the query set
+ * is prepared on a second stream while the scene builds.  Work runs on
+ * `stream` (NULL = the library's stream), which is synchronised before return. */
+RTDL_B200_API int rtdl_b200_run_fixed_radius_neighbors_device(
+    const void* query_points_dev, size_t query_count, const void* search_points_dev, size_t search_count,
+    int dimension, double radius, size_t k_max, void* rows_dev, size_t rows_capacity, size_t* row_count_out,
+    uint8_t* overflow_dev, void* stream, char* error_out, size_t error_size);
+
 /* bounded_knn_rows with ranks assigned on the device.  The reference builds
  * these rows in Python from the FRN rows (src/rtdsl/optix_runtime.py:15834-15862);
  * the rows equal src/rtdsl/reference.py:406-434. */

@@ -109,6 +109,8 @@ SIGNATURES = {
     "rtdl_b200_get_version": (_i, [ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "rtdl_b200_set_device": (_i, [_i]),
     "rtdl_b200_run_fixed_radius_neighbors": (_i, [_vp, _sz, _vp, _sz, _d, _sz, _vpp, _szp, _cp, _sz]),
+    "rtdl_b200_run_fixed_radius_neighbors_device": (_i, [_vp, _sz, _vp, _sz, _i, _d, _sz, _vp, _sz, _szp, _vp, _vp,
+                                                         _cp, _sz]),
     "rtdl_b200_run_fixed_radius_neighbors_3d": (_i, [_vp, _sz, _vp, _sz, _d, _sz, _vpp, _szp, _cp, _sz]),
     "rtdl_b200_run_bounded_knn_rows": (_i, [_vp, _sz, _vp, _sz, _d, _sz, _vpp, _szp, _cp, _sz]),
     "rtdl_b200_run_bounded_knn_rows_3d": (_i, [_vp, _sz, _vp, _sz, _d, _sz, _vpp, _szp, _cp, _sz]),

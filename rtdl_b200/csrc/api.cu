@@ -237,15 +237,14 @@ void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim,
   timer.mark("begin");
   const size_t rec = record_size(dim);
   void* d_search = upload(sp, rec * ns, s);
-  void* d_query = upload(q, rec * nq, s);
   timer.mark("upload");
   Scene* sc = nullptr;
+  void* d_query = nullptr;
   void* d_rows = nullptr;
   try {
-    sc = build_scene(d_search, (uint32_t)ns, dim, s, tuning().leaf_size);
-    timer.mark("build");
-    QueryResult r = run_query(sc, d_query, (uint32_t)nq, predicate, radius, (uint32_t)limit, nullptr, 0, &d_rows,
-                              nullptr, s, &timer);
+    BuildQueryInputs in{d_search, (uint32_t)ns, nullptr, q, (uint32_t)nq, dim};
+    QueryResult r = run_build_and_query(in, predicate, radius, (uint32_t)limit, nullptr, 0, &d_rows, nullptr, s,
+                                        aux_stream(), &timer, &sc, &d_query);
     const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
     void* host = download_rows(d_rows, row_size * r.rows, s);
     timer.mark("download");
@@ -253,6 +252,7 @@ void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim,
     *rows_out = host;
     *row_count_out = (size_t)r.rows;
   } catch (...) {
+    cudaStreamSynchronize(aux_stream());
     dev_free(d_rows, s);
     destroy_scene(sc);
     dev_free(d_search, s);
@@ -272,6 +272,18 @@ struct PreparedHandle {
 };
 
 }  // namespace
+
+cudaStream_t aux_stream() {
+  static thread_local std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  RTDL_CUDA_CHECK(cudaGetDevice(&dev));
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s;
+  RTDL_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  streams[dev] = s;
+  return s;
+}
 }  // namespace rtdl_b200
 
 using namespace rtdl_b200;
@@ -352,6 +364,52 @@ int rtdl_b200_run_fixed_radius_neighbors_3d(const RtdlPoint3D* query_points, siz
     if (query_count == 0 || search_count == 0) return;
     run_rows_call(query_points, query_count, search_points, search_count, 3, kFrn, radius, k_max,
                   reinterpret_cast<void**>(rows_out), row_count_out);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_fixed_radius_neighbors_device(const void* query_points_dev, size_t query_count,
+                                                const void* search_points_dev, size_t search_count, int dimension,
+                                                double radius, size_t k_max, void* rows_dev, size_t rows_capacity,
+                                                size_t* row_count_out, uint8_t* overflow_dev, void* stream,
+                                                char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!row_count_out) throw std::runtime_error("row_count_out must not be null");
+    if (dimension != 2 && dimension != 3) throw std::runtime_error("dimension must be 2 or 3");
+    validate_common(radius, k_max, query_count, search_count, true, "fixed_radius_neighbors", "k_max");
+    *row_count_out = 0;
+    if (query_count == 0) return;
+    if (!query_points_dev) throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    if (!search_points_dev && search_count)
+      throw std::runtime_error("search_points pointer must not be null when search_count is nonzero");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : library_stream();
+    int dev = 0;
+    RTDL_CUDA_CHECK(cudaGetDevice(&dev));
+    ensure_pool_configured(dev);
+    if (search_count == 0) {
+      if (overflow_dev) RTDL_CUDA_CHECK(cudaMemsetAsync(overflow_dev, 0, query_count, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      return;
+    }
+    PhaseTimer timer(s);
+    timer.mark("begin");
+    Scene* sc = nullptr;
+    void* owned = nullptr;
+    try {
+      BuildQueryInputs in{search_points_dev, (uint32_t)search_count, query_points_dev, nullptr, (uint32_t)query_count,
+                          dimension};
+      QueryResult r = run_build_and_query(in, kFrn, radius, (uint32_t)k_max, rows_dev, rows_capacity, nullptr,
+                                          overflow_dev, s, aux_stream(), &timer, &sc, &owned);
+      destroy_scene(sc);
+      sc = nullptr;
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      timer.publish();
+      *row_count_out = (size_t)r.rows;
+    } catch (...) {
+      cudaStreamSynchronize(aux_stream());
+      destroy_scene(sc);
+      cudaStreamSynchronize(s);
+      throw;
+    }
   }, error_out, error_size);
 }
 

@@ -248,6 +248,28 @@ QueryResult run_ranked_summaries(Scene* sc, const void* queries_dev, uint32_t nq
                                  RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
                                  RtdlFixedRadiusRankedNeighborAggregate* aggregate_host, cudaStream_t s,
                                  PhaseTimer* timer, const PreparedQueries* pq = nullptr);
+// The plain per-call form: builds the scene of the search records and answers
+// the query records (device, or host when query_host is set: uploaded inside).
+// fixed_radius_neighbors / bounded_knn_rows with k_max <= 64 prepare the query
+// set (statistics, own-box Morton order, output order) on `aux` while the scene
+// builds on `s`; the coordinates of both sets are checked at the query's first
+// read-back.  *scene_out and *query_owned (an uploaded copy) are the caller's to
+// release on `s` once the rows are used.
+struct BuildQueryInputs {
+  const void* search_dev;
+  uint32_t ns;
+  const void* query_dev;   // device records, or
+  const void* query_host;  // host records (uploaded on the query side's stream)
+  uint32_t nq;
+  int dim;
+};
+QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, double radius, uint32_t limit,
+                                void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev,
+                                cudaStream_t s, cudaStream_t aux, PhaseTimer* timer, Scene** scene_out,
+                                void** query_owned);
+// A second stream of this thread on the current device (the query side of run_build_and_query).
+cudaStream_t aux_stream();
+
 // Ranked-summary aggregates of several (radius, k_max) requests over one
 // prepared query set and one plain scene, captured once as a CUDA graph over
 // buffers allocated at creation (worst-case sizes) and replayed on the graph's

@@ -532,10 +532,24 @@ __device__ __forceinline__ void collect_init(const CollectParams& P, uint32_t t,
 
 // Tests the points of leaf bucket [first, first + cnt) against the lane's
 // query.  `test` false: the lane only takes part in the (warp-uniform) loads.
+// Four point loads are issued before their tests (more loads in flight per
+// warp; measured 6% faster at the 32-register budget than one at a time).
 template <bool STATS>
 __device__ __forceinline__ void collect_leaf(const CollectParams& P, const DevBands& B, int scene_inexact,
                                              CollectLane& L, int first, int cnt, bool test) {
-  for (int i = first; i < first + cnt; ++i) {
+  constexpr int kGroup = 4;
+  int i = first;
+  const int end = first + cnt;
+  for (; i + kGroup <= end; i += kGroup) {
+    float4 p[kGroup];
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) p[u] = __ldg(&P.S.pts[i + u]);
+    if (test) {
+#pragma unroll
+      for (int u = 0; u < kGroup; ++u) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)(i + u), p[u]);
+    }
+  }
+  for (; i < end; ++i) {
     const float4 p = __ldg(&P.S.pts[i]);
     if (test) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)i, p);
   }
@@ -2426,6 +2440,70 @@ QueryResult run_query_prepared(Scene* sc, const PreparedQueries* pq, double radi
   if (timer) timer->mark("start");
   return run_radius_query(sc, pq->raw, pq->n, kFrn, radius, kmax, rows_dev, rows_capacity, nullptr, overflow_dev, s,
                           timer, nullptr, nullptr, pq);
+}
+
+// ---- the plain per-call form: build and query in one call ---------------------
+QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, double radius, uint32_t limit,
+                                void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev,
+                                cudaStream_t s, cudaStream_t aux, PhaseTimer* timer, Scene** scene_out,
+                                void** query_owned) {
+  *scene_out = nullptr;
+  *query_owned = nullptr;
+  const size_t qbytes = (in.dim == 3 ? sizeof(RtdlPoint3D) : sizeof(RtdlPoint)) * (size_t)in.nq;
+  const bool overlap = predicate != kKnn && limit <= (uint32_t)kMaxList && in.nq > 0 && in.ns > 0 && aux != nullptr;
+  if (!overlap) {
+    const void* q = in.query_dev;
+    if (in.query_host && in.nq) {
+      *query_owned = dev_alloc(qbytes, s);
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(*query_owned, in.query_host, qbytes, cudaMemcpyHostToDevice, s));
+      q = *query_owned;
+    }
+    Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, tuning().leaf_size);
+    *scene_out = sc;
+    if (timer) timer->mark("build");
+    return run_query(sc, q, in.nq, predicate, radius, limit, rows_dev, rows_capacity, rows_alloc, overflow_dev, s,
+                     timer);
+  }
+  // the query side does not need the scene until its bands: it is prepared on
+  // `aux` (own-box Morton order) while the scene builds on `s`
+  static thread_local cudaEvent_t ev_start = nullptr, ev_ready = nullptr;
+  if (!ev_start) {
+    RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
+    RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_ready, cudaEventDisableTiming));
+  }
+  RTDL_CUDA_CHECK(cudaEventRecord(ev_start, s));
+  RTDL_CUDA_CHECK(cudaStreamWaitEvent(aux, ev_start, 0));  // whatever the caller queued on s comes first
+  Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, tuning().leaf_size);
+  *scene_out = sc;
+  const void* q = in.query_dev;
+  if (in.query_host) {  // a pageable copy holds the host; the build is already queued
+    *query_owned = dev_alloc(qbytes, aux);
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(*query_owned, in.query_host, qbytes, cudaMemcpyHostToDevice, aux));
+    q = *query_owned;
+  }
+  PreparedQueries* pq = nullptr;
+  try {
+    pq = prepare_query_set(q, in.nq, in.dim, aux);
+  } catch (...) {
+    cudaStreamSynchronize(aux);
+    throw;
+  }
+  RTDL_CUDA_CHECK(cudaEventRecord(ev_ready, aux));
+  RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ev_ready, 0));
+  pq->stream = s;  // from here the set is used and released on s
+  if (timer) timer->mark("build");
+  QueryResult r;
+  try {
+    r = run_radius_query(sc, q, in.nq, predicate, radius, limit, rows_dev, rows_capacity, rows_alloc, overflow_dev, s,
+                         timer, nullptr, nullptr, pq);
+  } catch (...) {
+    pq->raw = nullptr;
+    destroy_query_set(pq);
+    throw;
+  }
+  pq->raw = nullptr;  // the caller's records (or *query_owned)
+  destroy_query_set(pq);
+  return r;
 }
 
 // ---- captured summary graphs ------------------------------------------------

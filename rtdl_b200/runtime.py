@@ -263,6 +263,21 @@ def fixed_radius_neighbors(query, search, *, radius: float, k_max: int, dimensio
     return _row_view(rows.value or 0, count.value, ranked)
 
 
+def fixed_radius_neighbors_device(query_address: int, query_count: int, search_address: int, search_count: int, *,
+                                  dimension: int, radius: float, k_max: int, rows_address: int | None,
+                                  rows_capacity: int, overflow_address: int | None = None,
+                                  stream: int | None = None) -> int:
+    """One plain per-call launch on device-resident records (``rtdl_b200_run_fixed_radius_neighbors_device``):
+    builds the scene, writes the rows (``rows_address`` None: counts only); returns the row count."""
+    count = ctypes.c_size_t()
+    err = _native.error_buffer()
+    status = _native.load_library().rtdl_b200_run_fixed_radius_neighbors_device(
+        query_address, int(query_count), search_address, int(search_count), int(dimension), float(radius),
+        int(k_max), rows_address, int(rows_capacity), ctypes.byref(count), overflow_address, stream, err, len(err))
+    _native.check_status(status, err)
+    return int(count.value)
+
+
 def knn_rows(query, search, *, k: int, dimension: int | None = None) -> B200RowView:
     """One plain per-call launch of ``rtdl_b200_run_k_closest_hits[_3d]``."""
     lib = _native.load_library()

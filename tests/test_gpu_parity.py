@@ -284,3 +284,41 @@ def test_lattice_ball_generic_path(gpu):
         assert (counts > 256).all()
         _assert_same_rows(v.to_numpy(), exp, False)
         v.close()
+
+
+@pytest.mark.parametrize("dim,k_max", [(3, 64), (3, 7), (2, 16), (3, 200)])
+def test_device_per_call_entry_matches_oracle(gpu, dim, k_max):
+    """rtdl_b200_run_fixed_radius_neighbors_device (build + query in one call on resident records; the
+    probe set is prepared beside the build for k_max <= 64): rows, counts and overflow flags."""
+    import torch
+
+    from rtdl_b200.runtime import FRN_ROW_DTYPE
+
+    rng = np.random.default_rng(40 + dim + k_max)
+    centres = rng.random((12, 3))
+    s_pts, q_pts = _clustered(rng, 30000, centres)[:, :dim], _clustered(rng, 5000, centres)[:, :dim]
+    # query ids out of order: rows must still come grouped by ascending query id
+    s, q = _cols(s_pts), _cols(q_pts, ids=rng.permutation(len(q_pts)).astype(np.uint32) * 3)
+    sp, qp = _pack(s), _pack(q)
+    d_s = torch.from_numpy(sp.records.view(np.uint8).copy()).cuda()
+    d_q = torch.from_numpy(qp.records.view(np.uint8).copy()).cuda()
+    radius = 0.012
+    n = rt.runtime.fixed_radius_neighbors_device(d_q.data_ptr(), len(q_pts), d_s.data_ptr(), len(s_pts),
+                                                 dimension=dim, radius=radius, k_max=k_max, rows_address=None,
+                                                 rows_capacity=0)
+    rows = torch.empty(max(n, 1) * 16, dtype=torch.uint8, device="cuda")
+    flags = torch.empty(len(q_pts), dtype=torch.uint8, device="cuda")
+    assert rt.runtime.fixed_radius_neighbors_device(d_q.data_ptr(), len(q_pts), d_s.data_ptr(), len(s_pts),
+                                                    dimension=dim, radius=radius, k_max=k_max,
+                                                    rows_address=rows.data_ptr(), rows_capacity=n,
+                                                    overflow_address=flags.data_ptr()) == n
+    got = np.frombuffer(rows.cpu().numpy().tobytes(), dtype=FRN_ROW_DTYPE)[:n]
+    exp, counts = O.fixed_radius_neighbors(q, s, radius=radius, k_max=k_max, threads=8, with_counts=True)
+    _assert_same_rows(got, exp, False)
+    assert np.array_equal(flags.cpu().numpy().astype(bool), counts > k_max)
+    # no search points: no rows, flags cleared
+    flags.fill_(7)
+    assert rt.runtime.fixed_radius_neighbors_device(d_q.data_ptr(), len(q_pts), d_s.data_ptr(), 0, dimension=dim,
+                                                    radius=radius, k_max=k_max, rows_address=rows.data_ptr(),
+                                                    rows_capacity=n, overflow_address=flags.data_ptr()) == 0
+    assert int(flags.max()) == 0

@@ -669,6 +669,8 @@ def run_summary(args) -> int:
 
     torch.cuda.set_device(0)
     rt.set_device(0)
+    # these scenes serve only fixed-radius queries: the leaf buckets of a prepared fixed-radius scene
+    rt.set_tuning(leaf_size=24)
     golden = json.loads((ROOT / "tests" / "golden" / "rtnn_ranked_summary_262144.json").read_text())
     radius, k_max = golden["radius"], golden["k_max"]
     dev = torch.device("cuda", 0)
@@ -802,7 +804,7 @@ def main(argv=None) -> int:
     torch.cuda.set_device(local)
     rt.set_device(local)
     if args.traversal is not None or args.leaf_size is not None:
-        rt.set_tuning(leaf_size=args.leaf_size or 8, traversal=args.traversal or "packet")
+        rt.set_tuning(leaf_size=args.leaf_size or 0, traversal=args.traversal or "packet")
     dist = None
     if world > 1:
         import datetime

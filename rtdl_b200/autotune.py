@@ -27,14 +27,14 @@ import numpy as np
 from . import _native
 from .runtime import B200Scene, set_tuning
 
-LEAF_SIZES = (4, 8, 16)
+LEAF_SIZES = (8, 16, 24)
 TRAVERSALS = ("packet", "packet_cube", "lane")
 BLOCK_THREADS = (128, 256)
 
 
 @dataclass(frozen=True)
 class Config:
-    leaf_size: int = 8
+    leaf_size: int = 0  # 0: by the scene's use (see set_tuning)
     traversal: str = "packet"
     block_threads: int = 128
 

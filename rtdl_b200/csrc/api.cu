@@ -273,6 +273,11 @@ struct PreparedHandle {
 
 }  // namespace
 
+int leaf_size_for(bool fixed_radius_only) {
+  if (tuning().leaf_size > 0) return tuning().leaf_size;
+  return fixed_radius_only ? 24 : 8;
+}
+
 cudaStream_t aux_stream() {
   static thread_local std::map<int, cudaStream_t> streams;
   int dev = 0;
@@ -302,7 +307,7 @@ int rtdl_b200_set_device(int device) {
 }
 
 int rtdl_b200_set_tuning(int leaf_size, int block_threads, int traversal) {
-  if (leaf_size < 1 || leaf_size > 32) return 1;
+  if (leaf_size < 0 || leaf_size > 32) return 1;
   if (block_threads != 64 && block_threads != 128 && block_threads != 256) return 1;
   if (traversal < 0 || traversal > 2) return 1;
   tuning().leaf_size = leaf_size;
@@ -471,8 +476,10 @@ int rtdl_b200_run_k_closest_hits_3d(const RtdlPoint3D* query_points, size_t quer
   }, error_out, error_size);
 }
 
-int rtdl_b200_scene_create(const void* points, size_t count, int dimension, int points_on_device, void* stream,
-                           void** scene_out, char* error_out, size_t error_size) {
+namespace rtdl_b200 {
+namespace {
+int scene_create_impl(const void* points, size_t count, int dimension, int points_on_device, void* stream,
+                      bool fixed_radius_only, void** scene_out, char* error_out, size_t error_size) {
   return guarded([&]() {
     if (!scene_out) throw std::runtime_error("scene_out must not be null");
     *scene_out = nullptr;
@@ -491,7 +498,7 @@ int rtdl_b200_scene_create(const void* points, size_t count, int dimension, int 
     }
     Scene* sc = nullptr;
     try {
-      sc = build_scene(d_points, (uint32_t)count, dimension, s, tuning().leaf_size);
+      sc = build_scene(d_points, (uint32_t)count, dimension, s, leaf_size_for(fixed_radius_only));
       unsigned int bad = 0;
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
       RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -505,6 +512,14 @@ int rtdl_b200_scene_create(const void* points, size_t count, int dimension, int 
     dev_free(owned, s);
     *scene_out = sc;
   }, error_out, error_size);
+}
+}  // namespace
+}  // namespace rtdl_b200
+
+int rtdl_b200_scene_create(const void* points, size_t count, int dimension, int points_on_device, void* stream,
+                           void** scene_out, char* error_out, size_t error_size) {
+  return scene_create_impl(points, count, dimension, points_on_device, stream, false, scene_out, error_out,
+                           error_size);
 }
 
 void rtdl_b200_scene_destroy(void* scene) {
@@ -606,7 +621,7 @@ int rtdl_b200_batch_create(const void* points, const unsigned long long* point_o
         owned = upload(points, record_size(dimension) * count, s);
         d_points = owned;
       }
-      sc = build_scene_batch(d_points, point_offsets, problems, dimension, s, tuning().leaf_size);
+      sc = build_scene_batch(d_points, point_offsets, problems, dimension, s, leaf_size_for(true));
       unsigned int bad = 0;
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
       RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -809,7 +824,7 @@ int rtdl_b200_prepare_fixed_radius_neighbors_3d(const RtdlPoint3D* search_points
     *prepared_out = nullptr;
     void* scene = nullptr;
     char err[1024];
-    if (rtdl_b200_scene_create(search_points, search_count, 3, 0, nullptr, &scene, err, sizeof(err)) != 0)
+    if (scene_create_impl(search_points, search_count, 3, 0, nullptr, true, &scene, err, sizeof(err)) != 0)
       throw std::runtime_error(err);
     static_cast<Scene*>(scene)->max_radius = max_radius;
     *prepared_out = scene;

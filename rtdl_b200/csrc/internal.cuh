@@ -134,7 +134,7 @@ struct Scene {
 
 // ---- tuning ---------------------------------------------------------------
 struct Tuning {
-  int leaf_size = 8;
+  int leaf_size = 0;  // 0: automatic (leaf_size_for)
   int block_threads = 128;
   int traversal = 0;  // fixed-radius collect: 0 = one warp per 32 queries (packet), 1 = one thread per
                       // query, 2 = packet with cube tests at internal nodes
@@ -269,6 +269,11 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
                                 void** query_owned);
 // A second stream of this thread on the current device (the query side of run_build_and_query).
 cudaStream_t aux_stream();
+// Leaf-bucket size of a scene build: the tuning's when set, else 24 for scenes
+// that serve only fixed-radius queries (larger buckets shorten the walk and the
+// collect tests a bucket's points with four loads in flight) and 8 for general
+// scenes (the nearest-neighbour walk prunes better with small buckets).
+int leaf_size_for(bool fixed_radius_only);
 
 // Ranked-summary aggregates of several (radius, k_max) requests over one
 // prepared query set and one plain scene, captured once as a CUDA graph over

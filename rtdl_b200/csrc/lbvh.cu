@@ -302,9 +302,12 @@ __global__ void __launch_bounds__(kThreads) k_refit(uint32_t n, const float4* __
   int me = (int)i | kLeafFlag;  // child code of the subtree the thread stands on
   int p = parent_leaf[i];
   while (p >= 0) {
+    // the node's links (written by the previous kernel) are loaded before the
+    // arrival so their latency overlaps the atomic's; only the sibling's box
+    // has to wait for it
+    const int l = child_l[p], r = child_r[p], up = parent_int[p];
     cuda::atomic_ref<unsigned int, cuda::thread_scope_device> arrived(arrivals[p]);
     if (arrived.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) break;  // the sibling is not finished yet
-    const int l = child_l[p], r = child_r[p];
     float4 sl, sh;
     child_box(l == me ? r : l, pts, boxes, sl, sh);
     lo = make_float4(fminf(lo.x, sl.x), fminf(lo.y, sl.y), fminf(lo.z, sl.z), 0.f);
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(kThreads) k_refit(uint32_t n, const float4* __
     __stcg(&boxes[2 * p], lo);
     __stcg(&boxes[2 * p + 1], hi);
     me = p;
-    p = parent_int[p];
+    p = up;
   }
 }
 

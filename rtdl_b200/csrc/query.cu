@@ -2458,7 +2458,7 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
       RTDL_CUDA_CHECK(cudaMemcpyAsync(*query_owned, in.query_host, qbytes, cudaMemcpyHostToDevice, s));
       q = *query_owned;
     }
-    Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, tuning().leaf_size);
+    Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, leaf_size_for(predicate != kKnn));
     *scene_out = sc;
     if (timer) timer->mark("build");
     return run_query(sc, q, in.nq, predicate, radius, limit, rows_dev, rows_capacity, rows_alloc, overflow_dev, s,
@@ -2473,7 +2473,7 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
   }
   RTDL_CUDA_CHECK(cudaEventRecord(ev_start, s));
   RTDL_CUDA_CHECK(cudaStreamWaitEvent(aux, ev_start, 0));  // whatever the caller queued on s comes first
-  Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, tuning().leaf_size);
+  Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, leaf_size_for(true));
   *scene_out = sc;
   const void* q = in.query_dev;
   if (in.query_host) {  // a pageable copy holds the host; the build is already queued

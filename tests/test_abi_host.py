@@ -85,10 +85,13 @@ def test_prepare_validation():
 
 def test_set_tuning_bounds():
     with pytest.raises(ValueError):
-        rt.set_tuning(leaf_size=0, block_threads=128)
+        rt.set_tuning(leaf_size=-1, block_threads=128)
+    with pytest.raises(ValueError):
+        rt.set_tuning(leaf_size=33, block_threads=128)
     with pytest.raises(ValueError):
         rt.set_tuning(leaf_size=8, block_threads=96)
     rt.set_tuning(leaf_size=8, block_threads=128)
+    rt.set_tuning()  # back to the defaults: leaf size by the scene's use
 
 
 # ---- DSL mirror ---------------------------------------------------------------

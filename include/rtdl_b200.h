@@ -88,6 +88,14 @@ typedef struct RtdlFixedRadiusRankedNeighborAggregate {
   double sum_distance;            /* sum of sum_distance (fixed reduction order, run to run identical) */
 } RtdlFixedRadiusRankedNeighborAggregate;
 
+/* One row of fixed_radius_count_threshold: same layout as
+ * src/native/optix/rtdl_optix_prelude.h:276-280 (RtdlFixedRadiusCountRow, 12 B). */
+typedef struct RtdlFixedRadiusCountRow {
+  uint32_t query_id;
+  uint32_t neighbor_count;     /* in-radius count, capped at the threshold when it is positive */
+  uint32_t threshold_reached;  /* 1 when the threshold is positive and was reached */
+} RtdlFixedRadiusCountRow;
+
 /* Version triple (the reference exports rtdl_optix_get_version,
  * rtdl_optix_api.cpp:1-7). */
 RTDL_B200_API int rtdl_b200_get_version(int* major, int* minor, int* patch);
@@ -379,6 +387,73 @@ RTDL_B200_API int rtdl_b200_scene_ranked_summaries_prepared_device(
 RTDL_B200_API int rtdl_b200_scene_query_prepared_device(
     void* scene, void* queries, double radius, size_t k_max, void* rows_dev, size_t rows_capacity,
     size_t* row_count_out, uint8_t* overflow_dev, void* stream, char* error_out, size_t error_size);
+
+/* ---- fixed_radius_count_threshold and the nearest in-radius witness ------------
+ * Counts follow the reference's generic count (src/rtdsl/generic_primitives.py
+ * :198-227): a query's points within radius (inclusive, FP64 distances) are
+ * counted until a positive threshold is reached; threshold 0 counts them all.
+ * One RtdlFixedRadiusCountRow / output element per query, in input order.
+ * Prepared handles are scenes with a max_radius; radius may exceed it by at
+ * most 1e-7, as in the reference. */
+
+/* Replaces rtdl_optix_run_fixed_radius_count_threshold (rtdl_optix_api.cpp:4738-4765). */
+RTDL_B200_API int rtdl_b200_run_fixed_radius_count_threshold(
+    const RtdlPoint* query_points, size_t query_count, const RtdlPoint* search_points, size_t search_count,
+    double radius, size_t threshold, RtdlFixedRadiusCountRow** rows_out, size_t* row_count_out,
+    char* error_out, size_t error_size);
+
+/* Replace rtdl_optix_prepare_fixed_radius_count_threshold_2d[_device_search_columns]
+ * (rtdl_optix_api.cpp:4767-4810); the columns are device buffers. */
+RTDL_B200_API int rtdl_b200_prepare_fixed_radius_count_threshold_2d(
+    const RtdlPoint* search_points, size_t search_count, double max_radius, void** prepared_out,
+    char* error_out, size_t error_size);
+RTDL_B200_API int rtdl_b200_prepare_fixed_radius_count_threshold_2d_device_search_columns(
+    const uint32_t* search_ids, const double* search_x, const double* search_y, size_t search_count,
+    double max_radius, void** prepared_out, char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_run_prepared_fixed_radius_count_threshold_2d
+ * (rtdl_optix_workloads.cpp:13242-13320); rows are released with rtdl_b200_free_rows. */
+RTDL_B200_API int rtdl_b200_run_prepared_fixed_radius_count_threshold_2d(
+    void* prepared, const RtdlPoint* query_points, size_t query_count, double radius, size_t threshold,
+    RtdlFixedRadiusCountRow** rows_out, size_t* row_count_out, char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_write_prepared_fixed_radius_count_threshold_2d_device_query_columns
+ * (rtdl_optix_workloads.cpp:13322-13400): device query columns in, device output
+ * columns out; needs a handle prepared from device search columns. */
+RTDL_B200_API int rtdl_b200_write_prepared_fixed_radius_count_threshold_2d_device_query_columns(
+    void* prepared, const uint32_t* query_ids, const double* query_x, const double* query_y, size_t query_count,
+    double radius, size_t threshold, uint32_t* query_ids_out, uint32_t* neighbor_counts_out,
+    uint32_t* threshold_flags_out, char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_count_prepared_fixed_radius_threshold_reached_2d
+ * (rtdl_optix_workloads.cpp:13400-13466): how many queries reached the threshold. */
+RTDL_B200_API int rtdl_b200_count_prepared_fixed_radius_threshold_reached_2d(
+    void* prepared, const RtdlPoint* query_points, size_t query_count, double radius, size_t threshold,
+    size_t* threshold_reached_count_out, char* error_out, size_t error_size);
+
+/* Replaces rtdl_optix_run_prepared_fixed_radius_nearest_witness_2d
+ * (rtdl_optix_workloads.cpp:13468-13552): one row per query in input order,
+ * the nearest point within radius (ties to the smaller id; exact FP64
+ * distance), or neighbor_id 0xFFFFFFFF and distance FLT_MAX when none. */
+RTDL_B200_API int rtdl_b200_run_prepared_fixed_radius_nearest_witness_2d(
+    void* prepared, const RtdlPoint* query_points, size_t query_count, double radius,
+    RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out, char* error_out, size_t error_size);
+
+RTDL_B200_API void rtdl_b200_destroy_prepared_fixed_radius_count_threshold_2d(void* prepared);
+
+/* Replace rtdl_optix_prepare_fixed_radius_count_threshold_3d and
+ * rtdl_optix_write_prepared_fixed_radius_count_threshold_3d_device_outputs
+ * (rtdl_optix_api.cpp:4442-4470, rtdl_optix_workloads.cpp:16491-16560): host
+ * query records in, device output columns out.  As in the reference's 3-D
+ * contract, threshold 0 gives every query count 0 and flag 1. */
+RTDL_B200_API int rtdl_b200_prepare_fixed_radius_count_threshold_3d(
+    const RtdlPoint3D* search_points, size_t search_count, double max_radius, void** prepared_out,
+    char* error_out, size_t error_size);
+RTDL_B200_API int rtdl_b200_write_prepared_fixed_radius_count_threshold_3d_device_outputs(
+    void* prepared, const RtdlPoint3D* query_points, size_t query_count, double radius, size_t threshold,
+    uint32_t* query_ids_out, uint32_t* neighbor_counts_out, uint32_t* threshold_flags_out,
+    char* error_out, size_t error_size);
+RTDL_B200_API void rtdl_b200_destroy_prepared_fixed_radius_count_threshold_3d(void* prepared);
 
 /* ---- captured batch graph of prepared-query aggregates -----------------------
  * Replace the batch-graph entry points of rtdl_optix_api.cpp:4323-4396

@@ -127,6 +127,42 @@ def fixed_radius_neighbors(query, search, *, radius, k_max, threads=1, ranked=Fa
     return _call_rows(query, search, 0, radius, k_max, ranked, threads, with_counts)
 
 
+COUNT_ROW_DTYPE = np.dtype({"names": ["query_id", "neighbor_count", "threshold_reached"],
+                            "formats": ["<u4", "<u4", "<u4"], "offsets": [0, 4, 8], "itemsize": 12})
+
+
+def fixed_radius_count_threshold(query, search, *, radius, threshold, threads=1):
+    """The reference's generic count (``src/rtdsl/generic_primitives.py:198-227``): per query, in input
+    order, its points within radius counted until a positive threshold is reached (threshold 0 counts
+    them all); ``threshold_reached`` is 1 when a positive threshold was reached.  Restated from the
+    oracle's exact in-radius counts: the stopped count is min(count, threshold)."""
+    _, counts = _call_rows(query, search, 0, radius, 1, False, threads, True)
+    thr = int(threshold)
+    out = np.zeros(len(counts), dtype=COUNT_ROW_DTYPE)
+    out["query_id"] = np.asarray(query["id"], dtype=np.uint32)
+    out["neighbor_count"] = np.minimum(counts, thr) if thr > 0 else counts
+    out["threshold_reached"] = (counts >= thr) if thr > 0 else 0
+    return out
+
+
+def nearest_witness(query, search, *, radius, threads=1):
+    """Nearest in-radius neighbour of each query, in input order (the reference's prepared nearest
+    witness, ``rtdl_optix_core.cpp:6043-6090``: smaller distance, then smaller id); queries without
+    one get neighbor_id 0xFFFFFFFF and distance FLT_MAX.  Restated from the k_max = 1 rows, which
+    come grouped by query id, stable in input order."""
+    rows, counts = _call_rows(query, search, 0, radius, 1, False, threads, True)
+    ids = np.asarray(query["id"], dtype=np.uint32)
+    out = np.zeros(len(ids), dtype=FRN_ROW_DTYPE)
+    out["query_id"] = ids
+    out["neighbor_id"] = 0xFFFFFFFF
+    out["distance"] = 3.4028234663852886e38
+    order = np.argsort(ids, kind="stable")
+    hit = order[counts[order] > 0]
+    out["neighbor_id"][hit] = rows["neighbor_id"]
+    out["distance"][hit] = rows["distance"]
+    return out
+
+
 SUMMARY_DTYPE = np.dtype(
     {
         "names": ["query_id", "neighbor_count", "nearest_neighbor_id", "kth_neighbor_id", "nearest_distance",

@@ -43,7 +43,13 @@ from .runtime import (  # noqa: F401
     PreparedB200FixedRadiusNeighbors3D,
     PreparedB200FixedRadiusQueryPoints3D,
     PreparedB200FixedRadiusRankedSummaryAggregateBatchGraph3D,
+    PreparedB200FixedRadiusCountThreshold2D,
+    PreparedB200FixedRadiusCountThreshold3D,
     directed_hausdorff,
+    fixed_radius_count_threshold_2d,
+    prepare_b200_fixed_radius_count_threshold_2d,
+    prepare_b200_fixed_radius_count_threshold_2d_device_search_columns,
+    prepare_b200_fixed_radius_count_threshold_3d,
     hausdorff_distance,
     pack_points,
     prepare_b200,

@@ -160,6 +160,20 @@ SIGNATURES = {
     "rtdl_b200_update_fixed_radius_ranked_summary_aggregate_batch_graph_3d": (
         _i, [_vp, _dp, ctypes.POINTER(_sz), _sz, _cp, _sz]),
     "rtdl_b200_destroy_fixed_radius_ranked_summary_aggregate_batch_graph_3d": (None, [_vp]),
+    "rtdl_b200_run_fixed_radius_count_threshold": (_i, [_vp, _sz, _vp, _sz, _d, _sz, _vpp, _szp, _cp, _sz]),
+    "rtdl_b200_prepare_fixed_radius_count_threshold_2d": (_i, [_vp, _sz, _d, _vpp, _cp, _sz]),
+    "rtdl_b200_prepare_fixed_radius_count_threshold_2d_device_search_columns": (
+        _i, [_vp, _vp, _vp, _sz, _d, _vpp, _cp, _sz]),
+    "rtdl_b200_run_prepared_fixed_radius_count_threshold_2d": (_i, [_vp, _vp, _sz, _d, _sz, _vpp, _szp, _cp, _sz]),
+    "rtdl_b200_write_prepared_fixed_radius_count_threshold_2d_device_query_columns": (
+        _i, [_vp, _vp, _vp, _vp, _sz, _d, _sz, _vp, _vp, _vp, _cp, _sz]),
+    "rtdl_b200_count_prepared_fixed_radius_threshold_reached_2d": (_i, [_vp, _vp, _sz, _d, _sz, _szp, _cp, _sz]),
+    "rtdl_b200_run_prepared_fixed_radius_nearest_witness_2d": (_i, [_vp, _vp, _sz, _d, _vpp, _szp, _cp, _sz]),
+    "rtdl_b200_destroy_prepared_fixed_radius_count_threshold_2d": (None, [_vp]),
+    "rtdl_b200_prepare_fixed_radius_count_threshold_3d": (_i, [_vp, _sz, _d, _vpp, _cp, _sz]),
+    "rtdl_b200_write_prepared_fixed_radius_count_threshold_3d_device_outputs": (
+        _i, [_vp, _vp, _sz, _d, _sz, _vp, _vp, _vp, _cp, _sz]),
+    "rtdl_b200_destroy_prepared_fixed_radius_count_threshold_3d": (None, [_vp]),
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i, _i]),
     "rtdl_b200_get_launch_count": (_i, [ctypes.POINTER(ctypes.c_ulonglong)]),

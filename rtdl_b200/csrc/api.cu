@@ -1117,6 +1117,321 @@ void rtdl_b200_destroy_fixed_radius_ranked_summary_aggregate_batch_graph_3d(void
   summary_graph_destroy(static_cast<SummaryGraph*>(graph));
 }
 
+// ---- fixed_radius_count_threshold and the nearest witness ------------------------
+namespace rtdl_b200 {
+namespace {
+void count_checks(double radius, size_t query_count, size_t threshold, const char* what) {
+  const std::string w(what);
+  if (radius < 0.0) throw std::runtime_error(w + " radius must be non-negative");
+  if (query_count > (size_t)UINT32_MAX) throw std::runtime_error(w + " query_count exceeds uint32 limit");
+  if (threshold > (size_t)UINT32_MAX) throw std::runtime_error(w + " threshold exceeds uint32 limit");
+}
+
+Scene* prepared_count_scene(void* prepared, int dim, double radius, const char* what, const char* null_msg) {
+  Scene* sc = static_cast<Scene*>(prepared);
+  if (!sc) throw std::runtime_error(null_msg);
+  if (sc->dim != dim) throw std::runtime_error(dim == 3 ? "prepared scene is not 3D" : "prepared scene is not 2D");
+  if (radius > sc->max_radius + 1.0e-7) throw std::runtime_error(std::string(what) + " radius exceeds prepared max_radius");
+  return sc;
+}
+
+// Counts into 12-byte rows (device) and returns them in a pinned host buffer.
+void count_rows_to_host(Scene* sc, const void* d_query, uint32_t nq, double radius, uint32_t threshold,
+                        RtdlFixedRadiusCountRow** rows_out, size_t* row_count_out, cudaStream_t s) {
+  RtdlFixedRadiusCountRow* d_rows =
+      static_cast<RtdlFixedRadiusCountRow*>(dev_alloc(sizeof(RtdlFixedRadiusCountRow) * nq, s));
+  try {
+    CountOutputs out;
+    out.rows = d_rows;
+    run_count_threshold(sc, d_query, nq, radius, threshold, out, s);
+    *rows_out = static_cast<RtdlFixedRadiusCountRow*>(download_rows(d_rows, sizeof(RtdlFixedRadiusCountRow) * nq, s));
+    *row_count_out = nq;
+  } catch (...) {
+    dev_free(d_rows, s);
+    throw;
+  }
+  dev_free(d_rows, s);
+}
+
+int prepare_count_scene(const void* points, size_t count, int dim, int on_device, double max_radius,
+                        bool device_columns, void** prepared_out, char* error_out, size_t error_size) {
+  void* scene = nullptr;
+  char err[1024];
+  if (scene_create_impl(points, count, dim, on_device, nullptr, true, &scene, err, sizeof(err)) != 0) {
+    if (error_out && error_size) {
+      std::strncpy(error_out, err, error_size - 1);
+      error_out[error_size - 1] = 0;
+    }
+    return 1;
+  }
+  static_cast<Scene*>(scene)->max_radius = max_radius;
+  static_cast<Scene*>(scene)->device_columns = device_columns;
+  *prepared_out = scene;
+  return 0;
+}
+}  // namespace
+}  // namespace rtdl_b200
+
+int rtdl_b200_run_fixed_radius_count_threshold(const RtdlPoint* query_points, size_t query_count,
+                                               const RtdlPoint* search_points, size_t search_count, double radius,
+                                               size_t threshold, RtdlFixedRadiusCountRow** rows_out,
+                                               size_t* row_count_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    count_checks(radius, query_count, threshold, "fixed_radius_count_threshold");
+    if (search_count > (size_t)UINT32_MAX)
+      throw std::runtime_error("fixed_radius_count_threshold search_count exceeds uint32 limit");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || search_count == 0) return;
+    if (!query_points || !search_points) throw std::runtime_error("point pointers must not be null when counts are nonzero");
+    cudaStream_t s = library_stream();
+    void* d_search = upload(search_points, sizeof(RtdlPoint) * search_count, s);
+    void* d_query = nullptr;
+    Scene* sc = nullptr;
+    try {
+      sc = build_scene(d_search, (uint32_t)search_count, 2, s, leaf_size_for(true));
+      d_query = upload(query_points, sizeof(RtdlPoint) * query_count, s);
+      count_rows_to_host(sc, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, rows_out, row_count_out, s);
+    } catch (...) {
+      destroy_scene(sc);
+      dev_free(d_search, s);
+      dev_free(d_query, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    destroy_scene(sc);
+    dev_free(d_search, s);
+    dev_free(d_query, s);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_prepare_fixed_radius_count_threshold_2d(const RtdlPoint* search_points, size_t search_count,
+                                                      double max_radius, void** prepared_out, char* error_out,
+                                                      size_t error_size) {
+  if (!prepared_out) return guarded([] { throw std::runtime_error("prepared_out must not be null"); }, error_out, error_size);
+  *prepared_out = nullptr;
+  const int st = guarded([&]() {
+    if (!search_points && search_count != 0)
+      throw std::runtime_error("search_points pointer must not be null when search_count is nonzero");
+    if (max_radius < 0.0) throw std::runtime_error("fixed_radius_count_threshold max_radius must be non-negative");
+    if (search_count > (size_t)UINT32_MAX)
+      throw std::runtime_error("fixed_radius_count_threshold search_count exceeds uint32 limit");
+  }, error_out, error_size);
+  if (st != 0) return st;
+  return prepare_count_scene(search_points, search_count, 2, 0, max_radius, false, prepared_out, error_out, error_size);
+}
+
+int rtdl_b200_prepare_fixed_radius_count_threshold_2d_device_search_columns(
+    const uint32_t* search_ids, const double* search_x, const double* search_y, size_t search_count,
+    double max_radius, void** prepared_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!prepared_out) throw std::runtime_error("prepared_out must not be null");
+    *prepared_out = nullptr;
+    if ((!search_ids || !search_x || !search_y) && search_count != 0)
+      throw std::runtime_error("search column pointers must not be null when search_count is nonzero");
+    if (max_radius < 0.0) throw std::runtime_error("fixed_radius_count_threshold max_radius must be non-negative");
+    if (search_count > (size_t)UINT32_MAX)
+      throw std::runtime_error("fixed_radius_count_threshold search_count exceeds uint32 limit");
+    cudaStream_t s = library_stream();
+    void* recs = dev_alloc(sizeof(RtdlPoint) * (search_count ? search_count : 1), s);
+    columns_to_records_2d(search_ids, search_x, search_y, (uint32_t)search_count, recs, s);
+    char err[1024];
+    const int st = prepare_count_scene(recs, search_count, 2, 1, max_radius, true, prepared_out, err, sizeof(err));
+    dev_free(recs, s);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (st != 0) throw std::runtime_error(err);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_prepared_fixed_radius_count_threshold_2d(void* prepared, const RtdlPoint* query_points,
+                                                           size_t query_count, double radius, size_t threshold,
+                                                           RtdlFixedRadiusCountRow** rows_out, size_t* row_count_out,
+                                                           char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!prepared) throw std::runtime_error("prepared OptiX fixed-radius handle must not be null");
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    if (!query_points && query_count != 0)
+      throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    count_checks(radius, query_count, threshold, "fixed_radius_count_threshold");
+    Scene* sc = prepared_count_scene(prepared, 2, radius, "fixed_radius_count_threshold",
+                                     "prepared OptiX fixed-radius handle must not be null");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || sc->n == 0) return;
+    cudaStream_t s = sc->stream;
+    void* d_query = upload(query_points, sizeof(RtdlPoint) * query_count, s);
+    try {
+      count_rows_to_host(sc, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, rows_out, row_count_out, s);
+    } catch (...) {
+      dev_free(d_query, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(d_query, s);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_write_prepared_fixed_radius_count_threshold_2d_device_query_columns(
+    void* prepared, const uint32_t* query_ids, const double* query_x, const double* query_y, size_t query_count,
+    double radius, size_t threshold, uint32_t* query_ids_out, uint32_t* neighbor_counts_out,
+    uint32_t* threshold_flags_out, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!prepared) throw std::runtime_error("prepared OptiX fixed-radius handle must not be null");
+    Scene* sc = static_cast<Scene*>(prepared);
+    if (!sc->device_columns)
+      throw std::runtime_error("fixed-radius device-column output requires a device-search-column prepared scene");
+    count_checks(radius, query_count, threshold, "fixed_radius_count_threshold");
+    prepared_count_scene(prepared, 2, radius, "fixed_radius_count_threshold", "");
+    if (query_count == 0) return;
+    if (!query_ids || !query_x || !query_y)
+      throw std::runtime_error("query column pointers must not be null when query_count is nonzero");
+    if (!query_ids_out || !neighbor_counts_out || !threshold_flags_out)
+      throw std::runtime_error("device output pointers must not be null when query_count is nonzero");
+    cudaStream_t s = sc->stream;
+    void* recs = dev_alloc(sizeof(RtdlPoint) * query_count, s);
+    try {
+      columns_to_records_2d(query_ids, query_x, query_y, (uint32_t)query_count, recs, s);
+      CountOutputs out;
+      out.ids = query_ids_out;
+      out.counts = neighbor_counts_out;
+      out.flags = threshold_flags_out;
+      run_count_threshold(sc, recs, (uint32_t)query_count, radius, (uint32_t)threshold, out, s);
+    } catch (...) {
+      dev_free(recs, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(recs, s);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+  }, error_out, error_size);
+}
+
+int rtdl_b200_count_prepared_fixed_radius_threshold_reached_2d(void* prepared, const RtdlPoint* query_points,
+                                                               size_t query_count, double radius, size_t threshold,
+                                                               size_t* threshold_reached_count_out, char* error_out,
+                                                               size_t error_size) {
+  return guarded([&]() {
+    if (!prepared) throw std::runtime_error("prepared OptiX fixed-radius handle must not be null");
+    if (!threshold_reached_count_out) throw std::runtime_error("threshold_reached_count_out must not be null");
+    if (!query_points && query_count != 0)
+      throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    count_checks(radius, query_count, threshold, "fixed_radius_count_threshold");
+    Scene* sc = prepared_count_scene(prepared, 2, radius, "fixed_radius_count_threshold", "");
+    *threshold_reached_count_out = 0;
+    if (query_count == 0 || sc->n == 0) return;
+    cudaStream_t s = sc->stream;
+    void* d_query = upload(query_points, sizeof(RtdlPoint) * query_count, s);
+    unsigned long long reached = 0;
+    try {
+      CountOutputs out;
+      out.reached_host = &reached;
+      run_count_threshold(sc, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, out, s);
+    } catch (...) {
+      dev_free(d_query, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(d_query, s);
+    *threshold_reached_count_out = (size_t)reached;
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_prepared_fixed_radius_nearest_witness_2d(void* prepared, const RtdlPoint* query_points,
+                                                           size_t query_count, double radius,
+                                                           RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out,
+                                                           char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!prepared) throw std::runtime_error("prepared OptiX fixed-radius handle must not be null");
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    if (!query_points && query_count != 0)
+      throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    if (radius < 0.0) throw std::runtime_error("fixed_radius_nearest_witness radius must be non-negative");
+    Scene* sc = prepared_count_scene(prepared, 2, radius, "fixed_radius_nearest_witness", "");
+    if (query_count > (size_t)UINT32_MAX)
+      throw std::runtime_error("fixed_radius_nearest_witness query_count exceeds uint32 limit");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || sc->n == 0) return;
+    cudaStream_t s = sc->stream;
+    PhaseTimer timer(s);
+    timer.mark("begin");
+    void* d_query = upload(query_points, sizeof(RtdlPoint) * query_count, s);
+    void* d_rows = nullptr;
+    try {
+      QueryResult r = run_nearest_witness(sc, d_query, (uint32_t)query_count, radius, &d_rows, s, &timer);
+      *rows_out = static_cast<RtdlFixedRadiusNeighborRow*>(
+          download_rows(d_rows, sizeof(RtdlFixedRadiusNeighborRow) * r.rows, s));
+      *row_count_out = (size_t)r.rows;
+      timer.mark("download");
+      timer.publish();
+    } catch (...) {
+      dev_free(d_rows, s);
+      dev_free(d_query, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(d_rows, s);
+    dev_free(d_query, s);
+  }, error_out, error_size);
+}
+
+void rtdl_b200_destroy_prepared_fixed_radius_count_threshold_2d(void* prepared) { rtdl_b200_scene_destroy(prepared); }
+
+int rtdl_b200_prepare_fixed_radius_count_threshold_3d(const RtdlPoint3D* search_points, size_t search_count,
+                                                      double max_radius, void** prepared_out, char* error_out,
+                                                      size_t error_size) {
+  if (!prepared_out) return guarded([] { throw std::runtime_error("prepared_out must not be null"); }, error_out, error_size);
+  *prepared_out = nullptr;
+  const int st = guarded([&]() {
+    if (!search_points && search_count != 0)
+      throw std::runtime_error("search_points pointer must not be null when search_count is nonzero");
+    if (!(max_radius > 0.0)) throw std::runtime_error("fixed_radius_count_threshold_3d max_radius must be positive");
+    if (search_count > (size_t)UINT32_MAX)
+      throw std::runtime_error("fixed_radius_count_threshold_3d search_count exceeds uint32 limit");
+  }, error_out, error_size);
+  if (st != 0) return st;
+  return prepare_count_scene(search_points, search_count, 3, 0, max_radius, false, prepared_out, error_out, error_size);
+}
+
+int rtdl_b200_write_prepared_fixed_radius_count_threshold_3d_device_outputs(
+    void* prepared, const RtdlPoint3D* query_points, size_t query_count, double radius, size_t threshold,
+    uint32_t* query_ids_out, uint32_t* neighbor_counts_out, uint32_t* threshold_flags_out, char* error_out,
+    size_t error_size) {
+  return guarded([&]() {
+    const char* null_msg = "prepared OptiX fixed-radius count-threshold 3D handle must not be null";
+    if (!prepared) throw std::runtime_error(null_msg);
+    if (!query_points && query_count != 0)
+      throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    count_checks(radius, query_count, threshold, "fixed_radius_count_threshold_3d");
+    Scene* sc = prepared_count_scene(prepared, 3, radius, "fixed_radius_count_threshold_3d", null_msg);
+    if (query_count == 0) return;
+    if (!query_ids_out || !neighbor_counts_out || !threshold_flags_out)
+      throw std::runtime_error(
+          "fixed_radius_count_threshold_3d device output pointers must not be null when query_count is nonzero");
+    cudaStream_t s = sc->stream;
+    void* d_query = upload(query_points, sizeof(RtdlPoint3D) * query_count, s);
+    try {
+      CountOutputs out;
+      out.ids = query_ids_out;
+      out.counts = neighbor_counts_out;
+      out.flags = threshold_flags_out;
+      if (threshold == 0)
+        run_count_trivial(d_query, (uint32_t)query_count, 3, out, s);
+      else
+        run_count_threshold(sc, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, out, s);
+    } catch (...) {
+      dev_free(d_query, s);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+    dev_free(d_query, s);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+  }, error_out, error_size);
+}
+
+void rtdl_b200_destroy_prepared_fixed_radius_count_threshold_3d(void* prepared) { rtdl_b200_scene_destroy(prepared); }
+
 int rtdl_b200_scene_query_prepared_device(void* scene, void* queries, double radius, size_t k_max, void* rows_dev,
                                           size_t rows_capacity, size_t* row_count_out, uint8_t* overflow_dev,
                                           void* stream, char* error_out, size_t error_size) {

@@ -100,6 +100,7 @@ struct Scene {
   int device = 0;
   uint32_t n = 0;
   double max_radius = 0.0;  // prepared-FRN contract only
+  bool device_columns = false;  // built from partner-owned device columns (count-threshold contract)
   int leaf_size = 8;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -248,6 +249,30 @@ QueryResult run_ranked_summaries(Scene* sc, const void* queries_dev, uint32_t nq
                                  RtdlFixedRadiusRankedNeighborSummary* summaries_dev,
                                  RtdlFixedRadiusRankedNeighborAggregate* aggregate_host, cudaStream_t s,
                                  PhaseTimer* timer, const PreparedQueries* pq = nullptr);
+// fixed_radius_count_threshold over a scene: per query (input order) its id,
+// its in-radius count (capped at a positive threshold) and whether a positive
+// threshold was reached; every output is optional (device buffers, except
+// reached_host: the number of queries that reached the threshold).
+struct CountOutputs {
+  uint32_t* ids = nullptr;
+  uint32_t* counts = nullptr;
+  uint32_t* flags = nullptr;
+  RtdlFixedRadiusCountRow* rows = nullptr;
+  unsigned long long* reached_host = nullptr;
+};
+void run_count_threshold(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t threshold,
+                         const CountOutputs& out, cudaStream_t s);
+// Device id / x / y columns to RtdlPoint records (device).
+void columns_to_records_2d(const uint32_t* ids, const double* x, const double* y, uint32_t n, void* out,
+                           cudaStream_t s);
+// Every query reaches threshold 0 with a count of 0 (the 3-D device-output contract).
+void run_count_trivial(const void* queries_dev, uint32_t nq, int dim, const CountOutputs& out, cudaStream_t s);
+// Nearest in-radius neighbour of each query, one RtdlFixedRadiusNeighborRow per
+// query in input order (neighbor id 0xFFFFFFFF, distance FLT_MAX when none);
+// *rows_alloc receives a device buffer of nq rows.
+QueryResult run_nearest_witness(Scene* sc, const void* queries_dev, uint32_t nq, double radius, void** rows_alloc,
+                                cudaStream_t s, PhaseTimer* timer);
+
 // The plain per-call form: builds the scene of the search records and answers
 // the query records (device, or host when query_host is set: uploaded inside).
 // fixed_radius_neighbors / bounded_knn_rows with k_max <= 64 prepare the query

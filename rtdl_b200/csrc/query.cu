@@ -1230,6 +1230,123 @@ struct SummaryPartial {
   double sum;
 };
 
+// ---- nearest in-radius witness (k_max 1, one row per query) -------------------
+// offsets[o] = input index of output rank o, offsets[nq] = nq: the emit then
+// writes a query's first row at its input position.
+__global__ void k_witness_offsets(const uint32_t* oorder, const unsigned int* identity, uint32_t nq,
+                                  unsigned long long* offsets) {
+  const bool ident = *identity != 0;
+  for (uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; o <= nq; o += (uint64_t)gridDim.x * blockDim.x)
+    offsets[o] = o == nq ? nq : (ident ? o : oorder[o]);
+}
+
+// The row of a query without a neighbour in radius (rtdl_optix_core.cpp:6043-6090:
+// neighbor id 0xFFFFFFFF, distance FLT_MAX).
+__global__ void k_witness_fill(const float4* qpts, uint32_t nq, RtdlFixedRadiusNeighborRow* rows,
+                               unsigned long long capacity) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq && i < capacity;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    rows[i] = RtdlFixedRadiusNeighborRow{__float_as_uint(qpts[i].w), 0xFFFFFFFFu, 3.4028234663852886e38};
+}
+
+// ---- fixed-radius count with a threshold --------------------------------------
+// The reference's generic count (generic_primitives.py:198-227): a query's
+// in-radius points are counted (radius inclusive, FP64 distances) until the
+// threshold is reached; threshold 0 counts them all.  Here the count uses the
+// collect's accept rule (FP32 outside the band, FP64 inside) on a packet walk,
+// and a lane stops testing once its query reaches the threshold; the walk ends
+// when every lane of the warp has.
+struct CountParams {
+  SceneView S;
+  const float4* qpts;
+  const double* qraw;
+  int qstride;
+  const uint32_t* qorder;       // processing rank -> input index
+  uint32_t nq;
+  const DevBands* bands;
+  uint32_t threshold;
+  uint32_t* ids_out;            // per query, input order (each optional)
+  uint32_t* counts_out;
+  uint32_t* flags_out;
+  RtdlFixedRadiusCountRow* rows_out;
+  unsigned long long* reached;  // optional: queries that reached the threshold
+};
+
+__global__ void __launch_bounds__(256) k_count_packet(CountParams P) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!__any_sync(0xffffffffu, t < P.nq)) return;  // whole warp past the end
+  const bool valid = t < P.nq;
+  const DevBands B = *P.bands;
+  const SceneView& S = P.S;
+  const int scene_inexact = *S.inexact;
+  uint32_t qin = 0;
+  float4 q = make_float4(INFINITY, INFINITY, INFINITY, 0.f);  // never overlaps
+  if (valid) {
+    qin = P.qorder[t];
+    q = P.qpts[qin];
+  }
+  const uint32_t thr = P.threshold;
+  uint32_t count = 0;
+  bool active = valid;
+  int cur = S.n > 0 ? 0 : kRopeEnd;
+  while (cur != kRopeEnd) {
+    const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+    const int hit = __float_as_int(a.w);
+    const bool over = active && box_d2(q.x, q.y, q.z, a, b) <= B.box_hi2;
+    if (__any_sync(0xffffffffu, over)) {
+      if (hit >= 0) {
+        ++cur;  // internal node: its left child is the next record
+        continue;
+      }
+      const int first = leaf_first(hit), cnt = leaf_count(hit);
+      bool test = over;
+      for (int i = first; i < first + cnt; ++i) {
+        const float4 p = __ldg(&S.pts[i]);
+        if (!test) continue;
+        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+        const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        if (d2 > B.hi2) continue;
+        if (d2 >= B.lo2) {
+          const double* rq = P.qraw + (size_t)qin * P.qstride;
+          const double e2 = exact_d2_at(rq[1], rq[2], P.qstride == 4 ? rq[3] : 0.0, S.pts, S.pts64, scene_inexact,
+                                        (uint32_t)i);
+          if (e2 > B.r2) continue;
+        }
+        ++count;
+        if (thr != 0u && count >= thr) {
+          active = false;
+          test = false;
+        }
+      }
+      if (!__any_sync(0xffffffffu, active)) break;  // every query of the warp reached its threshold
+    }
+    cur = __float_as_int(b.w);
+  }
+  const bool reached = valid && thr != 0u && count >= thr;
+  if (valid) {
+    const uint32_t id = __float_as_uint(q.w);
+    if (P.ids_out) P.ids_out[qin] = id;
+    if (P.counts_out) P.counts_out[qin] = count;
+    if (P.flags_out) P.flags_out[qin] = reached ? 1u : 0u;
+    if (P.rows_out) P.rows_out[qin] = RtdlFixedRadiusCountRow{id, count, reached ? 1u : 0u};
+  }
+  if (P.reached) {
+    const unsigned int m = __ballot_sync(0xffffffffu, reached);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(P.reached, (unsigned long long)__popc(m));
+  }
+}
+
+// The 3-D device-output contract with threshold 0 (rtdl_optix_core.cpp:4189-4201):
+// every query reaches it with a count of 0, and no walk is needed.
+__global__ void k_count_trivial(const float4* qpts, uint32_t nq, uint32_t* ids_out, uint32_t* counts_out,
+                                uint32_t* flags_out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += (uint64_t)gridDim.x * blockDim.x) {
+    ids_out[i] = __float_as_uint(qpts[i].w);
+    counts_out[i] = 0u;
+    flags_out[i] = 1u;
+  }
+}
+
 struct SummarySpec {
   RtdlFixedRadiusRankedNeighborSummary* summaries_dev;  // per query, input order (optional)
   RtdlFixedRadiusRankedNeighborAggregate* aggregate_host;
@@ -2172,7 +2289,10 @@ void check_readback(const Readback& r) {
 QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius,
                              uint32_t kmax, void* rows_dev, size_t rows_capacity, void** rows_alloc,
                              uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer, const BatchSpec* bs = nullptr,
-                             const SummarySpec* ss = nullptr, const PreparedQueries* pq = nullptr) {
+                             const SummarySpec* ss = nullptr, const PreparedQueries* pq = nullptr,
+                             bool witness = false) {
+  // witness (k_max 1): one row per query at its input position, pre-filled
+  // with the no-witness row; the nearest in-radius neighbour overwrites it
   QueryResult res;
   void* summary_rows = nullptr;  // ranked summaries: the rows stay internal
   if (ss) rows_alloc = &summary_rows;
@@ -2269,7 +2389,12 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       dev_free(C.stats, s);
     }
     if (timer) timer->mark("traverse");
-    scan_counts_u64(counts, qp.oorder, qp.order_identity, nq, offsets, s);
+    if (witness) {
+      k_witness_offsets<<<grid_for(nq + 1, 256), 256, 0, s>>>(qp.oorder, qp.order_identity, nq, offsets);
+      RTDL_LAUNCHED(1);
+    } else {
+      scan_counts_u64(counts, qp.oorder, qp.order_identity, nq, offsets, s);
+    }
     if (bs) {
       k_problem_rows<<<div_up(bs->problems + 1, 256), 256, 0, s>>>(offsets, qp.qoff, bs->problems, prob_rows);
       RTDL_LAUNCHED(1);
@@ -2316,6 +2441,11 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
       rows_capacity = res.rows;
       *rows_alloc = rows_dev;
+    }
+    if (witness && rows_dev) {
+      k_witness_fill<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, static_cast<RtdlFixedRadiusNeighborRow*>(rows_dev),
+                                                       rows_capacity);
+      RTDL_LAUNCHED(1);
     }
     k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, np, poff);
     RTDL_LAUNCHED(1);
@@ -2440,6 +2570,89 @@ QueryResult run_query_prepared(Scene* sc, const PreparedQueries* pq, double radi
   if (timer) timer->mark("start");
   return run_radius_query(sc, pq->raw, pq->n, kFrn, radius, kmax, rows_dev, rows_capacity, nullptr, overflow_dev, s,
                           timer, nullptr, nullptr, pq);
+}
+
+namespace {
+// SoA point columns (partner-owned device buffers) -> RtdlPoint records.
+__global__ void k_columns_to_records_2d(const uint32_t* ids, const double* x, const double* y, uint32_t n,
+                                        RtdlPoint* out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = RtdlPoint{ids[i], x[i], y[i]};
+}
+}  // namespace
+
+void columns_to_records_2d(const uint32_t* ids, const double* x, const double* y, uint32_t n, void* out,
+                           cudaStream_t s) {
+  if (n == 0) return;
+  k_columns_to_records_2d<<<grid_for(n, 256), 256, 0, s>>>(ids, x, y, n, static_cast<RtdlPoint*>(out));
+  RTDL_LAUNCHED(1);
+}
+
+// ---- count with threshold, nearest witness --------------------------------------
+void run_count_threshold(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t threshold,
+                         const CountOutputs& out, cudaStream_t s) {
+  if (nq == 0) return;
+  if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
+  QueryPrep qp = prepare_queries(sc, queries_dev, nq, true, radius, false, s);
+  unsigned long long* reached = nullptr;
+  try {
+    if (out.reached_host) {
+      reached = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long), s));
+      RTDL_CUDA_CHECK(cudaMemsetAsync(reached, 0, sizeof(unsigned long long), s));
+    }
+    CountParams P;
+    P.S = sc->view();
+    P.qpts = qp.qpts;
+    P.qraw = static_cast<const double*>(queries_dev);
+    P.qstride = sc->dim == 3 ? 4 : 3;
+    P.qorder = qp.qorder;
+    P.nq = nq;
+    P.bands = qp.bands;
+    P.threshold = threshold;
+    P.ids_out = out.ids;
+    P.counts_out = out.counts;
+    P.flags_out = out.flags;
+    P.rows_out = out.rows;
+    P.reached = reached;
+    k_count_packet<<<div_up(nq, 256), 256, 0, s>>>(P);
+    RTDL_LAUNCHED(1);
+    Readback* rb = pinned_readback();
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    if (reached)
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, reached, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    check_readback(*rb);
+    if (out.reached_host) *out.reached_host = rb->rows;
+  } catch (...) {
+    cudaStreamSynchronize(s);
+    dev_free(reached, s);
+    free_prep(qp, s);
+    throw;
+  }
+  dev_free(reached, s);
+  free_prep(qp, s);
+}
+
+void run_count_trivial(const void* queries_dev, uint32_t nq, int dim, const CountOutputs& out, cudaStream_t s) {
+  if (nq == 0) return;
+  float4* qpts = static_cast<float4*>(dev_alloc(sizeof(float4) * nq, s));
+  PointStats* st = static_cast<PointStats*>(dev_alloc(sizeof(PointStats), s));
+  reset_stats(st, s);
+  prep_points(queries_dev, nq, dim, qpts, st, s);
+  k_count_trivial<<<grid_for(nq, 256), 256, 0, s>>>(qpts, nq, out.ids, out.counts, out.flags);
+  RTDL_LAUNCHED(1);
+  dev_free(qpts, s);
+  dev_free(st, s);
+}
+
+QueryResult run_nearest_witness(Scene* sc, const void* queries_dev, uint32_t nq, double radius, void** rows_alloc,
+                                cudaStream_t s, PhaseTimer* timer) {
+  if (rows_alloc) *rows_alloc = nullptr;
+  if (nq == 0 || sc->n == 0) return QueryResult{};
+  if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
+  return run_radius_query(sc, queries_dev, nq, kFrn, radius, 1, nullptr, 0, rows_alloc, nullptr, s, timer, nullptr,
+                          nullptr, nullptr, true);
 }
 
 // ---- the plain per-call form: build and query in one call ---------------------

@@ -48,6 +48,8 @@ SUMMARY_DTYPE = np.dtype(
     }
 )
 AGGREGATE_FIELDS = ("query_count", "bounded_neighbor_count", "nearest_id_checksum", "kth_id_checksum", "sum_distance")
+COUNT_ROW_DTYPE = np.dtype({"names": ["query_id", "neighbor_count", "threshold_reached"],
+                            "formats": ["<u4", "<u4", "<u4"], "offsets": [0, 4, 8], "itemsize": 12})
 KNN_ROW_DTYPE = np.dtype(
     {
         "names": ["query_id", "neighbor_id", "distance", "neighbor_rank"],
@@ -1044,6 +1046,291 @@ class PreparedB200FixedRadiusRankedSummaryAggregateBatchGraph3D:
             self.close()
         except Exception:
             pass
+
+
+def _device_address(obj) -> int:
+    """Device address of a partner buffer: a torch tensor, an object exposing
+    ``__cuda_array_interface__``, or an int address."""
+    if obj is None:
+        return 0
+    if isinstance(obj, int):
+        return obj
+    if hasattr(obj, "data_ptr"):
+        return int(obj.data_ptr())
+    cai = getattr(obj, "__cuda_array_interface__", None)
+    if cai is not None:
+        return int(cai["data"][0])
+    raise TypeError("expected a CUDA tensor, a __cuda_array_interface__ object or a device address")
+
+
+def _count_rows(view: B200RowView) -> tuple:
+    try:
+        return tuple({"query_id": int(r["query_id"]), "neighbor_count": int(r["neighbor_count"]),
+                      "threshold_reached": int(r["threshold_reached"])} for r in view.to_numpy())
+    finally:
+        view.close()
+
+
+def fixed_radius_count_threshold_2d(query_points, search_points=None, *, radius: float,
+                                    threshold: int = 0) -> tuple:
+    """One row per query: its in-radius count, stopped at ``threshold`` when positive, and whether it was
+    reached; mirrors ``fixed_radius_count_threshold_2d_optix`` (``optix_runtime.py:1430-1492``)."""
+    if radius < 0:
+        raise ValueError("radius must be non-negative")
+    if threshold < 0:
+        raise ValueError("threshold must be non-negative")
+    qa, qn, qd, qk = _pack_any(query_points, 2)
+    sa, sn, sd, sk = (qa, qn, qd, qk) if search_points is None else _pack_any(search_points, 2)
+    rows = ctypes.c_void_p()
+    count = ctypes.c_size_t()
+    err = _native.error_buffer()
+    status = _native.load_library().rtdl_b200_run_fixed_radius_count_threshold(
+        qa, qn, sa, sn, float(radius), int(threshold), ctypes.byref(rows), ctypes.byref(count), err, len(err))
+    del qk, sk
+    _native.check_status(status, err)
+    return _count_rows(B200RowView(rows.value or 0, count.value, COUNT_ROW_DTYPE, COUNT_ROW_DTYPE.names))
+
+
+class PreparedB200FixedRadiusCountThreshold2D:
+    """Prepared 2-D fixed-radius count-threshold scene; mirrors ``PreparedOptixFixedRadiusCountThreshold2D``
+    (``optix_runtime.py:1495-1842``)."""
+
+    def __init__(self, search_points, *, max_radius: float):
+        if max_radius < 0:
+            raise ValueError("max_radius must be non-negative")
+        addr, n, dim, keep = _pack_any(search_points, 2)
+        if dim != 2:
+            raise ValueError("prepare_b200_fixed_radius_count_threshold_2d requires 2-D points")
+        self._count = n
+        self._max_radius = float(max_radius)
+        self._handle = ctypes.c_void_p()
+        self._closed = False
+        self._search_scene_true_zero_copy = False
+        if n == 0:
+            return
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_prepare_fixed_radius_count_threshold_2d(
+            addr, n, ctypes.c_double(self._max_radius), ctypes.byref(self._handle), err, len(err))
+        del keep
+        _native.check_status(status, err)
+
+    @classmethod
+    def from_device_columns(cls, search_point_columns: dict, *, max_radius: float):
+        """From partner-owned device columns ``ids`` (u32), ``x``, ``y`` (f64); mirrors
+        ``prepare_optix_fixed_radius_count_threshold_2d_device_search_columns`` (``optix_runtime.py:4215-4270``)."""
+        if max_radius < 0:
+            raise ValueError("max_radius must be non-negative")
+        self = cls.__new__(cls)
+        n = int(search_point_columns.get("count", len(search_point_columns["ids"])))
+        self._count = n
+        self._max_radius = float(max_radius)
+        self._handle = ctypes.c_void_p()
+        self._closed = False
+        self._search_scene_true_zero_copy = True
+        if n == 0:
+            return self
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_prepare_fixed_radius_count_threshold_2d_device_search_columns(
+            _device_address(search_point_columns["ids"]), _device_address(search_point_columns["x"]),
+            _device_address(search_point_columns["y"]), n, ctypes.c_double(self._max_radius),
+            ctypes.byref(self._handle), err, len(err))
+        _native.check_status(status, err)
+        return self
+
+    @property
+    def max_radius(self) -> float:
+        return self._max_radius
+
+    @property
+    def closed(self) -> bool:
+        return self._closed
+
+    def _checks(self, radius: float, threshold: int = 0):
+        if self._closed:
+            raise RuntimeError("prepared b200 fixed-radius count handle is closed")
+        if radius < 0:
+            raise ValueError("radius must be non-negative")
+        if radius > self._max_radius:
+            raise ValueError("radius must be less than or equal to prepared max_radius")
+        if threshold < 0:
+            raise ValueError("threshold must be non-negative")
+
+    def _queries(self, query_points, what: str):
+        addr, n, dim, keep = _pack_any(query_points, 2)
+        if dim != 2:
+            raise ValueError(f"PreparedB200FixedRadiusCountThreshold2D.{what} requires 2-D points")
+        return addr, n, keep
+
+    def run(self, query_points, *, radius: float, threshold: int = 0) -> tuple:
+        self._checks(radius, threshold)
+        addr, n, keep = self._queries(query_points, "run")
+        if n == 0 or self._count == 0:
+            return ()
+        rows = ctypes.c_void_p()
+        count = ctypes.c_size_t()
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_run_prepared_fixed_radius_count_threshold_2d(
+            self._handle, addr, n, float(radius), int(threshold), ctypes.byref(rows), ctypes.byref(count), err,
+            len(err))
+        del keep
+        _native.check_status(status, err)
+        return _count_rows(B200RowView(rows.value or 0, count.value, COUNT_ROW_DTYPE, COUNT_ROW_DTYPE.names))
+
+    def count_threshold_reached(self, query_points, *, radius: float, threshold: int = 0) -> int:
+        """How many queries reached ``threshold`` (the scalar path, no rows)."""
+        self._checks(radius, threshold)
+        addr, n, keep = self._queries(query_points, "count_threshold_reached")
+        if n == 0 or self._count == 0:
+            return 0
+        out = ctypes.c_size_t()
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_count_prepared_fixed_radius_threshold_reached_2d(
+            self._handle, addr, n, float(radius), int(threshold), ctypes.byref(out), err, len(err))
+        del keep
+        _native.check_status(status, err)
+        return int(out.value)
+
+    def nearest_witness_rows(self, query_points, *, radius: float) -> tuple:
+        """One row per query: its nearest in-radius point (neighbor_id 0xFFFFFFFF, distance FLT_MAX when none)."""
+        self._checks(radius)
+        addr, n, keep = self._queries(query_points, "nearest_witness_rows")
+        if n == 0 or self._count == 0:
+            return ()
+        rows = ctypes.c_void_p()
+        count = ctypes.c_size_t()
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_run_prepared_fixed_radius_nearest_witness_2d(
+            self._handle, addr, n, float(radius), ctypes.byref(rows), ctypes.byref(count), err, len(err))
+        del keep
+        _native.check_status(status, err)
+        view = _row_view(rows.value or 0, count.value, False)
+        try:
+            return view.to_dict_rows()
+        finally:
+            view.close()
+
+    def write_device_count_threshold_columns(self, query_point_columns: dict, *, radius: float, threshold: int,
+                                             query_ids_out, neighbor_counts_out, threshold_flags_out) -> dict:
+        """Device query columns (``ids``, ``x``, ``y``) in, device output columns out; needs a scene prepared
+        from device columns (``from_device_columns``)."""
+        self._checks(radius, threshold)
+        if not self._search_scene_true_zero_copy:
+            raise RuntimeError("write_device_count_threshold_columns requires a device-search-column prepared scene")
+        n = int(query_point_columns.get("count", len(query_point_columns["ids"])))
+        meta = {"backend": "b200", "query_count": n, "radius": float(radius), "threshold": int(threshold)}
+        if n == 0 or self._count == 0:
+            return {"metadata": meta}
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_write_prepared_fixed_radius_count_threshold_2d_device_query_columns(
+            self._handle, _device_address(query_point_columns["ids"]), _device_address(query_point_columns["x"]),
+            _device_address(query_point_columns["y"]), n, float(radius), int(threshold),
+            _device_address(query_ids_out), _device_address(neighbor_counts_out), _device_address(threshold_flags_out),
+            err, len(err))
+        _native.check_status(status, err)
+        return {"metadata": meta}
+
+    def close(self) -> None:
+        if not self._closed:
+            if self._handle.value:
+                _native.load_library().rtdl_b200_destroy_prepared_fixed_radius_count_threshold_2d(self._handle)
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PreparedB200FixedRadiusCountThreshold3D:
+    """Prepared 3-D fixed-radius count-threshold scene; mirrors ``PreparedOptixFixedRadiusCountThreshold3D``
+    (``optix_runtime.py:2974-3110``): host query records in, caller-owned device columns out."""
+
+    def __init__(self, search_points, *, max_radius: float):
+        if max_radius <= 0:
+            raise ValueError("max_radius must be positive")
+        addr, n, dim, keep = _pack_any(search_points, 3)
+        if dim != 3:
+            raise ValueError("prepare_b200_fixed_radius_count_threshold_3d requires 3-D points")
+        self._count = n
+        self._max_radius = float(max_radius)
+        self._handle = ctypes.c_void_p()
+        self._closed = False
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_prepare_fixed_radius_count_threshold_3d(
+            addr, n, ctypes.c_double(self._max_radius), ctypes.byref(self._handle), err, len(err))
+        del keep
+        _native.check_status(status, err)
+
+    @property
+    def max_radius(self) -> float:
+        return self._max_radius
+
+    @property
+    def closed(self) -> bool:
+        return self._closed
+
+    def write_device_count_threshold_columns(self, query_points, *, radius: float, threshold: int,
+                                             query_ids_out, neighbor_counts_out, threshold_flags_out) -> dict:
+        if self._closed:
+            raise RuntimeError("prepared b200 fixed-radius count-threshold 3D handle is closed")
+        if radius < 0:
+            raise ValueError("radius must be non-negative")
+        if radius > self._max_radius:
+            raise ValueError("radius must be less than or equal to prepared max_radius")
+        if threshold < 0:
+            raise ValueError("threshold must be non-negative")
+        addr, n, dim, keep = _pack_any(query_points, 3)
+        if dim != 3:
+            raise ValueError("write_device_count_threshold_columns requires 3-D query points")
+        meta = {"backend": "b200", "query_count": n, "search_count": self._count, "radius": float(radius),
+                "threshold": int(threshold), "materializes_neighbor_rows": False}
+        if n == 0:
+            return {"metadata": meta}
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_write_prepared_fixed_radius_count_threshold_3d_device_outputs(
+            self._handle, addr, n, float(radius), int(threshold), _device_address(query_ids_out),
+            _device_address(neighbor_counts_out), _device_address(threshold_flags_out), err, len(err))
+        del keep
+        _native.check_status(status, err)
+        return {"metadata": meta}
+
+    def close(self) -> None:
+        if not self._closed:
+            if self._handle.value:
+                _native.load_library().rtdl_b200_destroy_prepared_fixed_radius_count_threshold_3d(self._handle)
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def prepare_b200_fixed_radius_count_threshold_2d(search_points, *, max_radius: float):
+    return PreparedB200FixedRadiusCountThreshold2D(search_points, max_radius=max_radius)
+
+
+def prepare_b200_fixed_radius_count_threshold_2d_device_search_columns(search_point_columns: dict, *,
+                                                                       max_radius: float):
+    return PreparedB200FixedRadiusCountThreshold2D.from_device_columns(search_point_columns, max_radius=max_radius)
+
+
+def prepare_b200_fixed_radius_count_threshold_3d(search_points, *, max_radius: float):
+    return PreparedB200FixedRadiusCountThreshold3D(search_points, max_radius=max_radius)
 
 
 def prepare_b200_fixed_radius_neighbors_3d(search_points, *, max_radius: float) -> PreparedB200FixedRadiusNeighbors3D:

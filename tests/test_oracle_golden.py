@@ -76,3 +76,24 @@ def test_restatement_agrees_with_reference_native_oracle():
     ours = O.fixed_radius_neighbors(q, s, radius=0.12, k_max=6)
     ref = O.reference_fixed_radius_neighbors(O.pack_reference_points(q), O.pack_reference_points(s), radius=0.12, k_max=6)
     assert G.rows_as_tuples(ours, False) == G.rows_as_tuples(ref, False)
+
+
+def _count_cases():
+    import json
+    from pathlib import Path
+
+    data = json.loads((Path(__file__).parent / "golden" / "count_threshold_2d.json").read_text())
+    return data["cases"]
+
+
+@pytest.mark.parametrize("case", _count_cases(), ids=lambda c: f"{c['name']}-r{c['radius']}-t{c['threshold']}")
+def test_oracle_count_threshold_matches_reference_generic_cpu(case):
+    """fixed_radius_count_threshold restated from the oracle's exact counts against rows of the
+    reference's own generic CPU count (tests/golden/make_count_threshold_golden.py)."""
+    q = {k: np.asarray(v, dtype=np.uint32 if k == "id" else np.float64) for k, v in case["query"].items()}
+    s = {k: np.asarray(v, dtype=np.uint32 if k == "id" else np.float64) for k, v in case["search"].items()}
+    got = O.fixed_radius_count_threshold(q, s, radius=case["radius"], threshold=case["threshold"])
+    exp = np.asarray(case["rows"], dtype=np.int64)
+    assert np.array_equal(got["query_id"], exp[:, 0])
+    assert np.array_equal(got["neighbor_count"], exp[:, 1])
+    assert np.array_equal(got["threshold_reached"], exp[:, 2])

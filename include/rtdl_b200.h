@@ -96,6 +96,16 @@ typedef struct RtdlFixedRadiusCountRow {
   uint32_t threshold_reached;  /* 1 when the threshold is positive and was reached */
 } RtdlFixedRadiusCountRow;
 
+/* A group of search points for the point-group witness: a span of the search
+ * array and its bounding box; same layout as
+ * src/native/optix/rtdl_optix_prelude.h:282-287 (RtdlPointGroupBounds2D, 48 B). */
+typedef struct RtdlPointGroupBounds2D {
+  uint32_t id;
+  uint32_t point_offset;
+  uint32_t point_count;
+  double min_x, min_y, max_x, max_y;
+} RtdlPointGroupBounds2D;
+
 /* Version triple (the reference exports rtdl_optix_get_version,
  * rtdl_optix_api.cpp:1-7). */
 RTDL_B200_API int rtdl_b200_get_version(int* major, int* minor, int* patch);
@@ -454,6 +464,38 @@ RTDL_B200_API int rtdl_b200_write_prepared_fixed_radius_count_threshold_3d_devic
     uint32_t* query_ids_out, uint32_t* neighbor_counts_out, uint32_t* threshold_flags_out,
     char* error_out, size_t error_size);
 RTDL_B200_API void rtdl_b200_destroy_prepared_fixed_radius_count_threshold_3d(void* prepared);
+
+/* ---- point-group witness (2-D) ----------------------------------------------------
+ * Replace the entry points of the reference's prepared point-group nearest
+ * witness (rtdl_optix_prelude.h:1480-1512; rtdl_optix_api.cpp:4885-4990 and
+ * rtdl_optix_workloads.cpp:13554-13880).  Groups are spans of the search array
+ * with a bounding box; a search point takes part for a query when it and its
+ * group's box are within radius (FP64, inclusive), once per group that holds
+ * it.  Threshold: counting stops at a positive threshold; the flag is 1 when it
+ * was reached (0 for threshold 0, except without groups, where threshold 0
+ * counts as reached, as in the reference).  Witness: per query (input order)
+ * the nearest such point by exact distance then smaller id, or neighbor_id
+ * 0xFFFFFFFF and distance FLT_MAX.  Max distance: the witness row of largest
+ * distance (then smaller query id, then smaller neighbour id), a query without
+ * a witness counting as infinitely far; {0xFFFFFFFF, 0xFFFFFFFF, inf} when
+ * there are no queries or groups. */
+RTDL_B200_API int rtdl_b200_prepare_point_group_nearest_witness_2d(
+    const RtdlPoint* search_points, size_t search_count, const RtdlPointGroupBounds2D* groups, size_t group_count,
+    double max_radius, void** prepared_out, char* error_out, size_t error_size);
+RTDL_B200_API int rtdl_b200_count_prepared_point_group_threshold_reached_2d(
+    void* prepared, const RtdlPoint* query_points, size_t query_count, double radius, size_t threshold,
+    size_t* threshold_reached_count_out, char* error_out, size_t error_size);
+/* threshold_flags_out: host array of query_count words. */
+RTDL_B200_API int rtdl_b200_write_prepared_point_group_threshold_flags_2d(
+    void* prepared, const RtdlPoint* query_points, size_t query_count, double radius, size_t threshold,
+    uint32_t* threshold_flags_out, char* error_out, size_t error_size);
+RTDL_B200_API int rtdl_b200_run_prepared_point_group_nearest_witness_2d(
+    void* prepared, const RtdlPoint* query_points, size_t query_count, double radius,
+    RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out, char* error_out, size_t error_size);
+RTDL_B200_API int rtdl_b200_reduce_prepared_point_group_nearest_max_distance_2d(
+    void* prepared, const RtdlPoint* query_points, size_t query_count, double radius,
+    RtdlFixedRadiusNeighborRow* row_out, char* error_out, size_t error_size);
+RTDL_B200_API void rtdl_b200_destroy_prepared_point_group_nearest_witness_2d(void* prepared);
 
 /* ---- captured batch graph of prepared-query aggregates -----------------------
  * Replace the batch-graph entry points of rtdl_optix_api.cpp:4323-4396

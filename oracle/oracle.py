@@ -163,6 +163,66 @@ def nearest_witness(query, search, *, radius, threads=1):
     return out
 
 
+def point_group_witness(query, search, groups, *, radius, threshold=0):
+    """The reference's prepared point-group kernels (``rtdl_optix_core.cpp:6119-6358``) restated in FP64
+    (numpy, small cases): a search point takes part for a query when it and its group's box are within
+    radius (inclusive), once per group holding it.  Returns (stopped counts, flags, witness rows, max row):
+    counting stops at a positive threshold; the flag is 1 when it was reached; the witness is the nearest
+    such point by distance then smaller id (0xFFFFFFFF / FLT_MAX when none); the max row is the witness of
+    largest distance, then smaller query id, then smaller neighbour id, a missing witness counting as
+    infinitely far."""
+    qx = np.asarray(query["x"], dtype=np.float64)
+    qy = np.asarray(query["y"], dtype=np.float64)
+    qid = np.asarray(query["id"], dtype=np.uint32)
+    sx = np.asarray(search["x"], dtype=np.float64)
+    sy = np.asarray(search["y"], dtype=np.float64)
+    sid = np.asarray(search["id"], dtype=np.uint32)
+    r2 = float(radius) * float(radius)
+    nq = len(qid)
+    counts = np.zeros(nq, dtype=np.int64)
+    best_d2 = np.full(nq, np.inf)
+    best_id = np.full(nq, 0xFFFFFFFF, dtype=np.int64)
+    for g in groups:
+        lo, n = int(g["point_offset"]), int(g["point_count"])
+        dxb = np.where(qx < g["min_x"], g["min_x"] - qx, np.where(qx > g["max_x"], qx - g["max_x"], 0.0))
+        dyb = np.where(qy < g["min_y"], g["min_y"] - qy, np.where(qy > g["max_y"], qy - g["max_y"], 0.0))
+        ok = (dxb * dxb + dyb * dyb) <= r2
+        if n == 0 or not ok.any():
+            continue
+        qi = np.flatnonzero(ok)
+        dx = sx[None, lo:lo + n] - qx[qi, None]
+        dy = sy[None, lo:lo + n] - qy[qi, None]
+        d2 = dx * dx + dy * dy
+        inr = d2 <= r2
+        counts[qi] += inr.sum(axis=1)
+        d2m = np.where(inr, d2, np.inf)
+        ids = sid[lo:lo + n].astype(np.int64)
+        for row, q in enumerate(qi):
+            m = d2m[row]
+            if not np.isfinite(m).any():
+                continue
+            mn = m.min()
+            cand = ids[m == mn].min()
+            if mn < best_d2[q] or (mn == best_d2[q] and cand < best_id[q]):
+                best_d2[q] = mn
+                best_id[q] = cand
+    thr = int(threshold)
+    stopped = np.minimum(counts, thr) if thr > 0 else counts
+    flags = (counts >= thr).astype(np.uint32) if thr > 0 else np.zeros(nq, dtype=np.uint32)
+    rows = np.zeros(nq, dtype=FRN_ROW_DTYPE)
+    rows["query_id"] = qid
+    found = np.isfinite(best_d2)
+    rows["neighbor_id"] = np.where(found, best_id, 0xFFFFFFFF).astype(np.uint32)
+    rows["distance"] = np.where(found, np.sqrt(np.where(found, best_d2, 0.0)), 3.4028234663852886e38)
+    key = np.where(found, rows["distance"], np.inf)
+    order = np.lexsort((rows["neighbor_id"], rows["query_id"], -key))
+    top = order[0] if nq else None
+    max_row = {"query_id": 0xFFFFFFFF, "neighbor_id": 0xFFFFFFFF, "distance": float("inf")} if top is None else {
+        "query_id": int(rows["query_id"][top]), "neighbor_id": int(rows["neighbor_id"][top]),
+        "distance": float(key[top])}
+    return stopped.astype(np.uint32), flags, rows, max_row
+
+
 SUMMARY_DTYPE = np.dtype(
     {
         "names": ["query_id", "neighbor_count", "nearest_neighbor_id", "kth_neighbor_id", "nearest_distance",

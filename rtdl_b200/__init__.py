@@ -45,11 +45,13 @@ from .runtime import (  # noqa: F401
     PreparedB200FixedRadiusRankedSummaryAggregateBatchGraph3D,
     PreparedB200FixedRadiusCountThreshold2D,
     PreparedB200FixedRadiusCountThreshold3D,
+    PreparedB200PointGroupNearestWitness2D,
     directed_hausdorff,
     fixed_radius_count_threshold_2d,
     prepare_b200_fixed_radius_count_threshold_2d,
     prepare_b200_fixed_radius_count_threshold_2d_device_search_columns,
     prepare_b200_fixed_radius_count_threshold_3d,
+    prepare_b200_point_group_nearest_witness_2d,
     hausdorff_distance,
     pack_points,
     prepare_b200,

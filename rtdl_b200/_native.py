@@ -174,6 +174,12 @@ SIGNATURES = {
     "rtdl_b200_write_prepared_fixed_radius_count_threshold_3d_device_outputs": (
         _i, [_vp, _vp, _sz, _d, _sz, _vp, _vp, _vp, _cp, _sz]),
     "rtdl_b200_destroy_prepared_fixed_radius_count_threshold_3d": (None, [_vp]),
+    "rtdl_b200_prepare_point_group_nearest_witness_2d": (_i, [_vp, _sz, _vp, _sz, _d, _vpp, _cp, _sz]),
+    "rtdl_b200_count_prepared_point_group_threshold_reached_2d": (_i, [_vp, _vp, _sz, _d, _sz, _szp, _cp, _sz]),
+    "rtdl_b200_write_prepared_point_group_threshold_flags_2d": (_i, [_vp, _vp, _sz, _d, _sz, _vp, _cp, _sz]),
+    "rtdl_b200_run_prepared_point_group_nearest_witness_2d": (_i, [_vp, _vp, _sz, _d, _vpp, _szp, _cp, _sz]),
+    "rtdl_b200_reduce_prepared_point_group_nearest_max_distance_2d": (_i, [_vp, _vp, _sz, _d, _vp, _cp, _sz]),
+    "rtdl_b200_destroy_prepared_point_group_nearest_witness_2d": (None, [_vp]),
     "rtdl_b200_get_last_phase_timings": (_i, [ctypes.POINTER(ctypes.c_char_p), _dp, _i]),
     "rtdl_b200_set_tuning": (_i, [_i, _i, _i]),
     "rtdl_b200_get_launch_count": (_i, [ctypes.POINTER(ctypes.c_ulonglong)]),

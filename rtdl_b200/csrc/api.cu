@@ -11,6 +11,8 @@
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <unordered_map>
@@ -1431,6 +1433,179 @@ int rtdl_b200_write_prepared_fixed_radius_count_threshold_3d_device_outputs(
 }
 
 void rtdl_b200_destroy_prepared_fixed_radius_count_threshold_3d(void* prepared) { rtdl_b200_scene_destroy(prepared); }
+
+// ---- point-group witness ---------------------------------------------------------
+namespace rtdl_b200 {
+namespace {
+PointGroupScene* point_group_checked(void* prepared, double radius, size_t query_count, const char* what) {
+  PointGroupScene* pg = static_cast<PointGroupScene*>(prepared);
+  if (!pg) throw std::runtime_error("prepared OptiX point-group handle must not be null");
+  const std::string w(what);
+  if (radius < 0.0) throw std::runtime_error(w + " radius must be non-negative");
+  if (radius > pg->max_radius + 1.0e-7) throw std::runtime_error(w + " radius exceeds prepared max_radius");
+  if (query_count > (size_t)UINT32_MAX) throw std::runtime_error(w + " query_count exceeds uint32 limit");
+  return pg;
+}
+
+// Uploads host query records, runs `fn(d_query, s)`, releases them.
+void with_queries(PointGroupScene* pg, const RtdlPoint* query_points, size_t query_count,
+                  const std::function<void(const void*, cudaStream_t)>& fn) {
+  cudaStream_t s = pg->sc->stream;
+  void* d_query = upload(query_points, sizeof(RtdlPoint) * query_count, s);
+  try {
+    fn(d_query, s);
+  } catch (...) {
+    dev_free(d_query, s);
+    cudaStreamSynchronize(s);
+    throw;
+  }
+  dev_free(d_query, s);
+}
+}  // namespace
+}  // namespace rtdl_b200
+
+int rtdl_b200_prepare_point_group_nearest_witness_2d(const RtdlPoint* search_points, size_t search_count,
+                                                     const RtdlPointGroupBounds2D* groups, size_t group_count,
+                                                     double max_radius, void** prepared_out, char* error_out,
+                                                     size_t error_size) {
+  return guarded([&]() {
+    if (!prepared_out) throw std::runtime_error("prepared_out must not be null");
+    *prepared_out = nullptr;
+    if (!search_points && search_count != 0)
+      throw std::runtime_error("point_group search_points pointer must not be null when search_count is nonzero");
+    if (!groups && group_count != 0)
+      throw std::runtime_error("point_group groups pointer must not be null when group_count is nonzero");
+    if (max_radius < 0.0) throw std::runtime_error("point_group_nearest_witness max_radius must be non-negative");
+    if (search_count > (size_t)UINT32_MAX)
+      throw std::runtime_error("point_group_nearest_witness search_count exceeds uint32 limit");
+    if (group_count > (size_t)UINT32_MAX)
+      throw std::runtime_error("point_group_nearest_witness group_count exceeds uint32 limit");
+    int dev = 0;
+    RTDL_CUDA_CHECK(cudaGetDevice(&dev));
+    ensure_pool_configured(dev);
+    *prepared_out = point_group_create(search_points, search_count, groups, group_count, max_radius,
+                                       leaf_size_for(true), library_stream());
+  }, error_out, error_size);
+}
+
+int rtdl_b200_count_prepared_point_group_threshold_reached_2d(void* prepared, const RtdlPoint* query_points,
+                                                              size_t query_count, double radius, size_t threshold,
+                                                              size_t* threshold_reached_count_out, char* error_out,
+                                                              size_t error_size) {
+  return guarded([&]() {
+    if (!prepared) throw std::runtime_error("prepared OptiX point-group handle must not be null");
+    if (!threshold_reached_count_out) throw std::runtime_error("threshold_reached_count_out must not be null");
+    if (!query_points && query_count != 0)
+      throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    PointGroupScene* pg = point_group_checked(prepared, radius, query_count, "point_group_threshold");
+    if (threshold > (size_t)UINT32_MAX) throw std::runtime_error("point_group_threshold threshold exceeds uint32 limit");
+    *threshold_reached_count_out = 0;
+    if (query_count == 0 || pg->groups == 0) return;
+    unsigned long long reached = 0;
+    with_queries(pg, query_points, query_count, [&](const void* d_query, cudaStream_t s) {
+      CountOutputs out;
+      out.reached_host = &reached;
+      point_group_count(pg, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, out, s);
+    });
+    *threshold_reached_count_out = (size_t)reached;
+  }, error_out, error_size);
+}
+
+int rtdl_b200_write_prepared_point_group_threshold_flags_2d(void* prepared, const RtdlPoint* query_points,
+                                                            size_t query_count, double radius, size_t threshold,
+                                                            uint32_t* threshold_flags_out, char* error_out,
+                                                            size_t error_size) {
+  return guarded([&]() {
+    if (!prepared) throw std::runtime_error("prepared OptiX point-group handle must not be null");
+    if (!threshold_flags_out && query_count != 0)
+      throw std::runtime_error("threshold_flags_out must not be null when query_count is nonzero");
+    if (!query_points && query_count != 0)
+      throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    PointGroupScene* pg = point_group_checked(prepared, radius, query_count, "point_group_threshold_flags");
+    if (threshold > (size_t)UINT32_MAX)
+      throw std::runtime_error("point_group_threshold_flags threshold exceeds uint32 limit");
+    if (query_count == 0) return;
+    if (pg->groups == 0) {  // as the reference: threshold 0 counts as reached without groups
+      for (size_t i = 0; i < query_count; ++i) threshold_flags_out[i] = threshold == 0 ? 1u : 0u;
+      return;
+    }
+    with_queries(pg, query_points, query_count, [&](const void* d_query, cudaStream_t s) {
+      uint32_t* d_flags = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * query_count, s));
+      try {
+        CountOutputs out;
+        out.flags = d_flags;
+        point_group_count(pg, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, out, s);
+        RTDL_CUDA_CHECK(cudaMemcpyAsync(threshold_flags_out, d_flags, sizeof(uint32_t) * query_count,
+                                        cudaMemcpyDeviceToHost, s));
+        RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      } catch (...) {
+        dev_free(d_flags, s);
+        throw;
+      }
+      dev_free(d_flags, s);
+    });
+  }, error_out, error_size);
+}
+
+int rtdl_b200_run_prepared_point_group_nearest_witness_2d(void* prepared, const RtdlPoint* query_points,
+                                                          size_t query_count, double radius,
+                                                          RtdlFixedRadiusNeighborRow** rows_out, size_t* row_count_out,
+                                                          char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!prepared) throw std::runtime_error("prepared OptiX point-group handle must not be null");
+    if (!rows_out || !row_count_out) throw std::runtime_error("output pointers must not be null");
+    if (!query_points && query_count != 0)
+      throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    PointGroupScene* pg = point_group_checked(prepared, radius, query_count, "point_group_nearest_witness");
+    *rows_out = nullptr;
+    *row_count_out = 0;
+    if (query_count == 0 || pg->groups == 0) return;
+    with_queries(pg, query_points, query_count, [&](const void* d_query, cudaStream_t s) {
+      RtdlFixedRadiusNeighborRow* d_rows =
+          static_cast<RtdlFixedRadiusNeighborRow*>(dev_alloc(sizeof(RtdlFixedRadiusNeighborRow) * query_count, s));
+      try {
+        point_group_nearest(pg, d_query, (uint32_t)query_count, radius, d_rows, nullptr, s);
+        *rows_out = static_cast<RtdlFixedRadiusNeighborRow*>(
+            download_rows(d_rows, sizeof(RtdlFixedRadiusNeighborRow) * query_count, s));
+        *row_count_out = query_count;
+      } catch (...) {
+        dev_free(d_rows, s);
+        throw;
+      }
+      dev_free(d_rows, s);
+    });
+  }, error_out, error_size);
+}
+
+int rtdl_b200_reduce_prepared_point_group_nearest_max_distance_2d(void* prepared, const RtdlPoint* query_points,
+                                                                  size_t query_count, double radius,
+                                                                  RtdlFixedRadiusNeighborRow* row_out,
+                                                                  char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!prepared) throw std::runtime_error("prepared OptiX point-group handle must not be null");
+    if (!row_out) throw std::runtime_error("row_out must not be null");
+    if (!query_points && query_count != 0)
+      throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
+    PointGroupScene* pg = point_group_checked(prepared, radius, query_count, "point_group_nearest_max_distance");
+    *row_out = RtdlFixedRadiusNeighborRow{0xFFFFFFFFu, 0xFFFFFFFFu, std::numeric_limits<double>::infinity()};
+    if (query_count == 0 || pg->groups == 0) return;
+    with_queries(pg, query_points, query_count, [&](const void* d_query, cudaStream_t s) {
+      RtdlFixedRadiusNeighborRow* d_rows =
+          static_cast<RtdlFixedRadiusNeighborRow*>(dev_alloc(sizeof(RtdlFixedRadiusNeighborRow) * query_count, s));
+      try {
+        point_group_nearest(pg, d_query, (uint32_t)query_count, radius, d_rows, row_out, s);
+      } catch (...) {
+        dev_free(d_rows, s);
+        throw;
+      }
+      dev_free(d_rows, s);
+    });
+  }, error_out, error_size);
+}
+
+void rtdl_b200_destroy_prepared_point_group_nearest_witness_2d(void* prepared) {
+  point_group_destroy(static_cast<PointGroupScene*>(prepared));
+}
 
 int rtdl_b200_scene_query_prepared_device(void* scene, void* queries, double radius, size_t k_max, void* rows_dev,
                                           size_t rows_capacity, size_t* row_count_out, uint8_t* overflow_dev,

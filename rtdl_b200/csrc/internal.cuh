@@ -262,6 +262,26 @@ struct CountOutputs {
 };
 void run_count_threshold(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t threshold,
                          const CountOutputs& out, cudaStream_t s);
+// Point groups (spans of a search array with their boxes): a scene over every
+// group's points, each tagged with its group; a candidate counts when it and its
+// group's box are within radius (a point in two groups counts twice).
+struct PointGroupScene {
+  Scene* sc = nullptr;
+  uint32_t* group_of = nullptr;  // device, group of each scene point (scene input order)
+  double* boxes = nullptr;       // device, min_x, min_y, max_x, max_y per group
+  uint32_t groups = 0, points = 0;
+  double max_radius = 0.0;
+};
+PointGroupScene* point_group_create(const RtdlPoint* points, size_t count, const RtdlPointGroupBounds2D* groups,
+                                    size_t group_count, double max_radius, int leaf_size, cudaStream_t s);
+void point_group_destroy(PointGroupScene* pg);
+void point_group_count(PointGroupScene* pg, const void* queries_dev, uint32_t nq, double radius, uint32_t threshold,
+                       const CountOutputs& out, cudaStream_t s);
+// One witness row per query (input order) into rows_dev; with max_row_host, also
+// the row of largest distance (a query without a witness counts as infinitely far).
+void point_group_nearest(PointGroupScene* pg, const void* queries_dev, uint32_t nq, double radius,
+                         RtdlFixedRadiusNeighborRow* rows_dev, RtdlFixedRadiusNeighborRow* max_row_host,
+                         cudaStream_t s);
 // Device id / x / y columns to RtdlPoint records (device).
 void columns_to_records_2d(const uint32_t* ids, const double* x, const double* y, uint32_t n, void* out,
                            cudaStream_t s);

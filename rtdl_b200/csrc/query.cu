@@ -1270,7 +1270,22 @@ struct CountParams {
   uint32_t* flags_out;
   RtdlFixedRadiusCountRow* rows_out;
   unsigned long long* reached;  // optional: queries that reached the threshold
+  // point groups (optional): a candidate also needs its group's box within radius
+  const uint32_t* group_of;     // group of each scene point (scene input order)
+  const double* group_boxes;    // min_x, min_y, max_x, max_y per group
 };
+
+// The reference's group test (rtdl_optix_core.cpp:6143-6147) in FP64: the
+// squared distance from the query to the group's box, within radius.
+__device__ __forceinline__ bool group_box_ok(const CountParams& P, const SceneView& S, uint32_t qin, uint32_t i,
+                                             double r2) {
+  const double* rq = P.qraw + (size_t)qin * P.qstride;
+  const double qx = rq[1], qy = rq[2];
+  const double* g = P.group_boxes + 4ull * P.group_of[S.perm[i]];
+  const double dx = qx < g[0] ? __dsub_rn(g[0], qx) : (qx > g[2] ? __dsub_rn(qx, g[2]) : 0.0);
+  const double dy = qy < g[1] ? __dsub_rn(g[1], qy) : (qy > g[3] ? __dsub_rn(qy, g[3]) : 0.0);
+  return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)) <= r2;
+}
 
 __global__ void __launch_bounds__(256) k_count_packet(CountParams P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1312,6 +1327,7 @@ __global__ void __launch_bounds__(256) k_count_packet(CountParams P) {
                                         (uint32_t)i);
           if (e2 > B.r2) continue;
         }
+        if (P.group_of && !group_box_ok(P, S, qin, (uint32_t)i, B.r2)) continue;
         ++count;
         if (thr != 0u && count >= thr) {
           active = false;
@@ -1334,6 +1350,89 @@ __global__ void __launch_bounds__(256) k_count_packet(CountParams P) {
     const unsigned int m = __ballot_sync(0xffffffffu, reached);
     if ((threadIdx.x & 31) == 0 && m) atomicAdd(P.reached, (unsigned long long)__popc(m));
   }
+}
+
+// Point groups: the nearest point within radius whose group box is also within
+// radius, by exact FP64 distance then smaller id (rtdl_optix_core.cpp:6215-6306);
+// one row per query at its input index, 0xFFFFFFFF / FLT_MAX when none.
+__global__ void __launch_bounds__(256) k_group_nearest_packet(CountParams P, RtdlFixedRadiusNeighborRow* rows) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!__any_sync(0xffffffffu, t < P.nq)) return;  // whole warp past the end
+  const bool valid = t < P.nq;
+  const DevBands B = *P.bands;
+  const SceneView& S = P.S;
+  const int scene_inexact = *S.inexact;
+  uint32_t qin = 0;
+  float4 q = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+  if (valid) {
+    qin = P.qorder[t];
+    q = P.qpts[qin];
+  }
+  double best = 0.0;
+  uint32_t best_id = 0xFFFFFFFFu;
+  bool found = false;
+  int cur = S.n > 0 ? 0 : kRopeEnd;
+  while (cur != kRopeEnd) {
+    const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+    const int hit = __float_as_int(a.w);
+    const bool over = valid && box_d2(q.x, q.y, q.z, a, b) <= B.box_hi2;
+    if (__any_sync(0xffffffffu, over)) {
+      if (hit >= 0) {
+        ++cur;
+        continue;
+      }
+      const int first = leaf_first(hit), cnt = leaf_count(hit);
+      for (int i = first; i < first + cnt; ++i) {
+        const float4 p = __ldg(&S.pts[i]);
+        if (!over) continue;
+        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+        if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) > B.hi2) continue;
+        const double* rq = P.qraw + (size_t)qin * P.qstride;
+        const double e2 = exact_d2_at(rq[1], rq[2], P.qstride == 4 ? rq[3] : 0.0, S.pts, S.pts64, scene_inexact,
+                                      (uint32_t)i);
+        if (e2 > B.r2) continue;
+        if (P.group_of && !group_box_ok(P, S, qin, (uint32_t)i, B.r2)) continue;
+        const uint32_t id = __float_as_uint(p.w);
+        if (!found || e2 < best || (e2 == best && id < best_id)) {
+          best = e2;
+          best_id = id;
+          found = true;
+        }
+      }
+    }
+    cur = __float_as_int(b.w);
+  }
+  if (valid)
+    rows[qin] = RtdlFixedRadiusNeighborRow{__float_as_uint(q.w), found ? best_id : 0xFFFFFFFFu,
+                                           found ? __dsqrt_rn(best) : 3.4028234663852886e38};
+}
+
+// The witness row of largest distance, ties to the smaller query id then
+// neighbour id; a query without a witness counts as infinitely far
+// (rtdl_optix_core.cpp:6310-6358).  One block.
+__device__ __forceinline__ bool witness_after(const RtdlFixedRadiusNeighborRow& c, const RtdlFixedRadiusNeighborRow& b) {
+  if (c.distance != b.distance) return c.distance > b.distance;
+  if (c.query_id != b.query_id) return c.query_id < b.query_id;
+  return c.neighbor_id < b.neighbor_id;
+}
+
+__global__ void __launch_bounds__(1024) k_witness_max(const RtdlFixedRadiusNeighborRow* rows, uint32_t n,
+                                                      RtdlFixedRadiusNeighborRow* out) {
+  __shared__ RtdlFixedRadiusNeighborRow sb[1024];
+  RtdlFixedRadiusNeighborRow best{0xFFFFFFFFu, 0xFFFFFFFFu, -1.0};
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    RtdlFixedRadiusNeighborRow r = rows[i];
+    if (r.neighbor_id == 0xFFFFFFFFu || !isfinite(r.distance)) r.distance = INFINITY;
+    if (witness_after(r, best)) best = r;
+  }
+  sb[threadIdx.x] = best;
+  __syncthreads();
+  for (unsigned int stride = blockDim.x >> 1; stride > 0; stride >>= 1) {
+    if (threadIdx.x < stride && witness_after(sb[threadIdx.x + stride], sb[threadIdx.x]))
+      sb[threadIdx.x] = sb[threadIdx.x + stride];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sb[0];
 }
 
 // The 3-D device-output contract with threshold 0 (rtdl_optix_core.cpp:4189-4201):
@@ -2589,8 +2688,12 @@ void columns_to_records_2d(const uint32_t* ids, const double* x, const double* y
 }
 
 // ---- count with threshold, nearest witness --------------------------------------
-void run_count_threshold(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t threshold,
-                         const CountOutputs& out, cudaStream_t s) {
+namespace {
+// The count (or, with nearest_rows, the point-group witness) walk over a scene;
+// group_of / group_boxes restrict candidates to groups whose box is in radius.
+void count_walk(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t threshold,
+                const CountOutputs& out, const uint32_t* group_of, const double* group_boxes,
+                RtdlFixedRadiusNeighborRow* nearest_rows, cudaStream_t s) {
   if (nq == 0) return;
   if (sc->problems) throw std::runtime_error("a problem batch is queried with the batch entry points");
   QueryPrep qp = prepare_queries(sc, queries_dev, nq, true, radius, false, s);
@@ -2614,7 +2717,12 @@ void run_count_threshold(Scene* sc, const void* queries_dev, uint32_t nq, double
     P.flags_out = out.flags;
     P.rows_out = out.rows;
     P.reached = reached;
-    k_count_packet<<<div_up(nq, 256), 256, 0, s>>>(P);
+    P.group_of = group_of;
+    P.group_boxes = group_boxes;
+    if (nearest_rows)
+      k_group_nearest_packet<<<div_up(nq, 256), 256, 0, s>>>(P, nearest_rows);
+    else
+      k_count_packet<<<div_up(nq, 256), 256, 0, s>>>(P);
     RTDL_LAUNCHED(1);
     Readback* rb = pinned_readback();
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
@@ -2632,6 +2740,101 @@ void run_count_threshold(Scene* sc, const void* queries_dev, uint32_t nq, double
   }
   dev_free(reached, s);
   free_prep(qp, s);
+}
+}  // namespace
+
+void run_count_threshold(Scene* sc, const void* queries_dev, uint32_t nq, double radius, uint32_t threshold,
+                         const CountOutputs& out, cudaStream_t s) {
+  count_walk(sc, queries_dev, nq, radius, threshold, out, nullptr, nullptr, nullptr, s);
+}
+
+PointGroupScene* point_group_create(const RtdlPoint* points, size_t count, const RtdlPointGroupBounds2D* groups,
+                                    size_t group_count, double max_radius, int leaf_size, cudaStream_t s) {
+  size_t total = 0;
+  for (size_t g = 0; g < group_count; ++g) {
+    const RtdlPointGroupBounds2D& G = groups[g];
+    if ((size_t)G.point_offset > count || (size_t)G.point_count > count - (size_t)G.point_offset)
+      throw std::runtime_error("point_group_nearest_witness group span exceeds search point count");
+    if (G.max_x < G.min_x || G.max_y < G.min_y)
+      throw std::runtime_error("point_group_nearest_witness group bounds must be ordered");
+    total += G.point_count;
+  }
+  if (total > (size_t)kMaxScenePoints) throw std::runtime_error("point groups reference more than 67,108,864 points");
+  // the scene holds every group's points (a point in two groups twice), each tagged with its group
+  std::vector<RtdlPoint> expanded(total);
+  std::vector<uint32_t> group_of(total);
+  std::vector<double> boxes(4 * group_count);
+  size_t k = 0;
+  for (size_t g = 0; g < group_count; ++g) {
+    const RtdlPointGroupBounds2D& G = groups[g];
+    for (uint32_t i = 0; i < G.point_count; ++i, ++k) {
+      expanded[k] = points[G.point_offset + i];
+      group_of[k] = (uint32_t)g;
+    }
+    boxes[4 * g] = G.min_x;
+    boxes[4 * g + 1] = G.min_y;
+    boxes[4 * g + 2] = G.max_x;
+    boxes[4 * g + 3] = G.max_y;
+  }
+  PointGroupScene* pg = new PointGroupScene();
+  pg->groups = (uint32_t)group_count;
+  pg->points = (uint32_t)total;
+  pg->max_radius = max_radius;
+  void* d_pts = nullptr;
+  try {
+    d_pts = dev_alloc(sizeof(RtdlPoint) * (total ? total : 1), s);
+    pg->group_of = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (total ? total : 1), s));
+    pg->boxes = static_cast<double*>(dev_alloc(sizeof(double) * (boxes.empty() ? 4 : boxes.size()), s));
+    if (total) {
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(d_pts, expanded.data(), sizeof(RtdlPoint) * total, cudaMemcpyHostToDevice, s));
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(pg->group_of, group_of.data(), sizeof(uint32_t) * total, cudaMemcpyHostToDevice,
+                                      s));
+    }
+    if (!boxes.empty())
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(pg->boxes, boxes.data(), sizeof(double) * boxes.size(), cudaMemcpyHostToDevice, s));
+    pg->sc = build_scene(d_pts, (uint32_t)total, 2, s, leaf_size);
+    unsigned int bad = 0;
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &pg->sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors stay alive until the copies are done
+    if (bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+  } catch (...) {
+    cudaStreamSynchronize(s);
+    dev_free(d_pts, s);
+    point_group_destroy(pg);
+    throw;
+  }
+  dev_free(d_pts, s);
+  return pg;
+}
+
+void point_group_destroy(PointGroupScene* pg) {
+  if (!pg) return;
+  cudaStream_t s = pg->sc ? pg->sc->stream : nullptr;
+  dev_free(pg->group_of, s);
+  dev_free(pg->boxes, s);
+  destroy_scene(pg->sc);
+  if (s) cudaStreamSynchronize(s);
+  delete pg;
+}
+
+void point_group_count(PointGroupScene* pg, const void* queries_dev, uint32_t nq, double radius, uint32_t threshold,
+                       const CountOutputs& out, cudaStream_t s) {
+  count_walk(pg->sc, queries_dev, nq, radius, threshold, out, pg->group_of, pg->boxes, nullptr, s);
+}
+
+void point_group_nearest(PointGroupScene* pg, const void* queries_dev, uint32_t nq, double radius,
+                         RtdlFixedRadiusNeighborRow* rows_dev, RtdlFixedRadiusNeighborRow* max_row_host,
+                         cudaStream_t s) {
+  count_walk(pg->sc, queries_dev, nq, radius, 0, CountOutputs{}, pg->group_of, pg->boxes, rows_dev, s);
+  if (max_row_host) {
+    RtdlFixedRadiusNeighborRow* d_max =
+        static_cast<RtdlFixedRadiusNeighborRow*>(dev_alloc(sizeof(RtdlFixedRadiusNeighborRow), s));
+    k_witness_max<<<1, 1024, 0, s>>>(rows_dev, nq, d_max);
+    RTDL_LAUNCHED(1);
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(max_row_host, d_max, sizeof(RtdlFixedRadiusNeighborRow), cudaMemcpyDeviceToHost, s));
+    dev_free(d_max, s);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+  }
 }
 
 void run_count_trivial(const void* queries_dev, uint32_t nq, int dim, const CountOutputs& out, cudaStream_t s) {

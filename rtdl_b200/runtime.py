@@ -1320,6 +1320,166 @@ class PreparedB200FixedRadiusCountThreshold3D:
             pass
 
 
+POINT_GROUP_DTYPE = np.dtype({"names": ["id", "point_offset", "point_count", "min_x", "min_y", "max_x", "max_y"],
+                              "formats": ["<u4", "<u4", "<u4", "<f8", "<f8", "<f8", "<f8"],
+                              "offsets": [0, 4, 8, 16, 24, 32, 40], "itemsize": 48})
+
+
+def pack_point_groups(groups) -> np.ndarray:
+    """Groups (mappings or objects with id, point_offset, point_count, min_x, min_y, max_x, max_y, or a
+    structured array) as ``RtdlPointGroupBounds2D`` records."""
+    if isinstance(groups, np.ndarray) and groups.dtype.names:
+        out = np.zeros(len(groups), dtype=POINT_GROUP_DTYPE)
+        for f in POINT_GROUP_DTYPE.names:
+            out[f] = groups[f]
+        return out
+    rows = tuple(groups)
+    out = np.zeros(len(rows), dtype=POINT_GROUP_DTYPE)
+    for i, g in enumerate(rows):
+        for f in POINT_GROUP_DTYPE.names:
+            out[f][i] = g[f] if isinstance(g, Mapping) else getattr(g, f)
+    return out
+
+
+class PreparedB200PointGroupNearestWitness2D:
+    """Prepared 2-D point-group scene; mirrors ``PreparedOptixPointGroupNearestWitness2D``
+    (``optix_runtime.py:4284-4540``): threshold coverage and one nearest in-radius witness per query over
+    search points that belong to groups whose box is within radius."""
+
+    def __init__(self, search_points, groups, *, max_radius: float):
+        if max_radius < 0:
+            raise ValueError("max_radius must be non-negative")
+        addr, n, dim, keep = _pack_any(search_points, 2)
+        if dim != 2:
+            raise ValueError("prepare_b200_point_group_nearest_witness_2d requires 2-D points")
+        self._groups = pack_point_groups(groups)
+        self._count = n
+        self._group_count = len(self._groups)
+        self._max_radius = float(max_radius)
+        self._handle = ctypes.c_void_p()
+        self._closed = False
+        if n == 0 or self._group_count == 0:
+            return
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_prepare_point_group_nearest_witness_2d(
+            addr, n, self._groups.ctypes.data, self._group_count, ctypes.c_double(self._max_radius),
+            ctypes.byref(self._handle), err, len(err))
+        del keep
+        _native.check_status(status, err)
+
+    @property
+    def max_radius(self) -> float:
+        return self._max_radius
+
+    @property
+    def closed(self) -> bool:
+        return self._closed
+
+    def _checks(self, radius: float, threshold: int = 0):
+        if self._closed:
+            raise RuntimeError("prepared b200 point-group handle is closed")
+        if radius < 0:
+            raise ValueError("radius must be non-negative")
+        if radius > self._max_radius:
+            raise ValueError("radius must be less than or equal to prepared max_radius")
+        if threshold < 0:
+            raise ValueError("threshold must be non-negative")
+
+    def _queries(self, query_points, what: str):
+        addr, n, dim, keep = _pack_any(query_points, 2)
+        if dim != 2:
+            raise ValueError(f"PreparedB200PointGroupNearestWitness2D.{what} requires 2-D points")
+        return addr, n, keep
+
+    @property
+    def _empty(self) -> bool:
+        return self._count == 0 or self._group_count == 0
+
+    def count_threshold_reached(self, query_points, *, radius: float, threshold: int = 0) -> int:
+        self._checks(radius, threshold)
+        addr, n, keep = self._queries(query_points, "count_threshold_reached")
+        if n == 0 or self._empty:
+            return 0
+        out = ctypes.c_size_t()
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_count_prepared_point_group_threshold_reached_2d(
+            self._handle, addr, n, float(radius), int(threshold), ctypes.byref(out), err, len(err))
+        del keep
+        _native.check_status(status, err)
+        return int(out.value)
+
+    def threshold_flags(self, query_points, *, radius: float, threshold: int = 0) -> np.ndarray:
+        """One uint32 threshold-reached flag per query point."""
+        self._checks(radius, threshold)
+        addr, n, keep = self._queries(query_points, "threshold_flags")
+        if n == 0:
+            return np.asarray([], dtype=np.uint32)
+        if self._empty:
+            return np.full(n, 1 if int(threshold) == 0 else 0, dtype=np.uint32)
+        flags = np.zeros(n, dtype=np.uint32)
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_write_prepared_point_group_threshold_flags_2d(
+            self._handle, addr, n, float(radius), int(threshold), flags.ctypes.data, err, len(err))
+        del keep
+        _native.check_status(status, err)
+        return flags
+
+    def nearest_witness_rows(self, query_points, *, radius: float) -> tuple:
+        self._checks(radius)
+        addr, n, keep = self._queries(query_points, "nearest_witness_rows")
+        if n == 0 or self._empty:
+            return ()
+        rows = ctypes.c_void_p()
+        count = ctypes.c_size_t()
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_run_prepared_point_group_nearest_witness_2d(
+            self._handle, addr, n, float(radius), ctypes.byref(rows), ctypes.byref(count), err, len(err))
+        del keep
+        _native.check_status(status, err)
+        view = _row_view(rows.value or 0, count.value, False)
+        try:
+            return view.to_dict_rows()
+        finally:
+            view.close()
+
+    def nearest_max_distance_row(self, query_points, *, radius: float) -> dict:
+        """The witness row of largest distance, reduced on the device."""
+        self._checks(radius)
+        addr, n, keep = self._queries(query_points, "nearest_max_distance_row")
+        if n == 0 or self._empty:
+            return {"query_id": 0xFFFFFFFF, "neighbor_id": 0xFFFFFFFF, "distance": float("inf")}
+        row = np.zeros(1, dtype=FRN_ROW_DTYPE)
+        err = _native.error_buffer()
+        status = _native.load_library().rtdl_b200_reduce_prepared_point_group_nearest_max_distance_2d(
+            self._handle, addr, n, float(radius), row.ctypes.data, err, len(err))
+        del keep
+        _native.check_status(status, err)
+        return {"query_id": int(row["query_id"][0]), "neighbor_id": int(row["neighbor_id"][0]),
+                "distance": float(row["distance"][0])}
+
+    def close(self) -> None:
+        if not self._closed:
+            if self._handle.value:
+                _native.load_library().rtdl_b200_destroy_prepared_point_group_nearest_witness_2d(self._handle)
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def prepare_b200_point_group_nearest_witness_2d(search_points, groups, *, max_radius: float):
+    return PreparedB200PointGroupNearestWitness2D(search_points, groups, max_radius=max_radius)
+
+
 def prepare_b200_fixed_radius_count_threshold_2d(search_points, *, max_radius: float):
     return PreparedB200FixedRadiusCountThreshold2D(search_points, max_radius=max_radius)
 

@@ -156,6 +156,37 @@ def cpu_baseline_port(probe, build, threads: int, budget_s: float = 10.0) -> dic
             "sample": f"{len(idx)} seeded probes x all {len(build)} build points, {len(rows)} rows in {dt:.2f} s"}
 
 
+def external_scipy_baseline(probe, build, threads: int, n_sample: int = 50_000) -> dict | None:
+    """The reference's external SciPy cKDTree baseline (``external_baselines.py``: ball query, hypot
+    distance, sort by (distance, id), first k_max) on a bounded probe sample, all host threads for the
+    ball queries.  Its hypot distances are not bit-identical to the reference's rows."""
+    try:
+        from scipy.spatial import cKDTree
+    except Exception:
+        return None
+    rng = np.random.default_rng(321)
+    idx = np.sort(rng.choice(len(probe), min(n_sample, len(probe)), replace=False))
+    b = np.stack([build["x"], build["y"], build["z"]], 1)
+    q = np.stack([probe["x"][idx], probe["y"][idx], probe["z"][idx]], 1)
+    bid = build["id"]
+    t0 = time.perf_counter()
+    tree = cKDTree(b)
+    hits = tree.query_ball_point(q, r=RADIUS, workers=threads)
+    rows = 0
+    for i, cand in enumerate(hits):
+        if not cand:
+            continue
+        c = np.asarray(cand)
+        d = np.hypot(np.hypot(b[c, 0] - q[i, 0], b[c, 1] - q[i, 1]), b[c, 2] - q[i, 2])
+        keep = d <= RADIUS
+        order = np.lexsort((bid[c][keep], d[keep]))
+        rows += min(len(order), K_MAX)
+    dt = time.perf_counter() - t0
+    return {"value": rows / dt, "unit": UNIT, "cores": threads, "kind": "external (scipy cKDTree)",
+            "sample": f"{len(idx)} seeded probes x all {len(build)} build points (tree build included), "
+                      f"{rows} rows in {dt:.2f} s"}
+
+
 def cpu_reference_step(probe_idx, packed_build, probe, threads):
     """One bounded sample of the reference's native oracle, sharded over threads."""
     from concurrent.futures import ThreadPoolExecutor
@@ -947,8 +978,10 @@ def main(argv=None) -> int:
                "entry_point": "rtdl_b200_run_fixed_radius_neighbors_3d (pinned host buffers)"}
 
     cpu = None
+    external = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(probe, build, os.cpu_count() or 1)
+        external = external_scipy_baseline(probe, build, os.cpu_count() or 1)
 
     if rank == 0:
         line = {
@@ -979,6 +1012,7 @@ def main(argv=None) -> int:
                                "frac": phase_achieved / hbm_peak, "algorithmic_bytes": phase_bytes},
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "external_baselines": {"scipy_ckdtree": external} if external else None,
             "clocks": clocks,
             "gpu_launches": launches,
         }

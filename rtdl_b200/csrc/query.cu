@@ -825,6 +825,47 @@ __device__ __forceinline__ void collect_refine_packet(const RefineParams& R, uin
   if (valid) R.cnt[j] = L.count;
 }
 
+// The same walk for one scene without problem subtrees (many heavy queries of a
+// plain or prepared scene): no per-lane roots, and close to the collect's occupancy.
+__global__ void __launch_bounds__(256, 6) k_collect_refine_packet_scene(RefineParams R) {
+  const uint32_t n = refine_count(R, true);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;  // warp-uniform
+  if (base >= n) return;  // whole warp
+  const CollectParams& P = R.C;
+  const SceneView& S = P.S;
+  const int scene_inexact = *S.inexact;
+  for (; base < n; base += stride) {
+    const uint32_t j = base + (threadIdx.x & 31);
+    const bool valid = j < n;
+    CollectLane L;
+    DevBands LB = P.bands[0];
+    if (valid) {
+      collect_init(P, R.work[j], L);
+      LB = bands_at_radius(P.bands[0], R.rad[j]);
+    } else {
+      L.q = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+      L.count = 0;
+      L.out = nullptr;
+    }
+    int cur = S.n > 0 ? 0 : kRopeEnd;
+    while (cur != kRopeEnd) {
+      const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+      const int hit = __float_as_int(a.w);
+      const bool over = valid && box_d2(L.q.x, L.q.y, L.q.z, a, b) <= LB.box_hi2;
+      if (__any_sync(0xffffffffu, over)) {
+        if (hit >= 0) {
+          ++cur;
+          continue;
+        }
+        collect_leaf<false>(P, LB, scene_inexact, L, leaf_first(hit), leaf_count(hit), over);
+      }
+      cur = __float_as_int(b.w);
+    }
+    if (valid) R.cnt[j] = L.count;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_collect_refine_packet(RefineParams R) {
   const uint32_t n = refine_count(R, true);
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -852,7 +893,8 @@ struct RefineUpdate {
   const double* rad;
   const double* lo;
   const double* hi;
-  const uint32_t* full;       // in-radius count at the original radius
+  const uint32_t* full;       // in-radius count at radius frad (at least kmax points)
+  const double* frad;         // the original radius, or a smaller tested one that held more than kSlab
   const uint32_t* cnt;
   uint32_t nwork;
   // next pass (or, on the last pass, the generic path's list)
@@ -861,15 +903,21 @@ struct RefineUpdate {
   double* next_lo;
   double* next_hi;
   uint32_t* next_full;
+  double* next_frad;
   unsigned int* next_count;
-  uint32_t* generic_qin;      // last pass: unresolved queries (input index) and their full counts
-  uint32_t* generic_m;
+  uint32_t* generic_qin;      // last pass: unresolved queries (input index), their counts at
+  uint32_t* generic_m;        // generic_rad: the generic path gathers within that radius
+  double* generic_rad;
   int last;
   const unsigned int* nwork_dev;  // non-null: the count is read here (captured graphs)
 };
 
-__device__ __forceinline__ void refine_update_one(const RefineUpdate& U, uint32_t j) {
-  const uint32_t t = U.work[j], qin = U.qorder[t], c = U.cnt[j];
+// One work item: resolves it (emit lists), lists it for the generic path (last
+// pass), or returns true with its next-pass radius, bracket and bound.
+__device__ __forceinline__ bool refine_update_one(const RefineUpdate& U, uint32_t j, uint32_t& t, double& est,
+                                                  double& l, double& h, uint32_t& f, double& fr) {
+  t = U.work[j];
+  const uint32_t qin = U.qorder[t], c = U.cnt[j];
   const uint32_t kmax = U.prob_kmax ? U.prob_kmax[U.qprob ? U.qprob[qin] : 0u] : U.kmax;
   if (c >= kmax && c <= (uint32_t)kSlab) {  // resolved: the slab holds every point within rad
     uint8_t fl = (uint8_t)((U.flags[qin] & ~6u) | (c > 64u ? 4u : 0u));
@@ -879,31 +927,59 @@ __device__ __forceinline__ void refine_update_one(const RefineUpdate& U, uint32_
       U.big_list[atomicAdd(&U.small[3], 1u)] = t;
     else if (c > 64u)
       U.mid_list[atomicAdd(&U.small[2], 1u)] = t;
-    return;
+    return false;
+  }
+  // a tested radius with more than kSlab (>= kmax) points in it also holds the
+  // kmax nearest; the smallest such radius bounds the generic path's gather
+  f = U.full[j];
+  fr = U.frad[j];
+  if (c > (uint32_t)kSlab && c < f) {
+    f = c;
+    fr = U.rad[j];
   }
   if (U.last) {
     const unsigned int k = atomicAdd(U.next_count, 1u);
     U.generic_qin[k] = qin;
-    U.generic_m[k] = U.full[j];
-    return;
+    U.generic_m[k] = f;
+    U.generic_rad[k] = fr;
+    return false;
   }
   const double r = U.rad[j];
-  double l = U.lo[j], h = U.hi[j];
+  l = U.lo[j];
+  h = U.hi[j];
   if (c < kmax) l = r; else h = r;
-  double est = r * cbrt(2.0 * kmax / (double)(c > 0u ? c : 1u));
+  est = r * cbrt(2.0 * kmax / (double)(c > 0u ? c : 1u));
   if (!(est > l && est < h)) est = 0.5 * (l + h);
-  const unsigned int k = atomicAdd(U.next_count, 1u);
-  U.next_work[k] = t;
-  U.next_rad[k] = est;
-  U.next_lo[k] = l;
-  U.next_hi[k] = h;
-  U.next_full[k] = U.full[j];
+  return true;
 }
 
+// The next pass's work keeps each warp's items in their order (one atomic per
+// warp): items come in processing (Morton) order, so a packet of the next pass
+// still walks one region.
 __global__ void k_refine_update(RefineUpdate U) {
   const uint32_t n = U.nwork_dev ? *U.nwork_dev : U.nwork;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-    refine_update_one(U, j);
+  const int lane = threadIdx.x & 31;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += stride) {  // warp-uniform
+    const uint32_t j = base + lane;
+    uint32_t t = 0, f = 0;
+    double est = 0.0, l = 0.0, h = 0.0, fr = 0.0;
+    const bool next = j < n && refine_update_one(U, j, t, est, l, h, f, fr);
+    const unsigned int m = __ballot_sync(0xffffffffu, next);
+    if (!m) continue;
+    unsigned int first = 0;
+    if (lane == 0) first = atomicAdd(U.next_count, (unsigned int)__popc(m));
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (next) {
+      const unsigned int k = first + __popc(m & ((1u << lane) - 1u));
+      U.next_work[k] = t;
+      U.next_rad[k] = est;
+      U.next_lo[k] = l;
+      U.next_hi[k] = h;
+      U.next_full[k] = f;
+      U.next_frad[k] = fr;
+    }
+  }
 }
 
 // The first refinement pass's work: the collect pass's heavy queries (listed
@@ -911,20 +987,22 @@ __global__ void k_refine_update(RefineUpdate U) {
 __global__ void k_refine_init(const uint32_t* heavy_qin, const uint32_t* heavy_m, const uint32_t* heavy_t,
                               uint32_t H, const uint32_t* qprob, const double* prob_radius, double radius,
                               const uint32_t* prob_kmax, uint32_t kmax, uint32_t* work, double* rad, double* lo,
-                              double* hi, uint32_t* full, const unsigned int* H_dev) {
+                              double* hi, uint32_t* full, double* frad, const unsigned int* H_dev) {
   if (H_dev) H = *H_dev;  // captured graphs: the collect pass's heavy count
   for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < H; h += gridDim.x * blockDim.x) {
     const uint32_t qin = heavy_qin[h], p = qprob ? qprob[qin] : 0u;
-    const double r = prob_radius ? prob_radius[p] : radius;
-    const uint32_t k = prob_kmax ? prob_kmax[p] : kmax;
     const uint32_t m = heavy_m[h];
     work[h] = heavy_t[h];
+    const double r = prob_radius ? prob_radius[p] : radius;
+    const uint32_t k = prob_kmax ? prob_kmax[p] : kmax;
     rad[h] = r * cbrt(2.0 * k / (double)m);
-    lo[h] = 0.0;
     hi[h] = r;
+    frad[h] = r;
+    lo[h] = 0.0;
     full[h] = m;
   }
 }
+
 
 // ---- emit: warp per query -----------------------------------------------------
 // Emitted row writer.
@@ -1699,12 +1777,13 @@ __global__ void __launch_bounds__(kHeavyThreads)
 __global__ void __launch_bounds__(32)
     k_heavy_gather_bvh(SceneView S, const float4* qpts, const double* qraw, int qstride, const uint32_t* heavy_list,
                        const unsigned long long* seg_off, const uint32_t* seg_size, const DevBands* bands,
-                       const uint32_t* qprob, HeavyEntry* scratch, unsigned int* error) {
+                       const uint32_t* qprob, const double* item_rad, HeavyEntry* scratch, unsigned int* error) {
   const int lane = threadIdx.x;
   const uint32_t h = blockIdx.x;
   const uint32_t qin = heavy_list[h];
   const uint32_t prob = qprob ? qprob[qin] : 0u;
-  const DevBands B = bands[prob];
+  // item_rad: the radius this query gathers within (a tested radius that holds its rows)
+  const DevBands B = item_rad ? bands_at_radius(bands[prob], item_rad[h]) : bands[prob];
   const Ctx c = make_ctx(S, qpts, qraw, qstride, qin, B);
   HeavyEntry* seg = scratch + seg_off[h];
   const uint32_t P2 = seg_size[h];
@@ -2200,7 +2279,7 @@ struct GenericOut {
 // force); otherwise gather in-radius candidates through the BVH.
 GenericOut run_generic_path(Scene* sc, const QueryPrep& qp, const void* queries_dev, int qstride, uint32_t H,
                             const uint32_t* heavy_list, const uint32_t* heavy_m, uint32_t limit, bool knn,
-                            unsigned int* error, cudaStream_t s) {
+                            unsigned int* error, cudaStream_t s, const double* item_rad = nullptr) {
   GenericOut g;
   std::vector<uint32_t> hm(H);
   RTDL_CUDA_CHECK(cudaMemcpyAsync(hm.data(), heavy_m, sizeof(uint32_t) * H, cudaMemcpyDeviceToHost, s));
@@ -2237,7 +2316,8 @@ GenericOut run_generic_path(Scene* sc, const QueryPrep& qp, const void* queries_
                                                heavy_list, d_seg_off, d_seg_size, 1, qp.bands, scratch, error);
   else
     k_heavy_gather_bvh<<<H, 32, 0, s>>>(qp.view, qp.qpts, static_cast<const double*>(queries_dev), qstride,
-                                        heavy_list, d_seg_off, d_seg_size, qp.bands, qp.qprob, scratch, error);
+                                        heavy_list, d_seg_off, d_seg_size, qp.bands, qp.qprob, item_rad, scratch,
+                                        error);
   k_heavy_sort<<<H, kHeavyThreads, sizeof(HeavyEntry) * kHeavySmemEntries, s>>>(d_seg_off, d_seg_size, scratch,
                                                                                 sc->perm);
   k_heavy_emit<<<H, kHeavyThreads, 0, s>>>(d_seg_off, g.heavy_out_off, d_out_cnt, scratch, g.heavy_out);
@@ -2260,6 +2340,7 @@ struct RefineOut {
   uint32_t generic = 0, mid = 0, big = 0;
   const uint32_t* generic_qin = nullptr;
   const uint32_t* generic_m = nullptr;
+  const double* generic_rad = nullptr;  // the radius each generic query gathers within
   std::vector<void*> buffers;  // released by the caller once the rows are out
 };
 
@@ -2274,7 +2355,7 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     return p;
   };
   uint32_t* work[2];
-  double *rad[2], *lo[2], *hi[2];
+  double *rad[2], *lo[2], *hi[2], *frad[2];
   uint32_t* full[2];
   for (int b = 0; b < 2; ++b) {
     work[b] = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
@@ -2282,20 +2363,23 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     lo[b] = static_cast<double*>(alloc(sizeof(double) * H));
     hi[b] = static_cast<double*>(alloc(sizeof(double) * H));
     full[b] = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
+    frad[b] = static_cast<double*>(alloc(sizeof(double) * H));
   }
+  double* gen_rad = static_cast<double*>(alloc(sizeof(double) * H));
   uint32_t* cnt = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
   uint32_t* gen_qin = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
   uint32_t* gen_m = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * H));
   unsigned int* next_count = static_cast<unsigned int*>(alloc(sizeof(unsigned int)));
   k_refine_init<<<div_up(H, 256), 256, 0, s>>>(heavy_list, heavy_m, heavy_t, H, qp.qprob, qp.prob_radius, radius,
                                                qp.prob_kmax, kmax, work[0], rad[0], lo[0], hi[0], full[0],
-                                               nullptr);
+                                               frad[0], nullptr);
   RTDL_LAUNCHED(1);
   Readback* rb = pinned_readback();
   uint32_t n = H;
   int cur = 0;
   for (int pass = 0; pass < kRefinePasses && n > 0; ++pass) {
     const bool last = pass == kRefinePasses - 1;
+
     RefineParams R;
     R.C = C;
     R.qprob = qp.qprob;
@@ -2305,9 +2389,13 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     R.cnt = cnt;
     R.nwork_dev = nullptr;
     R.packet_min = 0;
-    if (n >= qp.nproc / 8)  // many heavy queries: they cluster, a packet of them walks one region
-      k_collect_refine_packet<<<div_up(n, 256), 256, 0, s>>>(R);
-    else
+    const bool scene_packet = n >= qp.nproc / 8 && !qp.qprob && !qp.view.prob_root;
+    if (n >= qp.nproc / 8) {  // many heavy queries: they cluster, a packet of them walks one region
+      if (scene_packet)
+        k_collect_refine_packet_scene<<<div_up(n, 256), 256, 0, s>>>(R);
+      else
+        k_collect_refine_packet<<<div_up(n, 256), 256, 0, s>>>(R);
+    } else
       k_collect_refine<<<div_up((uint64_t)n * 32, 256), 256, 0, s>>>(R);
     RTDL_CUDA_CHECK(cudaMemsetAsync(next_count, 0, sizeof(unsigned int), s));
     RefineUpdate U;
@@ -2325,6 +2413,7 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     U.lo = lo[cur];
     U.hi = hi[cur];
     U.full = full[cur];
+    U.frad = frad[cur];
     U.cnt = cnt;
     U.nwork = n;
     U.nwork_dev = nullptr;
@@ -2333,12 +2422,15 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     U.next_lo = lo[cur ^ 1];
     U.next_hi = hi[cur ^ 1];
     U.next_full = full[cur ^ 1];
+    U.next_frad = frad[cur ^ 1];
     U.next_count = next_count;
     U.generic_qin = gen_qin;
     U.generic_m = gen_m;
+    U.generic_rad = gen_rad;
     U.last = last ? 1 : 0;
     k_refine_update<<<div_up(n, 256), 256, 0, s>>>(U);
     RTDL_LAUNCHED(2);
+
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->refine_left, next_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
     n = rb->refine_left;
@@ -2347,6 +2439,7 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
   }
   out.generic_qin = gen_qin;
   out.generic_m = gen_m;
+  out.generic_rad = gen_rad;
   RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->mid, small + 2, sizeof(unsigned int) * 2, cudaMemcpyDeviceToHost, s));
   RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
   out.mid = rb->mid;
@@ -2391,7 +2484,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
                              const SummarySpec* ss = nullptr, const PreparedQueries* pq = nullptr,
                              bool witness = false) {
   // witness (k_max 1): one row per query at its input position, pre-filled
-  // with the no-witness row; the nearest in-radius neighbour overwrites it
+  // with the no-witness row; the nearest in-radius neighbour overwrites it.
   QueryResult res;
   void* summary_rows = nullptr;  // ranked summaries: the rows stay internal
   if (ss) rows_alloc = &summary_rows;
@@ -2513,6 +2606,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     uint32_t mid = r.mid, big = r.big, generic = r.heavy;
     const uint32_t* generic_list = heavy_list;
     const uint32_t* generic_m = heavy_m;
+    const double* generic_rad = nullptr;
     if (r.heavy > 0) {
       // queries with more than kSlab points in radius: collect again at smaller radii
       RefineOut ro = refine_heavy(C, qp, radius, kmax, r.heavy, heavy_list, heavy_m, heavy_t, qinfo, flags, mid_list,
@@ -2521,6 +2615,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       generic = ro.generic;
       generic_list = ro.generic_qin;
       generic_m = ro.generic_m;
+      generic_rad = ro.generic_rad;
       mid = ro.mid;
       big = ro.big;
       if (timer) timer->mark("refine");
@@ -2532,7 +2627,9 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       last_stats()[kStatRefined] = r.heavy - generic;
     }
     if (generic > 0) {
-      g = run_generic_path(sc, qp, queries_dev, qstride, generic, generic_list, generic_m, kmax, false, small + 1, s);
+      // the gather is bounded by each query's smallest tested radius that holds its rows
+      g = run_generic_path(sc, qp, queries_dev, qstride, generic, generic_list, generic_m, kmax, false, small + 1, s,
+                           generic_rad);
       if (timer) timer->mark("generic_path");
     }
     if (rows_alloc != nullptr) {
@@ -2962,6 +3059,8 @@ struct SummaryGraph {
   uint32_t* work[2] = {nullptr, nullptr};
   double *rad[2] = {nullptr, nullptr}, *lo[2] = {nullptr, nullptr}, *hi[2] = {nullptr, nullptr};
   uint32_t* full[2] = {nullptr, nullptr};
+  double* frad[2] = {nullptr, nullptr};
+  double* gen_rad = nullptr;
   uint32_t *cnt = nullptr, *gen_qin = nullptr, *gen_m = nullptr;
   SummaryPartial* partial = nullptr;
   uint32_t summary_blocks = 0;
@@ -3029,7 +3128,7 @@ void graph_enqueue_request(SummaryGraph* g, uint32_t r, cudaStream_t s) {
   // heavy queries: every refinement pass is launched; each reads its work count
   k_refine_init<<<kSmCount * 4, 256, 0, s>>>(g->heavy_list, g->heavy_m, g->heavy_t, 0, nullptr, nullptr, radius,
                                              nullptr, kmax, g->work[0], g->rad[0], g->lo[0], g->hi[0], g->full[0],
-                                             small);
+                                             g->frad[0], small);
   RTDL_LAUNCHED(1);
   int cur = 0;
   for (int pass = 0; pass < kRefinePasses; ++pass) {
@@ -3060,6 +3159,7 @@ void graph_enqueue_request(SummaryGraph* g, uint32_t r, cudaStream_t s) {
     U.lo = g->lo[cur];
     U.hi = g->hi[cur];
     U.full = g->full[cur];
+    U.frad = g->frad[cur];
     U.cnt = g->cnt;
     U.nwork = 0;
     U.next_work = g->work[cur ^ 1];
@@ -3067,6 +3167,8 @@ void graph_enqueue_request(SummaryGraph* g, uint32_t r, cudaStream_t s) {
     U.next_lo = g->lo[cur ^ 1];
     U.next_hi = g->hi[cur ^ 1];
     U.next_full = g->full[cur ^ 1];
+    U.next_frad = g->frad[cur ^ 1];
+    U.generic_rad = g->gen_rad;
     U.next_count = pc + pass;
     U.generic_qin = g->gen_qin;
     U.generic_m = g->gen_m;
@@ -3215,10 +3317,12 @@ SummaryGraph* summary_graph_create(Scene* sc, const PreparedQueries* pq, const d
       g->lo[b] = static_cast<double*>(alloc(sizeof(double) * n));
       g->hi[b] = static_cast<double*>(alloc(sizeof(double) * n));
       g->full[b] = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+      g->frad[b] = static_cast<double*>(alloc(sizeof(double) * n));
     }
     g->cnt = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
     g->gen_qin = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
     g->gen_m = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->gen_rad = static_cast<double*>(alloc(sizeof(double) * n));
     g->summary_blocks = div_up((uint64_t)n * 32, kSummaryThreads);
     g->partial = static_cast<SummaryPartial*>(alloc(sizeof(SummaryPartial) * g->summary_blocks));
     g->agg = static_cast<RtdlFixedRadiusRankedNeighborAggregate*>(

@@ -397,6 +397,7 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
 // exact in-radius count is kept, so the overflow flag and the row offsets are
 // exact without any per-query list.
 constexpr int kSlab = 256;  // candidates kept per query
+constexpr unsigned int kStrideBlocks = kSmCount * 8;  // grid of the kernels that stride over device counts
 
 // Candidate slab: query-major, kSlab entries for the query at processing rank
 // t starting at t * kSlab.  An entry is (FP32 sort key bits << 32) | sorted
@@ -2472,6 +2473,84 @@ void launch_collect(const CollectParams& C, uint32_t np, uint32_t nq, bool batch
   RTDL_LAUNCHED(1);
 }
 
+// Buffers of the device-driven refinement (worst case: every processing rank).
+struct RefineDevice {
+  uint32_t* work[2];
+  double *rad[2], *lo[2], *hi[2], *frad[2];
+  uint32_t* full[2];
+  uint32_t *cnt, *gen_qin, *gen_m;
+  double* gen_rad;
+  unsigned int* pass_count;  // kRefinePasses: work left after each pass (after the last: the generic count)
+};
+
+// The radius refinement without host reads (captured graphs): every pass is
+// launched, each kernel reads its work count on the device and strides over it,
+// and both walk
+// forms are launched (the one the host-driven loop would not pick exits).
+// small[0] holds the collect pass's heavy count; D.pass_count[kRefinePasses-1]
+// ends with the number of queries left for the generic path.
+void enqueue_refine_device(const CollectParams& C, const uint32_t* qprob, const double* prob_radius, double radius,
+                           const uint32_t* prob_kmax, uint32_t kmax, uint32_t nproc, bool one_scene,
+                           QueryInfo* qinfo, uint8_t* flags, unsigned int* small, const RefineDevice& D,
+                           cudaStream_t s) {
+  RTDL_CUDA_CHECK(cudaMemsetAsync(D.pass_count, 0, sizeof(unsigned int) * kRefinePasses, s));
+  k_refine_init<<<kSmCount * 4, 256, 0, s>>>(C.heavy_list, C.heavy_m, C.heavy_t, 0, qprob, prob_radius, radius,
+                                             prob_kmax, kmax, D.work[0], D.rad[0], D.lo[0], D.hi[0], D.full[0],
+                                             D.frad[0], small);
+  RTDL_LAUNCHED(1);
+  int cur = 0;
+  for (int pass = 0; pass < kRefinePasses; ++pass) {
+    const unsigned int* n_dev = pass == 0 ? small : D.pass_count + pass - 1;
+    RefineParams R;
+    R.C = C;
+    R.qprob = qprob;
+    R.work = D.work[cur];
+    R.rad = D.rad[cur];
+    R.nwork = 0;
+    R.cnt = D.cnt;
+    R.nwork_dev = n_dev;
+    R.packet_min = nproc / 8;  // the host-driven loop's choice between the two forms
+    if (one_scene)
+      k_collect_refine_packet_scene<<<kStrideBlocks, 256, 0, s>>>(R);
+    else
+      k_collect_refine_packet<<<kStrideBlocks, 256, 0, s>>>(R);
+    k_collect_refine<<<kStrideBlocks, 256, 0, s>>>(R);
+    RefineUpdate U;
+    U.qorder = C.qorder;
+    U.qprob = qprob;
+    U.prob_kmax = prob_kmax;
+    U.kmax = kmax;
+    U.qinfo = qinfo;
+    U.flags = flags;
+    U.mid_list = C.mid_list;
+    U.big_list = C.big_list;
+    U.small = small;
+    U.work = D.work[cur];
+    U.rad = D.rad[cur];
+    U.lo = D.lo[cur];
+    U.hi = D.hi[cur];
+    U.full = D.full[cur];
+    U.frad = D.frad[cur];
+    U.cnt = D.cnt;
+    U.nwork = 0;
+    U.next_work = D.work[cur ^ 1];
+    U.next_rad = D.rad[cur ^ 1];
+    U.next_lo = D.lo[cur ^ 1];
+    U.next_hi = D.hi[cur ^ 1];
+    U.next_full = D.full[cur ^ 1];
+    U.next_frad = D.frad[cur ^ 1];
+    U.next_count = D.pass_count + pass;
+    U.generic_qin = D.gen_qin;
+    U.generic_m = D.gen_m;
+    U.generic_rad = D.gen_rad;
+    U.last = pass == kRefinePasses - 1 ? 1 : 0;
+    U.nwork_dev = n_dev;
+    k_refine_update<<<kSmCount * 4, 256, 0, s>>>(U);
+    RTDL_LAUNCHED(3);
+    cur ^= 1;
+  }
+}
+
 void check_readback(const Readback& r) {
   if (r.scene_bad || r.query_bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
   if (r.error & 1u) throw std::runtime_error("BVH traversal stack overflow");
@@ -2594,83 +2673,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
                                       cudaMemcpyDeviceToHost, s));
     }
     if (timer) timer->mark("scan");
-    Readback* rb = pinned_readback();
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-    const Readback r = *rb;
-    check_readback(r);
-    res.rows = r.rows;
-    uint32_t mid = r.mid, big = r.big, generic = r.heavy;
-    const uint32_t* generic_list = heavy_list;
-    const uint32_t* generic_m = heavy_m;
-    const double* generic_rad = nullptr;
-    if (r.heavy > 0) {
-      // queries with more than kSlab points in radius: collect again at smaller radii
-      RefineOut ro = refine_heavy(C, qp, radius, kmax, r.heavy, heavy_list, heavy_m, heavy_t, qinfo, flags, mid_list,
-                                  big_list, small, s);
-      refine_bufs = ro.buffers;
-      generic = ro.generic;
-      generic_list = ro.generic_qin;
-      generic_m = ro.generic_m;
-      generic_rad = ro.generic_rad;
-      mid = ro.mid;
-      big = ro.big;
-      if (timer) timer->mark("refine");
-    }
-    res.heavy = generic;
-    if (stats) {
-      last_stats()[kStatGenericQueries] = generic;
-      last_stats()[kStatLargeQueries] = mid + big;
-      last_stats()[kStatRefined] = r.heavy - generic;
-    }
-    if (generic > 0) {
-      // the gather is bounded by each query's smallest tested radius that holds its rows
-      g = run_generic_path(sc, qp, queries_dev, qstride, generic, generic_list, generic_m, kmax, false, small + 1, s,
-                           generic_rad);
-      if (timer) timer->mark("generic_path");
-    }
-    if (rows_alloc != nullptr) {
-      const size_t row_size = predicate == kFrn ? 16 : 24;
-      rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
-      rows_capacity = res.rows;
-      *rows_alloc = rows_dev;
-    }
-    if (witness && rows_dev) {
-      k_witness_fill<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, static_cast<RtdlFixedRadiusNeighborRow*>(rows_dev),
-                                                       rows_capacity);
-      RTDL_LAUNCHED(1);
-    }
-    k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, np, poff);
-    RTDL_LAUNCHED(1);
-    EmitParams E;
-    E.S = sc->view();
-    E.nq = np;
-    E.slab = slab;
-    E.qinfo = qinfo;
-    E.poff = poff;
-    E.sink.rows = rows_dev;
-    E.sink.capacity = rows_dev ? rows_capacity : 0;
-    E.sink.ranked = predicate == kFrn ? 0 : 1;
-    E.fix_list = fix_list;
-    E.fix_count = small + 4;
-    k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
-    RTDL_LAUNCHED(1);
-    if (mid > 0) {
-      k_emit_list<4, true><<<div_up((uint64_t)mid * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, mid_list,
-                                                                                                  mid, nullptr);
-      RTDL_LAUNCHED(1);
-    }
-    if (big > 0) {
-      k_emit_list<8, false><<<div_up((uint64_t)big * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, big_list,
-                                                                                                   big, nullptr);
-      RTDL_LAUNCHED(1);
-    }
-    k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
-    RTDL_LAUNCHED(1);
-    if (generic > 0) {
+    auto launch_expand = [&](uint32_t n_generic, const uint32_t* list) {
       ExpandParams X;
       X.S = sc->view();
       X.qpts = qp.qpts;
@@ -2678,7 +2681,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       X.qstride = qstride;
       X.oorder = qp.oorder;
       X.bands = qp.bands;
-      X.nq = generic;
+      X.nq = n_generic;
       X.L = kSlab;
       X.counts = counts;
       X.flags = flags;
@@ -2691,17 +2694,108 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       X.ranked = predicate == kFrn ? 0 : 1;
       X.overflow_out = nullptr;
       X.error = small + 1;
-      X.work_list = generic_list;
+      X.work_list = list;
       X.qrank = qrank;
-      k_expand<<<grid_for((uint64_t)generic * 32, kExpandThreads), kExpandThreads, 0, s>>>(X);
+      k_expand<<<grid_for((uint64_t)n_generic * 32, kExpandThreads), kExpandThreads, 0, s>>>(X);
       RTDL_LAUNCHED(1);
+    };
+    // Rows only counted: the total is known after the scan (no refinement, no emit).
+    const bool count_only = rows_alloc == nullptr && rows_dev == nullptr && !bs && !ss && !witness;
+    Readback* rb = pinned_readback();
+    if (count_only) {
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      check_readback(*rb);
+      res.rows = rb->rows;
+    } else {
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      const Readback r = *rb;
+      check_readback(r);
+      res.rows = r.rows;
+      uint32_t mid = r.mid, big = r.big, generic = r.heavy;
+      const uint32_t* generic_list = heavy_list;
+      const uint32_t* generic_m = heavy_m;
+      const double* generic_rad = nullptr;
+      if (r.heavy > 0) {
+        // queries with more than kSlab points in radius: collect again at smaller radii
+        RefineOut ro = refine_heavy(C, qp, radius, kmax, r.heavy, heavy_list, heavy_m, heavy_t, qinfo, flags, mid_list,
+                                    big_list, small, s);
+        refine_bufs = ro.buffers;
+        generic = ro.generic;
+        generic_list = ro.generic_qin;
+        generic_m = ro.generic_m;
+        generic_rad = ro.generic_rad;
+        mid = ro.mid;
+        big = ro.big;
+        if (timer) timer->mark("refine");
+      }
+      res.heavy = generic;
+      if (stats) {
+        last_stats()[kStatGenericQueries] = generic;
+        last_stats()[kStatLargeQueries] = mid + big;
+        last_stats()[kStatRefined] = r.heavy - generic;
+      }
+      if (generic > 0) {
+        // the gather is bounded by each query's smallest tested radius that holds its rows
+        g = run_generic_path(sc, qp, queries_dev, qstride, generic, generic_list, generic_m, kmax, false, small + 1, s,
+                             generic_rad);
+        if (timer) timer->mark("generic_path");
+      }
+      if (rows_alloc != nullptr) {
+        const size_t row_size = predicate == kFrn ? 16 : 24;
+        rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
+        rows_capacity = res.rows;
+        *rows_alloc = rows_dev;
+      }
+      if (witness && rows_dev) {
+        k_witness_fill<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, static_cast<RtdlFixedRadiusNeighborRow*>(rows_dev),
+                                                         rows_capacity);
+        RTDL_LAUNCHED(1);
+      }
+      k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, np, poff);
+      RTDL_LAUNCHED(1);
+      EmitParams E;
+      E.S = sc->view();
+      E.nq = np;
+      E.slab = slab;
+      E.qinfo = qinfo;
+      E.poff = poff;
+      E.sink.rows = rows_dev;
+      E.sink.capacity = rows_dev ? rows_capacity : 0;
+      E.sink.ranked = predicate == kFrn ? 0 : 1;
+      E.fix_list = fix_list;
+      E.fix_count = small + 4;
+      k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
+      RTDL_LAUNCHED(1);
+      if (mid > 0) {
+        k_emit_list<4, true><<<div_up((uint64_t)mid * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, mid_list,
+                                                                                                    mid, nullptr);
+        RTDL_LAUNCHED(1);
+      }
+      if (big > 0) {
+        k_emit_list<8, false><<<div_up((uint64_t)big * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, big_list,
+                                                                                                     big, nullptr);
+        RTDL_LAUNCHED(1);
+      }
+      k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
+      RTDL_LAUNCHED(1);
+      if (generic > 0) {
+        launch_expand(generic, generic_list);
+      }
+      if (timer) timer->mark("emit");
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
+      if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
     }
-    if (timer) timer->mark("emit");
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-    if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
-    if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
     if (ss) {
       const uint32_t blocks = div_up((uint64_t)nq * 32, kSummaryThreads);
       SummaryPartial* partial = static_cast<SummaryPartial*>(dev_alloc(sizeof(SummaryPartial) * blocks, s));
@@ -3032,7 +3126,6 @@ __global__ void k_graph_status(const unsigned int* small, const unsigned int* pa
                 (pass_count[(size_t)r * kRefinePasses + kRefinePasses - 1] ? kGraphStatusGeneric : 0u);
 }
 
-constexpr unsigned int kGraphStrideBlocks = kSmCount * 8;  // grid of the kernels that stride over device counts
 
 }  // namespace
 
@@ -3126,58 +3219,21 @@ void graph_enqueue_request(SummaryGraph* g, uint32_t r, cudaStream_t s) {
   launch_collect(C, np, nq, false, false, s);
   scan_counts_u64_ws(g->counts, pq->oorder, pq->identity, nq, g->offsets, g->scan_ws, s);
   // heavy queries: every refinement pass is launched; each reads its work count
-  k_refine_init<<<kSmCount * 4, 256, 0, s>>>(g->heavy_list, g->heavy_m, g->heavy_t, 0, nullptr, nullptr, radius,
-                                             nullptr, kmax, g->work[0], g->rad[0], g->lo[0], g->hi[0], g->full[0],
-                                             g->frad[0], small);
-  RTDL_LAUNCHED(1);
-  int cur = 0;
-  for (int pass = 0; pass < kRefinePasses; ++pass) {
-    const unsigned int* n_dev = pass == 0 ? small : pc + pass - 1;
-    RefineParams R;
-    R.C = C;
-    R.qprob = nullptr;
-    R.work = g->work[cur];
-    R.rad = g->rad[cur];
-    R.nwork = 0;
-    R.cnt = g->cnt;
-    R.nwork_dev = n_dev;
-    R.packet_min = np / 8;  // the plain call's choice between the two forms
-    k_collect_refine_packet<<<kGraphStrideBlocks, 256, 0, s>>>(R);
-    k_collect_refine<<<kGraphStrideBlocks, 256, 0, s>>>(R);
-    RefineUpdate U;
-    U.qorder = pq->qorder;
-    U.qprob = nullptr;
-    U.prob_kmax = nullptr;
-    U.kmax = kmax;
-    U.qinfo = g->qinfo;
-    U.flags = g->flags;
-    U.mid_list = g->mid_list;
-    U.big_list = g->big_list;
-    U.small = small;
-    U.work = g->work[cur];
-    U.rad = g->rad[cur];
-    U.lo = g->lo[cur];
-    U.hi = g->hi[cur];
-    U.full = g->full[cur];
-    U.frad = g->frad[cur];
-    U.cnt = g->cnt;
-    U.nwork = 0;
-    U.next_work = g->work[cur ^ 1];
-    U.next_rad = g->rad[cur ^ 1];
-    U.next_lo = g->lo[cur ^ 1];
-    U.next_hi = g->hi[cur ^ 1];
-    U.next_full = g->full[cur ^ 1];
-    U.next_frad = g->frad[cur ^ 1];
-    U.generic_rad = g->gen_rad;
-    U.next_count = pc + pass;
-    U.generic_qin = g->gen_qin;
-    U.generic_m = g->gen_m;
-    U.last = pass == kRefinePasses - 1 ? 1 : 0;
-    U.nwork_dev = n_dev;
-    k_refine_update<<<kSmCount * 4, 256, 0, s>>>(U);
-    RTDL_LAUNCHED(3);
-    cur ^= 1;
+  RefineDevice D;
+  for (int b2 = 0; b2 < 2; ++b2) {
+    D.work[b2] = g->work[b2];
+    D.rad[b2] = g->rad[b2];
+    D.lo[b2] = g->lo[b2];
+    D.hi[b2] = g->hi[b2];
+    D.frad[b2] = g->frad[b2];
+    D.full[b2] = g->full[b2];
   }
+  D.cnt = g->cnt;
+  D.gen_qin = g->gen_qin;
+  D.gen_m = g->gen_m;
+  D.gen_rad = g->gen_rad;
+  D.pass_count = pc;
+  enqueue_refine_device(C, nullptr, nullptr, radius, nullptr, kmax, np, true, g->qinfo, g->flags, small, D, s);
   k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(pq->qorder, pq->qrank, g->offsets, np, g->poff);
   RTDL_LAUNCHED(1);
   EmitParams E;
@@ -3192,8 +3248,8 @@ void graph_enqueue_request(SummaryGraph* g, uint32_t r, cudaStream_t s) {
   E.fix_list = g->fix_list;
   E.fix_count = small + 4;
   k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
-  k_emit_list<4, true><<<kGraphStrideBlocks, kEmitListThreads, 0, s>>>(E, g->mid_list, 0, small + 2);
-  k_emit_list<8, false><<<kGraphStrideBlocks, kEmitListThreads, 0, s>>>(E, g->big_list, 0, small + 3);
+  k_emit_list<4, true><<<kStrideBlocks, kEmitListThreads, 0, s>>>(E, g->mid_list, 0, small + 2);
+  k_emit_list<8, false><<<kStrideBlocks, kEmitListThreads, 0, s>>>(E, g->big_list, 0, small + 3);
   k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
   k_summarize<<<g->summary_blocks, kSummaryThreads, 0, s>>>(static_cast<const RtdlFixedRadiusNeighborRow*>(g->rows),
                                                             g->offsets, pq->oorder, pq->identity, pq->qpts, nq,

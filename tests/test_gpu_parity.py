@@ -322,3 +322,37 @@ def test_device_per_call_entry_matches_oracle(gpu, dim, k_max):
                                                     radius=radius, k_max=k_max, rows_address=rows.data_ptr(),
                                                     rows_capacity=n, overflow_address=flags.data_ptr()) == 0
     assert int(flags.max()) == 0
+
+
+def test_device_rows_path_heavy_and_generic_queries(gpu):
+    """Rows into a caller's device buffer take the refinement on device counts: queries with more than
+    256 candidates (a dense cluster) and queries no radius separates (400 coincident points) must still
+    get the oracle's rows, through the per-call device entry and a resident scene."""
+    import torch
+
+    from rtdl_b200.runtime import FRN_ROW_DTYPE
+
+    rng = np.random.default_rng(8)
+    dense = rng.normal(0.5, 0.01, (30000, 3))
+    same = np.full((400, 3), 0.25)
+    s_pts = np.concatenate([dense, same, rng.random((20000, 3))]).astype(np.float32).astype(np.float64)
+    q_pts = np.concatenate([rng.normal(0.5, 0.01, (3000, 3)), np.full((7, 3), 0.25),
+                            rng.random((2000, 3))]).astype(np.float32).astype(np.float64)
+    s, q = _cols(s_pts), _cols(q_pts)
+    d_s = torch.from_numpy(_pack(s).records.view(np.uint8).copy()).cuda()
+    d_q = torch.from_numpy(_pack(q).records.view(np.uint8).copy()).cuda()
+    for radius, k_max in ((0.01, 40), (0.004, 64), (0.02, 5)):
+        exp = O.fixed_radius_neighbors(q, s, radius=radius, k_max=k_max, threads=8)
+        n = len(exp)
+        rows = torch.empty(max(n, 1) * 16, dtype=torch.uint8, device="cuda")
+        assert rt.runtime.fixed_radius_neighbors_device(d_q.data_ptr(), len(q_pts), d_s.data_ptr(), len(s_pts),
+                                                        dimension=3, radius=radius, k_max=k_max,
+                                                        rows_address=rows.data_ptr(), rows_capacity=n) == n
+        got = np.frombuffer(rows.cpu().numpy().tobytes(), dtype=FRN_ROW_DTYPE)[:n]
+        _assert_same_rows(got, exp, False)
+        with rt.B200Scene(_pack(s)) as scene:
+            rows.zero_()
+            assert scene.query_device(d_q.data_ptr(), len(q_pts), predicate="fixed_radius_neighbors", radius=radius,
+                                      limit=k_max, rows_address=rows.data_ptr(), rows_capacity=n) == n
+            got = np.frombuffer(rows.cpu().numpy().tobytes(), dtype=FRN_ROW_DTYPE)[:n]
+            _assert_same_rows(got, exp, False)

@@ -544,7 +544,8 @@ RTDL_B200_API void rtdl_b200_destroy_fixed_radius_ranked_summary_aggregate_batch
 
 /* Result record of rtdl_b200_scene_directed_hausdorff_noalloc (device memory).
  * status: 0 = ok, 1 = a coordinate is non-finite or beyond 1e18, 2 = the
- * traversal stack overflowed. */
+ * traversal stack overflowed, 3 = a radix-sort wait of the scene build ran out
+ * (the scene is not valid). */
 typedef struct RtdlB200Witness {
   double distance;
   uint32_t source_id, target_id;

@@ -504,7 +504,7 @@ int scene_create_impl(const void* points, size_t count, int dimension, int point
       unsigned int bad = 0;
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
       RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-      if (bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+      throw_if_bad(bad);
     } catch (...) {
       destroy_scene(sc);
       dev_free(owned, s);
@@ -627,7 +627,7 @@ int rtdl_b200_batch_create(const void* points, const unsigned long long* point_o
       unsigned int bad = 0;
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
       RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-      if (bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+      throw_if_bad(bad);
     } catch (...) {
       destroy_scene(sc);
       dev_free(owned, s);
@@ -965,7 +965,7 @@ int rtdl_b200_queries_create(const void* points, size_t count, int dimension, in
       unsigned int bad = 0;
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &pq->qst->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
       RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-      if (bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+      throw_if_bad(bad);
     } catch (...) {
       if (pq) destroy_query_set(pq); else dev_free(owned, s);
       cudaStreamSynchronize(s);

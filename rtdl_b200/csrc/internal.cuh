@@ -43,11 +43,19 @@ struct PointStats {
   unsigned int hi[3];
   unsigned long long max_abs_bits;  // bits of the largest |coordinate| (double)
   unsigned int inexact;             // a coordinate is not exactly representable in FP32
-  unsigned int bad;                 // non-finite or |coordinate| > kMaxCoordinate
+  unsigned int bad;                 // kBadCoordinates | kBadSortWait bits
   unsigned int ids_unsorted;        // ids decrease somewhere in input order
   unsigned int pad;
 };
 constexpr double kMaxCoordinate = 1.0e18;
+constexpr unsigned int kBadCoordinates = 1u;  // non-finite or |coordinate| > kMaxCoordinate
+constexpr unsigned int kBadSortWait = 2u;     // a radix-sort look-back wait ran out (the order is not valid)
+
+// Turns a set's bad bits into the call's error.
+inline void throw_if_bad(unsigned int bad) {
+  if (bad & kBadSortWait) throw std::runtime_error("radix sort look-back wait exceeded its limit");
+  if (bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+}
 
 __host__ __device__ inline unsigned int float_to_ordered(float f) {
 #ifdef __CUDA_ARCH__
@@ -170,8 +178,10 @@ void scan_counts_u64_ws(const uint32_t* counts, const uint32_t* order, const uns
 // Stable LSD radix sort of (key, value) pairs over bits [begin_bit, end_bit),
 // 8 bits per pass.  The result is left in keys/vals.  When *skip_flag != 0
 // (device memory) every pass returns immediately and the input stays in place.
+// A look-back wait that runs out sets kBadSortWait in *wait_error (the sorted
+// set's PointStats::bad), which the caller's input check turns into an error.
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int begin_bit, int end_bit,
-                      const unsigned int* skip_flag, cudaStream_t s);
+                      const unsigned int* skip_flag, unsigned int* wait_error, cudaStream_t s);
 void iota_u32(uint32_t* out, uint32_t n, cudaStream_t s);
 
 // ---- scene build (lbvh.cu) -------------------------------------------------

@@ -13,12 +13,14 @@
 //               (Karras 2012, "Maximizing Parallelism in the Construction of
 //               BVHs, Octrees, and k-d Trees"; equal codes are split on the
 //               index, so duplicates are handled);
-//   6. refit:   bottom-up boxes, one thread per leaf, an atomic arrival
-//               counter per node lets the second child to arrive continue;
-//   7. compact: the tree the traversal sees keeps an internal node only while
-//               it covers more than leaf_size points; smaller subtrees (and
-//               single points hanging off large nodes) become leaf buckets.
-//               That collapsed tree is written in depth-first pre-order as
+//   6. collapse: the tree the traversal sees keeps an internal node only
+//               while it covers more than leaf_size points; smaller subtrees
+//               (and single points hanging off large nodes) become leaf
+//               buckets;
+//   7. refit:   bottom-up boxes of the collapsed tree, one thread per bucket,
+//               an atomic arrival counter per node lets the second child to
+//               arrive continue;
+//   8. compact: the collapsed tree is written in depth-first pre-order as
 //               32-B records {box, leaf reference or "internal", rope}: the
 //               left child of an internal node is the next record, and the
 //               rope is the record that follows the node's subtree.  A walk
@@ -134,7 +136,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(const double* __restrict_
     }
     atomicMax(&st->max_abs_bits, (unsigned long long)__double_as_longlong(max_abs));
     if (fl & 1u) atomicOr(&st->inexact, 1u);
-    if (fl & 2u) atomicOr(&st->bad, 1u);
+    if (fl & 2u) atomicOr(&st->bad, kBadCoordinates);
     if (fl & 4u) atomicOr(&st->ids_unsorted, 1u);
   }
 }
@@ -251,19 +253,20 @@ __global__ void k_karras(const uint32_t* __restrict__ codes, uint32_t n, int* __
     const int64_t lo = i < j ? i : j;
     const int64_t hi = i < j ? j : i;
     int cl, cr;
+    const int up_l = (int)i << 1, up_r = ((int)i << 1) | 1;
     if (lo == gamma) {
       cl = (int)gamma | kLeafFlag;
-      parent_leaf[gamma] = (int)i;
+      parent_leaf[gamma] = up_l;
     } else {
       cl = (int)gamma;
-      parent_int[gamma] = (int)i;
+      parent_int[gamma] = up_l;
     }
     if (hi == gamma + 1) {
       cr = (int)(gamma + 1) | kLeafFlag;
-      parent_leaf[gamma + 1] = (int)i;
+      parent_leaf[gamma + 1] = up_r;
     } else {
       cr = (int)(gamma + 1);
-      parent_int[gamma + 1] = (int)i;
+      parent_int[gamma + 1] = up_r;
     }
     child_l[i] = cl;
     child_r[i] = cr;
@@ -272,50 +275,6 @@ __global__ void k_karras(const uint32_t* __restrict__ codes, uint32_t n, int* __
     // node index of the right child: internal nodes keep their index, point
     // leaves follow the n - 1 internal nodes
     right_of_split[gamma] = (cr & kLeafFlag) ? (int)(nn - 1) + (cr & ~kLeafFlag) : cr;
-  }
-}
-
-__device__ __forceinline__ void child_box(int c, const float4* __restrict__ pts, const float4* boxes, float4& lo,
-                                          float4& hi) {
-  if (c & kLeafFlag) {
-    const float4 p = pts[c & ~kLeafFlag];
-    lo = p;
-    hi = p;
-  } else {
-    lo = __ldcg(&boxes[2 * c]);
-    hi = __ldcg(&boxes[2 * c + 1]);
-  }
-}
-
-// One thread per point walks towards the root; at each internal node an
-// acquire-release arrival counter lets the second child to arrive continue
-// (the first stops).  The walking thread carries its subtree's box in
-// registers, so it reads only the sibling's box.
-__global__ void __launch_bounds__(kThreads) k_refit(uint32_t n, const float4* __restrict__ pts,
-                                                   const int* __restrict__ child_l, const int* __restrict__ child_r,
-                                                   const int* __restrict__ parent_int, const int* __restrict__ parent_leaf,
-                                                   unsigned int* __restrict__ arrivals, float4* boxes) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float4 p0 = pts[i];
-  float4 lo = make_float4(p0.x, p0.y, p0.z, 0.f), hi = lo;
-  int me = (int)i | kLeafFlag;  // child code of the subtree the thread stands on
-  int p = parent_leaf[i];
-  while (p >= 0) {
-    // the node's links (written by the previous kernel) are loaded before the
-    // arrival so their latency overlaps the atomic's; only the sibling's box
-    // has to wait for it
-    const int l = child_l[p], r = child_r[p], up = parent_int[p];
-    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> arrived(arrivals[p]);
-    if (arrived.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) break;  // the sibling is not finished yet
-    float4 sl, sh;
-    child_box(l == me ? r : l, pts, boxes, sl, sh);
-    lo = make_float4(fminf(lo.x, sl.x), fminf(lo.y, sl.y), fminf(lo.z, sl.z), 0.f);
-    hi = make_float4(fmaxf(hi.x, sh.x), fmaxf(hi.y, sh.y), fmaxf(hi.z, sh.z), 0.f);
-    __stcg(&boxes[2 * p], lo);
-    __stcg(&boxes[2 * p + 1], hi);
-    me = p;
-    p = up;
   }
 }
 
@@ -331,8 +290,14 @@ struct Ent {
   __device__ __forceinline__ bool is_point(int e) const { return e >= (int)n - 1; }
   __device__ __forceinline__ int lo(int e) const { return is_point(e) ? e - ((int)n - 1) : first[e]; }
   __device__ __forceinline__ int hi(int e) const { return is_point(e) ? e - ((int)n - 1) : last[e]; }
-  __device__ __forceinline__ int parent(int e) const {
+  // parent link: (parent index << 1) | 1 when e is its parent's right child;
+  // -1 at the root
+  __device__ __forceinline__ int link(int e) const {
     return is_point(e) ? parent_leaf[e - ((int)n - 1)] : parent_int[e];
+  }
+  __device__ __forceinline__ int parent(int e) const {
+    const int v = link(e);
+    return v < 0 ? -1 : v >> 1;
   }
   __device__ __forceinline__ int child_code(int e) const {  // as stored in child_l / child_r
     return is_point(e) ? ((e - ((int)n - 1)) | kLeafFlag) : e;
@@ -350,11 +315,13 @@ __device__ __forceinline__ bool spans_problems(const Ent& E, int e, const uint32
 }
 
 // Marks the nodes of the collapsed tree (flag bit 0) and its leaf buckets
-// (bit 1); a bucket sets leaf_start at its first point.  In a problem batch a
+// (bit 1); a bucket sets leaf_start at its first point and records itself in
+// bucket_at there.  In a problem batch a
 // node whose points span problems is never a bucket, so each problem keeps a
 // subtree of its own.
 __global__ void k_mark_collapsed(Ent E, int leaf_size, const uint32_t* codes, int code_bits,
-                                 uint8_t* __restrict__ flags, uint32_t* __restrict__ leaf_start) {
+                                 uint8_t* __restrict__ flags, uint32_t* __restrict__ leaf_start,
+                                 int* __restrict__ bucket_at) {
   const int total = 2 * (int)E.n - 1;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
     const int par = e == 0 ? -1 : E.parent(e);
@@ -366,9 +333,76 @@ __global__ void k_mark_collapsed(Ent E, int leaf_size, const uint32_t* codes, in
       if (E.is_point(e) || (E.hi(e) - E.lo(e) + 1 <= leaf_size && !spans_problems(E, e, codes, code_bits))) {
         f |= 2;
         leaf_start[E.lo(e)] = 1u;
+        bucket_at[E.lo(e)] = e;
       }
     }
     flags[e] = f;
+  }
+}
+
+// Narrows the bucket counts to 32 bits and lists the buckets' entities in
+// point order (bucket b = the b-th bucket from the left).
+__global__ void k_bucket_list(const uint64_t* __restrict__ leaves_before, const uint32_t* __restrict__ leaf_start,
+                              const int* __restrict__ bucket_at, uint32_t n, uint32_t* __restrict__ leaves_before32,
+                              int* __restrict__ buckets) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t b = leaves_before[i];
+    leaves_before32[i] = (uint32_t)b;
+    if (i < n && leaf_start[i]) buckets[b] = bucket_at[i];
+  }
+}
+
+// Boxes of the collapsed tree, bottom-up from its leaf buckets: one thread
+// per bucket takes the min / max over the bucket's points (a contiguous run
+// of at most 32 sorted points), then walks towards the root; at each internal
+// node an acquire-release arrival counter lets the second child to arrive
+// continue (the first stops).  The walking thread carries its subtree's box
+// in registers and reads only the sibling's box.  Min and max are exact, so
+// the boxes equal a refit from the single points.  Only internal nodes of the
+// collapsed tree get a box; a single-point bucket's box is its point.
+__global__ void __launch_bounds__(kThreads) k_refit_buckets(Ent E, const int* __restrict__ buckets,
+                                                           const uint32_t* __restrict__ bucket_count,
+                                                           const float4* __restrict__ pts,
+                                                           unsigned int* __restrict__ arrivals, float4* boxes) {
+  const uint32_t m = *bucket_count;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
+    const int e = buckets[b];
+    const int a = E.lo(e), z = E.hi(e);
+    const float4 p0 = pts[a];
+    float4 lo = make_float4(p0.x, p0.y, p0.z, 0.f), hi = lo;
+#pragma unroll 4
+    for (int j = a + 1; j <= z; ++j) {
+      const float4 p = pts[j];
+      lo = make_float4(fminf(lo.x, p.x), fminf(lo.y, p.y), fminf(lo.z, p.z), 0.f);
+      hi = make_float4(fmaxf(hi.x, p.x), fmaxf(hi.y, p.y), fmaxf(hi.z, p.z), 0.f);
+    }
+    if (!E.is_point(e)) {
+      __stcg(&boxes[2 * e], lo);
+      __stcg(&boxes[2 * e + 1], hi);
+    }
+    int v = E.link(e);
+    while (v >= 0) {
+      const int p = v >> 1;
+      // the node's links are loaded before the arrival so their latency
+      // overlaps the atomic's; only the sibling's box waits for it
+      const int sib = (v & 1) ? E.child_l[p] : E.child_r[p];
+      const int up = E.parent_int[p];
+      cuda::atomic_ref<unsigned int, cuda::thread_scope_device> arrived(arrivals[p]);
+      if (arrived.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) break;  // the sibling is not finished yet
+      float4 sl, sh;
+      if (sib & kLeafFlag) {
+        sl = pts[sib & ~kLeafFlag];
+        sh = sl;
+      } else {
+        sl = __ldcg(&boxes[2 * sib]);
+        sh = __ldcg(&boxes[2 * sib + 1]);
+      }
+      lo = make_float4(fminf(lo.x, sl.x), fminf(lo.y, sl.y), fminf(lo.z, sl.z), 0.f);
+      hi = make_float4(fmaxf(hi.x, sh.x), fmaxf(hi.y, sh.y), fmaxf(hi.z, sh.z), 0.f);
+      __stcg(&boxes[2 * p], lo);
+      __stcg(&boxes[2 * p + 1], hi);
+      v = up;
+    }
   }
 }
 
@@ -384,10 +418,10 @@ __global__ void k_compact(Ent E, const uint8_t* __restrict__ flags, const uint32
     if (!(f & 1)) continue;
     int depth = 0, right = 0;
     for (int x = e; x != 0;) {
-      const int par = E.parent(x);
+      const int v = E.link(x);
       ++depth;
-      if (E.child_r[par] == E.child_code(x)) ++right;
-      x = par;
+      right += v & 1;
+      x = v >> 1;
     }
     const int a = E.lo(e), b = E.hi(e);
     const int pre = 2 * (int)leaves_before[a] + depth - right;
@@ -524,11 +558,6 @@ __global__ void k_batch_codes(const float4* __restrict__ pts, const uint32_t* __
   }
 }
 
-__global__ void k_narrow_u64(const uint64_t* __restrict__ in, uint64_t n, uint32_t* __restrict__ out) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-    out[i] = (uint32_t)in[i];
-}
-
 // A one-point scene: a single leaf bucket.
 __global__ void k_single_point(const float4* __restrict__ pts, float4* __restrict__ nodes) {
   const float4 p = pts[0];
@@ -644,7 +673,7 @@ Scene* build_scene_impl(const void* points_dev, uint32_t n, int dim, cudaStream_
   }
   sc->perm = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
   iota_u32(sc->perm, n, s);
-  radix_sort_pairs(codes, sc->perm, n, 0, batch ? 32 : (dim == 3 ? 30 : 32), nullptr, s);
+  radix_sort_pairs(codes, sc->perm, n, 0, batch ? 32 : (dim == 3 ? 30 : 32), nullptr, &sc->stats->bad, s);
   sc->pts = static_cast<float4*>(dev_alloc(sizeof(float4) * n, s));
   sc->pts64 = static_cast<double*>(dev_alloc(sizeof(double) * 3 * (size_t)n, s));
   if (dim == 3)
@@ -668,28 +697,31 @@ Scene* build_scene_impl(const void* points_dev, uint32_t n, int dim, cudaStream_
     RTDL_CUDA_CHECK(cudaMemsetAsync(parent_int, 0xFF, sizeof(int) * ni, s));  // root keeps -1
     k_karras<<<grid_for(ni), kThreads, 0, s>>>(codes, n, child_l, child_r, first, last, parent_int, parent_leaf,
                                               right_of_split);
-    k_refit<<<div_up(n, kThreads), kThreads, 0, s>>>(n, sc->pts, child_l, child_r, parent_int, parent_leaf, arrivals,
-                                                   boxes);
-    RTDL_LAUNCHED(2);
+    RTDL_LAUNCHED(1);
     Ent E{child_l, child_r, first, last, parent_int, parent_leaf, n};
     const uint64_t ents = 2ull * n - 1;
     uint8_t* flags = static_cast<uint8_t*>(dev_alloc(ents, s));
     uint32_t* leaf_start = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
+    int* bucket_at = static_cast<int*>(dev_alloc(sizeof(int) * n, s));
+    int* buckets = static_cast<int*>(dev_alloc(sizeof(int) * n, s));
     uint64_t* leaves_before = static_cast<uint64_t*>(dev_alloc(sizeof(uint64_t) * (n + 1), s));
     uint32_t* leaves_before32 = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (n + 1), s));
     int* ent2pre = static_cast<int*>(dev_alloc(sizeof(int) * ents, s));
     RTDL_CUDA_CHECK(cudaMemsetAsync(leaf_start, 0, sizeof(uint32_t) * n, s));
     RTDL_CUDA_CHECK(cudaMemsetAsync(ent2pre, 0xFF, sizeof(int) * ents, s));  // kRopeEnd for entities off the tree
     k_mark_collapsed<<<grid_for(ents), kThreads, 0, s>>>(E, leaf_size, batch ? codes : nullptr, sc->code_bits,
-                                                         flags, leaf_start);
+                                                         flags, leaf_start, bucket_at);
     RTDL_LAUNCHED(1);
     scan_counts_u64(leaf_start, nullptr, nullptr, n, reinterpret_cast<unsigned long long*>(leaves_before), s);
-    k_narrow_u64<<<grid_for(n + 1), kThreads, 0, s>>>(leaves_before, n + 1, leaves_before32);
+    k_bucket_list<<<grid_for(n + 1), kThreads, 0, s>>>(leaves_before, leaf_start, bucket_at, n, leaves_before32,
+                                                       buckets);
+    k_refit_buckets<<<grid_for(div_up(n, 4)), kThreads, 0, s>>>(E, buckets, leaves_before32 + n, sc->pts, arrivals,
+                                                               boxes);
     sc->nodes = static_cast<float4*>(dev_alloc(sizeof(float4) * 2 * ents, s));
     k_compact<<<grid_for(ents), kThreads, 0, s>>>(E, flags, leaves_before32, sc->pts, boxes, right_of_split, ent2pre,
                                                   sc->nodes);
     k_translate_ropes<<<grid_for(ents), kThreads, 0, s>>>(leaves_before32 + n, ent2pre, sc->nodes);
-    RTDL_LAUNCHED(3);
+    RTDL_LAUNCHED(4);
     if (batch) {
       k_batch_roots<<<grid_for(ents), kThreads, 0, s>>>(E, flags, codes, sc->code_bits, ent2pre, sc->prob_root);
       RTDL_LAUNCHED(1);
@@ -705,6 +737,8 @@ Scene* build_scene_impl(const void* points_dev, uint32_t n, int dim, cudaStream_
     dev_free(right_of_split, s);
     dev_free(flags, s);
     dev_free(leaf_start, s);
+    dev_free(bucket_at, s);
+    dev_free(buckets, s);
     dev_free(leaves_before, s);
     dev_free(leaves_before32, s);
     dev_free(ent2pre, s);

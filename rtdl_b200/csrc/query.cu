@@ -2150,14 +2150,14 @@ QueryPrep prepare_queries(Scene* sc, const void* queries_dev, uint32_t nq, bool 
   qp.qcodes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   morton_codes(qp.qpts, nq, sc->dim, sc->stats, qp.qcodes, s);
   iota_u32(qp.qorder, nq, s);
-  radix_sort_pairs(qp.qcodes, qp.qorder, nq, 0, sc->dim == 3 ? 30 : 32, nullptr, s);
+  radix_sort_pairs(qp.qcodes, qp.qorder, nq, 0, sc->dim == 3 ? 30 : 32, nullptr, &qp.qst->bad, s);
   if (want_output_order) {
     qp.oorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
     uint32_t* ids = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
     k_extract_ids<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, ids);
     RTDL_LAUNCHED(1);
     iota_u32(qp.oorder, nq, s);
-    radix_sort_pairs(ids, qp.oorder, nq, 0, 32, &qp.bands->ids_sorted, s);
+    radix_sort_pairs(ids, qp.oorder, nq, 0, 32, &qp.bands->ids_sorted, &qp.qst->bad, s);
     dev_free(ids, s);
   }
   return qp;
@@ -2219,7 +2219,7 @@ QueryPrep prepare_queries_batch(Scene* sc, const void* queries_dev, uint32_t nq,
   else
     batch_codes(qp.qpts, qp.qprob, nq, sc->dim, sc->prob_stats, 1, sc->code_bits, codes, s);
   iota_u32(sorted, nq, s);
-  radix_sort_pairs(codes, sorted, nq, 0, 32, nullptr, s);
+  radix_sort_pairs(codes, sorted, nq, 0, 32, nullptr, &qp.qst->bad, s);
   k_batch_pad<<<P, 256, 0, s>>>(qp.qoff, d_pstart, sorted, qp.qorder, qp.warp_prob);
   RTDL_LAUNCHED(1);
   // output order: by query id, then (stable) by problem; skipped when every
@@ -2228,10 +2228,10 @@ QueryPrep prepare_queries_batch(Scene* sc, const void* queries_dev, uint32_t nq,
   iota_u32(qp.oorder, nq, s);
   k_extract_ids<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, codes);
   RTDL_LAUNCHED(1);
-  radix_sort_pairs(codes, qp.oorder, nq, 0, 32, qp.sorted_flag, s);
+  radix_sort_pairs(codes, qp.oorder, nq, 0, 32, qp.sorted_flag, &qp.qst->bad, s);
   k_gather_u32<<<grid_for(nq, 256), 256, 0, s>>>(qp.qprob, qp.oorder, nq, qp.sorted_flag, codes);
   RTDL_LAUNCHED(1);
-  radix_sort_pairs(codes, qp.oorder, nq, 0, batch_problem_bits(P), qp.sorted_flag, s);
+  radix_sort_pairs(codes, qp.oorder, nq, 0, batch_problem_bits(P), qp.sorted_flag, &qp.qst->bad, s);
   dev_free(codes, s);
   dev_free(sorted, s);
   dev_free(d_pstart, s);
@@ -2552,7 +2552,7 @@ void enqueue_refine_device(const CollectParams& C, const uint32_t* qprob, const 
 }
 
 void check_readback(const Readback& r) {
-  if (r.scene_bad || r.query_bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+  throw_if_bad(r.scene_bad | r.query_bad);
   if (r.error & 1u) throw std::runtime_error("BVH traversal stack overflow");
 }
 
@@ -2772,17 +2772,37 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       E.sink.ranked = predicate == kFrn ? 0 : 1;
       E.fix_list = fix_list;
       E.fix_count = small + 4;
-      k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
-      RTDL_LAUNCHED(1);
+      // The list kernels (queries with 65..kSlab candidates: few warps, long
+      // sorts) run on the second stream beside k_emit, so each fills the
+      // other's partial waves; they write disjoint rows, and the fix-up waits
+      // for both.
+      static thread_local cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+      const bool side = mid > 0 || big > 0;
+      cudaStream_t ls = s;
+      if (side) {
+        if (!ev_fork) {
+          RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+          RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        }
+        ls = aux_stream();
+        RTDL_CUDA_CHECK(cudaEventRecord(ev_fork, s));
+        RTDL_CUDA_CHECK(cudaStreamWaitEvent(ls, ev_fork, 0));
+      }
       if (mid > 0) {
-        k_emit_list<4, true><<<div_up((uint64_t)mid * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, mid_list,
-                                                                                                    mid, nullptr);
+        k_emit_list<4, true><<<div_up((uint64_t)mid * 32, kEmitListThreads), kEmitListThreads, 0, ls>>>(E, mid_list,
+                                                                                                     mid, nullptr);
         RTDL_LAUNCHED(1);
       }
       if (big > 0) {
-        k_emit_list<8, false><<<div_up((uint64_t)big * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(E, big_list,
-                                                                                                     big, nullptr);
+        k_emit_list<8, false><<<div_up((uint64_t)big * 32, kEmitListThreads), kEmitListThreads, 0, ls>>>(E, big_list,
+                                                                                                      big, nullptr);
         RTDL_LAUNCHED(1);
+      }
+      k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
+      RTDL_LAUNCHED(1);
+      if (side) {
+        RTDL_CUDA_CHECK(cudaEventRecord(ev_join, ls));
+        RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ev_join, 0));
       }
       k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
       RTDL_LAUNCHED(1);
@@ -2987,7 +3007,7 @@ PointGroupScene* point_group_create(const RtdlPoint* points, size_t count, const
     unsigned int bad = 0;
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &pg->sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors stay alive until the copies are done
-    if (bad) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+    throw_if_bad(bad);
   } catch (...) {
     cudaStreamSynchronize(s);
     dev_free(d_pts, s);
@@ -3343,7 +3363,7 @@ SummaryGraph* summary_graph_create(Scene* sc, const PreparedQueries* pq, const d
     unsigned int bad[2] = {0, 0};
     RTDL_CUDA_CHECK(cudaMemcpy(&bad[0], &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost));
     RTDL_CUDA_CHECK(cudaMemcpy(&bad[1], &pq->qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost));
-    if (bad[0] || bad[1]) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+    throw_if_bad(bad[0] | bad[1]);
     auto alloc = [&](size_t bytes) {
       void* p = dev_alloc(bytes ? bytes : 1, s);
       g->buffers.push_back(p);
@@ -3482,11 +3502,11 @@ PreparedQueries* prepare_query_set(const void* records_dev, uint32_t n, int dim,
     uint32_t* codes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n1, s));
     morton_codes(pq->qpts, n, dim, pq->qst, codes, s);  // the set's own box: the order only groups neighbours
     iota_u32(pq->qorder, n, s);
-    radix_sort_pairs(codes, pq->qorder, n, 0, dim == 3 ? 30 : 32, nullptr, s);
+    radix_sort_pairs(codes, pq->qorder, n, 0, dim == 3 ? 30 : 32, nullptr, &pq->qst->bad, s);
     k_extract_ids<<<grid_for(n, 256), 256, 0, s>>>(pq->qpts, n, codes);
     RTDL_LAUNCHED(1);
     iota_u32(pq->oorder, n, s);
-    radix_sort_pairs(codes, pq->oorder, n, 0, 32, pq->identity, s);
+    radix_sort_pairs(codes, pq->oorder, n, 0, 32, pq->identity, &pq->qst->bad, s);
     k_invert<<<grid_for(n, 256), 256, 0, s>>>(pq->oorder, n, pq->identity, pq->qrank);
     RTDL_LAUNCHED(1);
     dev_free(codes, s);
@@ -3755,7 +3775,7 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   dev_free(partial, s);
   dev_free(best, s);
   free_prep(qp, s);
-  if (bad[0] || bad[1]) throw std::runtime_error("point coordinates must be finite with magnitude <= 1e18");
+  throw_if_bad(bad[0] | bad[1]);
   HausdorffResult out;
   unsigned long long db = w.dist;
   memcpy(&out.distance, &db, sizeof(double));
@@ -3809,7 +3829,8 @@ __global__ void k_noalloc_finish(const Witness* best, const PointStats* scene_st
   w.distance = __longlong_as_double((long long)db);
   w.source_id = best->qid;
   w.target_id = best->nid;
-  w.status = (scene_stats->bad || query_stats->bad) ? 1u : ((*error & 1u) ? 2u : 0u);
+  const unsigned int bad = scene_stats->bad | query_stats->bad;
+  w.status = (bad & kBadSortWait) ? 3u : bad ? 1u : ((*error & 1u) ? 2u : 0u);
   w.reserved = 0u;
   *out = w;
 }

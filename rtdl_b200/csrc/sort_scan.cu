@@ -6,12 +6,23 @@
 // Scan: reduce-then-scan over 2,048-element tiles (256 threads x 8 items), a
 // single-block pass over the tile sums, then a downsweep.  Deterministic and
 // free of inter-block waits.
-// Radix sort: 8-bit digits; per pass a tile histogram kernel, a scan of the
-// (digit, tile) histogram and a scatter kernel.  The scatter gives each warp a
-// contiguous run of the tile: the warp counts its digits (__match_any_sync,
-// one shared-memory add per digit group), one block-wide scan over
-// (digit, warp) turns the counts into bases, and the warp then places its
-// keys in order, so a tile costs two barriers and the sort stays stable.
+// Radix sort: 8-bit digits.  One kernel counts the digits of every pass in a
+// single read of the keys; then one scatter kernel per pass.  A scatter block
+// takes the next tile index from a counter, counts its tile's digits, and
+// finds each digit's offset among the earlier tiles by decoupled look-back
+// (Merrill and Garland, "Single-pass Parallel Prefix Scan with Decoupled
+// Look-back", 2016): per (tile, digit) a status word holds either the tile's
+// own count or the inclusive count over tiles 0..tile, and a block walks back
+// over the earlier tiles' words until it meets an inclusive one.  Tile indices
+// are handed out in the order blocks start, so every tile a block waits on
+// belongs to a block that is already running; each wait is still bounded and
+// reports through an error word when it runs out.  Inside a tile each warp
+// owns a contiguous run: the warp counts its digits (__match_any_sync, one
+// shared-memory add per digit group), a block-wide scan over (digit, warp)
+// turns the counts into bases, and the warp then places its keys in order, so
+// the sort stays stable.
+#include <cuda/atomic>
+
 #include "internal.cuh"
 
 namespace rtdl_b200 {
@@ -153,40 +164,58 @@ void scan_impl(const uint32_t* counts, const uint32_t* order, const unsigned int
   if (!workspace) dev_free(sums, s);
 }
 
-__global__ void k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift, uint32_t* hist,
-                             uint32_t num_tiles, const unsigned int* skip) {
+constexpr uint32_t kLookLocal = 1u << 30;       // status word: the tile's own count of the digit
+constexpr uint32_t kLookInclusive = 2u << 30;   // status word: the count over tiles 0..this one
+constexpr uint32_t kLookValue = (1u << 30) - 1u;
+constexpr int kLookSpinLimit = 1 << 22;         // polls of one status word before the wait gives up
+constexpr int kMaxPasses = 4;
+
+// Digit counts of every pass (counts[pass * 256 + digit]) in one read of the
+// keys; each warp keeps its own shared histograms.
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist_all(const uint32_t* __restrict__ keys, uint32_t n,
+                                                                int begin_bit, int passes, uint32_t* counts,
+                                                                const unsigned int* skip) {
   if (skip != nullptr && *skip) return;
-  __shared__ unsigned int h[256];
-  const int t = threadIdx.x;
-  h[t] = 0;
+  __shared__ unsigned int h[kSortWarps][kMaxPasses][256];
+  const int t = threadIdx.x, warp = t >> 5;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w)
+#pragma unroll
+    for (int p = 0; p < kMaxPasses; ++p) h[w][p][t] = 0;
   __syncthreads();
-  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
-#pragma unroll 4
-  for (int i = 0; i < kSortItems; ++i) {
-    uint64_t idx = base + (uint64_t)i * kSortThreads + t;
-    if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255u], 1u);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + t; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    for (int p = 0; p < passes; ++p) atomicAdd(&h[warp][p][(k >> (begin_bit + 8 * p)) & 255u], 1u);
   }
   __syncthreads();
-  hist[(uint64_t)t * num_tiles + blockIdx.x] = h[t];
+  for (int p = 0; p < passes; ++p) {
+    unsigned int c = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) c += h[w][p][t];
+    if (c) atomicAdd(&counts[p * 256 + t], c);
+  }
 }
 
 __global__ void __launch_bounds__(kSortThreads)
-    k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-                    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n, int shift,
-                    const uint32_t* __restrict__ hist_scanned, uint32_t num_tiles, const unsigned int* skip) {
+    k_radix_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n, int shift,
+                     const uint32_t* __restrict__ digit_counts, uint32_t* status, unsigned int* tile_counter,
+                     unsigned int* wait_error, const unsigned int* skip) {
   if (skip != nullptr && *skip) return;
   __shared__ unsigned int wcnt[kSortWarps][256];  // a warp's digit counts, then its tile-local digit bases
   __shared__ unsigned int dbase[256];             // tile-local start of each digit
   __shared__ unsigned int gbase[256];             // global start of each digit for this tile
-  __shared__ unsigned int total;
+  __shared__ unsigned int total, tile_s;
   __shared__ uint32_t skeys[kSortTile], svals[kSortTile];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const unsigned int lt_mask = (1u << lane) - 1u;
+  if (t == 0) tile_s = atomicAdd(tile_counter, 1u);
 #pragma unroll
   for (int w = 0; w < kSortWarps; ++w) wcnt[w][t] = 0;
   __syncthreads();
+  const uint32_t tile = tile_s;
   // the warp's run of the tile: kSortItems rounds of 32 consecutive keys
-  const uint64_t tile0 = (uint64_t)blockIdx.x * kSortTile;
+  const uint64_t tile0 = (uint64_t)tile * kSortTile;
   const uint64_t base = tile0 + (uint64_t)warp * (kSortItems * 32);
   uint32_t key[kSortItems];
 #pragma unroll
@@ -200,8 +229,8 @@ __global__ void __launch_bounds__(kSortThreads)
     __syncwarp();
   }
   __syncthreads();
-  // thread t owns digit t: offsets of the warps within the digit, then the
-  // digit's tile-local start (scan over digits) and its global start
+  // thread t owns digit t: offsets of the warps within the digit and the
+  // tile's count of the digit
   unsigned int r = 0;
 #pragma unroll
   for (int w = 0; w < kSortWarps; ++w) {
@@ -209,9 +238,40 @@ __global__ void __launch_bounds__(kSortThreads)
     wcnt[w][t] = r;
     r += c;
   }
+  // publish the count, then look back over the earlier tiles for the digit's
+  // offset among them
+  cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(status[(uint64_t)tile * 256 + t]);
+  uint32_t before = 0;
+  if (tile == 0) {
+    mine.store(kLookInclusive | r, cuda::memory_order_relaxed);
+  } else {
+    mine.store(kLookLocal | r, cuda::memory_order_relaxed);
+    int64_t j = (int64_t)tile - 1;
+    int spins = 0;
+    while (j >= 0) {
+      cuda::atomic_ref<uint32_t, cuda::thread_scope_device> w(status[(uint64_t)j * 256 + t]);
+      const uint32_t v = w.load(cuda::memory_order_relaxed);
+      if (v & kLookInclusive) {
+        before += v & kLookValue;
+        break;
+      }
+      if (v & kLookLocal) {
+        before += v & kLookValue;
+        --j;
+        continue;
+      }
+      if (++spins > kLookSpinLimit) {
+        atomicOr(wait_error, kBadSortWait);
+        break;
+      }
+      __nanosleep(64);
+    }
+    mine.store(kLookInclusive | ((before + r) & kLookValue), cuda::memory_order_relaxed);
+  }
   const unsigned int db = block_exclusive_scan<unsigned int>(r, &total);
+  const unsigned int dstart = block_exclusive_scan<unsigned int>(digit_counts[t], &total);
   dbase[t] = db;
-  gbase[t] = hist_scanned[(uint64_t)t * num_tiles + blockIdx.x];
+  gbase[t] = dstart + before;
 #pragma unroll
   for (int w = 0; w < kSortWarps; ++w) wcnt[w][t] += db;
   __syncthreads();
@@ -233,14 +293,17 @@ __global__ void __launch_bounds__(kSortThreads)
   }
   __syncthreads();
   // write out: consecutive threads take consecutive keys of a digit's run,
-  // so the global stores are contiguous
+  // so the global stores are contiguous; a position beyond n (possible only
+  // after a wait ran out) is not written
   const unsigned int tile_n = (unsigned int)(n - tile0 < (uint64_t)kSortTile ? n - tile0 : (uint64_t)kSortTile);
   for (unsigned int j = t; j < tile_n; j += kSortThreads) {
     const uint32_t k = skeys[j];
     const uint32_t d = (k >> shift) & 255u;
     const unsigned int pos = gbase[d] + (j - dbase[d]);
-    keys_out[pos] = k;
-    vals_out[pos] = svals[j];
+    if (pos < n) {
+      keys_out[pos] = k;
+      vals_out[pos] = svals[j];
+    }
   }
 }
 
@@ -275,28 +338,37 @@ void iota_u32(uint32_t* out, uint32_t n, cudaStream_t s) {
 }
 
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int begin_bit, int end_bit,
-                      const unsigned int* skip_flag, cudaStream_t s) {
+                      const unsigned int* skip_flag, unsigned int* wait_error, cudaStream_t s) {
   if (n <= 1 || end_bit <= begin_bit) return;
+  if (n > kLookValue) throw std::runtime_error("radix sort input too large");
+  if (begin_bit < 0 || end_bit > 32) throw std::runtime_error("radix sort bit range must lie in [0, 32)");
   int passes = (end_bit - begin_bit + 7) / 8;
   if (passes & 1) ++passes;  // even pass count leaves the result in the caller's buffers
+  int real = 0;              // passes that sort (the rest only copy)
+  while (real < passes && begin_bit + 8 * real < 32) ++real;
   const uint32_t tiles = div_up(n, kSortTile);
-  const uint64_t hist_n = (uint64_t)256 * tiles;
-  if (hist_n + 1 > 0xFFFFFFFFull) throw std::runtime_error("radix sort input too large");
   uint32_t* keys_alt = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
   uint32_t* vals_alt = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * n, s));
-  uint32_t* hist = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (hist_n + 1), s));
-  uint32_t* hist_sums = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (div_up(hist_n, kScanTile) + 1), s));
+  // per sorting pass: 256 digit counts, a tile counter and tiles x 256 status words
+  const size_t per_pass = 256 + 1 + (size_t)tiles * 256;
+  const size_t work_words = per_pass * (size_t)real;
+  uint32_t* work = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * work_words, s));
+  RTDL_CUDA_CHECK(cudaMemsetAsync(work, 0, sizeof(uint32_t) * work_words, s));
+  uint32_t* counts = work;                                    // real x 256
+  unsigned int* tile_counters = work + 256 * (size_t)real;    // real
+  uint32_t* status = work + 257 * (size_t)real;               // real x tiles x 256
+  unsigned int hist_blocks = div_up(n, kSortThreads * 8);
+  if (hist_blocks > (unsigned int)kSmCount * 2) hist_blocks = kSmCount * 2;
+  k_radix_hist_all<<<hist_blocks, kSortThreads, 0, s>>>(keys, n, begin_bit, real, counts, skip_flag);
+  RTDL_LAUNCHED(1);
   uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
-  const uint32_t htiles = div_up(hist_n, kScanTile);
   for (int p = 0; p < passes; ++p) {
     const int shift = begin_bit + 8 * p;
-    if (shift < 32) {
-      k_radix_hist<<<tiles, kSortThreads, 0, s>>>(ki, n, shift, hist, tiles, skip_flag);
-      k_scan_reduce<uint32_t><<<htiles, kScanThreads, 0, s>>>(hist, nullptr, nullptr, (uint32_t)hist_n, hist_sums);
-      k_scan_tile_sums<uint32_t><<<1, 1024, 0, s>>>(hist_sums, htiles, hist + hist_n);
-      k_scan_down<uint32_t><<<htiles, kScanThreads, 0, s>>>(hist, nullptr, nullptr, (uint32_t)hist_n, hist_sums, hist);
-      k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, shift, hist, tiles, skip_flag);
-      RTDL_LAUNCHED(5);
+    if (p < real) {
+      k_radix_onesweep<<<tiles, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, shift, counts + 256 * p, status +
+                                                      (size_t)p * tiles * 256, tile_counters + p, wait_error,
+                                                      skip_flag);
+      RTDL_LAUNCHED(1);
     } else {
       // A padding pass beyond the key width: a plain copy keeps the ping-pong even.
       RTDL_CUDA_CHECK(cudaMemcpyAsync(ko, ki, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
@@ -308,8 +380,7 @@ void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int begin_bit,
   }
   dev_free(keys_alt, s);
   dev_free(vals_alt, s);
-  dev_free(hist, s);
-  dev_free(hist_sums, s);
+  dev_free(work, s);
 }
 
 }  // namespace rtdl_b200

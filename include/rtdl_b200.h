@@ -599,7 +599,9 @@ RTDL_B200_API int rtdl_b200_get_launch_count(unsigned long long* count_out);
  * bounded_knn_rows -- and 8 for general scenes); block_threads: 64, 128
  * or 256; traversal: 0 = one warp walks the tree for 32 neighbouring queries
  * (packet), 1 = one thread per query, 2 = packet with the query's bounding
- * cube tested at internal nodes.  Returns 0 on success. */
+ * cube tested at internal nodes, 3 = packet whose leaf buckets are tested
+ * point-major (a lane per point, the reaching queries in turn).  Returns 0 on
+ * success. */
 RTDL_B200_API int rtdl_b200_set_tuning(int leaf_size, int block_threads, int traversal);
 
 #ifdef __cplusplus

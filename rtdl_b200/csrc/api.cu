@@ -311,7 +311,7 @@ int rtdl_b200_set_device(int device) {
 int rtdl_b200_set_tuning(int leaf_size, int block_threads, int traversal) {
   if (leaf_size < 0 || leaf_size > 32) return 1;
   if (block_threads != 64 && block_threads != 128 && block_threads != 256) return 1;
-  if (traversal < 0 || traversal > 2) return 1;
+  if (traversal < 0 || traversal > 3) return 1;
   tuning().leaf_size = leaf_size;
   tuning().block_threads = block_threads;
   tuning().traversal = traversal;

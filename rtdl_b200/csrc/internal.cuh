@@ -146,7 +146,8 @@ struct Tuning {
   int leaf_size = 0;  // 0: automatic (leaf_size_for)
   int block_threads = 128;
   int traversal = 0;  // fixed-radius collect: 0 = one warp per 32 queries (packet), 1 = one thread per
-                      // query, 2 = packet with cube tests at internal nodes
+                      // query, 2 = packet with cube tests at internal nodes, 3 = packet with
+                      // point-major leaf tests
 };
 Tuning& tuning();
 

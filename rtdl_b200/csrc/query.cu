@@ -455,11 +455,20 @@ struct CollectParams {
 struct CollectLane {
   uint32_t t, qin;
   float4 q;
-  double ex, ey, ez;
   uint32_t count;
   unsigned long long* out;  // this query's slab entries
   unsigned long long st_nodes, st_points, st_band, st_pairs;
 };
+
+// The query's exact coordinates, read when needed (the band's FP64 test and
+// the query record) rather than held in registers through the walk.
+__device__ __forceinline__ void query_exact(const CollectParams& P, uint32_t qin, double& ex, double& ey,
+                                            double& ez) {
+  const double* r = P.qraw + (size_t)qin * P.qstride;
+  ex = r[1];
+  ey = r[2];
+  ez = P.qstride == 4 ? r[3] : 0.0;
+}
 
 // Tests sorted point i against the lane's query and appends it when it is in
 // radius: FP32 decides outside the band, FP64 inside.  The stored key is the
@@ -472,7 +481,9 @@ __device__ __forceinline__ void collect_point(const CollectParams& P, const DevB
   if (d2 > B.hi2) return;
   if (d2 >= B.lo2 || B.any_inexact) {
     if (STATS && d2 >= B.lo2) ++L.st_band;
-    const double e2 = exact_d2_at(L.ex, L.ey, L.ez, P.S.pts, P.S.pts64, scene_inexact, i);
+    double ex, ey, ez;
+    query_exact(P, L.qin, ex, ey, ez);
+    const double e2 = exact_d2_at(ex, ey, ez, P.S.pts, P.S.pts64, scene_inexact, i);
     if (d2 >= B.lo2 && e2 > B.r2) return;
     if (B.any_inexact) d2 = __double2float_rn(e2);
   }
@@ -507,9 +518,7 @@ __device__ __forceinline__ void collect_finish(const CollectParams& P, const Col
     P.mid_list[atomicAdd(&P.small[2], 1u)] = L.t;
   }
   QueryInfo qi;
-  qi.ex = L.ex;
-  qi.ey = L.ey;
-  qi.ez = L.ez;
+  query_exact(P, L.qin, qi.ex, qi.ey, qi.ez);
   qi.qid = __float_as_uint(L.q.w);
   qi.meta = (count < (uint32_t)kSlab ? count : (uint32_t)kSlab) | ((fl & 1) ? kQueryOverflow : 0u) |
             ((fl & 2) ? kQueryGeneric : 0u) | ((fl & 4) ? kQueryBig : 0u) | (kmax << kQueryKmaxShift);
@@ -522,10 +531,6 @@ __device__ __forceinline__ void collect_init(const CollectParams& P, uint32_t t,
   L.t = t;
   L.qin = P.qorder[t];
   L.q = P.qpts[L.qin];
-  const double* r = P.qraw + (size_t)L.qin * P.qstride;
-  L.ex = r[1];
-  L.ey = r[2];
-  L.ez = P.qstride == 4 ? r[3] : 0.0;
   L.count = 0;
   L.out = P.slab + slab_base(t);
   L.st_nodes = L.st_points = L.st_band = L.st_pairs = 0;
@@ -553,6 +558,62 @@ __device__ __forceinline__ void collect_leaf(const CollectParams& P, const DevBa
   for (; i < end; ++i) {
     const float4 p = __ldg(&P.S.pts[i]);
     if (test) collect_point<STATS>(P, B, scene_inexact, L, (uint32_t)i, p);
+  }
+}
+
+// Point-major form of collect_leaf for a packet: lane j holds point
+// first + j of the bucket (cnt <= 32), and the warp takes the queries whose
+// sphere reaches the bucket (`active`, one bit per lane) one at a time: the
+// query's coordinates are broadcast, every lane tests its point, and the hits
+// go to consecutive entries of that query's slab row (one coalesced store).
+// The loop runs once per reaching query instead of once per point, and lanes
+// whose query misses the bucket cost nothing.  The decisions are
+// collect_point's (FP32 outside the band, FP64 inside); only the order of a
+// query's slab entries differs, which the emit's sort does not see.
+template <bool STATS>
+__device__ __forceinline__ void collect_leaf_pm(const CollectParams& P, const DevBands& B, int scene_inexact,
+                                                CollectLane& L, uint32_t t0, int lane, int first, int cnt,
+                                                unsigned int active) {
+  const bool has = lane < cnt;
+  const uint32_t i = (uint32_t)(first + (has ? lane : 0));
+  const float4 p = __ldg(&P.S.pts[i]);
+  const unsigned int lt_mask = (1u << lane) - 1u;
+  if (STATS) {
+    L.st_points += cnt;
+    if ((active >> lane) & 1u) L.st_pairs += cnt;
+  }
+  while (active) {
+    const int q = __ffs(active) - 1;
+    active &= active - 1u;
+    const float qx = __shfl_sync(0xffffffffu, L.q.x, q);
+    const float qy = __shfl_sync(0xffffffffu, L.q.y, q);
+    const float qz = __shfl_sync(0xffffffffu, L.q.z, q);
+    const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+    float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    bool hit = has && d2 <= B.hi2;
+    const bool check = hit && (d2 >= B.lo2 || B.any_inexact);
+    if (__any_sync(0xffffffffu, check)) {
+      const uint32_t qin = __shfl_sync(0xffffffffu, L.qin, q);
+      if (check) {
+        double ex, ey, ez;
+        query_exact(P, qin, ex, ey, ez);
+        if (STATS && d2 >= B.lo2) ++L.st_band;
+        const double e2 = exact_d2_at(ex, ey, ez, P.S.pts, P.S.pts64, scene_inexact, i);
+        if (d2 >= B.lo2 && e2 > B.r2)
+          hit = false;
+        else if (B.any_inexact)
+          d2 = __double2float_rn(e2);
+      }
+    }
+    const unsigned int hits = __ballot_sync(0xffffffffu, hit);
+    if (hits) {
+      const uint32_t c0 = __shfl_sync(0xffffffffu, L.count, q);
+      if (hit) {
+        const uint32_t pos = c0 + (uint32_t)__popc(hits & lt_mask);
+        if (pos < (uint32_t)kSlab) P.slab[slab_base(t0 + (uint32_t)q) + pos] = slab_entry(d2, i);
+      }
+      if (lane == q) L.count = c0 + (uint32_t)__popc(hits);
+    }
   }
 }
 
@@ -608,7 +669,7 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
 // one scene): each warp walks its problem's subtree with its problem's bands
 // and kmax; kept out of the single-problem instantiation, whose registers it
 // would cost.
-template <bool STATS, bool CUBE, bool BATCH, int MIN_BLOCKS>
+template <bool STATS, bool CUBE, bool BATCH, int MIN_BLOCKS, bool PM = false>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParams P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!__any_sync(0xffffffffu, t < P.nq)) return;  // whole warp past the end
@@ -649,17 +710,22 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParam
       over = valid && a.x <= chi.x && b.x >= clo.x && a.y <= chi.y && b.y >= clo.y && a.z <= chi.z && b.z >= clo.z;
     else
       over = valid && box_d2(L.q.x, L.q.y, L.q.z, a, b) <= B.box_hi2;
-    if (__any_sync(0xffffffffu, over)) {
+    const unsigned int reach = __ballot_sync(0xffffffffu, over);
+    if (reach) {
       if (hit >= 0) {
         ++cur;  // internal node: its left child is the next record
         continue;
       }
       const int first = leaf_first(hit), cnt = leaf_count(hit);
-      if (STATS) {
-        L.st_points += cnt;
-        if (over) L.st_pairs += cnt;
+      if (PM) {
+        collect_leaf_pm<STATS>(P, B, scene_inexact, L, t & ~31u, (int)(threadIdx.x & 31), first, cnt, reach);
+      } else {
+        if (STATS) {
+          L.st_points += cnt;
+          if (over) L.st_pairs += cnt;
+        }
+        collect_leaf<STATS>(P, B, scene_inexact, L, first, cnt, over);
       }
-      collect_leaf<STATS>(P, B, scene_inexact, L, first, cnt, over);
     }
     cur = __float_as_int(b.w);
   }
@@ -2458,6 +2524,9 @@ void launch_collect(const CollectParams& C, uint32_t np, uint32_t nq, bool batch
     // occupancy bounds chosen so neither variant spills (32 and 40 registers)
     if (batch)  // several problems (traversal counters are not gathered here)
       k_collect_packet<false, false, true, 5><<<grid, threads, 0, s>>>(C);
+    else if (tuning().traversal == 3)
+      stats ? k_collect_packet<true, false, false, 1, true><<<grid, threads, 0, s>>>(C)
+            : k_collect_packet<false, false, false, 6, true><<<grid, threads, 0, s>>>(C);
     else if (stats)
       cube ? k_collect_packet<true, true, false, 1><<<grid, threads, 0, s>>>(C)
            : k_collect_packet<true, false, false, 1><<<grid, threads, 0, s>>>(C);

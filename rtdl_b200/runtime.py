@@ -1522,9 +1522,9 @@ def hausdorff_distance(points_a, points_b, *, dimension: int | None = None) -> d
 def set_tuning(*, leaf_size: int = 0, block_threads: int = 128, traversal: str = "packet") -> None:
     """Set the kernel tuning knobs (see ``rtdl_b200_set_tuning``); ``leaf_size`` 0 picks the leaf
     bucket size by the scene's use (24 points for fixed-radius-only scenes, 8 otherwise)."""
-    modes = {"packet": 0, "lane": 1, "packet_cube": 2}
+    modes = {"packet": 0, "lane": 1, "packet_cube": 2, "packet_points": 3}
     if traversal not in modes:
-        raise ValueError("traversal must be 'packet', 'lane' or 'packet_cube'")
+        raise ValueError("traversal must be 'packet', 'lane', 'packet_cube' or 'packet_points'")
     status = _native.load_library().rtdl_b200_set_tuning(int(leaf_size), int(block_threads), modes[traversal])
     if status != 0:
         raise ValueError("leaf_size must be in [0, 32] and block_threads one of 64, 128, 256")

@@ -119,6 +119,32 @@ def test_clustered_frn_3d_matches_oracle(gpu, k_max):
     assert (counts > k_max).any()
 
 
+@pytest.mark.parametrize("traversal", ["packet", "packet_cube", "lane", "packet_points"])
+def test_every_traversal_matches_oracle(gpu, traversal):
+    """Each collect traversal of the tuning knob, on FP32-exact clustered
+    points and on FP64 inputs (every candidate takes the exact band test)."""
+    rng = np.random.default_rng(31)
+    centres = rng.random((12, 3))
+    s = _cols(_clustered(rng, 30000, centres))
+    q = _cols(_clustered(rng, 5000, centres))
+    s64 = _cols(0.25 + rng.random((6000, 3)) * 0.5)
+    q64 = _cols(0.25 + rng.random((1500, 3)) * 0.5)
+    rt.set_tuning(traversal=traversal)
+    try:
+        for search, query, radius, k_max in ((s, q, 0.01, 64), (s64, q64, 0.05, 12)):
+            with rt.B200Scene(_pack(search)) as scene:
+                view, overflow = scene.query(_pack(query), predicate="fixed_radius_neighbors", radius=radius,
+                                             limit=k_max, with_overflow=True)
+                got = view.to_numpy()
+                view.close()
+            exp, counts = O.fixed_radius_neighbors(query, search, radius=radius, k_max=k_max, threads=8,
+                                                   with_counts=True)
+            _assert_same_rows(got, exp, False)
+            assert np.array_equal(overflow.astype(bool), counts > k_max)
+    finally:
+        rt.set_tuning()
+
+
 def test_bounded_knn_and_knn_3d_match_oracle(gpu):
     rng = np.random.default_rng(5)
     centres = rng.random((8, 3))

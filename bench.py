@@ -936,8 +936,8 @@ def main(argv=None) -> int:
         dom, dom_kernel, dom_ms, dom_bytes = ("k_collect_packet (packet LBVH walk, FP32 test + FP64 band)",
                                               "k_collect_packet", traverse_ms, traverse_bytes)
     else:
-        dom, dom_kernel, dom_ms, dom_bytes = ("k_emit_lanes + k_emit_warp (exact FP64 sort and row emission)",
-                                              "k_emit_lanes", emit_ms, emit_bytes)
+        dom, dom_kernel, dom_ms, dom_bytes = ("k_emit + k_emit_list (exact FP64 sort and row emission)",
+                                              "k_emit", emit_ms, emit_bytes)
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     traffic = measured_traffic(dom_kernel, "clustered_3d_fixed_radius", N_PROBE, N_BUILD)
     phase_bytes = N_PROBE * 16 + N_BUILD * 16 + R * 16 + N_PROBE * 4 + N_PROBE // 8

@@ -90,6 +90,12 @@ def test_set_tuning_bounds():
         rt.set_tuning(leaf_size=33, block_threads=128)
     with pytest.raises(ValueError):
         rt.set_tuning(leaf_size=8, block_threads=96)
+    with pytest.raises(ValueError, match="traversal"):
+        rt.set_tuning(traversal="packet_pairs")
+    from rtdl_b200 import _native as nat
+    assert nat.load_library().rtdl_b200_set_tuning(0, 128, 4) != 0  # traversal codes are 0..3
+    for mode in ("packet", "lane", "packet_cube", "packet_points"):
+        rt.set_tuning(traversal=mode)
     rt.set_tuning(leaf_size=8, block_threads=128)
     rt.set_tuning()  # back to the defaults: leaf size by the scene's use
 

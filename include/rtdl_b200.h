@@ -543,9 +543,9 @@ RTDL_B200_API int rtdl_b200_update_fixed_radius_ranked_summary_aggregate_batch_g
 RTDL_B200_API void rtdl_b200_destroy_fixed_radius_ranked_summary_aggregate_batch_graph_3d(void* graph);
 
 /* Result record of rtdl_b200_scene_directed_hausdorff_noalloc (device memory).
- * status: 0 = ok, 1 = a coordinate is non-finite or beyond 1e18, 2 = the
- * traversal stack overflowed, 3 = a radix-sort wait of the scene build ran out
- * (the scene is not valid). */
+ * status: 0 = ok, 1 = a coordinate is non-finite or beyond 1e18, 3 = a
+ * radix-sort wait of the scene build ran out (the scene is not valid).  The
+ * value 2 is not used (the nearest walk is stackless and cannot overflow). */
 typedef struct RtdlB200Witness {
   double distance;
   uint32_t source_id, target_id;
@@ -600,7 +600,9 @@ RTDL_B200_API int rtdl_b200_get_launch_count(unsigned long long* count_out);
  * or 256; traversal: 0 = one warp walks the tree for 32 neighbouring queries
  * (packet), 1 = one thread per query, 2 = packet with the query's bounding
  * cube tested at internal nodes, 3 = packet whose leaf buckets are tested
- * point-major (a lane per point, the reaching queries in turn).  Returns 0 on
+ * point-major (a lane per point, the reaching queries in turn), 4 = packet
+ * choosing lane- or point-major per bucket (point-major when at most half as
+ * many of the packet's queries reach it as it holds points).  Returns 0 on
  * success. */
 RTDL_B200_API int rtdl_b200_set_tuning(int leaf_size, int block_threads, int traversal);
 

@@ -30,9 +30,55 @@ std::atomic<unsigned long long> g_launches{0};
 void count_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 unsigned long long launches_counted() { return g_launches.load(std::memory_order_relaxed); }
 
-Tuning& tuning() {
+void check_launch(int n, const char* file, int line) {
+  count_launches(n);
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return;
+  const char* base = std::strrchr(file, '/');
+  throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e) + " at kernel launch (" +
+                           (base ? base + 1 : file) + ":" + std::to_string(line) + ")");
+}
+
+namespace {
+thread_local std::string g_cleanup_error;
+
+std::mutex& tuning_mutex() {
+  static std::mutex m;
+  return m;
+}
+Tuning& tuning_global() {
   static Tuning t;
   return t;
+}
+Tuning tuning_copy() {
+  std::lock_guard<std::mutex> g(tuning_mutex());
+  return tuning_global();
+}
+thread_local Tuning g_tuning_snapshot;
+thread_local int g_tuning_depth = 0;
+}  // namespace
+
+void note_cleanup_error(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();  // consumed here: a later launch check must not report it
+  if (g_cleanup_error.empty())
+    g_cleanup_error = std::string("CUDA error: ") + cudaGetErrorString(e) + " at " + what;
+}
+
+TuningScope::TuningScope() : outer(g_tuning_depth == 0) {
+  if (outer) g_tuning_snapshot = tuning_copy();
+  ++g_tuning_depth;
+}
+TuningScope::~TuningScope() { --g_tuning_depth; }
+
+const Tuning& tuning() {
+  if (g_tuning_depth == 0) g_tuning_snapshot = tuning_copy();  // outside an entry point: the current setting
+  return g_tuning_snapshot;
+}
+
+void set_tuning(const Tuning& t) {
+  std::lock_guard<std::mutex> g(tuning_mutex());
+  tuning_global() = t;
 }
 
 void ensure_pool_configured(int device) {
@@ -60,7 +106,7 @@ void* dev_alloc(size_t bytes, cudaStream_t s) {
 }
 
 void dev_free(void* p, cudaStream_t s) {
-  if (p) cudaFreeAsync(p, s);
+  if (p) note_cleanup_error(cudaFreeAsync(p, s), "cudaFreeAsync");
 }
 
 namespace {
@@ -71,7 +117,7 @@ thread_local std::vector<std::pair<const char*, double>> g_last_timings;
 
 PhaseTimer::PhaseTimer(cudaStream_t s) : stream(s) {}
 PhaseTimer::~PhaseTimer() {
-  for (auto& m : marks) cudaEventDestroy(m.second);
+  for (auto& m : marks) note_cleanup_error(cudaEventDestroy(m.second), "cudaEventDestroy");
 }
 void PhaseTimer::mark(const char* name) {
   cudaEvent_t e;
@@ -129,7 +175,7 @@ class PinnedPool {
     const size_t sz = it->second;
     live_.erase(it);
     if (cached_ + sz > limit()) {
-      cudaFreeHost(p);
+      note_cleanup_error(cudaFreeHost(p), "cudaFreeHost");
     } else {
       free_.emplace(sz, p);
       cached_ += sz;
@@ -177,20 +223,37 @@ void set_error(const char* msg, char* error_out, size_t error_size) {
   error_out[error_size - 1] = '\0';
 }
 
+// Every entry point runs through here: the thread's last runtime error is
+// cleared first (an error left by earlier, unrelated runtime calls on this
+// thread is not this call's), the call runs with one tuning snapshot, and a
+// cleanup error that nothing else reported fails the call.
 template <typename Fn>
 int guarded(Fn&& fn, char* error_out, size_t error_size) {
+  TuningScope scope;
   try {
     if (error_out && error_size) error_out[0] = '\0';
+    if (scope.outer) {
+      cudaGetLastError();
+      g_cleanup_error.clear();
+    }
     fn();
+    if (scope.outer && !g_cleanup_error.empty()) {
+      set_error(g_cleanup_error.c_str(), error_out, error_size);
+      g_cleanup_error.clear();
+      return 1;
+    }
     return 0;
   } catch (const std::exception& ex) {
     set_error(ex.what(), error_out, error_size);
+    if (scope.outer) g_cleanup_error.clear();
     return 1;
   } catch (...) {
     set_error("unknown native error", error_out, error_size);
+    if (scope.outer) g_cleanup_error.clear();
     return 1;
   }
 }
+
 
 size_t record_size(int dim) { return dim == 3 ? sizeof(RtdlPoint3D) : sizeof(RtdlPoint); }
 
@@ -254,12 +317,12 @@ void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim,
     *rows_out = host;
     *row_count_out = (size_t)r.rows;
   } catch (...) {
-    cudaStreamSynchronize(aux_stream());
+    sync_quietly(aux_stream());
     dev_free(d_rows, s);
     destroy_scene(sc);
     dev_free(d_search, s);
     dev_free(d_query, s);
-    cudaStreamSynchronize(s);
+    sync_quietly(s);
     throw;
   }
   dev_free(d_rows, s);
@@ -311,10 +374,12 @@ int rtdl_b200_set_device(int device) {
 int rtdl_b200_set_tuning(int leaf_size, int block_threads, int traversal) {
   if (leaf_size < 0 || leaf_size > 32) return 1;
   if (block_threads != 64 && block_threads != 128 && block_threads != 256) return 1;
-  if (traversal < 0 || traversal > 3) return 1;
-  tuning().leaf_size = leaf_size;
-  tuning().block_threads = block_threads;
-  tuning().traversal = traversal;
+  if (traversal < 0 || traversal > 4) return 1;
+  Tuning t;
+  t.leaf_size = leaf_size;
+  t.block_threads = block_threads;
+  t.traversal = traversal;
+  set_tuning(t);
   return 0;
 }
 
@@ -412,9 +477,9 @@ int rtdl_b200_run_fixed_radius_neighbors_device(const void* query_points_dev, si
       timer.publish();
       *row_count_out = (size_t)r.rows;
     } catch (...) {
-      cudaStreamSynchronize(aux_stream());
+      sync_quietly(aux_stream());
       destroy_scene(sc);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
   }, error_out, error_size);
@@ -508,7 +573,7 @@ int scene_create_impl(const void* points, size_t count, int dimension, int point
     } catch (...) {
       destroy_scene(sc);
       dev_free(owned, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(owned, s);
@@ -568,7 +633,7 @@ int rtdl_b200_scene_query(void* scene, const void* query_points, size_t query_co
       dev_free(d_rows, s);
       dev_free(d_query, s);
       dev_free(d_overflow, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(d_rows, s);
@@ -631,7 +696,7 @@ int rtdl_b200_batch_create(const void* points, const unsigned long long* point_o
     } catch (...) {
       destroy_scene(sc);
       dev_free(owned, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(owned, s);
@@ -679,7 +744,7 @@ int rtdl_b200_batch_fixed_radius_neighbors(void* batch, const void* query_points
       dev_free(d_rows, s);
       dev_free(d_query, s);
       dev_free(d_overflow, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(d_rows, s);
@@ -769,7 +834,7 @@ int rtdl_b200_scene_directed_hausdorff(void* scene, const void* query_points, si
       dev_free(d_query, s);
       dev_free(d_nd, s);
       dev_free(d_ni, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(d_query, s);
@@ -907,7 +972,7 @@ int rtdl_b200_run_prepared_ranked_fixed_radius_neighbor_summaries_3d(
     } catch (...) {
       dev_free(d_sum, s);
       dev_free(d_query, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(d_sum, s);
@@ -935,7 +1000,7 @@ int rtdl_b200_aggregate_prepared_ranked_fixed_radius_neighbor_summaries_3d(
       timer.publish();
     } catch (...) {
       dev_free(d_query, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(d_query, s);
@@ -968,7 +1033,7 @@ int rtdl_b200_queries_create(const void* points, size_t count, int dimension, in
       throw_if_bad(bad);
     } catch (...) {
       if (pq) destroy_query_set(pq); else dev_free(owned, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     *queries_out = pq;
@@ -1199,7 +1264,7 @@ int rtdl_b200_run_fixed_radius_count_threshold(const RtdlPoint* query_points, si
       destroy_scene(sc);
       dev_free(d_search, s);
       dev_free(d_query, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     destroy_scene(sc);
@@ -1267,7 +1332,7 @@ int rtdl_b200_run_prepared_fixed_radius_count_threshold_2d(void* prepared, const
       count_rows_to_host(sc, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, rows_out, row_count_out, s);
     } catch (...) {
       dev_free(d_query, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(d_query, s);
@@ -1301,7 +1366,7 @@ int rtdl_b200_write_prepared_fixed_radius_count_threshold_2d_device_query_column
       run_count_threshold(sc, recs, (uint32_t)query_count, radius, (uint32_t)threshold, out, s);
     } catch (...) {
       dev_free(recs, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(recs, s);
@@ -1331,7 +1396,7 @@ int rtdl_b200_count_prepared_fixed_radius_threshold_reached_2d(void* prepared, c
       run_count_threshold(sc, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, out, s);
     } catch (...) {
       dev_free(d_query, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(d_query, s);
@@ -1370,7 +1435,7 @@ int rtdl_b200_run_prepared_fixed_radius_nearest_witness_2d(void* prepared, const
     } catch (...) {
       dev_free(d_rows, s);
       dev_free(d_query, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(d_rows, s);
@@ -1424,7 +1489,7 @@ int rtdl_b200_write_prepared_fixed_radius_count_threshold_3d_device_outputs(
         run_count_threshold(sc, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, out, s);
     } catch (...) {
       dev_free(d_query, s);
-      cudaStreamSynchronize(s);
+      sync_quietly(s);
       throw;
     }
     dev_free(d_query, s);
@@ -1456,7 +1521,7 @@ void with_queries(PointGroupScene* pg, const RtdlPoint* query_points, size_t que
     fn(d_query, s);
   } catch (...) {
     dev_free(d_query, s);
-    cudaStreamSynchronize(s);
+    sync_quietly(s);
     throw;
   }
   dev_free(d_query, s);

@@ -22,14 +22,25 @@ namespace rtdl_b200 {
   } while (0)
 
 // Counts kernel launches made by this library (reported by
-// rtdl_b200_get_launch_count) and checks the launch status.
+// rtdl_b200_get_launch_count) and checks the launch status right after the
+// launch.  Every entry point clears the thread's last runtime error before it
+// starts and every cleanup call consumes its own, so an error reported here
+// belongs to the launch at `file:line` (the message names it).
 void count_launches(int n);
 unsigned long long launches_counted();
-#define RTDL_LAUNCHED(n)                              \
-  do {                                                \
-    ::rtdl_b200::count_launches(n);                   \
-    RTDL_CUDA_CHECK(cudaGetLastError());              \
-  } while (0)
+void check_launch(int n, const char* file, int line);
+#define RTDL_LAUNCHED(n) ::rtdl_b200::check_launch((n), __FILE__, __LINE__)
+
+// A runtime error met while releasing resources (cudaFreeAsync, event
+// destruction) is consumed at once, so it cannot surface at an unrelated later
+// check, and kept for the entry point, which reports it as the call's error
+// when nothing failed before it.
+void note_cleanup_error(cudaError_t e, const char* what);
+// Synchronizes a stream on an error path or in a destructor: the original
+// exception is the one reported, so a failure here is only consumed.
+inline void sync_quietly(cudaStream_t s) {
+  if (cudaStreamSynchronize(s) != cudaSuccess) cudaGetLastError();
+}
 
 constexpr int kSmCount = 148;          // B200: 2 dies x 74 SMs
 constexpr int kMaxList = 64;           // per-query list capacity held in shared memory
@@ -147,9 +158,18 @@ struct Tuning {
   int block_threads = 128;
   int traversal = 0;  // fixed-radius collect: 0 = one warp per 32 queries (packet), 1 = one thread per
                       // query, 2 = packet with cube tests at internal nodes, 3 = packet with
-                      // point-major leaf tests
+                      // point-major leaf tests, 4 = packet choosing lane- or point-major per leaf
 };
-Tuning& tuning();
+// The tuning a call runs with: a copy of the process-wide setting taken when
+// the entry point starts (rtdl_b200_set_tuning from another thread changes the
+// next call, never one in progress).
+const Tuning& tuning();
+void set_tuning(const Tuning& t);
+struct TuningScope {  // takes the calling thread's snapshot for one entry point
+  TuningScope();
+  ~TuningScope();
+  bool outer;
+};
 
 // ---- phase timing (CUDA events, read after the call's final sync) ----------
 struct PhaseTimer {

@@ -786,8 +786,8 @@ void destroy_scene(Scene* sc) {
   dev_free(sc->prob_stats, s);
   dev_free(sc->prob_root, s);
   if (sc->own_stream && s) {
-    cudaStreamSynchronize(s);
-    cudaStreamDestroy(s);
+    sync_quietly(s);
+    note_cleanup_error(cudaStreamDestroy(s), "cudaStreamDestroy");
   }
   delete sc;
 }

@@ -669,7 +669,13 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
 // one scene): each warp walks its problem's subtree with its problem's bands
 // and kmax; kept out of the single-problem instantiation, whose registers it
 // would cost.
-template <bool STATS, bool CUBE, bool BATCH, int MIN_BLOCKS, bool PM = false>
+// LEAF: how a reached leaf bucket is tested -- 0 lane-major (collect_leaf:
+// every lane loops over the bucket's points), 1 point-major (collect_leaf_pm:
+// the warp loops over the reaching queries), 2 either, chosen per bucket
+// (warp-uniform): point-major when at most kHybridRatio reaching queries per
+// point, i.e. when few of the packet's spheres reach the bucket.
+constexpr int kLeafLaneMajor = 0, kLeafPointMajor = 1, kLeafHybrid = 2;
+template <bool STATS, bool CUBE, bool BATCH, int MIN_BLOCKS, int LEAF = kLeafLaneMajor>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParams P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!__any_sync(0xffffffffu, t < P.nq)) return;  // whole warp past the end
@@ -717,7 +723,8 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParam
         continue;
       }
       const int first = leaf_first(hit), cnt = leaf_count(hit);
-      if (PM) {
+      const bool pm = LEAF == kLeafPointMajor || (LEAF == kLeafHybrid && 2 * __popc(reach) <= cnt);
+      if (pm) {
         collect_leaf_pm<STATS>(P, B, scene_inexact, L, t & ~31u, (int)(threadIdx.x & 31), first, cnt, reach);
       } else {
         if (STATS) {
@@ -2525,8 +2532,11 @@ void launch_collect(const CollectParams& C, uint32_t np, uint32_t nq, bool batch
     if (batch)  // several problems (traversal counters are not gathered here)
       k_collect_packet<false, false, true, 5><<<grid, threads, 0, s>>>(C);
     else if (tuning().traversal == 3)
-      stats ? k_collect_packet<true, false, false, 1, true><<<grid, threads, 0, s>>>(C)
-            : k_collect_packet<false, false, false, 6, true><<<grid, threads, 0, s>>>(C);
+      stats ? k_collect_packet<true, false, false, 1, kLeafPointMajor><<<grid, threads, 0, s>>>(C)
+            : k_collect_packet<false, false, false, 6, kLeafPointMajor><<<grid, threads, 0, s>>>(C);
+    else if (tuning().traversal == 4)
+      stats ? k_collect_packet<true, false, false, 1, kLeafHybrid><<<grid, threads, 0, s>>>(C)
+            : k_collect_packet<false, false, false, 6, kLeafHybrid><<<grid, threads, 0, s>>>(C);
     else if (stats)
       cube ? k_collect_packet<true, true, false, 1><<<grid, threads, 0, s>>>(C)
            : k_collect_packet<true, false, false, 1><<<grid, threads, 0, s>>>(C);
@@ -2902,7 +2912,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       if (timer) timer->mark("summarize");
     }
   } catch (...) {
-    cudaStreamSynchronize(s);
+    sync_quietly(s);
     dev_free(summary_rows, s);
     cleanup();
     throw;
@@ -3013,7 +3023,7 @@ void count_walk(Scene* sc, const void* queries_dev, uint32_t nq, double radius, 
     check_readback(*rb);
     if (out.reached_host) *out.reached_host = rb->rows;
   } catch (...) {
-    cudaStreamSynchronize(s);
+    sync_quietly(s);
     dev_free(reached, s);
     free_prep(qp, s);
     throw;
@@ -3078,7 +3088,7 @@ PointGroupScene* point_group_create(const RtdlPoint* points, size_t count, const
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors stay alive until the copies are done
     throw_if_bad(bad);
   } catch (...) {
-    cudaStreamSynchronize(s);
+    sync_quietly(s);
     dev_free(d_pts, s);
     point_group_destroy(pg);
     throw;
@@ -3181,7 +3191,7 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
   try {
     pq = prepare_query_set(q, in.nq, in.dim, aux);
   } catch (...) {
-    cudaStreamSynchronize(aux);
+    sync_quietly(aux);
     throw;
   }
   RTDL_CUDA_CHECK(cudaEventRecord(ev_ready, aux));
@@ -3535,8 +3545,8 @@ void summary_graph_destroy(SummaryGraph* g) {
   for (void* p : g->buffers) dev_free(p, g->stream);
   dev_free(g->rows, g->stream);
   if (g->stream) {
-    cudaStreamSynchronize(g->stream);
-    cudaStreamDestroy(g->stream);
+    sync_quietly(g->stream);
+    note_cleanup_error(cudaStreamDestroy(g->stream), "cudaStreamDestroy");
   }
   if (g->agg_host) cudaFreeHost(g->agg_host);
   if (g->status_host) cudaFreeHost(g->status_host);
@@ -3622,6 +3632,27 @@ QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec&
                           overflow_dev, s, timer, &bs);
 }
 
+// The list kernels take their per-lane lists in dynamic shared memory
+// (block_threads x list length x 8 B, at most kMaxList x 256 x 8 = 128 KiB).
+// The limit a launch may ask for is a per-function attribute of each device:
+// it is raised once per device to that largest size, never per launch, so
+// concurrent calls with different k cannot lower it under one another.
+void ensure_pass1_shared_memory() {
+  static std::mutex m;
+  static std::vector<bool> done;
+  int dev = 0;
+  RTDL_CUDA_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(m);
+  if ((int)done.size() <= dev) done.resize(dev + 1, false);
+  if (done[dev]) return;
+  const int most = kMaxList * 256 * 8;
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+  done[dev] = true;
+}
+
 QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius, uint32_t limit,
                       void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
                       PhaseTimer* timer) {
@@ -3700,10 +3731,8 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
         P.stats = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * kStatCount, s));
         RTDL_CUDA_CHECK(cudaMemsetAsync(P.stats, 0, sizeof(unsigned long long) * kStatCount, s));
       }
-      auto launch = [&](auto kernel) {
-        RTDL_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        kernel<<<blocks, threads, shm, s>>>(P);
-      };
+      ensure_pass1_shared_memory();
+      auto launch = [&](auto kernel) { kernel<<<blocks, threads, shm, s>>>(P); };
       if (knn) {
         if (stats) launch(k_pass1<true, true>);
         else launch(k_pass1<true, false>);
@@ -3774,7 +3803,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
     if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
   } catch (...) {
-    cudaStreamSynchronize(s);
+    sync_quietly(s);
     cleanup();
     throw;
   }
@@ -3891,7 +3920,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::
 // Converts the reduced witness into the public record and folds in the
 // input checks, so the call never needs a host round trip.
 __global__ void k_noalloc_finish(const Witness* best, const PointStats* scene_stats, const PointStats* query_stats,
-                                 const unsigned int* error, RtdlB200Witness* out) {
+                                 RtdlB200Witness* out) {
   if (threadIdx.x != 0) return;
   RtdlB200Witness w;
   unsigned long long db = best->dist;
@@ -3899,7 +3928,7 @@ __global__ void k_noalloc_finish(const Witness* best, const PointStats* scene_st
   w.source_id = best->qid;
   w.target_id = best->nid;
   const unsigned int bad = scene_stats->bad | query_stats->bad;
-  w.status = (bad & kBadSortWait) ? 3u : bad ? 1u : ((*error & 1u) ? 2u : 0u);
+  w.status = (bad & kBadSortWait) ? 3u : bad ? 1u : 0u;
   w.reserved = 0u;
   *out = w;
 }
@@ -3980,7 +4009,7 @@ void run_directed_hausdorff_noalloc(Scene* sc, const void* queries_dev, uint32_t
   k_nearest_reduce<<<blocks, 256, 0, s>>>(sc->view(), qpts, static_cast<const double*>(queries_dev), P.qstride, nq,
                                           temp, nearest_dist_dev, nearest_id_dev, partial);
   k_witness_final<<<1, 32, 0, s>>>(partial, (int)blocks, best);
-  k_noalloc_finish<<<1, 32, 0, s>>>(best, sc->stats, qst, small + 1, witness_dev);
+  k_noalloc_finish<<<1, 32, 0, s>>>(best, sc->stats, qst, witness_dev);
   RTDL_LAUNCHED(3);
 }
 

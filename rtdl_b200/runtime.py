@@ -27,6 +27,7 @@ import numpy as np
 
 from . import _native
 from . import dsl
+from .lowering import _is_plan, lower_to_b200_plan
 
 NEIGHBOR_PREDICATES = ("fixed_radius_neighbors", "bounded_knn_rows", "knn_rows")
 PREDICATE_CODE = {"fixed_radius_neighbors": 0, "bounded_knn_rows": 1, "knn_rows": 2}
@@ -317,14 +318,6 @@ def _validate_kernel(compiled) -> None:
         raise ValueError("RTDL CPU simulator requires a fully compiled kernel with traverse/refine/emit")
 
 
-def _layout_dimension(geometry_input) -> int:
-    layout = geometry_input.layout
-    names = set(layout.field_names())
-    if layout.name.endswith("3D") or "z" in names:
-        return 3
-    return 2
-
-
 def _check_inputs(expected, inputs, label="RTDL b200"):
     missing = [n for n in expected if n not in inputs]
     unexpected = [n for n in inputs if n not in expected]
@@ -334,38 +327,49 @@ def _check_inputs(expected, inputs, label="RTDL b200"):
         raise ValueError(f"unexpected {label} inputs: {', '.join(sorted(unexpected))}")
 
 
-def _call_packed(compiled, packed: dict) -> B200RowView:
-    pred = compiled.refine_op.predicate
-    query = packed[compiled.candidates.left.name]
-    search = packed[compiled.candidates.right.name]
-    if pred.name == "knn_rows":
-        return knn_rows(query, search, k=int(pred.options["k"]))
-    return fixed_radius_neighbors(query, search, radius=float(pred.options["radius"]), k_max=int(pred.options["k_max"]),
-                                  ranked=pred.name == "bounded_knn_rows")
+def _call_plan(plan, packed: dict) -> B200RowView:
+    """Executes a lowered plan: the plan's query/search binding, predicate and options reach the C ABI."""
+    query = packed[plan.query_input]
+    search = packed[plan.search_input]
+    opts = plan.predicate_options
+    if plan.predicate == "knn_rows":
+        return knn_rows(query, search, k=int(opts["k"]))
+    return fixed_radius_neighbors(query, search, radius=float(opts["radius"]), k_max=int(opts["k_max"]),
+                                  ranked=plan.predicate == "bounded_knn_rows")
+
+
+def _lower(kernel_fn_or_compiled_or_plan):
+    """A B200ExecutionPlan for a kernel function, a compiled kernel or a plan
+    (the reference's RTExecutionPlan or this backend's); kernels are checked
+    with the runner's messages first (src/rtdsl/runtime.py:145-149)."""
+    if _is_plan(kernel_fn_or_compiled_or_plan):
+        return lower_to_b200_plan(kernel_fn_or_compiled_or_plan)
+    compiled = _resolve_kernel(kernel_fn_or_compiled_or_plan)
+    _validate_kernel(compiled)
+    pred = compiled.refine_op.predicate.name
+    if pred not in NEIGHBOR_PREDICATES:
+        raise ValueError(f"unsupported predicate for b200 backend: {pred!r}")
+    return lower_to_b200_plan(compiled)
 
 
 class PreparedB200Kernel:
-    """Compiled-once handle; mirrors ``PreparedOptixKernel`` for the neighbor predicates."""
+    """Compiled-once handle; mirrors ``PreparedOptixKernel`` for the neighbor predicates.  It holds the
+    kernel's B200ExecutionPlan (``.plan``), which every run executes."""
 
     def __init__(self, kernel_fn_or_compiled):
-        compiled = _resolve_kernel(kernel_fn_or_compiled)
-        _validate_kernel(compiled)
-        pred = compiled.refine_op.predicate.name
-        if pred not in NEIGHBOR_PREDICATES:
-            raise ValueError(f"unsupported predicate for b200 backend: {pred!r}")
-        self.compiled = compiled
-        self.expected_inputs = {item.name: item for item in compiled.inputs}
-        self.predicate_name = pred
+        self.plan = _lower(kernel_fn_or_compiled)
+        self.compiled = None if _is_plan(kernel_fn_or_compiled) else _resolve_kernel(kernel_fn_or_compiled)
+        self.expected_inputs = {name: self.plan.dimension for name in self.plan.input_names}
+        self.predicate_name = self.plan.predicate
         _native.load_library()
 
     def bind(self, **inputs) -> "PreparedB200Execution":
         _check_inputs(self.expected_inputs, inputs)
         packed = {}
         for name, payload in inputs.items():
-            dim = _layout_dimension(self.expected_inputs[name])
-            _addr, _n, _d, keep = _pack_any(payload, dim)
+            _addr, _n, _d, keep = _pack_any(payload, self.expected_inputs[name])
             packed[name] = keep
-        return PreparedB200Execution(self.compiled, packed)
+        return PreparedB200Execution(self.plan, packed)
 
     def run(self, **inputs) -> tuple:
         return self.bind(**inputs).run()
@@ -373,22 +377,22 @@ class PreparedB200Kernel:
 
 @dataclass
 class PreparedB200Execution:
-    compiled: object
+    plan: object
     packed_inputs: dict
 
     def run_raw(self) -> B200RowView:
-        return _call_packed(self.compiled, self.packed_inputs)
+        return _call_plan(self.plan, self.packed_inputs)
 
     def run(self) -> tuple:
         view = self.run_raw()
         try:
-            return _project(self.compiled, view)
+            return _project(self.plan.emit_fields, view)
         finally:
             view.close()
 
 
-def _project(compiled, view: B200RowView) -> tuple:
-    fields = tuple(compiled.emit_op.fields)
+def _project(fields, view: B200RowView) -> tuple:
+    fields = tuple(fields)
     missing = [f for f in fields if f not in view.field_names]
     if missing:
         raise ValueError("b200 row is missing emitted fields: " + ", ".join(missing))
@@ -402,20 +406,18 @@ def prepare_b200(kernel_fn_or_compiled) -> PreparedB200Kernel:
 def run_b200(kernel_fn_or_compiled, *, result_mode: str = "dict", **inputs):
     """Execute a neighbor kernel on the B200 backend (mirrors ``run_optix``).
 
+    Takes an ``@rt.kernel`` function, a compiled kernel, or an execution plan
+    (the reference's ``RTExecutionPlan`` or a ``B200ExecutionPlan``); a kernel
+    is lowered to its plan first and the plan executes.
     ``result_mode="dict"`` returns ``tuple[dict, ...]`` projected onto the
     kernel's emitted fields; ``"raw"`` returns a ``B200RowView`` the caller
     closes.
     """
-    compiled = _resolve_kernel(kernel_fn_or_compiled)
-    _validate_kernel(compiled)
-    expected = {item.name: item for item in compiled.inputs}
-    _check_inputs(expected, inputs)
+    plan = _lower(kernel_fn_or_compiled)
+    _check_inputs({name: None for name in plan.input_names}, inputs)
     if result_mode not in {"dict", "raw"}:
         raise ValueError("b200 result_mode must be 'dict' or 'raw'")
-    pred = compiled.refine_op.predicate.name
-    if pred not in NEIGHBOR_PREDICATES:
-        raise ValueError(f"unsupported predicate for b200 backend: {pred!r}")
-    execution = PreparedB200Kernel(compiled).bind(**inputs)
+    execution = PreparedB200Kernel(plan).bind(**inputs)
     return execution.run_raw() if result_mode == "raw" else execution.run()
 
 
@@ -1522,9 +1524,9 @@ def hausdorff_distance(points_a, points_b, *, dimension: int | None = None) -> d
 def set_tuning(*, leaf_size: int = 0, block_threads: int = 128, traversal: str = "packet") -> None:
     """Set the kernel tuning knobs (see ``rtdl_b200_set_tuning``); ``leaf_size`` 0 picks the leaf
     bucket size by the scene's use (24 points for fixed-radius-only scenes, 8 otherwise)."""
-    modes = {"packet": 0, "lane": 1, "packet_cube": 2, "packet_points": 3}
+    modes = {"packet": 0, "lane": 1, "packet_cube": 2, "packet_points": 3, "packet_hybrid": 4}
     if traversal not in modes:
-        raise ValueError("traversal must be 'packet', 'lane', 'packet_cube' or 'packet_points'")
+        raise ValueError("traversal must be 'packet', 'lane', 'packet_cube', 'packet_points' or 'packet_hybrid'")
     status = _native.load_library().rtdl_b200_set_tuning(int(leaf_size), int(block_threads), modes[traversal])
     if status != 0:
         raise ValueError("leaf_size must be in [0, 32] and block_threads one of 64, 128, 256")

@@ -93,8 +93,8 @@ def test_set_tuning_bounds():
     with pytest.raises(ValueError, match="traversal"):
         rt.set_tuning(traversal="packet_pairs")
     from rtdl_b200 import _native as nat
-    assert nat.load_library().rtdl_b200_set_tuning(0, 128, 4) != 0  # traversal codes are 0..3
-    for mode in ("packet", "lane", "packet_cube", "packet_points"):
+    assert nat.load_library().rtdl_b200_set_tuning(0, 128, 5) != 0  # traversal codes are 0..4
+    for mode in ("packet", "lane", "packet_cube", "packet_points", "packet_hybrid"):
         rt.set_tuning(traversal=mode)
     rt.set_tuning(leaf_size=8, block_threads=128)
     rt.set_tuning()  # back to the defaults: leaf size by the scene's use
@@ -174,8 +174,10 @@ def test_register_with_reference_dispatch(monkeypatch):
     import os
     import sys
 
-    ref = os.environ.get("RTDL_REFERENCE_ROOT", "/root/reference")
-    if not Path(ref, "src", "rtdsl").exists():
+    from oracle.oracle import reference_root
+
+    ref = reference_root()
+    if ref is None:
         pytest.skip("reference tree not present")
     monkeypatch.syspath_prepend(str(Path(ref) / "src"))
     rtdsl = importlib.import_module("rtdsl")

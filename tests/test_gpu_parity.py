@@ -119,7 +119,7 @@ def test_clustered_frn_3d_matches_oracle(gpu, k_max):
     assert (counts > k_max).any()
 
 
-@pytest.mark.parametrize("traversal", ["packet", "packet_cube", "lane", "packet_points"])
+@pytest.mark.parametrize("traversal", ["packet", "packet_cube", "lane", "packet_points", "packet_hybrid"])
 def test_every_traversal_matches_oracle(gpu, traversal):
     """Each collect traversal of the tuning knob, on FP32-exact clustered
     points and on FP64 inputs (every candidate takes the exact band test)."""

@@ -63,6 +63,41 @@ def test_noalloc_matches_regular_entry_point_twice(gpu, case):
             assert np.array_equal(d_ids.cpu().numpy().view(np.uint32), exp_ids)
 
 
+def _check_against_regular(scene, queries, stream):
+    import torch
+
+    nq = len(queries)
+    expected, exp_dist, exp_ids = scene.directed_hausdorff(rt.pack_points(records=queries), with_nearest=True)
+    d_queries = _device_records(queries)
+    d_dist = torch.full((nq,), -1.0, dtype=torch.float64, device="cuda")
+    d_ids = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    d_witness = torch.zeros(24, dtype=torch.uint8, device="cuda")
+    status, msg = _noalloc(scene, d_queries, nq, d_dist, d_ids, d_witness, stream)
+    assert status == 0, msg
+    torch.cuda.synchronize()
+    w = _native.RtdlB200Witness.from_buffer_copy(d_witness.cpu().numpy().tobytes())
+    assert w.status == 0
+    assert w.distance == expected["distance"]
+    assert (w.source_id, w.target_id) == (expected["source_id"], expected["target_id"])
+    assert np.array_equal(d_dist.cpu().numpy().view(np.uint64), exp_dist.view(np.uint64))
+    assert np.array_equal(d_ids.cpu().numpy().view(np.uint32), exp_ids)
+
+
+def test_noalloc_large_3d_then_small_2d(gpu):
+    """A smaller call after a larger one on another scene and dimension: the
+    scratch still holds the large call's per-query data past the small call's
+    end and its reduction partials, which the small call must not read."""
+    import torch
+
+    stream = torch.cuda.current_stream().cuda_stream
+    big_q, big_s = workloads.clustered_3d(250_000, 180_000)
+    with rt.B200Scene(rt.pack_points(records=big_s)) as scene:
+        _check_against_regular(scene, big_q, stream)
+    a, b = workloads.hausdorff_2d(3_000)
+    with rt.B200Scene(rt.pack_points(records=b)) as scene:
+        _check_against_regular(scene, a, stream)
+
+
 def test_noalloc_rejects_more_queries_than_its_scratch_holds(gpu):
     import torch
 

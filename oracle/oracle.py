@@ -39,11 +39,24 @@ KNN_ROW_DTYPE = np.dtype(
 _lib = None
 
 
+# Where the reference tree is read from (test infrastructure only: fixture
+# generation, the cross-checks of the CPU tests, and compiling the reference's
+# own oracle).  RTDL_REFERENCE_ROOT names it; when unset, the read-only mount of
+# the build container is tried.  Nothing run on a GPU machine reads it.
+_DEFAULT_REFERENCE_MOUNT = "/root/reference"
+
+
+def reference_root() -> Path | None:
+    """The reference tree, or None when it is not present on this machine."""
+    root = Path(os.environ.get("RTDL_REFERENCE_ROOT") or _DEFAULT_REFERENCE_MOUNT)
+    return root if (root / "src" / "rtdsl").is_dir() else None
+
+
 def build() -> Path:
     """Compile ``libnn_oracle.so`` (and the reference's own oracle when its tree is present)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    ref_root = os.environ.get("RTDL_REFERENCE_ROOT", "/root/reference")
-    if Path(ref_root, "src", "native", "rtdl_oracle.cpp").exists():
+    ref_root = reference_root()
+    if ref_root is not None and (ref_root / "src" / "native" / "rtdl_oracle.cpp").exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={ref_root}"], check=True)
     return LIB_PATH
 
@@ -70,6 +83,10 @@ def _load():
         ctypes.c_int, f64p, u32p,
     ]
     lib.nn_oracle_nearest.restype = ctypes.c_int
+    lib.nn_oracle_rows_grid.argtypes = lib.nn_oracle_rows.argtypes
+    lib.nn_oracle_rows_grid.restype = ctypes.c_int
+    lib.nn_oracle_nearest_grid.argtypes = lib.nn_oracle_nearest.argtypes
+    lib.nn_oracle_nearest_grid.restype = ctypes.c_int
     lib.nn_oracle_free.argtypes = [ctypes.c_void_p]
     lib.nn_oracle_free.restype = None
     _lib = lib
@@ -92,8 +109,9 @@ def _ptr(a, ctype):
     return a.ctypes.data_as(ctypes.POINTER(ctype))
 
 
-def _call_rows(query, search, mode, radius, k, ranked, threads, want_counts):
+def _call_rows(query, search, mode, radius, k, ranked, threads, want_counts, grid=False):
     lib = _load()
+    fn = lib.nn_oracle_rows_grid if grid else lib.nn_oracle_rows
     qid, qx, qy, qz = _columns(query)
     sid, sx, sy, sz = _columns(search)
     if (qz is None) != (sz is None):
@@ -101,7 +119,7 @@ def _call_rows(query, search, mode, radius, k, ranked, threads, want_counts):
     rows_ptr = ctypes.c_void_p()
     count = ctypes.c_size_t()
     counts = np.zeros(len(qid), dtype=np.uint32) if want_counts else None
-    status = lib.nn_oracle_rows(
+    status = fn(
         _ptr(qid, ctypes.c_uint32), _ptr(qx, ctypes.c_double), _ptr(qy, ctypes.c_double), _ptr(qz, ctypes.c_double), len(qid),
         _ptr(sid, ctypes.c_uint32), _ptr(sx, ctypes.c_double), _ptr(sy, ctypes.c_double), _ptr(sz, ctypes.c_double), len(sid),
         mode, float(radius), int(k), int(ranked), int(threads),
@@ -122,9 +140,11 @@ def _call_rows(query, search, mode, radius, k, ranked, threads, want_counts):
     return (rows, counts) if want_counts else rows
 
 
-def fixed_radius_neighbors(query, search, *, radius, k_max, threads=1, ranked=False, with_counts=False):
-    """FRN rows (``reference.py:349-376``); ``ranked=True`` gives bounded_knn_rows (``:406-434``)."""
-    return _call_rows(query, search, 0, radius, k_max, ranked, threads, with_counts)
+def fixed_radius_neighbors(query, search, *, radius, k_max, threads=1, ranked=False, with_counts=False, grid=False):
+    """FRN rows (``reference.py:349-376``); ``ranked=True`` gives bounded_knn_rows (``:406-434``).
+    ``grid=True`` takes the candidates from a uniform grid over the search set instead of every
+    search point (same arithmetic and keys, the same rows; for the full-size sets)."""
+    return _call_rows(query, search, 0, radius, k_max, ranked, threads, with_counts, grid)
 
 
 COUNT_ROW_DTYPE = np.dtype({"names": ["query_id", "neighbor_count", "threshold_reached"],
@@ -276,19 +296,20 @@ def ranked_summaries(query, search, *, radius, k_max, threads=1):
     return out, agg
 
 
-def knn_rows(query, search, *, k, threads=1):
-    """KNN rows (``reference.py:379-403``)."""
-    return _call_rows(query, search, 1, 0.0, k, True, threads, False)
+def knn_rows(query, search, *, k, threads=1, grid=False):
+    """KNN rows (``reference.py:379-403``); ``grid`` as for fixed_radius_neighbors."""
+    return _call_rows(query, search, 1, 0.0, k, True, threads, False, grid)
 
 
-def nearest(query, search, *, threads=1):
+def nearest(query, search, *, threads=1, grid=False):
     """Per-query nearest (distance, neighbor_id) in query-input order (knn_rows with k=1)."""
     lib = _load()
+    fn = lib.nn_oracle_nearest_grid if grid else lib.nn_oracle_nearest
     qid, qx, qy, qz = _columns(query)
     sid, sx, sy, sz = _columns(search)
     dist = np.zeros(len(qid), dtype=np.float64)
     nid = np.zeros(len(qid), dtype=np.uint32)
-    status = lib.nn_oracle_nearest(
+    status = fn(
         _ptr(qid, ctypes.c_uint32), _ptr(qx, ctypes.c_double), _ptr(qy, ctypes.c_double), _ptr(qz, ctypes.c_double), len(qid),
         _ptr(sid, ctypes.c_uint32), _ptr(sx, ctypes.c_double), _ptr(sy, ctypes.c_double), _ptr(sz, ctypes.c_double), len(sid),
         int(threads), _ptr(dist, ctypes.c_double), _ptr(nid, ctypes.c_uint32),

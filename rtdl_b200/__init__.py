@@ -35,6 +35,7 @@ from .dsl import (  # noqa: F401
     traverse,
 )
 from .execution import ExecutionPolicy, ExecutionResult, register_with_rtdsl, run  # noqa: F401
+from .lowering import B200ExecutionPlan, lower_to_b200_plan  # noqa: F401
 from .runtime import (  # noqa: F401
     B200Queries,
     B200RowView,

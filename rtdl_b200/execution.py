@@ -16,7 +16,7 @@ import platform
 from dataclasses import asdict, dataclass, field
 from typing import Any, Mapping
 
-from .runtime import run_b200
+from .runtime import _lower, run_b200
 
 SUPPORTED_BACKENDS = ("b200",)
 
@@ -76,17 +76,16 @@ def run(kernel_fn_or_compiled, inputs: Mapping[str, object] | None = None, *, ex
     policy = execution or ExecutionPolicy()
     merged = dict(inputs or {})
     merged.update(input_kwargs)
-    compiled = kernel_fn_or_compiled if hasattr(kernel_fn_or_compiled, "refine_op") else kernel_fn_or_compiled()
-    rows = run_b200(compiled, result_mode=policy.result_mode, **merged)
-    pred = compiled.refine_op.predicate.name if compiled.refine_op is not None else None
+    plan = _lower(kernel_fn_or_compiled)
+    rows = run_b200(plan, result_mode=policy.result_mode, **merged)
     report = ExecutionReport(
         requested_backend=policy.backend,
         selected_backend="b200",
         primitive_family="nearest_neighbor",
-        predicate=pred,
-        output_schema=tuple(compiled.emit_op.fields) if compiled.emit_op is not None else (),
-        accel_kind="lbvh",
-        exact_mode="fp64_band_recheck",
+        predicate=plan.predicate,
+        output_schema=tuple(plan.emit_fields),
+        accel_kind=plan.accel_kind,
+        exact_mode=plan.exact_refine_mode,
         reproducibility={"python": platform.python_version(), "platform": platform.platform()},
         notes=("Rows from librtdl_b200 (sm_100a); FP32 traversal with FP64 re-decision inside the error band.",),
     )
@@ -114,3 +113,6 @@ def register_with_rtdsl(rtdsl_module=None) -> None:
     _run_selected_backend._rtdl_b200_patched = True
     ex._run_selected_backend = _run_selected_backend
     rtdsl_module.run_b200 = run_b200
+    from .lowering import lower_to_b200_plan
+
+    rtdsl_module.lower_to_b200_plan = lower_to_b200_plan

@@ -1,7 +1,7 @@
 """Writes tests/golden/count_threshold_2d.json with rows from the reference's
 own generic CPU count (run here, where the reference tree exists):
 
-    python tests/golden/make_count_threshold_golden.py /root/reference
+    python tests/golden/make_count_threshold_golden.py <reference tree>
 
 The cases are small seeded 2-D sets (a lattice whose spacing puts points
 exactly on the radius, duplicates, ids out of order) counted by
@@ -61,4 +61,12 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    else:
+        sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
+        from oracle.oracle import reference_root
+
+        if reference_root() is None:
+            raise SystemExit("give the reference tree as the argument or set RTDL_REFERENCE_ROOT")
+        main(str(reference_root()))

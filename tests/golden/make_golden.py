@@ -1,7 +1,8 @@
 """Generate golden fixtures by running the reference's own ``cpu_python_reference``.
 
-Run in a container where the rubaolee/rtdl tree is present (default
-``/root/reference``, override with ``RTDL_REFERENCE_ROOT``)::
+Run in a container where the rubaolee/rtdl tree is present (located by
+``oracle.reference_root()``: ``RTDL_REFERENCE_ROOT``, else the build
+container's read-only mount)::
 
     python tests/golden/make_golden.py
 
@@ -30,7 +31,12 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(os.environ.get("RTDL_REFERENCE_ROOT", "/root/reference"))
+sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
+from oracle.oracle import reference_root  # noqa: E402
+
+REF = reference_root()
+if REF is None:
+    raise SystemExit("the reference tree is not present: set RTDL_REFERENCE_ROOT")
 sys.path.insert(0, str(REF / "src"))
 sys.path.insert(0, str(REF))
 

@@ -1,7 +1,7 @@
 """Writes tests/golden/rtnn_ranked_summary_262144.json from the reference's own
 published ranked-summary report (run here, where the reference tree exists):
 
-    python tests/golden/make_rtnn_golden.py /root/reference
+    python tests/golden/make_rtnn_golden.py <reference tree>
 
 For each distribution it keeps the seed and sizes, the aggregate of the
 reference's CuPy grid opponent and of its OptiX float32 path, and the median
@@ -56,4 +56,12 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    else:
+        sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
+        from oracle.oracle import reference_root
+
+        if reference_root() is None:
+            raise SystemExit("give the reference tree as the argument or set RTDL_REFERENCE_ROOT")
+        main(str(reference_root()))

@@ -1,6 +1,13 @@
-"""Full-size 1,048,576 x 1,048,576 3D clustered workload: properties that do not
-depend on size, plus exact agreement with the oracle on a seeded sample of
-queries against the full build set."""
+"""Full-size workloads of the benchmark: the 1,048,576 x 1,048,576 3D clustered
+sets (fixed radius with k_max 64, and KNN with k = 16) and the 4,194,304 x
+4,194,304 2D Hausdorff sets.  Each complete output is compared with the
+oracle's digest of it (tests/golden/full_scale_digests.json, every row of
+every query), a seeded sample of queries is compared row by row with the
+oracle run here, and the size-independent properties are checked."""
+import hashlib
+import json
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -9,6 +16,24 @@ from oracle import oracle as O
 from rtdl_b200 import workloads
 
 pytestmark = pytest.mark.gpu
+
+DIGESTS = json.loads((Path(__file__).resolve().parent / "golden" / "full_scale_digests.json").read_text())
+
+
+def _sha(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).view(np.uint8).tobytes()).hexdigest()
+
+
+def _first_bad_block(rows, per_q, ref):
+    """The first block of queries whose rows differ from the oracle's (None when all agree)."""
+    offsets = np.zeros(len(per_q) + 1, dtype=np.int64)
+    np.cumsum(per_q, out=offsets[1:])
+    b = ref["block_queries"]
+    for i, want in enumerate(ref["block_sha256_16"]):
+        lo, hi = i * b, min((i + 1) * b, len(per_q))
+        if _sha(rows[offsets[lo]:offsets[hi]])[:16] != want:
+            return lo, hi
+    return None
 
 
 @pytest.fixture(scope="module")
@@ -52,6 +77,12 @@ def test_full_scale_fixed_radius_rows(gpu, clustered):
         assert np.array_equal(got[f], exp[f])
     assert np.array_equal(got["distance"].view(np.uint64), exp["distance"].view(np.uint64))
     assert np.array_equal(overflow[sample].astype(bool), counts > 64)
+    # the complete row set against the oracle's
+    ref = DIGESTS["frn_1m"]
+    assert int(overflow.astype(bool).sum()) == ref["overflow_queries"]
+    assert _sha(per_q.astype(np.uint32)) == ref["counts_sha256"]
+    assert len(rows) == ref["rows"]
+    assert _sha(rows) == ref["rows_sha256"], f"rows differ from the oracle's in queries {_first_bad_block(rows, per_q, ref)}"
 
 
 def test_full_scale_knn16_rows(gpu, clustered):
@@ -68,3 +99,21 @@ def test_full_scale_knn16_rows(gpu, clustered):
     for f in ("query_id", "neighbor_id", "neighbor_rank"):
         assert np.array_equal(got[f], exp[f])
     assert np.array_equal(got["distance"].view(np.uint64), exp["distance"].view(np.uint64))
+    # the complete row set against the oracle's (fields packed without the struct's padding)
+    packed = np.zeros(len(rows), dtype=np.dtype({"names": ["query_id", "neighbor_id", "distance", "neighbor_rank"],
+                                                 "formats": ["<u4", "<u4", "<f8", "<u4"],
+                                                 "offsets": [0, 4, 8, 16], "itemsize": 20}))
+    for f in packed.dtype.names:
+        packed[f] = rows[f]
+    assert _sha(packed) == DIGESTS["knn16_1m"]["rows_packed_sha256"]
+
+
+def test_full_scale_hausdorff_4m(gpu):
+    a, b = workloads.hausdorff_2d()
+    with rt.B200Scene(rt.pack_points(records=b)) as scene:
+        w, dist, nid = scene.directed_hausdorff(rt.pack_points(records=a), with_nearest=True)
+    ref = DIGESTS["hausdorff_4m"]
+    assert _sha(np.asarray(dist, dtype=np.float64)) == ref["nearest_distance_sha256"]
+    assert _sha(np.asarray(nid, dtype=np.uint32)) == ref["nearest_id_sha256"]
+    assert w["distance"] == float.fromhex(ref["witness"]["distance_hex"])
+    assert (w["source_id"], w["target_id"]) == (ref["witness"]["source_id"], ref["witness"]["target_id"])

@@ -97,3 +97,41 @@ def test_oracle_count_threshold_matches_reference_generic_cpu(case):
     assert np.array_equal(got["query_id"], exp[:, 0])
     assert np.array_equal(got["neighbor_count"], exp[:, 1])
     assert np.array_equal(got["threshold_reached"], exp[:, 2])
+
+
+def test_python_restatement_matches_reference_config1_prefix():
+    """The pure-Python restatement (the timed stand-in for cpu_python_reference) against the reference's
+    own config-1 rows, on the first 512 queries (a few seconds of Python)."""
+    from oracle import reference_py
+
+    z = G.load_config1()
+    q, s = G.config1_points()
+    recs = lambda d: np.rec.fromarrays([d["id"], d["x"], d["y"]], names="id,x,y")  # noqa: E731
+    rows = reference_py.fixed_radius_neighbors(reference_py.points(recs(q)[:512]), reference_py.points(recs(s)),
+                                               radius=0.02, k_max=4096)
+    n = int(np.searchsorted(z["query_id"], 512))
+    assert len(rows) == n
+    assert [r["query_id"] for r in rows] == z["query_id"][:n].tolist()
+    assert [r["neighbor_id"] for r in rows] == z["neighbor_id"][:n].tolist()
+    assert np.array_equal(np.array([r["distance"] for r in rows]).view(np.uint64), z["distance"][:n].view(np.uint64))
+
+
+@pytest.mark.parametrize("case", CASES[:12], ids=[c["name"] for c in CASES[:12]])
+def test_python_restatement_matches_reference_case(case):
+    from oracle import reference_py
+
+    dim = case["dimension"]
+    cols = lambda p: G.points_columns(p, dim)  # noqa: E731
+    def recs(d):
+        names = ["id", "x", "y"] + (["z"] if dim == 3 else [])
+        return np.rec.fromarrays([np.asarray(d[n]) for n in names], names=",".join(names))
+    q, s = reference_py.points(recs(cols(case["query_points"]))), reference_py.points(recs(cols(case["search_points"])))
+    opts = case["options"]
+    if case["predicate"] == "knn_rows":
+        rows = reference_py.knn_rows(q, s, k=opts["k"])
+        got = [(r["query_id"], r["neighbor_id"], r["distance"], r["neighbor_rank"]) for r in rows]
+    else:
+        ranked = case["predicate"] == "bounded_knn_rows"
+        rows = reference_py.fixed_radius_neighbors(q, s, radius=opts["radius"], k_max=opts["k_max"], ranked=ranked)
+        got = [(r["query_id"], r["neighbor_id"], r["distance"]) + ((r["neighbor_rank"],) if ranked else ()) for r in rows]
+    assert got == G.expected_rows(case)

@@ -261,32 +261,82 @@ def run_reference_arm(args) -> int:
 # secondary workloads (one GPU): knn k=16 and directed Hausdorff
 # ---------------------------------------------------------------------------
 
-def run_secondary(args) -> int:
+def _hbm_peak():
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def full_scale_digests() -> dict:
+    """Digests of the complete row sets computed by the oracle (tests/golden/full_scale_digests.json)."""
+    try:
+        return json.loads((ROOT / "tests" / "golden" / "full_scale_digests.json").read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def _sha(a) -> str:
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(a).view(np.uint8).tobytes()).hexdigest()
+
+
+def _bits_equal(a, b) -> bool:
+    return bool(np.array_equal(np.asarray(a, dtype=np.float64).view(np.uint64),
+                               np.asarray(b, dtype=np.float64).view(np.uint64)))
+
+
+def frn_exactness(rows: np.ndarray, probe, build, sample_n: int = 512) -> dict:
+    """The headline's rows against the oracle: every row of a seeded sample of queries (ids and FP64
+    distance bits, oracle over the full build set) and the complete row set against the oracle's
+    digest of it.  Probe ids are their input indices, so rows come in probe order."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(99)
+    sample = np.sort(rng.choice(len(probe), sample_n, replace=False))
+    exp = O.fixed_radius_neighbors(probe[sample], build, radius=RADIUS, k_max=K_MAX, threads=os.cpu_count() or 1)
+    starts = np.searchsorted(rows["query_id"], sample, side="left")
+    ends = np.searchsorted(rows["query_id"], sample, side="right")
+    got = np.concatenate([rows[a:b] for a, b in zip(starts, ends)]) if len(sample) else rows[:0]
+    same = (len(got) == len(exp) and np.array_equal(got["query_id"], exp["query_id"])
+            and np.array_equal(got["neighbor_id"], exp["neighbor_id"]) and _bits_equal(got["distance"], exp["distance"]))
+    err = float(np.max(np.abs(got["distance"] - exp["distance"]))) if same and len(exp) else (0.0 if same else None)
+    out = {"sample_queries": int(sample_n), "sample_rows": int(len(exp)), "sample_rows_equal_to_oracle": bool(same),
+           "max_abs_distance_error_vs_fp64_oracle": err}
+    ref = full_scale_digests().get("frn_1m")
+    if ref and len(probe) == N_PROBE == 1 << 20 and len(build) == N_BUILD == 1 << 20:
+        out["full_set_rows"] = int(len(rows))
+        out["full_set_rows_sha256_equal_to_oracle"] = _sha(rows) == ref["rows_sha256"]
+    return out
+
+
+def secondary_leg(workload: str, steps: int, warmup: int) -> dict:
+    """knn k=16 at 1M x 1M 3D, or directed Hausdorff at 4M x 4M 2D: CUDA-event ms per step (scene build +
+    query), rows/s, the query kernel's roofline fraction and exactness against the oracle (a sample of
+    queries, plus the complete output against the oracle's digest)."""
     import torch
 
     import rtdl_b200 as rt
     from oracle import oracle as O
     from rtdl_b200 import _native, workloads
 
-    torch.cuda.set_device(0)
-    rt.set_device(0)
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.Stream(device=dev)
     sh = stream.cuda_stream
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
-    if args.workload == "knn":
+    knn = workload == "knn"
+    if knn:
         probe, build = workloads.clustered_3d()
         k = 16
         units = len(probe) * k
-        metric, unit = "knn rows/s at 1M x 1M 3D, k=16 (exact row set)", "rows/s"
     else:
         probe, build = workloads.hausdorff_2d()
         units = len(probe)
-        metric, unit = "directed Hausdorff nearest rows/s at 4M x 4M 2D (FP64 max-min)", "rows/s"
-    dim = 3 if args.workload == "knn" else 2
+    dim = 3 if knn else 2
     d_build = torch.from_numpy(build.view(np.uint8)).to(dev)
     d_probe = torch.from_numpy(probe.view(np.uint8)).to(dev)
-    rows_buf = torch.empty(units * 24, dtype=torch.uint8, device=dev) if args.workload == "knn" else None
+    rows_buf = torch.empty(units * 24, dtype=torch.uint8, device=dev) if knn else None
     nd = torch.empty(len(probe), dtype=torch.float64, device=dev)
     ni = torch.empty(len(probe), dtype=torch.int32, device=dev)
     result = {}
@@ -294,7 +344,7 @@ def run_secondary(args) -> int:
     def step():
         scene = rt.B200Scene(None, dimension=dim, stream=sh, device_points=(d_build.data_ptr(), len(build)))
         try:
-            if args.workload == "knn":
+            if knn:
                 n = scene.query_device(d_probe.data_ptr(), len(probe), predicate="knn_rows", limit=k,
                                        rows_address=rows_buf.data_ptr(), rows_capacity=units, stream=sh)
                 assert n == units
@@ -306,16 +356,12 @@ def run_secondary(args) -> int:
         finally:
             scene.close()
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
-    sampler = ClockSampler(0)
-    sampler.start()
-    time.sleep(0.3)
     launches0 = _native.launch_count()
-    torch.cuda.synchronize()
     ms, phases = [], []
-    for _ in range(args.steps):
+    for _ in range(steps):
         with torch.cuda.stream(stream):
             flush.zero_()
             a = torch.cuda.Event(enable_timing=True)
@@ -328,44 +374,187 @@ def run_secondary(args) -> int:
         ms.append(a.elapsed_time(b))
     torch.cuda.synchronize()
     launches = _native.launch_count() - launches0
-    clocks = sampler.stop()
     ms_step = sum(ms) / len(ms)
     trav = sum(p.get("traverse", 0.0) for p in phases) / len(phases)
-    # exactness against the FP64 oracle on a seeded sample of queries
+    threads = os.cpu_count() or 1
     rng = np.random.default_rng(99)
     sample = np.sort(rng.choice(len(probe), 256, replace=False))
-    if args.workload == "knn":
-        got = np.frombuffer(rows_buf.cpu().numpy().tobytes(), dtype=rt.runtime.KNN_ROW_DTYPE).reshape(-1, k)[sample]
-        exp = O.knn_rows(probe[sample], build, k=k, threads=os.cpu_count() or 1).reshape(-1, k)
-        ids_equal = bool(np.array_equal(got["neighbor_id"], exp["neighbor_id"]))
+    digests = full_scale_digests()
+    if knn:
+        rows = np.frombuffer(rows_buf.cpu().numpy().tobytes(), dtype=rt.runtime.KNN_ROW_DTYPE)
+        got = rows.reshape(-1, k)[sample]
+        exp = O.knn_rows(probe[sample], build, k=k, threads=threads).reshape(-1, k)
+        ids_equal = bool(np.array_equal(got["neighbor_id"], exp["neighbor_id"])
+                         and np.array_equal(got["neighbor_rank"], exp["neighbor_rank"]))
+        dist_equal = _bits_equal(got["distance"], exp["distance"])
         max_err = float(np.max(np.abs(got["distance"] - exp["distance"])))
         alg_bytes = len(probe) * 16 + len(build) * 16 + units * 24
+        kernel = "k_pass1<KNN> (nearest-list LBVH walk)"
+        full = {}
+        ref = digests.get("knn16_1m")
+        if ref:
+            packed = np.zeros(len(rows), dtype=np.dtype({"names": ["query_id", "neighbor_id", "distance", "neighbor_rank"],
+                                                         "formats": ["<u4", "<u4", "<f8", "<u4"],
+                                                         "offsets": [0, 4, 8, 16], "itemsize": 20}))
+            for n in packed.dtype.names:
+                packed[n] = rows[n]
+            full = {"full_set_rows": int(len(rows)),
+                    "full_set_rows_sha256_equal_to_oracle": _sha(packed) == ref["rows_packed_sha256"]}
+        extra = {"k": k, "rows": units}
     else:
-        dist, nid = O.nearest(probe[sample], build, threads=os.cpu_count() or 1)
-        got_d = nd.cpu().numpy()[sample]
-        ids_equal = bool(np.array_equal(ni.cpu().numpy().view(np.uint32)[sample], nid))
-        max_err = float(np.max(np.abs(got_d - dist)))
+        dist, nid = O.nearest(probe[sample], build, threads=threads)
+        got_d = nd.cpu().numpy()
+        got_i = ni.cpu().numpy().view(np.uint32)
+        ids_equal = bool(np.array_equal(got_i[sample], nid))
+        dist_equal = _bits_equal(got_d[sample], dist)
+        max_err = float(np.max(np.abs(got_d[sample] - dist)))
         alg_bytes = len(probe) * 16 + len(build) * 16 + len(probe) * 12
-    try:
-        hbm_peak = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
-    except Exception:
-        hbm_peak = 6650.0
+        kernel = "k_pass1<KNN> with k = 1 (nearest LBVH walk)"
+        full = {}
+        ref = digests.get("hausdorff_4m")
+        if ref:
+            w = ref["witness"]
+            full = {"full_set_nearest_sha256_equal_to_oracle": _sha(got_d) == ref["nearest_distance_sha256"]
+                    and _sha(got_i) == ref["nearest_id_sha256"],
+                    "witness_equal_to_oracle": (float.fromhex(w["distance_hex"]) == result.get("distance")
+                                                and w["source_id"] == result.get("source_id")
+                                                and w["target_id"] == result.get("target_id"))}
+        extra = {"hausdorff": result, "queries": len(probe)}
+    hbm_peak, peak_note = _hbm_peak()
     achieved = alg_bytes / (trav / 1e3) / 1e9 if trav > 0 else None
-    line = {
-        "metric": metric, "value": units / (ms_step / 1e3), "unit": unit, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 traversal + f64 band recheck and distances", "data": "synthetic",
-        "config": {"workload": args.workload, "build": len(build), "probe": len(probe),
-                   "l2": "flushed between steps (512 MiB write)"},
-        "phases_ms": {k2: sum(p.get(k2, 0.0) for p in phases) / len(phases) for k2 in ("query_prep", "traverse", "scan", "emit", "reduce")},
-        "roofline": {"bound": "hbm", "kernel": "k_pass1 (KNN list traversal)", "achieved": achieved, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": (achieved / hbm_peak) if achieved else None, "traffic": None,
-                     "algorithmic_bytes": alg_bytes},
+    return {
+        "metric": ("knn rows/s at 1M x 1M 3D, k=16 (exact row set)" if knn
+                   else "directed Hausdorff nearest rows/s at 4M x 4M 2D (FP64 max-min)"),
+        "value": units / (ms_step / 1e3), "unit": "rows/s", "ms_per_step": ms_step, "steps": steps, "warmup": warmup,
+        "config": {"workload": workload, "build": len(build), "probe": len(probe),
+                   "l2": "flushed between steps (512 MiB write)", **extra},
+        "phases_ms": {k2: sum(p.get(k2, 0.0) for p in phases) / len(phases)
+                      for k2 in ("build", "query_prep", "traverse", "scan", "emit", "reduce")},
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": (achieved / hbm_peak) if achieved else None, "traffic": None,
+                     "peak_source": peak_note, "algorithmic_bytes": alg_bytes},
         "exactness": {"sample_queries": int(len(sample)), "ids_equal_to_oracle": ids_equal,
-                      "max_abs_distance_error_vs_fp64_oracle": max_err},
-        "hausdorff": result if args.workload == "hausdorff" else None,
+                      "distance_bits_equal_to_oracle": dist_equal,
+                      "max_abs_distance_error_vs_fp64_oracle": max_err, **full},
+        "gpu_launches": launches,
+    }
+
+
+def run_config1(args) -> int:
+    """The reference's CPU-runnable case: 4,096 x 4,096 2D fixed radius (float64 uniform, seed 0, radius
+    0.02, no k_max truncation), rows checked against the reference's own rows (tests/golden), GPU
+    rows/s through the plain C ABI call beside the CPU runners timed here on one core each."""
+    import ctypes
+
+    import torch
+
+    import rtdl_b200 as rt
+    from oracle import oracle as O
+    from oracle import reference_py
+    from rtdl_b200 import _native
+    from rtdl_b200.runtime import FRN_ROW_DTYPE, POINT2D_DTYPE
+
+    torch.cuda.set_device(0)
+    rt.set_device(0)
+    rng = np.random.default_rng(0)
+    b, p = rng.random((4096, 2)), rng.random((4096, 2))
+    build = np.zeros(4096, dtype=POINT2D_DTYPE)
+    probe = np.zeros(4096, dtype=POINT2D_DTYPE)
+    for arr, pts in ((build, b), (probe, p)):
+        arr["id"] = np.arange(4096, dtype=np.uint32)
+        arr["x"], arr["y"] = pts[:, 0], pts[:, 1]
+    radius, k_max = 0.02, 4096
+    lib = _native.load_library()
+
+    def call():
+        rows = ctypes.c_void_p()
+        count = ctypes.c_size_t()
+        err = _native.error_buffer()
+        st = lib.rtdl_b200_run_fixed_radius_neighbors(probe.ctypes.data, 4096, build.ctypes.data, 4096, radius,
+                                                      k_max, ctypes.byref(rows), ctypes.byref(count), err, len(err))
+        _native.check_status(st, err)
+        n = count.value
+        out = np.frombuffer((ctypes.c_char * (n * 16)).from_address(rows.value), dtype=FRN_ROW_DTYPE).copy()
+        lib.rtdl_b200_free_rows(rows)
+        return out
+
+    for _ in range(args.warmup):
+        call()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = _native.launch_count()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rows = call()
+    dt = (time.perf_counter() - t0) / args.steps
+    launches = _native.launch_count() - launches0
+    clocks = sampler.stop()
+    golden = ROOT / "tests" / "golden" / "config1_frn_2d.npz"
+    exact = None
+    if golden.exists():
+        z = np.load(golden)
+        exact = bool(len(rows) == len(z["query_id"]) and np.array_equal(rows["query_id"], z["query_id"])
+                     and np.array_equal(rows["neighbor_id"], z["neighbor_id"])
+                     and _bits_equal(rows["distance"], z["distance"]))
+    # CPU runners on the same input, one core each
+    t = time.perf_counter()
+    py_rows = reference_py.fixed_radius_neighbors(reference_py.points(probe), reference_py.points(build),
+                                                  radius=radius, k_max=k_max)
+    t_py = time.perf_counter() - t
+    t = time.perf_counter()
+    c_rows = O.fixed_radius_neighbors(probe, build, radius=radius, k_max=k_max, threads=1)
+    t_c = time.perf_counter() - t
+    ref = None
+    if O.reference_library_available():
+        pq, pb = O.pack_reference_points(probe), O.pack_reference_points(build)
+        t = time.perf_counter()
+        ref_rows = O.reference_fixed_radius_neighbors(pq, pb, radius=radius, k_max=k_max)
+        t_ref = time.perf_counter() - t
+        ref = {"value": len(ref_rows) / t_ref, "unit": "rows/s", "cores": 1, "kind": "reference",
+               "sample": f"full set, {len(ref_rows)} rows in {t_ref:.3f} s (the reference's native oracle, "
+                         "compiled from its sources)"}
+    line = {
+        "metric": "fixed-radius neighbor rows/s at 4,096 x 4,096 2D (float64, radius 0.02; exact row set)",
+        "value": len(rows) / dt, "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 inputs: f32 traversal + f64 band recheck and distances", "data": "synthetic",
+        "config": {"workload": "config1_frn_2d (rng(0) uniform, 4,096 build then 4,096 probe points)",
+                   "radius": radius, "k_max": k_max, "rows": int(len(rows)),
+                   "timing": "host wall clock around rtdl_b200_run_fixed_radius_neighbors (host records in, "
+                             "rows in host memory out)", "l2": "input far below L2 (latency-bound case)"},
+        "exactness": {"rows_equal_to_reference_rows": exact, "reference_rows": "tests/golden/config1_frn_2d.npz "
+                      "(the reference's cpu_python_reference)"},
+        "cpu_baseline": {"value": len(py_rows) / t_py, "unit": "rows/s", "cores": 1, "kind": "port",
+                         "sample": f"full set, {len(py_rows)} rows in {t_py:.2f} s (oracle/reference_py.py: the "
+                                   "reference's cpu_python_reference algorithm in plain Python)"},
+        "cpu_baselines": {"reference_native_oracle": ref,
+                          "c_port": {"value": len(c_rows) / t_c, "unit": "rows/s", "cores": 1, "kind": "port",
+                                     "sample": f"full set, {len(c_rows)} rows in {t_c:.3f} s (oracle/nn_oracle.c)"}},
+        "e2e": {"value": len(rows) / dt, "unit": "rows/s", "h2d_bytes_per_step": 2 * 4096 * 24,
+                "d2h_bytes_per_step": int(len(rows)) * 16},
         "clocks": clocks, "gpu_launches": launches,
     }
+    print(json.dumps(line))
+    return 0
+
+
+def run_secondary(args) -> int:
+    import torch
+
+    import rtdl_b200 as rt
+
+    torch.cuda.set_device(0)
+    rt.set_device(0)
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    leg = secondary_leg(args.workload, args.steps, args.warmup)
+    clocks = sampler.stop()
+    line = {"metric": leg.pop("metric"), "value": leg.pop("value"), "unit": leg.pop("unit"), "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg.pop("ms_per_step"),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 traversal + f64 band recheck and distances", "data": "synthetic", **leg, "clocks": clocks}
     print(json.dumps(line))
     return 0
 
@@ -552,8 +741,85 @@ def run_batch(args) -> int:
                       "oracle_checked": oracle_checked, "rows_equal_to_oracle": equal_oracle},
         "e2e": None, "cpu_baseline": None, "clocks": clocks, "gpu_launches": launches,
     }
+    if not args.no_graph:
+        del plain_buf, rows_buf
+        torch.cuda.empty_cache()
+        line["graph"] = batch_graph_leg(args, nb, nq, boff, qoff, radius, kmax, d_build, d_probe, stream, flush,
+                                        rows_total, sample, alg, hbm_peak)
+        g = line["graph"]
+        line["speedup_graph_vs_plain"] = plain_ms[0] / g["ms_per_step"]
     print(json.dumps(line))
     return 0
+
+
+def batch_graph_leg(args, nb, nq, boff, qoff, radius, kmax, d_build, d_probe, stream, flush, rows_total, sample,
+                    alg, hbm_peak) -> dict:
+    """All problems answered by one replay of the captured graph over prepared problem batches (one persistent
+    collect launch per batch, nothing read back inside), rows of every problem into one device buffer."""
+    import torch
+
+    import rtdl_b200 as rt
+    from rtdl_b200 import _native
+    from rtdl_b200.batch import B200ProblemBatch, B200ProblemBatchGraph
+
+    sh = stream.cuda_stream
+    chunks = _plan_chunks(nb, nq, (1 << 26) - 1, args.graph_batch_probes)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batches = [B200ProblemBatch(None, dimension=3, stream=sh,
+                                device_points=(d_build.data_ptr() + 32 * int(boff[a]), boff[a:b + 1] - boff[a]))
+               for a, b in chunks]
+    d_rows = torch.empty(rows_total * 16, dtype=torch.uint8, device=d_build.device)
+    graph = B200ProblemBatchGraph(batches, d_probe.data_ptr(), qoff, radius=radius, k_max=kmax,
+                                  rows_address=d_rows.data_ptr(), rows_capacity=rows_total)
+    torch.cuda.synchronize()
+    prepare_s = time.perf_counter() - t0
+    try:
+        off, status = graph.replay()
+        assert int(off[-1]) == rows_total and status == 0, (int(off[-1]), rows_total, status)
+        for _ in range(args.warmup):
+            graph.launch(sh)
+        torch.cuda.synchronize()
+        launches0 = _native.launch_count()
+        ms = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            graph.launch(sh)
+            with torch.cuda.stream(stream):
+                b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        launches = _native.launch_count() - launches0
+        # sampled problems: graph rows against one plain call per problem
+        equal = True
+        for i in sample:
+            lo, hi = int(off[i]), int(off[i + 1])
+            got = np.frombuffer(d_rows[lo * 16: hi * 16].cpu().numpy().tobytes(), dtype=rt.runtime.FRN_ROW_DTYPE)
+            probe_i = np.frombuffer(d_probe[32 * int(qoff[i]): 32 * int(qoff[i + 1])].cpu().numpy().tobytes(),
+                                    dtype=rt.runtime.POINT3D_DTYPE)
+            build_i = np.frombuffer(d_build[32 * int(boff[i]): 32 * int(boff[i + 1])].cpu().numpy().tobytes(),
+                                    dtype=rt.runtime.POINT3D_DTYPE)
+            view = rt.runtime.fixed_radius_neighbors(probe_i, build_i, radius=float(radius[i]), k_max=int(kmax[i]))
+            ref = view.to_numpy()
+            view.close()
+            equal &= bool(len(ref) == len(got) and np.array_equal(ref.view(np.uint8), got.view(np.uint8)))
+        info = graph.info()
+    finally:
+        graph.close()
+        for b in batches:
+            b.close()
+    ms_step = sum(ms) / len(ms)
+    return {"value": rows_total / (ms_step / 1e3), "unit": "rows/s", "ms_per_step": ms_step,
+            "step": "one replay of the captured graph over prepared problem batches (queries of all problems)",
+            "batches": len(chunks), "persistent_collect_launches": len(chunks), "kernel_nodes": info["kernel_nodes"],
+            "prepare_s": prepare_s, "fallback_batches": info["fallbacks"], "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": alg / (ms_step / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": alg / (ms_step / 1e3) / 1e9 / hbm_peak, "algorithmic_bytes": alg},
+            "exactness": {"problems_checked": len(sample), "rows_equal_to_plain_call": equal}}
 
 
 def serve_trace(seconds: float, rate: float, scenes: dict, pools: dict, seed: int = 6):
@@ -599,19 +865,17 @@ def run_serve(args) -> int:
               for i, n in enumerate(sizes)}
     pools = {name: workloads.records(workloads._mixture(np.random.default_rng(200 + i), 1 << 20, c))
              for i, name in enumerate(points)}
-    trace = serve_trace(args.serve_seconds, args.rate, {k: len(v) for k, v in points.items()}, pools)
-    with B200Server(memory_budget=120 << 30, streams=4) as server:
-        for name, p in points.items():
-            server.add_scene(name, p)
-        replay(server, trace[: min(len(trace), 32)], keep=set())  # warm-up: allocator pools, pinned buffers
+    scene_sizes = {k: len(v) for k, v in points.items()}
+    trace = serve_trace(args.serve_seconds, args.rate, scene_sizes, pools)
+
+    def measure(server, trace, sampler=None):
+        """Replays a trace through the served loop and the plain path; sampled requests checked."""
         server.completed.clear()
         sample = set(np.random.default_rng(3).choice(len(trace), min(24, len(trace)), replace=False).tolist())
-        sampler = ClockSampler(0)
-        sampler.start()
         launches0 = _native.launch_count()
         reqs = replay(server, trace, keep=sample)  # rows of the sampled requests are kept for the check
         launches = _native.launch_count() - launches0
-        clocks = sampler.stop()
+        clocks = sampler.stop() if sampler else None
         served = server.stats()
         failed = [r.error for r in reqs if r.error]
         equal = True
@@ -621,6 +885,24 @@ def run_serve(args) -> int:
             equal &= same_rows(r.rows, view.to_numpy())
             view.close()
         plain = run_plain(server.scenes, reqs, [t[0] for t in trace])
+        return served, plain, {"requests_checked": len(sample), "rows_equal_to_plain_call": equal,
+                               "failed": len(failed)}, launches, clocks
+
+    with B200Server(memory_budget=120 << 30, streams=4) as server:
+        for name, p in points.items():
+            server.add_scene(name, p)
+        replay(server, trace[: min(len(trace), 32)], keep=set())  # warm-up: allocator pools, pinned buffers
+        sampler = ClockSampler(0)
+        sampler.start()
+        served, plain, exact, launches, clocks = measure(server, trace, sampler)
+        sustained = None
+        if args.sustained_rate > 0:  # a rate the loop keeps up with: latencies are service times, not queueing
+            strace = serve_trace(args.serve_seconds, args.sustained_rate, scene_sizes, pools, seed=7)
+            s_served, s_plain, s_exact, _, _ = measure(server, strace)
+            sustained = {"rate_req_per_s": args.sustained_rate, "requests": len(strace), "served": s_served,
+                         "plain_per_call": s_plain, "exactness": s_exact,
+                         "throughput_vs_plain": (s_served["rows_per_s"] / s_plain["rows_per_s"])
+                         if s_served.get("rows_per_s") and s_plain.get("rows_per_s") else None}
     line = {
         "metric": f"served neighbor rows/s with continuous batching ({args.scenes} resident 3D scenes, "
                   "Poisson arrivals)",
@@ -635,7 +917,8 @@ def run_serve(args) -> int:
                    "timing": "host wall clock per request (arrival to rows in pinned host memory)"},
         "served": served, "plain_per_call": plain,
         "throughput_vs_plain": (served["rows_per_s"] / plain["rows_per_s"]) if served.get("rows_per_s") else None,
-        "exactness": {"requests_checked": len(sample), "rows_equal_to_plain_call": equal, "failed": len(failed)},
+        "exactness": exact,
+        "sustained": sustained,
         "e2e": None, "cpu_baseline": None, "roofline": None, "clocks": clocks, "gpu_launches": launches,
     }
     print(json.dumps(line))
@@ -793,20 +1076,30 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="leave out the exactness check and the knn16 / hausdorff_4m legs of the headline line")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--probes", type=int, default=N_PROBE, help="probe points per GPU (profiling a smaller case)")
     ap.add_argument("--build", type=int, default=N_BUILD, help="build points (profiling a smaller case)")
-    ap.add_argument("--workload", choices=("frn", "knn", "hausdorff", "batch", "serve", "summary"), default="frn",
+    ap.add_argument("--workload", choices=("frn", "knn", "hausdorff", "batch", "serve", "summary", "config1"),
+                    default="frn",
                     help="frn: the headline fixed-radius config; knn: k=16 on the same 3D sets; "
                          "hausdorff: 4,194,304 x 4,194,304 2D directed nearest-distance reduction; "
                          "batch: 2,048 uneven fixed-radius problems, batched vs one call per problem; "
                          "serve: request loop over resident scenes vs the plain per-call path; "
-                         "summary: the reference's published ranked-summary benchmark")
+                         "summary: the reference's published ranked-summary benchmark; "
+                         "config1: 4,096 x 4,096 2D fixed radius beside the reference's CPU runners")
     ap.add_argument("--problems", type=int, default=2048, help="problems of the batch workload")
+    ap.add_argument("--no-graph", action="store_true", help="batch workload: leave out the captured-graph leg")
+    ap.add_argument("--graph-batch-probes", type=int, default=24 << 20,
+                    help="batch workload: probes per prepared batch of the captured graph")
     ap.add_argument("--scenes", type=int, default=16, help="resident scenes of the serve workload")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve workload arrivals per second")
+    ap.add_argument("--sustained-rate", type=float, default=250.0,
+                    help="serve workload: a second trace at a rate the loop keeps up with (0: none)")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="serve workload trace length")
-    ap.add_argument("--traversal", choices=("packet", "lane", "packet_cube"), default=None,
+    ap.add_argument("--traversal", choices=("packet", "lane", "packet_cube", "packet_points", "packet_hybrid"),
+                    default=None,
                     help="collect-pass traversal (library default when omitted)")
     ap.add_argument("--leaf-size", type=int, default=None, help="LBVH leaf bucket size (library default when omitted)")
     args = ap.parse_args(argv)
@@ -815,12 +1108,18 @@ def main(argv=None) -> int:
     N_PROBE, N_BUILD = args.probes, args.build
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.traversal is not None or args.leaf_size is not None:
+        import rtdl_b200 as rt
+
+        rt.set_tuning(leaf_size=args.leaf_size or 0, traversal=args.traversal or "packet")
     if args.workload == "batch":
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
     if args.workload == "summary":
         return run_summary(args)
+    if args.workload == "config1":
+        return run_config1(args)
     if args.workload != "frn":
         return run_secondary(args)
 
@@ -834,8 +1133,6 @@ def main(argv=None) -> int:
     local = _env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
     rt.set_device(local)
-    if args.traversal is not None or args.leaf_size is not None:
-        rt.set_tuning(leaf_size=args.leaf_size or 0, traversal=args.traversal or "packet")
     dist = None
     if world > 1:
         import datetime
@@ -920,12 +1217,7 @@ def main(argv=None) -> int:
     # "build" spans the scene build and, on a second stream beside it, the probe set's preparation
     build_ms = mean_phase("build")
     query_ms = mean_phase("total") - build_ms
-    peaks = {}
-    try:
-        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
-        hbm_peak, peak_note = float(peaks["hbm_gbs"]), "measured"
-    except Exception:
-        hbm_peak, peak_note = 6650.0, "fallback"
+    hbm_peak, peak_note = _hbm_peak()
     R = rows_total
     # algorithmic bytes (per launch) of the two query phases: the collect kernel reads every probe and build
     # point once and keeps a 4-byte neighbour index per row plus a count and a flag per probe; the emit
@@ -977,6 +1269,19 @@ def main(argv=None) -> int:
                "d2h_bytes_per_step": rows_total * 16, "ms_per_step": t_job / e2e_steps * 1e3,
                "entry_point": "rtdl_b200_run_fixed_radius_neighbors_3d (pinned host buffers)"}
 
+    # exactness of the timed rows against the oracle, then the KNN and Hausdorff legs (one GPU only)
+    exactness = knn16 = hausdorff4m = None
+    if rank == 0 and world == 1 and not args.no_secondary:
+        from rtdl_b200.runtime import FRN_ROW_DTYPE
+
+        rows_np = np.frombuffer(rows_buf.cpu().numpy().tobytes(), dtype=FRN_ROW_DTYPE)
+        del rows_buf, flush
+        torch.cuda.empty_cache()
+        exactness = frn_exactness(rows_np, probe, build)
+        del rows_np
+        knn16 = secondary_leg("knn", steps=5, warmup=3)
+        hausdorff4m = secondary_leg("hausdorff", steps=5, warmup=3)
+
     cpu = None
     external = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1011,6 +1316,9 @@ def main(argv=None) -> int:
             "phase_roofline": {"phase": "query+emit", "achieved": phase_achieved, "peak": hbm_peak, "unit": "GB/s",
                                "frac": phase_achieved / hbm_peak, "algorithmic_bytes": phase_bytes},
             "e2e": e2e,
+            "exactness": exactness,
+            "knn16": knn16,
+            "hausdorff_4m": hausdorff4m,
             "cpu_baseline": cpu,
             "external_baselines": {"scipy_ckdtree": external} if external else None,
             "clocks": clocks,

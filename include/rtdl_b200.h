@@ -311,6 +311,45 @@ RTDL_B200_API int rtdl_b200_batch_fixed_radius_neighbors_device(
     unsigned long long* row_offsets_out, uint8_t* overflow_dev, void* stream,
     char* error_out, size_t error_size);
 
+/* ---- captured graph over prepared problem batches ---------------------------
+ * The reference's batch graph (rtdl_optix_api.cpp:4323-4396,
+ * rtdl_optix_workloads.cpp:14378-14393: capture once, replay a launch over
+ * prepared inputs) for problem batches.  `batches` are batch_count handles of
+ * rtdl_b200_batch_create; their problems are numbered in order (batch 0's
+ * first).  query_points_dev holds every problem's device query records back
+ * to back, problem p at [query_offsets[p], query_offsets[p + 1]) (host array,
+ * total problems + 1 entries), with radius[p] and k_max[p] (1..64).  One
+ * replay answers every problem: per batch one persistent collect launch takes
+ * 32-query packets from a device work queue, then the scan, the radius
+ * refinement and the emit run device-driven (nothing is read back inside the
+ * graph).  Rows go to rows_dev (device, capacity rows_capacity rows) problem
+ * by problem, each problem's exactly as rtdl_b200_batch_fixed_radius_neighbors
+ * returns them.  The query records, the batches and rows_dev must stay valid
+ * until the graph is destroyed. */
+RTDL_B200_API int rtdl_b200_batch_graph_create(
+    void* const* batches, uint32_t batch_count, const void* query_points_dev,
+    const unsigned long long* query_offsets, const double* radius, const uint32_t* k_max,
+    void* rows_dev, size_t rows_capacity, void** graph_out, char* error_out, size_t error_size);
+
+/* Replays the graph and waits: row_offsets_out (optional, problems + 1
+ * entries) receives each problem's first row and the total; status_out
+ * (optional) the OR of the batches' status bits (4: the rows exceeded
+ * rows_capacity, rows past it were not written).  A batch with heavy queries
+ * the refinement did not resolve is recomputed by the plain batch call. */
+RTDL_B200_API int rtdl_b200_batch_graph_replay(
+    void* graph, unsigned long long* row_offsets_out, uint32_t* status_out, char* error_out, size_t error_size);
+
+/* Enqueues one replay ordered after `stream`'s earlier work and before its
+ * later work, without waiting or reading anything back (no recompute of
+ * flagged batches: check with a replay when unsure). */
+RTDL_B200_API int rtdl_b200_batch_graph_launch(void* graph, void* stream, char* error_out, size_t error_size);
+
+/* Problems, kernel nodes of one replay, batches recomputed so far. */
+RTDL_B200_API int rtdl_b200_batch_graph_info(void* graph, uint32_t* problems_out, int* kernel_nodes_out,
+                                             unsigned long long* fallbacks_out);
+
+RTDL_B200_API void rtdl_b200_batch_graph_destroy(void* graph);
+
 /* Several fixed_radius_neighbors requests against one resident scene (from
  * rtdl_b200_scene_create) answered by one launch sequence: request r's
  * queries are [query_offsets[r], query_offsets[r + 1]) of query_points_dev,

@@ -130,6 +130,12 @@ SIGNATURES = {
     # batch arrays (offsets, radius, k_max, row offsets) are passed as addresses of numpy buffers
     "rtdl_b200_batch_create": (_i, [_vp, _vp, ctypes.c_uint32, _i, _i, _vp, _vpp, _cp, _sz]),
     "rtdl_b200_batch_destroy": (None, [_vp]),
+    "rtdl_b200_batch_graph_create": (_i, [_vp, ctypes.c_uint32, _vp, _vp, _vp, _vp, _vp, _sz, _vpp, _cp, _sz]),
+    "rtdl_b200_batch_graph_replay": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32), _cp, _sz]),
+    "rtdl_b200_batch_graph_launch": (_i, [_vp, _vp, _cp, _sz]),
+    "rtdl_b200_batch_graph_info": (_i, [_vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_i),
+                                        ctypes.POINTER(ctypes.c_ulonglong)]),
+    "rtdl_b200_batch_graph_destroy": (None, [_vp]),
     "rtdl_b200_batch_fixed_radius_neighbors": (_i, [_vp, _vp, _vp, _vp, _vp, _vpp, _vp, _vp, _cp, _sz]),
     "rtdl_b200_batch_fixed_radius_neighbors_device": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp,
                                                            _cp, _sz]),

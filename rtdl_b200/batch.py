@@ -194,3 +194,80 @@ class B200ProblemBatch:
             self.close()
         except Exception:
             pass
+
+
+class B200ProblemBatchGraph:
+    """Every problem of several prepared :class:`B200ProblemBatch` objects
+    answered by one captured CUDA graph (``rtdl_b200_batch_graph_create``).
+
+    ``query_address`` holds all problems' device query records back to back
+    (problem p at ``query_offsets[p]:query_offsets[p + 1]``, problems numbered
+    batch after batch); rows go to the device buffer at ``rows_address``
+    (capacity ``rows_capacity`` rows) problem by problem.  Per batch, one
+    persistent collect launch takes 32-query packets from a device work queue;
+    nothing is read back inside the graph.  Mirrors the reference's captured
+    batch graph (``rtdl_optix_api.cpp:4323-4396``), for problem batches.
+    """
+
+    def __init__(self, batches: Sequence[B200ProblemBatch], query_address: int, query_offsets, *, radius, k_max,
+                 rows_address: int | None, rows_capacity: int):
+        lib = _native.load_library()
+        self._lib = lib
+        self._batches = list(batches)  # kept alive with the graph
+        self.problems = sum(b.problems for b in self._batches)
+        self._qoff = np.ascontiguousarray(np.asarray(query_offsets, dtype=np.uint64))
+        if len(self._qoff) != self.problems + 1:
+            raise ValueError("query_offsets needs problems + 1 entries")
+        self._radius = _per_problem(radius, self.problems, np.float64, "radius")
+        self._kmax = _per_problem(k_max, self.problems, np.uint32, "k_max")
+        handles = (ctypes.c_void_p * len(self._batches))(*[b.handle for b in self._batches])
+        self._handle = ctypes.c_void_p()
+        self._closed = True
+        err = _native.error_buffer()
+        status = lib.rtdl_b200_batch_graph_create(
+            handles, len(self._batches), query_address, self._qoff.ctypes.data, self._radius.ctypes.data,
+            self._kmax.ctypes.data, rows_address, int(rows_capacity), ctypes.byref(self._handle), err, len(err))
+        _native.check_status(status, err)
+        self._closed = False
+
+    def replay(self) -> tuple[np.ndarray, int]:
+        """One replay; returns (row_offsets with problems + 1 entries, status bits)."""
+        if self._closed:
+            raise RuntimeError("graph is closed")
+        offsets = np.zeros(self.problems + 1, dtype=np.uint64)
+        status = ctypes.c_uint32()
+        err = _native.error_buffer()
+        st = self._lib.rtdl_b200_batch_graph_replay(self._handle, offsets.ctypes.data, ctypes.byref(status), err,
+                                                    len(err))
+        _native.check_status(st, err)
+        return offsets, int(status.value)
+
+    def launch(self, stream: int | None = None) -> None:
+        """Enqueue one replay after `stream`'s work, without waiting."""
+        if self._closed:
+            raise RuntimeError("graph is closed")
+        err = _native.error_buffer()
+        _native.check_status(self._lib.rtdl_b200_batch_graph_launch(self._handle, stream, err, len(err)), err)
+
+    def info(self) -> dict:
+        problems, kernels, fallbacks = ctypes.c_uint32(), ctypes.c_int(), ctypes.c_ulonglong()
+        self._lib.rtdl_b200_batch_graph_info(self._handle, ctypes.byref(problems), ctypes.byref(kernels),
+                                             ctypes.byref(fallbacks))
+        return {"problems": problems.value, "kernel_nodes": kernels.value, "fallbacks": fallbacks.value}
+
+    def close(self) -> None:
+        if not self._closed:
+            self._lib.rtdl_b200_batch_graph_destroy(self._handle)
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -110,6 +110,26 @@ void dev_free(void* p, cudaStream_t s) {
 }
 
 namespace {
+thread_local RowBufferHook g_row_hook;
+thread_local void* g_hook_rows = nullptr;  // the buffer the hook handed out for this call
+}  // namespace
+
+RowBufferHook& row_buffer_hook() { return g_row_hook; }
+
+void* alloc_rows(size_t bytes, cudaStream_t s) {
+  if (g_row_hook.alloc) {
+    void* p = g_row_hook.alloc(bytes);
+    if (p) {
+      g_hook_rows = p;
+      return p;
+    }
+  }
+  return dev_alloc(bytes, s);
+}
+
+bool rows_on_host(const void* p) { return p != nullptr && p == g_hook_rows; }
+
+namespace {
 
 thread_local std::vector<std::pair<const char*, double>> g_last_timings;
 
@@ -200,6 +220,54 @@ class PinnedPool {
 PinnedPool& pinned_pool() {
   static PinnedPool* p = new PinnedPool();  // never destroyed: outlives static teardown order
   return *p;
+}
+
+void* download_rows(const void* d_rows, size_t bytes, cudaStream_t s);
+
+// Rows written by the kernels straight into the pinned buffer handed to the
+// caller (RTDL_B200_DIRECT_ROWS=0 keeps them in device memory and copies them
+// after the emit).
+bool direct_rows_enabled() {
+  static const bool on = [] {
+    const char* env = std::getenv("RTDL_B200_DIRECT_ROWS");
+    return !(env && env[0] == '0');
+  }();
+  return on;
+}
+
+// Sets the pinned-host row allocator for one host-buffer call on this thread.
+struct DirectRowsScope {
+  DirectRowsScope() {
+    if (direct_rows_enabled()) g_row_hook.alloc = [](size_t bytes) { return pinned_pool().get(bytes); };
+  }
+  ~DirectRowsScope() {
+    g_row_hook.alloc = nullptr;
+    g_hook_rows = nullptr;
+  }
+};
+
+// Releases a call's row buffer: pinned host rows go back to the pool once the
+// stream has finished writing them, device rows to the device pool.
+void release_rows(void* rows, cudaStream_t s) {
+  if (!rows) return;
+  if (rows_on_host(rows)) {
+    sync_quietly(s);
+    pinned_pool().put(rows);
+  } else {
+    dev_free(rows, s);
+  }
+}
+
+// The rows of a host-buffer call as the caller receives them: already in the
+// pinned buffer (written there by the kernels) or copied from device memory.
+void* rows_for_caller(void*& d_rows, size_t bytes, cudaStream_t s) {
+  if (rows_on_host(d_rows)) {
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    void* host = d_rows;
+    d_rows = nullptr;
+    return host;
+  }
+  return download_rows(d_rows, bytes, s);
 }
 
 cudaStream_t library_stream() {
@@ -298,6 +366,7 @@ void validate_common(double radius, size_t limit, size_t nq, size_t ns, bool has
 void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim, int predicate, double radius,
                    size_t limit, void** rows_out, size_t* row_count_out) {
   cudaStream_t s = library_stream();
+  DirectRowsScope direct;
   PhaseTimer timer(s);
   timer.mark("begin");
   const size_t rec = record_size(dim);
@@ -311,21 +380,21 @@ void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim,
     QueryResult r = run_build_and_query(in, predicate, radius, (uint32_t)limit, nullptr, 0, &d_rows, nullptr, s,
                                         aux_stream(), &timer, &sc, &d_query);
     const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
-    void* host = download_rows(d_rows, row_size * r.rows, s);
+    void* host = rows_for_caller(d_rows, row_size * r.rows, s);
     timer.mark("download");
     timer.publish();
     *rows_out = host;
     *row_count_out = (size_t)r.rows;
   } catch (...) {
     sync_quietly(aux_stream());
-    dev_free(d_rows, s);
+    release_rows(d_rows, s);
     destroy_scene(sc);
     dev_free(d_search, s);
     dev_free(d_query, s);
     sync_quietly(s);
     throw;
   }
-  dev_free(d_rows, s);
+  release_rows(d_rows, s);
   destroy_scene(sc);
   dev_free(d_search, s);
   dev_free(d_query, s);
@@ -612,6 +681,7 @@ int rtdl_b200_scene_query(void* scene, const void* query_points, size_t query_co
     if (query_count == 0) return;
     if (!query_points) throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
     cudaStream_t s = sc->stream;
+    DirectRowsScope direct;
     PhaseTimer timer(s);
     timer.mark("begin");
     void* d_query = upload(query_points, record_size(sc->dim) * query_count, s);
@@ -624,19 +694,19 @@ int rtdl_b200_scene_query(void* scene, const void* query_points, size_t query_co
                                 &d_rows, d_overflow, s, &timer);
       const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
       if (d_overflow) RTDL_CUDA_CHECK(cudaMemcpyAsync(overflow_out, d_overflow, query_count, cudaMemcpyDeviceToHost, s));
-      void* host = download_rows(d_rows, row_size * r.rows, s);
+      void* host = rows_for_caller(d_rows, row_size * r.rows, s);
       timer.mark("download");
       timer.publish();
       *rows_out = host;
       *row_count_out = (size_t)r.rows;
     } catch (...) {
-      dev_free(d_rows, s);
+      release_rows(d_rows, s);
       dev_free(d_query, s);
       dev_free(d_overflow, s);
       sync_quietly(s);
       throw;
     }
-    dev_free(d_rows, s);
+    release_rows(d_rows, s);
     dev_free(d_query, s);
     dev_free(d_overflow, s);
   }, error_out, error_size);
@@ -776,6 +846,50 @@ int rtdl_b200_batch_fixed_radius_neighbors_device(void* batch, const void* query
     timer.publish();
   }, error_out, error_size);
 }
+
+int rtdl_b200_batch_graph_create(void* const* batches, uint32_t batch_count, const void* query_points_dev,
+                                 const unsigned long long* query_offsets, const double* radius,
+                                 const uint32_t* k_max, void* rows_dev, size_t rows_capacity, void** graph_out,
+                                 char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!graph_out) throw std::runtime_error("graph_out must not be null");
+    *graph_out = nullptr;
+    if (!batches) throw std::runtime_error("batches must not be null");
+    std::vector<Scene*> scenes(batch_count);
+    for (uint32_t i = 0; i < batch_count; ++i) scenes[i] = static_cast<Scene*>(batches[i]);
+    *graph_out = batch_graph_create(scenes.data(), batch_count, query_points_dev, query_offsets, radius, k_max,
+                                    rows_dev, rows_capacity);
+  }, error_out, error_size);
+}
+
+int rtdl_b200_batch_graph_replay(void* graph, unsigned long long* row_offsets_out, uint32_t* status_out,
+                                 char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!graph) throw std::runtime_error("graph must not be null");
+    unsigned int st = 0;
+    batch_graph_replay(static_cast<BatchGraph*>(graph), row_offsets_out, &st);
+    if (status_out) *status_out = st;
+  }, error_out, error_size);
+}
+
+int rtdl_b200_batch_graph_launch(void* graph, void* stream, char* error_out, size_t error_size) {
+  return guarded([&]() {
+    if (!graph) throw std::runtime_error("graph must not be null");
+    batch_graph_launch(static_cast<BatchGraph*>(graph), static_cast<cudaStream_t>(stream));
+  }, error_out, error_size);
+}
+
+int rtdl_b200_batch_graph_info(void* graph, uint32_t* problems_out, int* kernel_nodes_out,
+                               unsigned long long* fallbacks_out) {
+  if (!graph) return 1;
+  const BatchGraph* g = static_cast<const BatchGraph*>(graph);
+  if (problems_out) *problems_out = batch_graph_problems(g);
+  if (kernel_nodes_out) *kernel_nodes_out = batch_graph_kernels(g);
+  if (fallbacks_out) *fallbacks_out = (unsigned long long)batch_graph_fallbacks(g);
+  return 0;
+}
+
+void rtdl_b200_batch_graph_destroy(void* graph) { batch_graph_destroy(static_cast<BatchGraph*>(graph)); }
 
 int rtdl_b200_scene_fixed_radius_neighbors_multi_device(void* scene, const void* query_points_dev,
                                                         const unsigned long long* query_offsets, uint32_t requests,

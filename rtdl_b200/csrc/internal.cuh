@@ -186,6 +186,21 @@ void* dev_alloc(size_t bytes, cudaStream_t s);
 void dev_free(void* p, cudaStream_t s);
 void ensure_pool_configured(int device);
 
+// ---- where a call's own row buffer goes --------------------------------------
+// A call that allocates its row buffer itself (the rows_alloc argument of the
+// query functions) takes it from device memory, unless the calling thread has
+// set a host allocator for the call: the host-buffer entry points hand out
+// rows in pinned host memory, and with the allocator set the emit kernels
+// write the rows across PCIe straight into that buffer, so the transfer
+// overlaps the emit instead of following it.  The allocator returns nullptr
+// to fall back to device memory.
+struct RowBufferHook {
+  void* (*alloc)(size_t bytes) = nullptr;
+};
+RowBufferHook& row_buffer_hook();  // the calling thread's
+void* alloc_rows(size_t bytes, cudaStream_t s);
+bool rows_on_host(const void* p);  // p came from the hook (pinned host memory)
+
 // ---- sort / scan (sort_scan.cu) -------------------------------------------
 // Exclusive scan of `counts` (optionally gathered through `order`, or identity
 // when *identity_flag != 0) into out[0..n] (u64); out[n] is the total.
@@ -373,6 +388,24 @@ cudaStream_t summary_graph_stream(const SummaryGraph* g);
 uint32_t summary_graph_requests(const SummaryGraph* g);
 uint64_t summary_graph_fallbacks(const SummaryGraph* g);
 void summary_graph_destroy(SummaryGraph* g);
+
+// Prepared problem batches answered by one captured CUDA graph (one
+// persistent collect launch per batch, rows of all problems problem-major into
+// the caller's buffer); see query.cu.
+struct BatchGraph;
+BatchGraph* batch_graph_create(Scene* const* batches, uint32_t batch_count, const void* queries_dev,
+                               const unsigned long long* query_offsets, const double* radius, const uint32_t* kmax,
+                               void* rows_dev, unsigned long long rows_capacity);
+// Enqueues one replay (the graph runs on its own stream, ordered after `s`'s
+// work and before `s`'s later work); nothing is read back.
+void batch_graph_launch(BatchGraph* g, cudaStream_t s);
+// Replays, reads the per-problem row offsets and status back, and recomputes
+// flagged batches by the plain batch call.
+void batch_graph_replay(BatchGraph* g, unsigned long long* row_offsets_out, unsigned int* status_out);
+uint32_t batch_graph_problems(const BatchGraph* g);
+int batch_graph_kernels(const BatchGraph* g);
+uint64_t batch_graph_fallbacks(const BatchGraph* g);
+void batch_graph_destroy(BatchGraph* g);
 
 QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec& bs, void* rows_dev,
                             size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,

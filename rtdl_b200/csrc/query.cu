@@ -28,6 +28,7 @@
 //     k_max, or k > 64) go to a generic block-per-query path (gather, bitonic
 //     sort in global memory, emit).
 #include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 #include "internal.cuh"
@@ -216,16 +217,22 @@ enum Stat { kStatNodes, kStatLeafPoints, kStatInRadius, kStatInserts, kStatShift
 
 // One thread per query, queries in Morton order so a warp walks neighbouring
 // subtrees.  KNN == false: radius-limited (fixed_radius_neighbors and
-// bounded_knn_rows); KNN == true: k nearest.
-template <bool KNN, bool STATS>
+// bounded_knn_rows); KNN == true: k nearest.  PACKET: the warp walks the tree
+// together -- each node is read once for the warp and entered when any lane's
+// current bound needs it -- while every lane keeps its own list and tests a
+// leaf's points only when its own bound reaches the leaf; the lists, and so
+// the rows, are the per-lane walk's.
+template <bool KNN, bool STATS, bool PACKET = false>
 __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
   extern __shared__ uint32_t smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int L = P.L;
   uint32_t* lkey = smem + (size_t)warp * 64 * L;
   uint32_t* lidx = lkey + 32 * L;
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.nq) return;
+  const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (PACKET ? !__any_sync(0xffffffffu, t0 < P.nq) : t0 >= P.nq) return;
+  const bool active = t0 < P.nq;  // PACKET: lanes past the end take part in the warp's walk only
+  const uint32_t t = active ? t0 : P.nq - 1;
   const uint32_t qin = P.qorder[t];
   const float4 q = P.qpts[qin];
   const DevBands B = *P.bands;
@@ -348,18 +355,36 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
   }
   // stackless depth-first walk over the pre-order records
   int cur = S.n > 0 ? 0 : kRopeEnd;
-  while (cur != kRopeEnd) {
-    const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
-    if (STATS) ++st_nodes;
-    const int hit = __float_as_int(a.w);
-    if (box_ok(box_d2(c.qx, c.qy, c.qz, a, b))) {
-      if (hit >= 0) {
-        ++cur;  // internal node: its left child is the next record
-        continue;
+  if (PACKET) {
+    while (cur != kRopeEnd) {
+      const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+      if (STATS) ++st_nodes;
+      const int hit = __float_as_int(a.w);
+      const bool need = active && box_ok(box_d2(c.qx, c.qy, c.qz, a, b));
+      if (__ballot_sync(0xffffffffu, need)) {
+        if (hit >= 0) {
+          ++cur;  // internal node: its left child is the next record
+          continue;
+        }
+        if (need) visit_leaf(leaf_first(hit), leaf_count(hit));
       }
-      visit_leaf(leaf_first(hit), leaf_count(hit));
+      cur = __float_as_int(b.w);
     }
-    cur = __float_as_int(b.w);
+    if (!active) return;
+  } else {
+    while (cur != kRopeEnd) {
+      const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
+      if (STATS) ++st_nodes;
+      const int hit = __float_as_int(a.w);
+      if (box_ok(box_d2(c.qx, c.qy, c.qz, a, b))) {
+        if (hit >= 0) {
+          ++cur;  // internal node: its left child is the next record
+          continue;
+        }
+        visit_leaf(leaf_first(hit), leaf_count(hit));
+      }
+      cur = __float_as_int(b.w);
+    }
   }
 
   if (STATS) {
@@ -675,10 +700,9 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
 // (warp-uniform): point-major when at most kHybridRatio reaching queries per
 // point, i.e. when few of the packet's spheres reach the bucket.
 constexpr int kLeafLaneMajor = 0, kLeafPointMajor = 1, kLeafHybrid = 2;
-template <bool STATS, bool CUBE, bool BATCH, int MIN_BLOCKS, int LEAF = kLeafLaneMajor>
-__global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParams P) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!__any_sync(0xffffffffu, t < P.nq)) return;  // whole warp past the end
+// The packet walk for processing ranks t & ~31 .. (t & ~31) + 31 (lane t & 31).
+template <bool STATS, bool CUBE, bool BATCH, int LEAF>
+__device__ __forceinline__ void collect_packet_body(const CollectParams& P, uint32_t t) {
   // a problem batch pads every problem to whole warps, so a warp has one problem
   const uint32_t prob = BATCH ? P.warp_prob[t >> 5] : 0u;
   const bool valid = t < P.nq && (!BATCH || P.qorder[t] != kNone);
@@ -737,6 +761,13 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParam
     cur = __float_as_int(b.w);
   }
   if (valid) collect_finish<STATS>(P, L, BATCH ? P.prob_kmax[prob] : P.kmax);
+}
+
+template <bool STATS, bool CUBE, bool BATCH, int MIN_BLOCKS, int LEAF = kLeafLaneMajor>
+__global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParams P) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!__any_sync(0xffffffffu, t < P.nq)) return;  // whole warp past the end
+  collect_packet_body<STATS, CUBE, BATCH, LEAF>(P, t);
 }
 
 // ---- heavy queries: radius refinement -------------------------------------------
@@ -1766,6 +1797,50 @@ __global__ void k_mark_all_heavy(const uint32_t* qorder, uint32_t nq, uint32_t n
     counts[qin] = k < n ? k : n;
     flags[qin] = 2;
     temp[qin] = (uint32_t)t;
+  }
+}
+
+// Density class of each query of a nearest search, by processing rank: the
+// FP32 exponent of the largest d2 over the seed window of 2w scene points
+// around the query's Morton code (the window the nearest walk seeds from, so
+// the class tracks the k-th bound the walk starts with).  Queries in a dense
+// cluster get small classes, queries in the sparse background large ones.
+__global__ void k_knn_class(const float4* qpts, const uint32_t* qorder, const uint32_t* qcodes, uint32_t nq,
+                            const float4* spts, const uint32_t* scodes, uint32_t ns, int w, uint32_t* cls,
+                            uint32_t* rank) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += gridDim.x * blockDim.x) {
+    const float4 q = qpts[qorder[t]];
+    const uint32_t code = qcodes[t];
+    uint32_t lo = 0, hi = ns;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(&scodes[mid]) < code) lo = mid + 1;
+      else hi = mid;
+    }
+    int a = (int)lo - w;
+    if (a < 0) a = 0;
+    int b = a + 2 * w;
+    if (b > (int)ns) {
+      b = (int)ns;
+      a = b - 2 * w < 0 ? 0 : b - 2 * w;
+    }
+    float far = 0.f;
+    for (int i = a; i < b; ++i) {
+      const float4 p = __ldg(&spts[i]);
+      const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+      far = fmaxf(far, fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+    }
+    cls[t] = (__float_as_uint(far) >> 23) & 0xFFu;
+    rank[t] = t;
+  }
+}
+
+__global__ void k_permute_pair(const uint32_t* a, const uint32_t* b, const uint32_t* perm, uint32_t n, uint32_t* a_out,
+                               uint32_t* b_out) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t p = perm[j];
+    a_out[j] = a[p];
+    b_out[j] = b[p];
   }
 }
 
@@ -2829,7 +2904,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       }
       if (rows_alloc != nullptr) {
         const size_t row_size = predicate == kFrn ? 16 : 24;
-        rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
+        rows_dev = res.rows ? alloc_rows(row_size * res.rows, s) : nullptr;
         rows_capacity = res.rows;
         *rows_alloc = rows_dev;
       }
@@ -3217,6 +3292,7 @@ namespace {
 
 constexpr unsigned int kGraphStatusOverflow = 1u;  // traversal stack overflow (the plain call raises it)
 constexpr unsigned int kGraphStatusGeneric = 2u;   // heavy queries left for the generic path
+constexpr unsigned int kBatchGraphStatusRows = 4u;  // a batch graph's rows exceed the caller's row buffer
 
 __global__ void k_graph_status(const unsigned int* small, const unsigned int* pass_count, uint32_t requests,
                                unsigned int* status) {
@@ -3646,11 +3722,38 @@ void ensure_pass1_shared_memory() {
   if ((int)done.size() <= dev) done.resize(dev + 1, false);
   if (done[dev]) return;
   const int most = kMaxList * 256 * 8;
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
   RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
   RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
   RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
   RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
   done[dev] = true;
+}
+
+// Nearest searches walk in warp packets; a packet mixing queries of a dense
+// cluster with queries of the sparse background walks the union of very
+// different k-th bounds.  The Morton processing order is therefore reordered,
+// stably, by the queries' density class: packets hold queries of alike bounds
+// and keep Morton order within a class.  Only the processing order changes
+// (each query's rows do not depend on it).
+void order_by_density_class(Scene* sc, QueryPrep& qp, uint32_t nq, int w, cudaStream_t s) {
+  uint32_t* cls = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  uint32_t* rank = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  uint32_t* order = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  uint32_t* codes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
+  k_knn_class<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, qp.qorder, qp.qcodes, nq, sc->pts, sc->codes, sc->n, w, cls,
+                                                rank);
+  RTDL_LAUNCHED(1);
+  radix_sort_pairs(cls, rank, nq, 0, 8, nullptr, &qp.qst->bad, s);
+  k_permute_pair<<<grid_for(nq, 256), 256, 0, s>>>(qp.qorder, qp.qcodes, rank, nq, order, codes);
+  RTDL_LAUNCHED(1);
+  dev_free(qp.qorder, s);
+  dev_free(qp.qcodes, s);
+  qp.qorder = order;
+  qp.qcodes = codes;
+  dev_free(cls, s);
+  dev_free(rank, s);
 }
 
 QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius, uint32_t limit,
@@ -3671,10 +3774,12 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
     return run_radius_query(sc, queries_dev, nq, predicate, radius, limit, rows_dev, rows_capacity, rows_alloc,
                             overflow_dev, s, timer);
   QueryPrep qp = prepare_queries(sc, queries_dev, nq, !knn, radius, true, s);
-  if (timer) timer->mark("query_prep");
-
   const bool all_heavy = knn && limit > (uint32_t)kMaxList;
   const int L = all_heavy ? 1 : (int)(limit < (uint32_t)kMaxList ? limit : (uint32_t)kMaxList);
+  if (knn && !all_heavy && tuning().traversal != 1 && nq > 32)
+    order_by_density_class(sc, qp, nq, L < 8 ? 8 : L, s);
+  if (timer) timer->mark("query_prep");
+
   uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq, s));
   uint32_t* temp = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * (size_t)nq * L, s));
@@ -3733,9 +3838,10 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
       }
       ensure_pass1_shared_memory();
       auto launch = [&](auto kernel) { kernel<<<blocks, threads, shm, s>>>(P); };
+      const bool packet = tuning().traversal != 1;  // "lane": one thread per query walks alone
       if (knn) {
-        if (stats) launch(k_pass1<true, true>);
-        else launch(k_pass1<true, false>);
+        if (stats) packet ? launch(k_pass1<true, true, true>) : launch(k_pass1<true, true>);
+        else packet ? launch(k_pass1<true, false, true>) : launch(k_pass1<true, false>);
       } else {
         if (stats) launch(k_pass1<false, true>);
         else launch(k_pass1<false, false>);
@@ -3767,7 +3873,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
     }
     if (rows_alloc != nullptr) {
       const size_t row_size = predicate == kFrn ? 16 : 24;
-      rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
+      rows_dev = res.rows ? alloc_rows(row_size * res.rows, s) : nullptr;
       rows_capacity = res.rows;
       *rows_alloc = rows_dev;
     }
@@ -3818,6 +3924,7 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   const int qstride = sc->dim == 3 ? 4 : 3;
   if (timer) timer->mark("start");
   QueryPrep qp = prepare_queries(sc, queries_dev, nq, false, 0.0, false, s);
+  if (tuning().traversal != 1 && nq > 32) order_by_density_class(sc, qp, nq, 8, s);
   if (timer) timer->mark("query_prep");
   uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq, s));
@@ -3845,7 +3952,10 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   P.stats = nullptr;
   P.qcodes = qp.qcodes;
   P.scodes = sc->codes;
-  k_pass1<true, false><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
+  if (tuning().traversal != 1)
+    k_pass1<true, false, true><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
+  else
+    k_pass1<true, false><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
   RTDL_LAUNCHED(1);
   if (timer) timer->mark("traverse");
   const unsigned int blocks = grid_for(nq, 256) < 2 * kSmCount ? grid_for(nq, 256) : 2 * kSmCount;
@@ -4011,6 +4121,429 @@ void run_directed_hausdorff_noalloc(Scene* sc, const void* queries_dev, uint32_t
   k_witness_final<<<1, 32, 0, s>>>(partial, (int)blocks, best);
   k_noalloc_finish<<<1, 32, 0, s>>>(best, sc->stats, qst, witness_dev);
   RTDL_LAUNCHED(3);
+}
+
+
+// ---- captured graphs over prepared problem batches --------------------------
+// Many uneven fixed-radius problems, already built into problem batches
+// (build_scene_batch: one LBVH per batch, each problem one subtree), answered
+// by one CUDA graph replay with no host read-back inside.  Per batch the graph
+// holds ONE persistent collect launch -- a grid that fills the GPU once, whose
+// warps take 32-query packets (one problem each) from a device work queue
+// until the batch's packets are gone, so small and large problems share the
+// SMs -- then the scan (rows of this batch start where the previous batch's
+// end), the device-driven radius refinement, and the emit kernels striding
+// over device list lengths.  Batches run one after another in the graph and
+// share one set of scratch buffers sized for the largest.  A batch whose heavy
+// queries the refinement passes do not resolve is flagged in its status word
+// and recomputed by the plain batch call at replay, so rows always equal it.
+namespace {
+
+__global__ void k_add_row_base(unsigned long long* offsets, uint32_t n, const unsigned long long* base,
+                               unsigned long long* next_base) {
+  const unsigned long long b = *base;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
+    const unsigned long long v = offsets[i] + b;
+    offsets[i] = v;
+    if (i == n) *next_base = v;
+  }
+}
+
+__global__ void k_empty_batch_rows(const unsigned long long* base, uint32_t problems, unsigned long long* prob_rows,
+                                   unsigned long long* next_base) {
+  const unsigned long long b = *base;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p <= problems; p += gridDim.x * blockDim.x) prob_rows[p] = b;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *next_base = b;
+}
+
+// Persistent collect over one batch: 32-query packets from a work queue.
+template <int MIN_BLOCKS>
+__global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_persistent(CollectParams P, unsigned int* queue) {
+  const uint32_t packets = (P.nq + 31u) / 32u;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(queue, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= packets) return;
+    collect_packet_body<false, false, true, kLeafLaneMajor>(P, item * 32u + lane);
+  }
+}
+
+constexpr int kPersistentMinBlocks = 5;
+
+__global__ void k_batch_graph_status(const unsigned int* small, const unsigned int* pass_count, uint32_t batches,
+                                     const unsigned long long* total, unsigned long long capacity,
+                                     unsigned int* status) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < batches; b += gridDim.x * blockDim.x)
+    status[b] = ((small[8 * (size_t)b + 1] & 1u) ? kGraphStatusOverflow : 0u) |
+                (pass_count[(size_t)b * kRefinePasses + kRefinePasses - 1] ? kGraphStatusGeneric : 0u) |
+                (*total > capacity ? kBatchGraphStatusRows : 0u);
+}
+
+}  // namespace
+
+struct BatchGraphPart {  // one prepared problem batch
+  Scene* sc = nullptr;                        // borrowed
+  const void* queries = nullptr;              // the caller's records of this batch's problems
+  uint32_t p0 = 0, problems = 0;              // global problem range
+  uint32_t nq = 0;
+  std::vector<unsigned long long> qoff;       // problems + 1, local
+  std::vector<double> radius;
+  std::vector<uint32_t> kmax;
+  QueryPrep qp;
+  uint32_t* qrank = nullptr;
+  unsigned long long* offsets = nullptr;      // nq + 1, global row offsets once the base is added
+};
+
+struct BatchGraph {
+  std::vector<BatchGraphPart> parts;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t problems = 0;
+  void* rows = nullptr;                       // the caller's
+  unsigned long long capacity = 0;
+  std::vector<void*> buffers;
+  // scratch shared by the batches (sized for the largest)
+  unsigned long long* slab = nullptr;
+  uint32_t* counts = nullptr;
+  QueryInfo* qinfo = nullptr;
+  uint8_t* flags = nullptr;
+  uint32_t *heavy_list = nullptr, *heavy_m = nullptr, *heavy_t = nullptr;
+  uint32_t *mid_list = nullptr, *big_list = nullptr, *fix_list = nullptr;
+  unsigned long long* poff = nullptr;
+  void* scan_ws = nullptr;
+  RefineDevice D{};
+  // per batch
+  unsigned int* small = nullptr;        // 8 counters per batch
+  unsigned int* pass_count = nullptr;   // kRefinePasses per batch
+  unsigned int* queue = nullptr;        // work-queue counter per batch
+  unsigned long long* base = nullptr;   // batches + 1: first row of each batch, then the total
+  unsigned long long* prob_rows = nullptr;  // problems + 1: first row of each problem, then the total
+  unsigned int* status = nullptr;
+  unsigned int* status_host = nullptr;      // pinned
+  unsigned long long* rows_host = nullptr;  // pinned, problems + 1
+  unsigned int persistent_grid = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int kernels = 0;
+  uint64_t fallbacks = 0;
+};
+
+namespace {
+
+void batch_graph_enqueue(BatchGraph* g, uint32_t i, cudaStream_t s) {
+  BatchGraphPart& b = g->parts[i];
+  unsigned int* small = g->small + 8 * (size_t)i;
+  if (b.nq == 0) {  // no queries in this batch: its problems get no rows
+    k_empty_batch_rows<<<div_up(b.problems + 1, 256), 256, 0, s>>>(g->base + i, b.problems, g->prob_rows + b.p0,
+                                                                  g->base + i + 1);
+    RTDL_LAUNCHED(1);
+    return;
+  }
+  uint32_t kmax = 1;
+  for (uint32_t k : b.kmax) kmax = k > kmax ? k : kmax;
+  CollectParams C;
+  C.S = b.qp.view;
+  C.qpts = b.qp.qpts;
+  C.qraw = static_cast<const double*>(b.queries);
+  C.qstride = b.sc->dim == 3 ? 4 : 3;
+  C.qorder = b.qp.qorder;
+  C.nq = b.qp.nproc;
+  C.kmax = kmax;
+  C.bands = b.qp.bands;
+  C.warp_prob = b.qp.warp_prob;
+  C.prob_kmax = b.qp.prob_kmax;
+  C.slab = g->slab;
+  C.counts = g->counts;
+  C.qinfo = g->qinfo;
+  C.flags = g->flags;
+  C.heavy_list = g->heavy_list;
+  C.heavy_m = g->heavy_m;
+  C.heavy_t = g->heavy_t;
+  C.mid_list = g->mid_list;
+  C.big_list = g->big_list;
+  C.small = small;
+  C.overflow_out = nullptr;
+  C.stats = nullptr;
+  const uint32_t np = b.qp.nproc;
+  k_collect_persistent<kPersistentMinBlocks><<<g->persistent_grid, 256, 0, s>>>(C, g->queue + i);
+  RTDL_LAUNCHED(1);
+  scan_counts_u64_ws(g->counts, b.qp.oorder, b.qp.order_identity, b.nq, b.offsets, g->scan_ws, s);
+  k_add_row_base<<<grid_for(b.nq + 1, 256), 256, 0, s>>>(b.offsets, b.nq, g->base + i, g->base + i + 1);
+  k_problem_rows<<<div_up(b.problems + 1, 256), 256, 0, s>>>(b.offsets, b.qp.qoff, b.problems, g->prob_rows + b.p0);
+  RTDL_LAUNCHED(2);
+  RefineDevice D = g->D;
+  D.pass_count = g->pass_count + (size_t)i * kRefinePasses;
+  enqueue_refine_device(C, b.qp.qprob, b.qp.prob_radius, 0.0, b.qp.prob_kmax, kmax, np, false, g->qinfo, g->flags,
+                        small, D, s);
+  k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(b.qp.qorder, b.qrank, b.offsets, np, g->poff);
+  RTDL_LAUNCHED(1);
+  EmitParams E;
+  E.S = b.sc->view();
+  E.nq = np;
+  E.slab = g->slab;
+  E.qinfo = g->qinfo;
+  E.poff = g->poff;
+  E.sink.rows = g->rows;
+  E.sink.capacity = g->rows ? g->capacity : 0;
+  E.sink.ranked = 0;
+  E.fix_list = g->fix_list;
+  E.fix_count = small + 4;
+  k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
+  k_emit_list<4, true><<<kStrideBlocks, kEmitListThreads, 0, s>>>(E, g->mid_list, 0, small + 2);
+  k_emit_list<8, false><<<kStrideBlocks, kEmitListThreads, 0, s>>>(E, g->big_list, 0, small + 3);
+  k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
+  RTDL_LAUNCHED(4);
+}
+
+void batch_graph_release(BatchGraph* g) {
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  g->exec = nullptr;
+  g->graph = nullptr;
+}
+
+void batch_graph_capture(BatchGraph* g) {
+  batch_graph_release(g);
+  cudaStream_t s = g->stream;
+  const uint32_t B = (uint32_t)g->parts.size();
+  const unsigned long long before = launches_counted();
+  RTDL_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  try {
+    RTDL_CUDA_CHECK(cudaMemsetAsync(g->small, 0, sizeof(unsigned int) * 8 * (size_t)B, s));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(g->pass_count, 0, sizeof(unsigned int) * kRefinePasses * (size_t)B, s));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(g->queue, 0, sizeof(unsigned int) * B, s));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(g->base, 0, sizeof(unsigned long long), s));
+    for (uint32_t i = 0; i < B; ++i) batch_graph_enqueue(g, i, s);
+    k_batch_graph_status<<<div_up(B, 256), 256, 0, s>>>(g->small, g->pass_count, B, g->base + B, g->capacity,
+                                                        g->status);
+    RTDL_LAUNCHED(1);
+  } catch (...) {
+    cudaGraph_t partial = nullptr;
+    cudaStreamEndCapture(s, &partial);
+    if (partial) cudaGraphDestroy(partial);
+    cudaGetLastError();
+    count_launches(-(int)(launches_counted() - before));
+    throw;
+  }
+  count_launches(-(int)(launches_counted() - before));  // counted when a replay launches them
+  RTDL_CUDA_CHECK(cudaStreamEndCapture(s, &g->graph));
+  RTDL_CUDA_CHECK(cudaGraphInstantiate(&g->exec, g->graph, 0));
+  size_t n = 0;
+  RTDL_CUDA_CHECK(cudaGraphGetNodes(g->graph, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  RTDL_CUDA_CHECK(cudaGraphGetNodes(g->graph, nodes.data(), &n));
+  g->kernels = 0;
+  for (size_t i = 0; i < n; ++i) {
+    cudaGraphNodeType t;
+    RTDL_CUDA_CHECK(cudaGraphNodeGetType(nodes[i], &t));
+    if (t == cudaGraphNodeTypeKernel) ++g->kernels;
+  }
+}
+
+}  // namespace
+
+BatchGraph* batch_graph_create(Scene* const* batches, uint32_t batch_count, const void* queries_dev,
+                               const unsigned long long* query_offsets, const double* radius, const uint32_t* kmax,
+                               void* rows_dev, unsigned long long rows_capacity) {
+  if (batch_count == 0) throw std::runtime_error("a batch graph needs at least one problem batch");
+  if (!batches || !query_offsets || !radius || !kmax)
+    throw std::runtime_error("batches, query_offsets, radius and k_max must not be null");
+  for (uint32_t i = 0; i < batch_count; ++i) {
+    if (!batches[i] || batches[i]->problems == 0)
+      throw std::runtime_error("batch graph inputs must be problem batch handles");
+    if (batches[i]->dim != batches[0]->dim) throw std::runtime_error("problem batches of a graph must share a dimension");
+  }
+  BatchGraph* g = new BatchGraph();
+  try {
+    RTDL_CUDA_CHECK(cudaGetDevice(&g->device));
+    RTDL_CUDA_CHECK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    cudaStream_t s = g->stream;
+    g->rows = rows_dev;
+    g->capacity = rows_dev ? rows_capacity : 0;
+    uint32_t p0 = 0, most_np = 0, most_nq = 0;
+    const size_t rec = batches[0]->dim == 2 ? sizeof(RtdlPoint) : sizeof(RtdlPoint3D);
+    g->parts.reserve(batch_count);
+    for (uint32_t i = 0; i < batch_count; ++i) {
+      Scene* sc = batches[i];
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(sc->stream));  // built on its own stream
+      g->parts.emplace_back();
+      BatchGraphPart& b = g->parts.back();
+      b.sc = sc;
+      b.p0 = p0;
+      b.problems = sc->problems;
+      const unsigned long long q0 = query_offsets[p0], q1 = query_offsets[p0 + sc->problems];
+      if (q1 < q0 || q1 - q0 > 0xFFFFFFFFull - 32) throw std::runtime_error("query offsets must be non-decreasing");
+      b.nq = (uint32_t)(q1 - q0);
+      if (b.nq > 0 && !queries_dev) throw std::runtime_error("query_points_dev must not be null when queries exist");
+      b.queries = static_cast<const char*>(queries_dev) + q0 * rec;
+      b.qoff.resize(sc->problems + 1);
+      for (uint32_t p = 0; p <= sc->problems; ++p) b.qoff[p] = query_offsets[p0 + p] - q0;
+      b.radius.assign(radius + p0, radius + p0 + sc->problems);
+      b.kmax.assign(kmax + p0, kmax + p0 + sc->problems);
+      for (uint32_t p = 0; p < sc->problems; ++p) {
+        if (b.qoff[p + 1] < b.qoff[p]) throw std::runtime_error("query offsets must be non-decreasing");
+        if (!(b.radius[p] >= 0.0)) throw std::runtime_error("radius must be non-negative");
+        if (b.kmax[p] < 1 || b.kmax[p] > 64) throw std::runtime_error("a problem batch takes k_max in [1, 64]");
+      }
+      if (b.nq > 0) {
+        BatchSpec bs;
+        bs.problems = sc->problems;
+        bs.qoff = b.qoff.data();
+        bs.radius = b.radius.data();
+        bs.kmax = b.kmax.data();
+        b.qp = prepare_queries_batch(sc, b.queries, b.nq, bs, s);
+        b.qrank = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * b.nq, s));
+        k_invert<<<grid_for(b.nq, 256), 256, 0, s>>>(b.qp.oorder, b.nq, b.qp.order_identity, b.qrank);
+        RTDL_LAUNCHED(1);
+      }
+      b.offsets = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * ((size_t)b.nq + 1), s));
+      RTDL_CUDA_CHECK(cudaMemsetAsync(b.offsets, 0, sizeof(unsigned long long) * ((size_t)b.nq + 1), s));
+      most_np = b.qp.nproc > most_np ? b.qp.nproc : most_np;
+      most_nq = b.nq > most_nq ? b.nq : most_nq;
+      p0 += sc->problems;
+    }
+    g->problems = p0;
+    const size_t n = most_np ? most_np : 1, nqm = most_nq ? most_nq : 1, B = batch_count;
+    auto alloc = [&](size_t bytes) {
+      void* p = dev_alloc(bytes ? bytes : 1, s);
+      g->buffers.push_back(p);
+      return p;
+    };
+    g->slab = static_cast<unsigned long long*>(alloc(sizeof(unsigned long long) * slab_base((uint32_t)n)));
+    g->counts = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * nqm));
+    g->qinfo = static_cast<QueryInfo*>(alloc(sizeof(QueryInfo) * n));
+    g->flags = static_cast<uint8_t*>(alloc(nqm));
+    g->heavy_list = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * nqm));
+    g->heavy_m = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * nqm));
+    g->heavy_t = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * nqm));
+    g->mid_list = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->big_list = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->fix_list = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+    g->poff = static_cast<unsigned long long*>(alloc(sizeof(unsigned long long) * n));
+    g->scan_ws = alloc(scan_workspace_bytes((uint32_t)nqm));
+    for (int k = 0; k < 2; ++k) {
+      g->D.work[k] = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+      g->D.rad[k] = static_cast<double*>(alloc(sizeof(double) * n));
+      g->D.lo[k] = static_cast<double*>(alloc(sizeof(double) * n));
+      g->D.hi[k] = static_cast<double*>(alloc(sizeof(double) * n));
+      g->D.full[k] = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * n));
+      g->D.frad[k] = static_cast<double*>(alloc(sizeof(double) * n));
+    }
+    g->D.cnt = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * nqm));
+    g->D.gen_qin = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * nqm));
+    g->D.gen_m = static_cast<uint32_t*>(alloc(sizeof(uint32_t) * nqm));
+    g->D.gen_rad = static_cast<double*>(alloc(sizeof(double) * nqm));
+    g->small = static_cast<unsigned int*>(alloc(sizeof(unsigned int) * 8 * B));
+    g->pass_count = static_cast<unsigned int*>(alloc(sizeof(unsigned int) * kRefinePasses * B));
+    g->queue = static_cast<unsigned int*>(alloc(sizeof(unsigned int) * B));
+    g->base = static_cast<unsigned long long*>(alloc(sizeof(unsigned long long) * (B + 1)));
+    g->prob_rows = static_cast<unsigned long long*>(alloc(sizeof(unsigned long long) * ((size_t)g->problems + 1)));
+    g->status = static_cast<unsigned int*>(alloc(sizeof(unsigned int) * B));
+    RTDL_CUDA_CHECK(cudaMemsetAsync(g->prob_rows, 0, sizeof(unsigned long long) * ((size_t)g->problems + 1), s));
+    RTDL_CUDA_CHECK(cudaMallocHost(&g->status_host, sizeof(unsigned int) * B));
+    RTDL_CUDA_CHECK(cudaMallocHost(&g->rows_host, sizeof(unsigned long long) * ((size_t)g->problems + 1)));
+    int per_sm = 0;
+    RTDL_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_collect_persistent<kPersistentMinBlocks>, 256, 0));
+    int sms = kSmCount;
+    RTDL_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+    g->persistent_grid = (unsigned int)(sms * (per_sm > 0 ? per_sm : 1));
+    // bad coordinates or a failed sort wait in a batch or its queries fail creation
+    Readback* rb = pinned_readback();
+    for (auto& b : g->parts) {
+      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &b.sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                      s));
+      rb->query_bad = 0;
+      if (b.qp.qst)
+        RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &b.qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                        s));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      throw_if_bad(rb->query_bad | rb->scene_bad);
+    }
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // everything allocated and prepared before capture
+    batch_graph_capture(g);
+  } catch (...) {
+    batch_graph_destroy(g);
+    throw;
+  }
+  return g;
+}
+
+void batch_graph_launch(BatchGraph* g, cudaStream_t s) {
+  count_launches(g->kernels);
+  if (s && s != g->stream) {
+    cudaEvent_t e;
+    RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    RTDL_CUDA_CHECK(cudaEventRecord(e, s));
+    RTDL_CUDA_CHECK(cudaStreamWaitEvent(g->stream, e, 0));
+    RTDL_CUDA_CHECK(cudaGraphLaunch(g->exec, g->stream));
+    RTDL_CUDA_CHECK(cudaEventRecord(e, g->stream));
+    RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, e, 0));
+    note_cleanup_error(cudaEventDestroy(e), "cudaEventDestroy");
+  } else {
+    RTDL_CUDA_CHECK(cudaGraphLaunch(g->exec, g->stream));
+  }
+}
+
+void batch_graph_replay(BatchGraph* g, unsigned long long* row_offsets_out, unsigned int* status_out) {
+  batch_graph_launch(g, nullptr);
+  cudaStream_t s = g->stream;
+  const uint32_t B = (uint32_t)g->parts.size();
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(g->status_host, g->status, sizeof(unsigned int) * B, cudaMemcpyDeviceToHost, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(g->rows_host, g->prob_rows, sizeof(unsigned long long) * ((size_t)g->problems + 1),
+                                  cudaMemcpyDeviceToHost, s));
+  RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+  unsigned int all = 0;
+  for (uint32_t i = 0; i < B; ++i) {
+    const unsigned int st = g->status_host[i];
+    all |= st;
+    if (st & kGraphStatusOverflow) throw std::runtime_error("LBVH traversal stack overflow");
+    if ((st & kGraphStatusGeneric) && g->rows && !(st & kBatchGraphStatusRows)) {
+      // heavy queries the refinement did not resolve: this batch's rows by the plain batch call
+      BatchGraphPart& b = g->parts[i];
+      const unsigned long long first = g->rows_host[b.p0];
+      std::vector<unsigned long long> local(b.problems + 1);
+      BatchSpec bs;
+      bs.problems = b.problems;
+      bs.qoff = b.qoff.data();
+      bs.radius = b.radius.data();
+      bs.kmax = b.kmax.data();
+      bs.row_offsets = local.data();
+      run_query_batch(b.sc, b.queries, bs, static_cast<char*>(g->rows) + first * sizeof(RtdlFixedRadiusNeighborRow),
+                      g->capacity - first, nullptr, nullptr, s, nullptr);
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      ++g->fallbacks;
+    }
+  }
+  if (status_out) *status_out = all;
+  if (row_offsets_out)
+    std::memcpy(row_offsets_out, g->rows_host, sizeof(unsigned long long) * ((size_t)g->problems + 1));
+}
+
+uint32_t batch_graph_problems(const BatchGraph* g) { return g->problems; }
+int batch_graph_kernels(const BatchGraph* g) { return g->kernels; }
+uint64_t batch_graph_fallbacks(const BatchGraph* g) { return g->fallbacks; }
+
+void batch_graph_destroy(BatchGraph* g) {
+  if (!g) return;
+  if (g->stream) sync_quietly(g->stream);
+  batch_graph_release(g);
+  cudaStream_t s = g->stream;
+  for (auto& b : g->parts) {
+    if (b.nq > 0) free_prep(b.qp, s);
+    dev_free(b.qrank, s);
+    dev_free(b.offsets, s);
+  }
+  for (void* p : g->buffers) dev_free(p, s);
+  if (g->status_host) note_cleanup_error(cudaFreeHost(g->status_host), "cudaFreeHost");
+  if (g->rows_host) note_cleanup_error(cudaFreeHost(g->rows_host), "cudaFreeHost");
+  if (s) {
+    sync_quietly(s);
+    note_cleanup_error(cudaStreamDestroy(s), "cudaStreamDestroy");
+  }
+  delete g;
 }
 
 }  // namespace rtdl_b200

@@ -145,6 +145,36 @@ def test_every_traversal_matches_oracle(gpu, traversal):
         rt.set_tuning()
 
 
+@pytest.mark.parametrize("traversal", ["packet", "lane"])
+def test_knn_walks_match_oracle(gpu, traversal):
+    """The nearest-list walk in warp packets over density-class order (default)
+    and one thread per query in Morton order ("lane"): KNN rows and the
+    Hausdorff nearest, on clustered 3D sets with a query count that leaves a
+    partial last warp, and on a 2D lattice whose equal distances are broken
+    by id."""
+    rng = np.random.default_rng(33)
+    centres = rng.random((10, 3))
+    s = _cols(_clustered(rng, 25000, centres))
+    q = _cols(_clustered(rng, 4001, centres))
+    g = np.stack(np.meshgrid(np.arange(60), np.arange(60)), -1).reshape(-1, 2).astype(np.float64) * 0.5
+    s2 = {"id": np.arange(len(g), dtype=np.uint32), "x": g[:, 0], "y": g[:, 1]}
+    q2 = {"id": np.arange(720, dtype=np.uint32), "x": g[::5, 0][:720] + 0.25, "y": g[::5, 1][:720]}
+    rt.set_tuning(traversal=traversal)
+    try:
+        for search, query in ((s, q), (s2, q2)):
+            with rt.B200Scene(_pack(search)) as scene:
+                for k in (1, 5, 16, 40):
+                    v = scene.query(_pack(query), predicate="knn_rows", limit=k)
+                    _assert_same_rows(v.to_numpy(), O.knn_rows(query, search, k=k, threads=8), True)
+                    v.close()
+                w = scene.directed_hausdorff(_pack(query))
+                exp = O.directed_hausdorff(query, search, threads=8)
+                assert (w["distance"], w["source_id"], w["target_id"]) == \
+                    (exp["distance"], exp["source_id"], exp["target_id"])
+    finally:
+        rt.set_tuning()
+
+
 def test_bounded_knn_and_knn_3d_match_oracle(gpu):
     rng = np.random.default_rng(5)
     centres = rng.random((8, 3))

@@ -327,7 +327,7 @@ def secondary_leg(workload: str, steps: int, warmup: int) -> dict:
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     knn = workload == "knn"
     if knn:
-        probe, build = workloads.clustered_3d()
+        probe, build = workloads.clustered_3d(N_BUILD, N_PROBE)  # --build / --probes for a smaller case
         k = 16
         units = len(probe) * k
     else:
@@ -392,7 +392,7 @@ def secondary_leg(workload: str, steps: int, warmup: int) -> dict:
         kernel = "k_pass1<KNN> (nearest-list LBVH walk)"
         full = {}
         ref = digests.get("knn16_1m")
-        if ref:
+        if ref and len(probe) == len(build) == 1 << 20:
             packed = np.zeros(len(rows), dtype=np.dtype({"names": ["query_id", "neighbor_id", "distance", "neighbor_rank"],
                                                          "formats": ["<u4", "<u4", "<f8", "<u4"],
                                                          "offsets": [0, 4, 8, 16], "itemsize": 20}))

@@ -83,6 +83,33 @@ def test_prepare_validation():
     assert err.value.decode() == "fixed_radius_neighbors_3d max_radius must be positive"
 
 
+def test_batch_graph_validation_before_any_gpu_work():
+    lib = _native.load_library()
+    g = ctypes.c_void_p()
+    err = _native.error_buffer()
+    qoff = (ctypes.c_ulonglong * 2)(0, 0)
+    radius = (ctypes.c_double * 1)(0.1)
+    kmax = (ctypes.c_uint32 * 1)(8)
+    assert lib.rtdl_b200_batch_graph_create(None, 1, None, qoff, radius, kmax, None, 0, None, err, len(err)) == 1
+    assert err.value.decode() == "graph_out must not be null"
+    assert lib.rtdl_b200_batch_graph_create(None, 1, None, qoff, radius, kmax, None, 0, ctypes.byref(g), err,
+                                            len(err)) == 1
+    assert err.value.decode() == "batches must not be null"
+    batches = (ctypes.c_void_p * 1)(None)
+    assert lib.rtdl_b200_batch_graph_create(batches, 0, None, qoff, radius, kmax, None, 0, ctypes.byref(g), err,
+                                            len(err)) == 1
+    assert err.value.decode() == "a batch graph needs at least one problem batch"
+    assert lib.rtdl_b200_batch_graph_create(batches, 1, None, qoff, radius, kmax, None, 0, ctypes.byref(g), err,
+                                            len(err)) == 1
+    assert err.value.decode() == "batch graph inputs must be problem batch handles"
+    assert g.value is None
+    assert lib.rtdl_b200_batch_graph_replay(None, None, None, err, len(err)) == 1
+    assert err.value.decode() == "graph must not be null"
+    assert lib.rtdl_b200_batch_graph_launch(None, None, err, len(err)) == 1
+    assert lib.rtdl_b200_batch_graph_info(None, None, None, None) == 1
+    lib.rtdl_b200_batch_graph_destroy(None)  # no-op
+
+
 def test_set_tuning_bounds():
     with pytest.raises(ValueError):
         rt.set_tuning(leaf_size=-1, block_threads=128)

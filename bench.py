@@ -613,7 +613,7 @@ def run_batch(args) -> int:
     from rtdl_b200.autotune import Autotuner
 
     med = int(np.argsort(nb * nq)[len(nb) // 2])
-    tuner = Autotuner(repeats=2, traversals=("packet",))
+    tuner = Autotuner(repeats=2, traversals=("packet_hybrid", "packet"))
     tune_key, tune_cfg = tuner.tune(d_build.data_ptr() + 32 * int(boff[med]), int(nb[med]),
                                     d_probe.data_ptr() + 32 * int(qoff[med]), int(nq[med]), dimension=3,
                                     radius=float(radius[med]), k_max=int(kmax[med]), stream=sh)
@@ -1111,7 +1111,7 @@ def main(argv=None) -> int:
     if args.traversal is not None or args.leaf_size is not None:
         import rtdl_b200 as rt
 
-        rt.set_tuning(leaf_size=args.leaf_size or 0, traversal=args.traversal or "packet")
+        rt.set_tuning(leaf_size=args.leaf_size or 0, traversal=args.traversal or "packet_hybrid")
     if args.workload == "batch":
         return run_batch(args)
     if args.workload == "serve":

@@ -639,10 +639,10 @@ RTDL_B200_API int rtdl_b200_get_launch_count(unsigned long long* count_out);
  * or 256; traversal: 0 = one warp walks the tree for 32 neighbouring queries
  * (packet), 1 = one thread per query, 2 = packet with the query's bounding
  * cube tested at internal nodes, 3 = packet whose leaf buckets are tested
- * point-major (a lane per point, the reaching queries in turn), 4 = packet
- * choosing lane- or point-major per bucket (point-major when at most half as
- * many of the packet's queries reach it as it holds points).  Returns 0 on
- * success. */
+ * point-major (a lane per point, the reaching queries in turn), 4 (the
+ * default) = packet choosing lane- or point-major per bucket (point-major when
+ * at most half as many of the packet's queries reach it as it holds points).
+ * Every setting returns the same rows.  Returns 0 on success. */
 RTDL_B200_API int rtdl_b200_set_tuning(int leaf_size, int block_threads, int traversal);
 
 #ifdef __cplusplus

@@ -5,7 +5,9 @@ leaf, the traversal's tile), the collect traversal (``packet``: one warp walks
 the tree for 32 neighbouring queries; ``packet_cube``: the same with the
 query's bounding cube tested at internal nodes; ``packet_points``: the same
 with leaf buckets tested a lane per point, the reaching queries in turn;
-``lane``: one thread per query) and the collect block size.  A shape class is the dimension plus the
+``packet_hybrid``, the library default: the one of those two leaf tests that
+costs less for each bucket; ``lane``: one thread per query) and the collect
+block size.  A shape class is the dimension plus the
 log2 buckets of the build size, the query count and the mean in-radius count
 (from a sampled query).  :meth:`Autotuner.tune` times every candidate on the
 caller's device-resident data with CUDA events (min of ``repeats``), keeps
@@ -29,14 +31,14 @@ from . import _native
 from .runtime import B200Scene, set_tuning
 
 LEAF_SIZES = (8, 16, 24)
-TRAVERSALS = ("packet", "packet_cube", "packet_points", "lane")
+TRAVERSALS = ("packet_hybrid", "packet", "packet_cube", "packet_points", "lane")
 BLOCK_THREADS = (128, 256)
 
 
 @dataclass(frozen=True)
 class Config:
     leaf_size: int = 0  # 0: by the scene's use (see set_tuning)
-    traversal: str = "packet"
+    traversal: str = "packet_hybrid"
     block_threads: int = 128
 
     def apply(self) -> None:

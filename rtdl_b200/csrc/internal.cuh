@@ -156,9 +156,10 @@ struct Scene {
 struct Tuning {
   int leaf_size = 0;  // 0: automatic (leaf_size_for)
   int block_threads = 128;
-  int traversal = 0;  // fixed-radius collect: 0 = one warp per 32 queries (packet), 1 = one thread per
+  int traversal = 4;  // fixed-radius collect: 0 = one warp per 32 queries (packet), 1 = one thread per
                       // query, 2 = packet with cube tests at internal nodes, 3 = packet with
-                      // point-major leaf tests, 4 = packet choosing lane- or point-major per leaf
+                      // point-major leaf tests, 4 (default) = packet choosing lane- or point-major
+                      // per leaf
 };
 // The tuning a call runs with: a copy of the process-wide setting taken when
 // the entry point starts (rtdl_b200_set_tuning from another thread changes the

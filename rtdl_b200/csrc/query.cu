@@ -2605,7 +2605,8 @@ void launch_collect(const CollectParams& C, uint32_t np, uint32_t nq, bool batch
     const bool cube = tuning().traversal == 2;
     // occupancy bounds chosen so neither variant spills (32 and 40 registers)
     if (batch)  // several problems (traversal counters are not gathered here)
-      k_collect_packet<false, false, true, 5><<<grid, threads, 0, s>>>(C);
+      tuning().traversal == 4 ? k_collect_packet<false, false, true, 5, kLeafHybrid><<<grid, threads, 0, s>>>(C)
+                              : k_collect_packet<false, false, true, 5><<<grid, threads, 0, s>>>(C);
     else if (tuning().traversal == 3)
       stats ? k_collect_packet<true, false, false, 1, kLeafPointMajor><<<grid, threads, 0, s>>>(C)
             : k_collect_packet<false, false, false, 6, kLeafPointMajor><<<grid, threads, 0, s>>>(C);
@@ -4157,7 +4158,7 @@ __global__ void k_empty_batch_rows(const unsigned long long* base, uint32_t prob
 }
 
 // Persistent collect over one batch: 32-query packets from a work queue.
-template <int MIN_BLOCKS>
+template <int MIN_BLOCKS, int LEAF>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_persistent(CollectParams P, unsigned int* queue) {
   const uint32_t packets = (P.nq + 31u) / 32u;
   const uint32_t lane = threadIdx.x & 31u;
@@ -4166,7 +4167,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_persistent(CollectP
     if (lane == 0) item = atomicAdd(queue, 1u);
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= packets) return;
-    collect_packet_body<false, false, true, kLeafLaneMajor>(P, item * 32u + lane);
+    collect_packet_body<false, false, true, LEAF>(P, item * 32u + lane);
   }
 }
 
@@ -4224,6 +4225,7 @@ struct BatchGraph {
   unsigned int* status_host = nullptr;      // pinned
   unsigned long long* rows_host = nullptr;  // pinned, problems + 1
   unsigned int persistent_grid = 0;
+  bool hybrid = true;  // leaf buckets tested lane- or point-major per bucket (the tuning at creation)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int kernels = 0;
@@ -4267,7 +4269,10 @@ void batch_graph_enqueue(BatchGraph* g, uint32_t i, cudaStream_t s) {
   C.overflow_out = nullptr;
   C.stats = nullptr;
   const uint32_t np = b.qp.nproc;
-  k_collect_persistent<kPersistentMinBlocks><<<g->persistent_grid, 256, 0, s>>>(C, g->queue + i);
+  if (g->hybrid)
+    k_collect_persistent<kPersistentMinBlocks, kLeafHybrid><<<g->persistent_grid, 256, 0, s>>>(C, g->queue + i);
+  else
+    k_collect_persistent<kPersistentMinBlocks, kLeafLaneMajor><<<g->persistent_grid, 256, 0, s>>>(C, g->queue + i);
   RTDL_LAUNCHED(1);
   scan_counts_u64_ws(g->counts, b.qp.oorder, b.qp.order_identity, b.nq, b.offsets, g->scan_ws, s);
   k_add_row_base<<<grid_for(b.nq + 1, 256), 256, 0, s>>>(b.offsets, b.nq, g->base + i, g->base + i + 1);
@@ -4444,9 +4449,14 @@ BatchGraph* batch_graph_create(Scene* const* batches, uint32_t batch_count, cons
     RTDL_CUDA_CHECK(cudaMemsetAsync(g->prob_rows, 0, sizeof(unsigned long long) * ((size_t)g->problems + 1), s));
     RTDL_CUDA_CHECK(cudaMallocHost(&g->status_host, sizeof(unsigned int) * B));
     RTDL_CUDA_CHECK(cudaMallocHost(&g->rows_host, sizeof(unsigned long long) * ((size_t)g->problems + 1)));
+    g->hybrid = tuning().traversal == 4;
     int per_sm = 0;
-    RTDL_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, k_collect_persistent<kPersistentMinBlocks>, 256, 0));
+    if (g->hybrid)
+      RTDL_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, k_collect_persistent<kPersistentMinBlocks, kLeafHybrid>, 256, 0));
+    else
+      RTDL_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, k_collect_persistent<kPersistentMinBlocks, kLeafLaneMajor>, 256, 0));
     int sms = kSmCount;
     RTDL_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
     g->persistent_grid = (unsigned int)(sms * (per_sm > 0 ? per_sm : 1));

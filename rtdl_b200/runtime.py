@@ -1521,7 +1521,7 @@ def hausdorff_distance(points_a, points_b, *, dimension: int | None = None) -> d
     }
 
 
-def set_tuning(*, leaf_size: int = 0, block_threads: int = 128, traversal: str = "packet") -> None:
+def set_tuning(*, leaf_size: int = 0, block_threads: int = 128, traversal: str = "packet_hybrid") -> None:
     """Set the kernel tuning knobs (see ``rtdl_b200_set_tuning``); ``leaf_size`` 0 picks the leaf
     bucket size by the scene's use (24 points for fixed-radius-only scenes, 8 otherwise)."""
     modes = {"packet": 0, "lane": 1, "packet_cube": 2, "packet_points": 3, "packet_hybrid": 4}

@@ -15,7 +15,7 @@ def test_every_configuration_gives_the_same_rows(gpu):
     ref = None
     try:
         for leaf in (4, 8, 16):
-            for trav in ("packet", "packet_cube", "lane"):
+            for trav in ("packet_hybrid", "packet", "packet_cube", "lane"):
                 for bt in (128, 256):
                     Config(leaf, trav, bt).apply()
                     view = rt.runtime.fixed_radius_neighbors(probe, build, radius=0.006, k_max=48)

@@ -473,7 +473,6 @@ struct CollectParams {
                              // [3] big_list length, [4] emit fixup queue length
   uint8_t* overflow_out;     // optional: 1 per query (input order) when count > kmax
   unsigned long long* stats;
-  const double* qradius = nullptr;  // nearest searches: each query's own radius (input order), else nullptr
 };
 
 // Per-query state of the collect pass and its accept / finish steps, shared by
@@ -695,22 +694,6 @@ __global__ void __launch_bounds__(256) k_collect(CollectParams P) {
 // one scene): each warp walks its problem's subtree with its problem's bands
 // and kmax; kept out of the single-problem instantiation, whose registers it
 // would cost.
-// The bands of DevBands recomputed for another radius (same formulas; the
-// FP32 e_abs is rounded up, which only widens them).
-__device__ __forceinline__ DevBands bands_at_radius(const DevBands& base, double radius) {
-  DevBands b = base;
-  const double rho = (double)base.rho, e_abs = (double)base.e_abs;
-  const double r_hi = radius * (1.0 + rho) + e_abs + 1.0e-18;
-  const double r_lo = radius * (1.0 - rho) - e_abs;
-  float hi2 = __double2float_ru(r_hi * r_hi);
-  if (hi2 < b.floor2) hi2 = b.floor2;
-  b.hi2 = hi2;
-  b.lo2 = r_lo > 0.0 ? __double2float_rd(r_lo * r_lo) : 0.0f;
-  b.box_hi2 = __double2float_ru((double)hi2 * (1.0 + 1.0e-6));
-  b.r2 = radius * radius;
-  return b;
-}
-
 // LEAF: how a reached leaf bucket is tested -- 0 lane-major (collect_leaf:
 // every lane loops over the bucket's points), 1 point-major (collect_leaf_pm:
 // the warp loops over the reaching queries), 2 either, chosen per bucket
@@ -718,18 +701,13 @@ __device__ __forceinline__ DevBands bands_at_radius(const DevBands& base, double
 // point, i.e. when few of the packet's spheres reach the bucket.
 constexpr int kLeafLaneMajor = 0, kLeafPointMajor = 1, kLeafHybrid = 2;
 // The packet walk for processing ranks t & ~31 .. (t & ~31) + 31 (lane t & 31).
-// PERQ: every query has its own radius (P.qradius, nearest searches routed
-// through this pass): each lane tests nodes and points against its own bands,
-// and leaf buckets are tested lane-major.
-template <bool STATS, bool CUBE, bool BATCH, int LEAF, bool PERQ = false>
+template <bool STATS, bool CUBE, bool BATCH, int LEAF>
 __device__ __forceinline__ void collect_packet_body(const CollectParams& P, uint32_t t) {
-  static_assert(!PERQ || (LEAF == 0 && !BATCH && !CUBE), "per-query radii are tested lane-major on one problem");
   // a problem batch pads every problem to whole warps, so a warp has one problem
   const uint32_t prob = BATCH ? P.warp_prob[t >> 5] : 0u;
   const bool valid = t < P.nq && (!BATCH || P.qorder[t] != kNone);
   if (BATCH && !valid && t < P.nq) P.qinfo[t] = QueryInfo{0.0, 0.0, 0.0, 0u, 0u};  // padding: nothing to emit
-  DevBands B = P.bands[prob];
-  if (PERQ && valid) B = bands_at_radius(B, P.qradius[P.qorder[t]]);
+  const DevBands B = P.bands[prob];
   const SceneView& S = P.S;
   const int scene_inexact = *S.inexact;
   CollectLane L;
@@ -785,11 +763,11 @@ __device__ __forceinline__ void collect_packet_body(const CollectParams& P, uint
   if (valid) collect_finish<STATS>(P, L, BATCH ? P.prob_kmax[prob] : P.kmax);
 }
 
-template <bool STATS, bool CUBE, bool BATCH, int MIN_BLOCKS, int LEAF = kLeafLaneMajor, bool PERQ = false>
+template <bool STATS, bool CUBE, bool BATCH, int MIN_BLOCKS, int LEAF = kLeafLaneMajor>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParams P) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!__any_sync(0xffffffffu, t < P.nq)) return;  // whole warp past the end
-  collect_packet_body<STATS, CUBE, BATCH, LEAF, PERQ>(P, t);
+  collect_packet_body<STATS, CUBE, BATCH, LEAF>(P, t);
 }
 
 // ---- heavy queries: radius refinement -------------------------------------------
@@ -801,6 +779,22 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) k_collect_packet(CollectParam
 // in-radius count (cube-root scaling towards ~2 kmax points) inside a bracket
 // [lo, hi] that every pass narrows; queries still unresolved after a few
 // passes (for instance many points at one distance) take the generic path.
+
+// The bands of DevBands recomputed for another radius (same formulas; the
+// FP32 e_abs is rounded up, which only widens them).
+__device__ __forceinline__ DevBands bands_at_radius(const DevBands& base, double radius) {
+  DevBands b = base;
+  const double rho = (double)base.rho, e_abs = (double)base.e_abs;
+  const double r_hi = radius * (1.0 + rho) + e_abs + 1.0e-18;
+  const double r_lo = radius * (1.0 - rho) - e_abs;
+  float hi2 = __double2float_ru(r_hi * r_hi);
+  if (hi2 < b.floor2) hi2 = b.floor2;
+  b.hi2 = hi2;
+  b.lo2 = r_lo > 0.0 ? __double2float_rd(r_lo * r_lo) : 0.0f;
+  b.box_hi2 = __double2float_ru((double)hi2 * (1.0 + 1.0e-6));
+  b.r2 = radius * radius;
+  return b;
+}
 
 struct RefineParams {
   CollectParams C;         // scene, queries, processing order, bands, slab
@@ -1098,14 +1092,13 @@ __global__ void k_refine_update(RefineUpdate U) {
 __global__ void k_refine_init(const uint32_t* heavy_qin, const uint32_t* heavy_m, const uint32_t* heavy_t,
                               uint32_t H, const uint32_t* qprob, const double* prob_radius, double radius,
                               const uint32_t* prob_kmax, uint32_t kmax, uint32_t* work, double* rad, double* lo,
-                              double* hi, uint32_t* full, double* frad, const unsigned int* H_dev,
-                              const double* qradius) {
+                              double* hi, uint32_t* full, double* frad, const unsigned int* H_dev) {
   if (H_dev) H = *H_dev;  // captured graphs: the collect pass's heavy count
   for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < H; h += gridDim.x * blockDim.x) {
     const uint32_t qin = heavy_qin[h], p = qprob ? qprob[qin] : 0u;
     const uint32_t m = heavy_m[h];
     work[h] = heavy_t[h];
-    const double r = qradius ? qradius[qin] : prob_radius ? prob_radius[p] : radius;
+    const double r = prob_radius ? prob_radius[p] : radius;
     const uint32_t k = prob_kmax ? prob_kmax[p] : kmax;
     rad[h] = r * cbrt(2.0 * k / (double)m);
     hi[h] = r;
@@ -1842,66 +1835,6 @@ __global__ void k_knn_class(const float4* qpts, const uint32_t* qorder, const ui
   }
 }
 
-// Nearest searches routed through the radius pass: each query's radius bounds
-// its k-th nearest distance from above.  It is taken from the seed window of
-// 2w scene points around the query's Morton code (w >= k): the k-th smallest
-// FP32 d2 among them, widened by the bands' error model (relative 2 rho,
-// absolute 2 e_abs), so those k points lie within it in exact arithmetic and
-// the k nearest overall do too.  One warp per query (processing rank t): the
-// window's keys are sorted across the warp.  The FP32 exponent of that k-th d2
-// is the query's density class, used to order the processing ranks.
-template <int E>
-__global__ void __launch_bounds__(256) k_knn_seed(const float4* qpts, const uint32_t* qorder, const uint32_t* qcodes,
-                                                  uint32_t nq, const float4* spts, const uint32_t* scodes,
-                                                  uint32_t ns, int k, int w, const DevBands* base, double* qradius,
-                                                  uint32_t* cls, uint32_t* rank) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  const double rho = (double)base->rho, e_abs = (double)base->e_abs;
-  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nq; t += warps) {
-    const uint32_t qin = qorder[t];
-    const float4 q = qpts[qin];
-    const uint32_t code = qcodes[t];
-    uint32_t lo = 0, hi = ns;
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (__ldg(&scodes[mid]) < code) lo = mid + 1;
-      else hi = mid;
-    }
-    int a = (int)lo - w;
-    if (a < 0) a = 0;
-    int b = a + 2 * w;
-    if (b > (int)ns) {
-      b = (int)ns;
-      a = b - 2 * w < 0 ? 0 : b - 2 * w;
-    }
-    uint32_t v[E];
-#pragma unroll
-    for (int r = 0; r < E; ++r) {
-      const int i = a + (r << 5) + lane;
-      if (i < b) {
-        const float4 p = __ldg(&spts[i]);
-        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-        v[r] = __float_as_uint(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));  // d2 >= 0: bit order is value order
-      } else {
-        v[r] = 0xFFFFFFFFu;
-      }
-    }
-    warp_bitonic_striped<E>(v, lane);
-    uint32_t sel = v[0];
-#pragma unroll
-    for (int r = 1; r < E; ++r)
-      if (r == ((k - 1) >> 5)) sel = v[r];
-    const uint32_t kth = __shfl_sync(0xffffffffu, sel, (k - 1) & 31);
-    if (lane == 0) {
-      const double d = sqrt((double)__uint_as_float(kth));
-      qradius[qin] = d * (1.0 + 2.0 * rho) + 2.0 * e_abs + 1.0e-30;
-      cls[t] = (kth >> 23) & 0xFFu;
-      rank[t] = t;
-    }
-  }
-}
-
 __global__ void k_permute_pair(const uint32_t* a, const uint32_t* b, const uint32_t* perm, uint32_t n, uint32_t* a_out,
                                uint32_t* b_out) {
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
@@ -2325,7 +2258,6 @@ struct QueryPrep {
   double* prob_radius = nullptr;       // radius of each problem
   int* shared_roots = nullptr;         // requests against one plain scene: every problem's root is the scene's
   SceneView view{};                    // the scene as the traversal kernels see it
-  double* qradius = nullptr;            // nearest searches routed through the radius pass: radius per query
   const PreparedQueries* borrowed = nullptr;  // set: the query-side buffers belong to a prepared query set
 };
 
@@ -2471,13 +2403,10 @@ void free_prep(QueryPrep& qp, cudaStream_t s) {
   dev_free(qp.sorted_flag, s);
   dev_free(qp.qoff, s);
   dev_free(qp.shared_roots, s);
-  dev_free(qp.qradius, s);
   dev_free(qp.prob_radius, s);
 }
 
 }  // namespace
-
-void seed_knn_radius(Scene* sc, QueryPrep& qp, uint32_t nq, uint32_t k, cudaStream_t s);
 
 namespace {
 
@@ -2592,7 +2521,7 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
   unsigned int* next_count = static_cast<unsigned int*>(alloc(sizeof(unsigned int)));
   k_refine_init<<<div_up(H, 256), 256, 0, s>>>(heavy_list, heavy_m, heavy_t, H, qp.qprob, qp.prob_radius, radius,
                                                qp.prob_kmax, kmax, work[0], rad[0], lo[0], hi[0], full[0],
-                                               frad[0], nullptr, qp.qradius);
+                                               frad[0], nullptr);
   RTDL_LAUNCHED(1);
   Readback* rb = pinned_readback();
   uint32_t n = H;
@@ -2675,10 +2604,7 @@ void launch_collect(const CollectParams& C, uint32_t np, uint32_t nq, bool batch
     const unsigned int grid = div_up(np, threads);
     const bool cube = tuning().traversal == 2;
     // occupancy bounds chosen so neither variant spills (32 and 40 registers)
-    if (C.qradius)  // nearest searches: a radius per query
-      stats ? k_collect_packet<true, false, false, 1, kLeafLaneMajor, true><<<grid, threads, 0, s>>>(C)
-            : k_collect_packet<false, false, false, 5, kLeafLaneMajor, true><<<grid, threads, 0, s>>>(C);
-    else if (batch)  // several problems (traversal counters are not gathered here)
+    if (batch)  // several problems (traversal counters are not gathered here)
       tuning().traversal == 4 ? k_collect_packet<false, false, true, 5, kLeafHybrid><<<grid, threads, 0, s>>>(C)
                               : k_collect_packet<false, false, true, 5><<<grid, threads, 0, s>>>(C);
     else if (tuning().traversal == 3)
@@ -2725,7 +2651,7 @@ void enqueue_refine_device(const CollectParams& C, const uint32_t* qprob, const 
   RTDL_CUDA_CHECK(cudaMemsetAsync(D.pass_count, 0, sizeof(unsigned int) * kRefinePasses, s));
   k_refine_init<<<kSmCount * 4, 256, 0, s>>>(C.heavy_list, C.heavy_m, C.heavy_t, 0, qprob, prob_radius, radius,
                                              prob_kmax, kmax, D.work[0], D.rad[0], D.lo[0], D.hi[0], D.full[0],
-                                             D.frad[0], small, C.qradius);
+                                             D.frad[0], small);
   RTDL_LAUNCHED(1);
   int cur = 0;
   for (int pass = 0; pass < kRefinePasses; ++pass) {
@@ -2790,10 +2716,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
                              uint32_t kmax, void* rows_dev, size_t rows_capacity, void** rows_alloc,
                              uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer, const BatchSpec* bs = nullptr,
                              const SummarySpec* ss = nullptr, const PreparedQueries* pq = nullptr,
-                             bool witness = false, bool knn_seed = false) {
-  // knn_seed: a nearest search (predicate kKnn, kmax = k): every query is
-  // collected within its own radius bounding its k-th nearest distance
-  // (seed_knn_radius), and its k nearest are its rows.
+                             bool witness = false) {
   // witness (k_max 1): one row per query at its input position, pre-filled
   // with the no-witness row; the nearest in-radius neighbour overwrites it.
   QueryResult res;
@@ -2808,7 +2731,6 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
   QueryPrep qp = pq   ? borrow_prepared(sc, pq, radius, s)
                  : bs ? prepare_queries_batch(sc, queries_dev, nq, *bs, s)
                       : prepare_queries(sc, queries_dev, nq, true, radius, true, s);
-  if (knn_seed) seed_knn_radius(sc, qp, nq, kmax, s);
   const uint32_t np = qp.nproc;  // processing ranks
   const size_t nq1 = nq ? nq : 1, np1 = np ? np : 1;
   uint32_t* qrank = pq ? pq->qrank : static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
@@ -2880,7 +2802,6 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     C.small = small;
     C.overflow_out = overflow_dev;
     C.stats = nullptr;
-    C.qradius = qp.qradius;
     const bool stats = stats_enabled();
     if (stats) {
       C.stats = static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * kStatCount, s));
@@ -3836,39 +3757,6 @@ void order_by_density_class(Scene* sc, QueryPrep& qp, uint32_t nq, int w, cudaSt
   dev_free(rank, s);
 }
 
-// The per-query radii of a nearest search routed through the radius pass
-// (k_knn_seed), and the processing order by density class.  The scene must
-// hold at least 2 max(8, k) points.
-void seed_knn_radius(Scene* sc, QueryPrep& qp, uint32_t nq, uint32_t k, cudaStream_t s) {
-  const int w = k < 8 ? 8 : (int)k;  // 2w <= 128
-  qp.qradius = static_cast<double*>(dev_alloc(sizeof(double) * nq, s));
-  uint32_t* cls = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* rank = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* order = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* codes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  unsigned int blocks = div_up((uint64_t)nq * 32, 256);
-  if (blocks > (unsigned int)kSmCount * 16) blocks = kSmCount * 16;
-  if (2 * w <= 32)
-    k_knn_seed<1><<<blocks, 256, 0, s>>>(qp.qpts, qp.qorder, qp.qcodes, nq, sc->pts, sc->codes, sc->n, (int)k, w,
-                                         qp.bands, qp.qradius, cls, rank);
-  else if (2 * w <= 64)
-    k_knn_seed<2><<<blocks, 256, 0, s>>>(qp.qpts, qp.qorder, qp.qcodes, nq, sc->pts, sc->codes, sc->n, (int)k, w,
-                                         qp.bands, qp.qradius, cls, rank);
-  else
-    k_knn_seed<4><<<blocks, 256, 0, s>>>(qp.qpts, qp.qorder, qp.qcodes, nq, sc->pts, sc->codes, sc->n, (int)k, w,
-                                         qp.bands, qp.qradius, cls, rank);
-  RTDL_LAUNCHED(1);
-  radix_sort_pairs(cls, rank, nq, 0, 8, nullptr, &qp.qst->bad, s);
-  k_permute_pair<<<grid_for(nq, 256), 256, 0, s>>>(qp.qorder, qp.qcodes, rank, nq, order, codes);
-  RTDL_LAUNCHED(1);
-  dev_free(qp.qorder, s);
-  dev_free(qp.qcodes, s);
-  qp.qorder = order;
-  qp.qcodes = codes;
-  dev_free(cls, s);
-  dev_free(rank, s);
-}
-
 QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius, uint32_t limit,
                       void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
                       PhaseTimer* timer) {
@@ -3886,10 +3774,6 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
   if (!knn && limit <= (uint32_t)kMaxList)
     return run_radius_query(sc, queries_dev, nq, predicate, radius, limit, rows_dev, rows_capacity, rows_alloc,
                             overflow_dev, s, timer);
-  // k nearest as a radius search with a radius per query (tuning "lane": the list walk)
-  if (knn && limit <= (uint32_t)kMaxList && tuning().traversal != 1 && sc->n >= 2 * (limit < 8 ? 8 : limit))
-    return run_radius_query(sc, queries_dev, nq, predicate, 0.0, limit, rows_dev, rows_capacity, rows_alloc,
-                            overflow_dev, s, timer, nullptr, nullptr, nullptr, false, true);
   QueryPrep qp = prepare_queries(sc, queries_dev, nq, !knn, radius, true, s);
   const bool all_heavy = knn && limit > (uint32_t)kMaxList;
   const int L = all_heavy ? 1 : (int)(limit < (uint32_t)kMaxList ? limit : (uint32_t)kMaxList);

@@ -109,25 +109,6 @@ void dev_free(void* p, cudaStream_t s) {
   if (p) note_cleanup_error(cudaFreeAsync(p, s), "cudaFreeAsync");
 }
 
-namespace {
-thread_local RowBufferHook g_row_hook;
-thread_local void* g_hook_rows = nullptr;  // the buffer the hook handed out for this call
-}  // namespace
-
-RowBufferHook& row_buffer_hook() { return g_row_hook; }
-
-void* alloc_rows(size_t bytes, cudaStream_t s) {
-  if (g_row_hook.alloc) {
-    void* p = g_row_hook.alloc(bytes);
-    if (p) {
-      g_hook_rows = p;
-      return p;
-    }
-  }
-  return dev_alloc(bytes, s);
-}
-
-bool rows_on_host(const void* p) { return p != nullptr && p == g_hook_rows; }
 
 namespace {
 
@@ -220,54 +201,6 @@ class PinnedPool {
 PinnedPool& pinned_pool() {
   static PinnedPool* p = new PinnedPool();  // never destroyed: outlives static teardown order
   return *p;
-}
-
-void* download_rows(const void* d_rows, size_t bytes, cudaStream_t s);
-
-// Rows written by the kernels straight into the pinned buffer handed to the
-// caller (RTDL_B200_DIRECT_ROWS=0 keeps them in device memory and copies them
-// after the emit).
-bool direct_rows_enabled() {
-  static const bool on = [] {
-    const char* env = std::getenv("RTDL_B200_DIRECT_ROWS");
-    return !(env && env[0] == '0');
-  }();
-  return on;
-}
-
-// Sets the pinned-host row allocator for one host-buffer call on this thread.
-struct DirectRowsScope {
-  DirectRowsScope() {
-    if (direct_rows_enabled()) g_row_hook.alloc = [](size_t bytes) { return pinned_pool().get(bytes); };
-  }
-  ~DirectRowsScope() {
-    g_row_hook.alloc = nullptr;
-    g_hook_rows = nullptr;
-  }
-};
-
-// Releases a call's row buffer: pinned host rows go back to the pool once the
-// stream has finished writing them, device rows to the device pool.
-void release_rows(void* rows, cudaStream_t s) {
-  if (!rows) return;
-  if (rows_on_host(rows)) {
-    sync_quietly(s);
-    pinned_pool().put(rows);
-  } else {
-    dev_free(rows, s);
-  }
-}
-
-// The rows of a host-buffer call as the caller receives them: already in the
-// pinned buffer (written there by the kernels) or copied from device memory.
-void* rows_for_caller(void*& d_rows, size_t bytes, cudaStream_t s) {
-  if (rows_on_host(d_rows)) {
-    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-    void* host = d_rows;
-    d_rows = nullptr;
-    return host;
-  }
-  return download_rows(d_rows, bytes, s);
 }
 
 cudaStream_t library_stream() {
@@ -366,7 +299,6 @@ void validate_common(double radius, size_t limit, size_t nq, size_t ns, bool has
 void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim, int predicate, double radius,
                    size_t limit, void** rows_out, size_t* row_count_out) {
   cudaStream_t s = library_stream();
-  DirectRowsScope direct;
   PhaseTimer timer(s);
   timer.mark("begin");
   const size_t rec = record_size(dim);
@@ -380,21 +312,21 @@ void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim,
     QueryResult r = run_build_and_query(in, predicate, radius, (uint32_t)limit, nullptr, 0, &d_rows, nullptr, s,
                                         aux_stream(), &timer, &sc, &d_query);
     const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
-    void* host = rows_for_caller(d_rows, row_size * r.rows, s);
+    void* host = download_rows(d_rows, row_size * r.rows, s);
     timer.mark("download");
     timer.publish();
     *rows_out = host;
     *row_count_out = (size_t)r.rows;
   } catch (...) {
     sync_quietly(aux_stream());
-    release_rows(d_rows, s);
+    dev_free(d_rows, s);
     destroy_scene(sc);
     dev_free(d_search, s);
     dev_free(d_query, s);
     sync_quietly(s);
     throw;
   }
-  release_rows(d_rows, s);
+  dev_free(d_rows, s);
   destroy_scene(sc);
   dev_free(d_search, s);
   dev_free(d_query, s);
@@ -681,7 +613,6 @@ int rtdl_b200_scene_query(void* scene, const void* query_points, size_t query_co
     if (query_count == 0) return;
     if (!query_points) throw std::runtime_error("query_points pointer must not be null when query_count is nonzero");
     cudaStream_t s = sc->stream;
-    DirectRowsScope direct;
     PhaseTimer timer(s);
     timer.mark("begin");
     void* d_query = upload(query_points, record_size(sc->dim) * query_count, s);
@@ -694,19 +625,19 @@ int rtdl_b200_scene_query(void* scene, const void* query_points, size_t query_co
                                 &d_rows, d_overflow, s, &timer);
       const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
       if (d_overflow) RTDL_CUDA_CHECK(cudaMemcpyAsync(overflow_out, d_overflow, query_count, cudaMemcpyDeviceToHost, s));
-      void* host = rows_for_caller(d_rows, row_size * r.rows, s);
+      void* host = download_rows(d_rows, row_size * r.rows, s);
       timer.mark("download");
       timer.publish();
       *rows_out = host;
       *row_count_out = (size_t)r.rows;
     } catch (...) {
-      release_rows(d_rows, s);
+      dev_free(d_rows, s);
       dev_free(d_query, s);
       dev_free(d_overflow, s);
       sync_quietly(s);
       throw;
     }
-    release_rows(d_rows, s);
+    dev_free(d_rows, s);
     dev_free(d_query, s);
     dev_free(d_overflow, s);
   }, error_out, error_size);

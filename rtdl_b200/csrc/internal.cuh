@@ -187,21 +187,6 @@ void* dev_alloc(size_t bytes, cudaStream_t s);
 void dev_free(void* p, cudaStream_t s);
 void ensure_pool_configured(int device);
 
-// ---- where a call's own row buffer goes --------------------------------------
-// A call that allocates its row buffer itself (the rows_alloc argument of the
-// query functions) takes it from device memory, unless the calling thread has
-// set a host allocator for the call: the host-buffer entry points hand out
-// rows in pinned host memory, and with the allocator set the emit kernels
-// write the rows across PCIe straight into that buffer, so the transfer
-// overlaps the emit instead of following it.  The allocator returns nullptr
-// to fall back to device memory.
-struct RowBufferHook {
-  void* (*alloc)(size_t bytes) = nullptr;
-};
-RowBufferHook& row_buffer_hook();  // the calling thread's
-void* alloc_rows(size_t bytes, cudaStream_t s);
-bool rows_on_host(const void* p);  // p came from the hook (pinned host memory)
-
 // ---- sort / scan (sort_scan.cu) -------------------------------------------
 // Exclusive scan of `counts` (optionally gathered through `order`, or identity
 // when *identity_flag != 0) into out[0..n] (u64); out[n] is the total.
@@ -414,7 +399,7 @@ QueryResult run_query_batch(Scene* sc, const void* queries_dev, const BatchSpec&
 
 // Runs a neighbor query on a scene.  All buffers are device buffers; rows are
 // written as RtdlFixedRadiusNeighborRow (kFrn) or RtdlKnnNeighborRow.  When
-// rows_dev is null the rows are only counted.  When alloc_rows is set, a
+// rows_dev is null the rows are only counted.  When rows_alloc is set, a
 // device buffer of exactly the row count is allocated into *rows_alloc.
 QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius,
                       uint32_t limit, void* rows_dev, size_t rows_capacity, void** rows_alloc,

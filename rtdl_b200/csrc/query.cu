@@ -2905,7 +2905,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       }
       if (rows_alloc != nullptr) {
         const size_t row_size = predicate == kFrn ? 16 : 24;
-        rows_dev = res.rows ? alloc_rows(row_size * res.rows, s) : nullptr;
+        rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
         rows_capacity = res.rows;
         *rows_alloc = rows_dev;
       }
@@ -3874,7 +3874,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
     }
     if (rows_alloc != nullptr) {
       const size_t row_size = predicate == kFrn ? 16 : 24;
-      rows_dev = res.rows ? alloc_rows(row_size * res.rows, s) : nullptr;
+      rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
       rows_capacity = res.rows;
       *rows_alloc = rows_dev;
     }

@@ -576,7 +576,7 @@ def _plan_chunks(nb: np.ndarray, nq: np.ndarray, max_build: int, max_probe: int)
     return chunks
 
 
-def run_batch(args) -> int:
+def batch_workload(args) -> dict:
     """2,048 uneven 3D fixed-radius problems: problem batches (one build + one launch sequence per batch)
     against one plain per-call launch per problem, in the same run."""
     import torch
@@ -748,7 +748,11 @@ def run_batch(args) -> int:
                                         rows_total, sample, alg, hbm_peak)
         g = line["graph"]
         line["speedup_graph_vs_plain"] = plain_ms[0] / g["ms_per_step"]
-    print(json.dumps(line))
+    return line
+
+
+def run_batch(args) -> int:
+    print(json.dumps(batch_workload(args)))
     return 0
 
 
@@ -847,7 +851,7 @@ def serve_trace(seconds: float, rate: float, scenes: dict, pools: dict, seed: in
             out.append((t, name, KNN, q, 0.0, (1, 8, 32)[op - 1]))
 
 
-def run_serve(args) -> int:
+def serve_workload(args) -> dict:
     """Served loop: resident scenes, Poisson arrivals, continuous batching, p50/p99 against the plain
     per-call path on the same trace."""
     import torch
@@ -921,7 +925,11 @@ def run_serve(args) -> int:
         "sustained": sustained,
         "e2e": None, "cpu_baseline": None, "roofline": None, "clocks": clocks, "gpu_launches": launches,
     }
-    print(json.dumps(line))
+    return line
+
+
+def run_serve(args) -> int:
+    print(json.dumps(serve_workload(args)))
     return 0
 
 
@@ -1077,7 +1085,8 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
-                    help="leave out the exactness check and the knn16 / hausdorff_4m legs of the headline line")
+                    help="leave out the exactness check and the knn16 / hausdorff_4m / batch_2048 / serve legs of "
+                         "the headline line")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--probes", type=int, default=N_PROBE, help="probe points per GPU (profiling a smaller case)")
     ap.add_argument("--build", type=int, default=N_BUILD, help="build points (profiling a smaller case)")
@@ -1270,7 +1279,7 @@ def main(argv=None) -> int:
                "entry_point": "rtdl_b200_run_fixed_radius_neighbors_3d (pinned host buffers)"}
 
     # exactness of the timed rows against the oracle, then the KNN and Hausdorff legs (one GPU only)
-    exactness = knn16 = hausdorff4m = None
+    exactness = knn16 = hausdorff4m = batch2048 = serve = None
     if rank == 0 and world == 1 and not args.no_secondary:
         from rtdl_b200.runtime import FRN_ROW_DTYPE
 
@@ -1281,6 +1290,20 @@ def main(argv=None) -> int:
         del rows_np
         knn16 = secondary_leg("knn", steps=5, warmup=3)
         hausdorff4m = secondary_leg("hausdorff", steps=5, warmup=3)
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup = 3, 3
+        b = batch_workload(sub)
+        rt.set_tuning()  # the batch leg's autotuner leaves its winner set
+        batch2048 = {"metric": b["metric"], "value": b["value"], "unit": b["unit"], "ms_per_step": b["ms_per_step"],
+                     "step": "one build + query per batch of problems", "config": b["config"],
+                     "plain_per_call": b["plain_per_call"], "speedup_vs_plain": b["speedup_vs_plain"],
+                     "graph": b.get("graph"), "speedup_graph_vs_plain": b.get("speedup_graph_vs_plain"),
+                     "exactness": b["exactness"], "roofline": b["roofline"], "gpu_launches": b["gpu_launches"]}
+        v = serve_workload(sub)
+        serve = {"metric": v["metric"], "value": v["value"], "unit": v["unit"], "config": v["config"],
+                 "served": v["served"], "plain_per_call": v["plain_per_call"],
+                 "throughput_vs_plain": v["throughput_vs_plain"], "sustained": v["sustained"],
+                 "exactness": v["exactness"], "gpu_launches": v["gpu_launches"]}
 
     cpu = None
     external = None
@@ -1319,6 +1342,8 @@ def main(argv=None) -> int:
             "exactness": exactness,
             "knn16": knn16,
             "hausdorff_4m": hausdorff4m,
+            "batch_2048": batch2048,
+            "serve": serve,
             "cpu_baseline": cpu,
             "external_baselines": {"scipy_ckdtree": external} if external else None,
             "clocks": clocks,

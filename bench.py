@@ -311,10 +311,10 @@ def frn_exactness(rows: np.ndarray, probe, build, sample_n: int = 512) -> dict:
     return out
 
 
-def secondary_leg(workload: str, steps: int, warmup: int) -> dict:
-    """knn k=16 at 1M x 1M 3D, or directed Hausdorff at 4M x 4M 2D: CUDA-event ms per step (scene build +
-    query), rows/s, the query kernel's roofline fraction and exactness against the oracle (a sample of
-    queries, plus the complete output against the oracle's digest)."""
+def secondary_leg(workload: str, steps: int, warmup: int, k: int = 16) -> dict:
+    """knn (k=16 unless given) at 1M x 1M 3D, or directed Hausdorff at 4M x 4M 2D: CUDA-event ms per step
+    (scene build + query), rows/s, the query kernel's roofline fraction and exactness against the oracle (a
+    sample of queries, plus the complete output against the oracle's digest)."""
     import torch
 
     import rtdl_b200 as rt
@@ -328,7 +328,6 @@ def secondary_leg(workload: str, steps: int, warmup: int) -> dict:
     knn = workload == "knn"
     if knn:
         probe, build = workloads.clustered_3d(N_BUILD, N_PROBE)  # --build / --probes for a smaller case
-        k = 16
         units = len(probe) * k
     else:
         probe, build = workloads.hausdorff_2d()
@@ -392,7 +391,7 @@ def secondary_leg(workload: str, steps: int, warmup: int) -> dict:
         kernel = "k_pass1<KNN> (nearest-list LBVH walk)"
         full = {}
         ref = digests.get("knn16_1m")
-        if ref and len(probe) == len(build) == 1 << 20:
+        if ref and k == 16 and len(probe) == len(build) == 1 << 20:
             packed = np.zeros(len(rows), dtype=np.dtype({"names": ["query_id", "neighbor_id", "distance", "neighbor_rank"],
                                                          "formats": ["<u4", "<u4", "<f8", "<u4"],
                                                          "offsets": [0, 4, 8, 16], "itemsize": 20}))
@@ -423,7 +422,7 @@ def secondary_leg(workload: str, steps: int, warmup: int) -> dict:
     hbm_peak, peak_note = _hbm_peak()
     achieved = alg_bytes / (trav / 1e3) / 1e9 if trav > 0 else None
     return {
-        "metric": ("knn rows/s at 1M x 1M 3D, k=16 (exact row set)" if knn
+        "metric": (f"knn rows/s at 1M x 1M 3D, k={k} (exact row set)" if knn
                    else "directed Hausdorff nearest rows/s at 4M x 4M 2D (FP64 max-min)"),
         "value": units / (ms_step / 1e3), "unit": "rows/s", "ms_per_step": ms_step, "steps": steps, "warmup": warmup,
         "config": {"workload": workload, "build": len(build), "probe": len(probe),
@@ -549,7 +548,7 @@ def run_secondary(args) -> int:
     sampler = ClockSampler(0)
     sampler.start()
     time.sleep(0.3)
-    leg = secondary_leg(args.workload, args.steps, args.warmup)
+    leg = secondary_leg(args.workload, args.steps, args.warmup, k=args.k)
     clocks = sampler.stop()
     line = {"metric": leg.pop("metric"), "value": leg.pop("value"), "unit": leg.pop("unit"), "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg.pop("ms_per_step"),
@@ -1098,6 +1097,7 @@ def main(argv=None) -> int:
                          "serve: request loop over resident scenes vs the plain per-call path; "
                          "summary: the reference's published ranked-summary benchmark; "
                          "config1: 4,096 x 4,096 2D fixed radius beside the reference's CPU runners")
+    ap.add_argument("--k", type=int, default=16, help="knn workload: neighbours per query")
     ap.add_argument("--problems", type=int, default=2048, help="problems of the batch workload")
     ap.add_argument("--no-graph", action="store_true", help="batch workload: leave out the captured-graph leg")
     ap.add_argument("--graph-batch-probes", type=int, default=24 << 20,

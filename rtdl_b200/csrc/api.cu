@@ -295,7 +295,20 @@ void validate_common(double radius, size_t limit, size_t nq, size_t ns, bool has
     throw std::runtime_error(std::string(what) + " " + limit_name + " exceeds uint32 limit");
 }
 
-// Plain per-call launch: upload, build, query, download.
+// Host buffer for rows copied range by range: pinned from the pool, else malloc'd.
+void* rows_host_buffer(size_t bytes, bool* pinned) {
+  void* host = pinned_pool().get(bytes);
+  *pinned = host != nullptr;
+  if (!host) {
+    host = std::malloc(bytes ? bytes : 1);
+    if (!host) throw std::runtime_error("host allocation of rows failed");
+  }
+  return host;
+}
+
+// Plain per-call launch: upload, build, query, download.  Fixed-radius rows
+// are copied to the host range by range while later ranges are still being
+// emitted (the copy stream is this thread's second stream, idle by then).
 void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim, int predicate, double radius,
                    size_t limit, void** rows_out, size_t* row_count_out) {
   cudaStream_t s = library_stream();
@@ -307,18 +320,37 @@ void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim,
   Scene* sc = nullptr;
   void* d_query = nullptr;
   void* d_rows = nullptr;
+  RowDownload dl;
+  dl.alloc = rows_host_buffer;
+  dl.copy = aux_stream();
+  auto release_host = [&]() {
+    if (dl.host && !(dl.pinned && pinned_pool().put(dl.host))) std::free(dl.host);
+    dl.host = nullptr;
+  };
   try {
     BuildQueryInputs in{d_search, (uint32_t)ns, nullptr, q, (uint32_t)nq, dim};
     QueryResult r = run_build_and_query(in, predicate, radius, (uint32_t)limit, nullptr, 0, &d_rows, nullptr, s,
-                                        aux_stream(), &timer, &sc, &d_query);
+                                        aux_stream(), &timer, &sc, &d_query, &dl);
     const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
-    void* host = download_rows(d_rows, row_size * r.rows, s);
+    void* host;
+    if (dl.host) {  // the copies were queued while the rows were emitted
+      static thread_local cudaEvent_t ev_copied = nullptr;
+      if (!ev_copied) RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
+      RTDL_CUDA_CHECK(cudaEventRecord(ev_copied, dl.copy));
+      RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ev_copied, 0));
+      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+      host = dl.host;
+      dl.host = nullptr;
+    } else {
+      host = download_rows(d_rows, row_size * r.rows, s);
+    }
     timer.mark("download");
     timer.publish();
     *rows_out = host;
     *row_count_out = (size_t)r.rows;
   } catch (...) {
     sync_quietly(aux_stream());
+    release_host();
     dev_free(d_rows, s);
     destroy_scene(sc);
     dev_free(d_search, s);

@@ -340,10 +340,23 @@ struct BuildQueryInputs {
   uint32_t nq;
   int dim;
 };
+// Rows copied to the host while they are written: once the row count is known
+// the query takes a host buffer from `alloc` and, for each range of queries in
+// output order whose rows are complete, queues the copy of those rows on
+// `copy` behind an event on the query's stream, so the copies overlap the
+// emission of later ranges.  `copies` counts the copies queued; the caller
+// makes its stream wait for `copy` before it uses or releases the rows.
+struct RowDownload {
+  void* (*alloc)(size_t bytes, bool* pinned) = nullptr;
+  cudaStream_t copy = nullptr;
+  void* host = nullptr;
+  bool pinned = false;
+  int copies = 0;
+};
 QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, double radius, uint32_t limit,
                                 void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev,
                                 cudaStream_t s, cudaStream_t aux, PhaseTimer* timer, Scene** scene_out,
-                                void** query_owned);
+                                void** query_owned, RowDownload* download = nullptr);
 // A second stream of this thread on the current device (the query side of run_build_and_query).
 cudaStream_t aux_stream();
 // Leaf-bucket size of a scene build: the tuning's when set, else 24 for scenes

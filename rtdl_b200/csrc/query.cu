@@ -217,12 +217,19 @@ enum Stat { kStatNodes, kStatLeafPoints, kStatInRadius, kStatInserts, kStatShift
 
 // One thread per query, queries in Morton order so a warp walks neighbouring
 // subtrees.  KNN == false: radius-limited (fixed_radius_neighbors and
-// bounded_knn_rows); KNN == true: k nearest.  PACKET: the warp walks the tree
-// together -- each node is read once for the warp and entered when any lane's
-// current bound needs it -- while every lane keeps its own list and tests a
-// leaf's points only when its own bound reaches the leaf; the lists, and so
-// the rows, are the per-lane walk's.
-template <bool KNN, bool STATS, bool PACKET = false>
+// bounded_knn_rows); KNN == true: k nearest.  Every lane keeps its own list.
+// WALK: kWalkLane -- each lane walks the rope-linked records alone;
+// kWalkRope -- the warp walks them together in pre-order, entering a node
+// when any lane's current k-th bound reaches it; kWalkNear -- the warp walks
+// nearer child first with a stack (fewer nodes for longer lists, a dearer
+// step: 14% faster than kWalkRope at k = 16, 10% slower at k = 1 on the
+// benchmark's clustered 1M x 1M sets).  In the packet forms each lane tests a
+// leaf only when its own bound reaches it, so lists and rows are the
+// per-lane walk's.
+constexpr int kWalkLane = 0, kWalkRope = 1, kWalkNear = 2;
+// Lists at least this long take kWalkNear (k = 4: both packet forms equal).
+constexpr int kNearFirstMinList = 4;
+template <bool KNN, bool STATS, int WALK = kWalkLane>
 __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
   extern __shared__ uint32_t smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -230,6 +237,7 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
   uint32_t* lkey = smem + (size_t)warp * 64 * L;
   uint32_t* lidx = lkey + 32 * L;
   const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr bool PACKET = WALK != kWalkLane;
   if (PACKET ? !__any_sync(0xffffffffu, t0 < P.nq) : t0 >= P.nq) return;
   const bool active = t0 < P.nq;  // PACKET: lanes past the end take part in the warp's walk only
   const uint32_t t = active ? t0 : P.nq - 1;
@@ -349,13 +357,27 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
       b = (int)S.n;
       a = b - 2 * w < 0 ? 0 : b - 2 * w;
     }
-    visit_leaf(a, b - a);
+    if (L >= kNearFirstMinList) {
+      // outward from the query's position (lo, lo - 1, lo + 1, ...): points
+      // nearer in the curve tend to be nearer in space, so more inserts land
+      // at the list's end instead of shifting it (k = 16: 178 shifts per
+      // query instead of 249); the list is the same
+      int right = (int)lo < a ? a : (int)lo < b ? (int)lo : b - 1, left = right - 1;
+      for (int j = a; j < b; ++j) {
+        const bool take_right = right < b && (((j - a) & 1) == 0 || left < a);
+        visit_leaf(take_right ? right : left, 1);
+        if (take_right) ++right;
+        else --left;
+      }
+    } else {
+      visit_leaf(a, b - a);
+    }
     win_lo = a;
     win_hi = b;
   }
-  // stackless depth-first walk over the pre-order records
+  // depth-first walk over the pre-order records
   int cur = S.n > 0 ? 0 : kRopeEnd;
-  if (PACKET) {
+  if constexpr (WALK == kWalkRope) {
     while (cur != kRopeEnd) {
       const float4 a = __ldg(&S.nodes[2 * cur]), b = __ldg(&S.nodes[2 * cur + 1]);
       if (STATS) ++st_nodes;
@@ -369,6 +391,81 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
         if (need) visit_leaf(leaf_first(hit), leaf_count(hit));
       }
       cur = __float_as_int(b.w);
+    }
+    if (!active) return;
+  } else if constexpr (WALK == kWalkNear) {
+    // Nearer child first.  A node's two children are tested together, by the
+    // lanes that needed the node; the packet enters the child that most of
+    // those lanes find nearer and keeps the other, if any lane needs it, on a
+    // warp-uniform stack in shared memory.  A kept child is tested again when
+    // it comes off the stack, against bounds that have shrunk meanwhile (a
+    // child's box lies inside its parent's, so a lane that did not need the
+    // parent never needs the child).  The right child of an internal record
+    // is its left child's rope; the depth, and so the stack, stays below
+    // kStackDepth (30 code bits plus 32 index bits).
+    __shared__ int stack_all[256 / 32][kStackDepth];
+    int* stack = stack_all[warp];
+    int sp = 0;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+    bool need = false;
+    if (cur != kRopeEnd) {
+      a = __ldg(&S.nodes[0]);
+      b = __ldg(&S.nodes[1]);
+      if (STATS) ++st_nodes;
+      need = active && box_ok(box_d2(c.qx, c.qy, c.qz, a, b));
+      if (!__any_sync(0xffffffffu, need)) cur = kRopeEnd;
+    }
+    // at the loop top (a, b) is cur's record, `need` this lane's test of it,
+    // and some lane needs it
+    while (cur != kRopeEnd) {
+      const int hit = __float_as_int(a.w);
+      bool descended = false;
+      if (hit < 0) {
+        if (need) visit_leaf(leaf_first(hit), leaf_count(hit));
+      } else {
+        const int left = cur + 1;
+        const float4 la = __ldg(&S.nodes[2 * left]), lb = __ldg(&S.nodes[2 * left + 1]);
+        const int right = __float_as_int(lb.w);
+        const float4 ra = __ldg(&S.nodes[2 * right]), rb = __ldg(&S.nodes[2 * right + 1]);
+        if (STATS) st_nodes += 2;
+        const float dl = box_d2(c.qx, c.qy, c.qz, la, lb), dr = box_d2(c.qx, c.qy, c.qz, ra, rb);
+        const bool nl = need && box_ok(dl), nr = need && box_ok(dr);
+        const unsigned int bl = __ballot_sync(0xffffffffu, nl), br = __ballot_sync(0xffffffffu, nr);
+        if (bl | br) {
+          bool right_first = br != 0;
+          if (bl && br) {
+            const unsigned int vote_r = __ballot_sync(0xffffffffu, nr && (!nl || dr < dl));
+            right_first = 2 * __popc(vote_r) > __popc(bl | br);
+            if (sp == kStackDepth) {  // cannot happen for a valid tree; the call reports it
+              if (lane == 0) atomicOr(P.error, 8u);
+              break;
+            }
+            if (lane == 0) stack[sp] = right_first ? left : right;
+            ++sp;
+          }
+          cur = right_first ? right : left;
+          a = right_first ? ra : la;
+          b = right_first ? rb : lb;
+          need = right_first ? nr : nl;
+          descended = true;
+        }
+      }
+      if (!descended) {  // the next kept node some lane still needs
+        cur = kRopeEnd;
+        while (sp > 0) {
+          __syncwarp();
+          const int k = stack[--sp];
+          __syncwarp();
+          a = __ldg(&S.nodes[2 * k]);
+          b = __ldg(&S.nodes[2 * k + 1]);
+          if (STATS) ++st_nodes;
+          need = active && box_ok(box_d2(c.qx, c.qy, c.qz, a, b));
+          if (__any_sync(0xffffffffu, need)) {
+            cur = k;
+            break;
+          }
+        }
+      }
     }
     if (!active) return;
   } else {
@@ -1139,6 +1236,17 @@ struct EmitParams {
   RowSink sink;
   uint32_t* fix_list;         // processing ranks queued for k_emit_fixup
   unsigned int* fix_count;
+  // Emission of one range [out_lo, out_hi) of output ranks (rows copied to the
+  // host range by range): k_emit takes the range's queries through `order`
+  // (output rank -> processing rank), k_emit_list the range's part
+  // [list_start[range], list_start[range + 1]) of its list partitioned by
+  // range, and the fix-up the queue from `*fix_begin`.  All null: every
+  // query at once.
+  const uint32_t* order = nullptr;
+  const unsigned int* list_start = nullptr;
+  const unsigned int* fix_begin = nullptr;
+  uint32_t out_lo = 0, out_hi = 0;
+  int range = 0;
 };
 
 // A deferred query's sorted packed keys live in slab entries its candidates do
@@ -1330,11 +1438,17 @@ __device__ __forceinline__ void emit_query(const EmitParams& P, uint32_t t, cons
 // the generic path get their rows from k_expand.
 constexpr int kEmitThreads = 256;
 
-__global__ void __launch_bounds__(kEmitThreads) k_emit(EmitParams P) {
+__global__ void __launch_bounds__(kEmitThreads, 8) k_emit(EmitParams P) {
   const int lane = threadIdx.x & 31;
   const uint64_t t64 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (t64 >= P.nq) return;  // whole warp
-  const uint32_t t = (uint32_t)t64;
+  uint32_t t;
+  if (P.order) {  // one range of output ranks
+    if (t64 >= (uint64_t)(P.out_hi - P.out_lo)) return;  // whole warp
+    t = P.order[P.out_lo + (uint32_t)t64];
+  } else {
+    if (t64 >= P.nq) return;  // whole warp
+    t = (uint32_t)t64;
+  }
   EmitQuery q;
   emit_load(P, t, lane, q);
   const uint32_t meta = q.qi.meta;
@@ -1357,11 +1471,12 @@ constexpr int kFixupThreads = 128;
 __global__ void __launch_bounds__(kFixupThreads) k_emit_fixup(EmitParams P) {
   __shared__ uint32_t sk[kFixupThreads / 32][128];
   const unsigned int m = *P.fix_count;
+  const unsigned int first = P.fix_begin ? *P.fix_begin : 0u;
   const int lane = threadIdx.x & 31;
   uint32_t* keys = sk[threadIdx.x >> 5];
   const int inexact = *P.S.inexact;
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < m; j += warps) {
+  for (uint64_t j = first + (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); j < m; j += warps) {
     const uint32_t t = P.fix_list[j];
     const QueryInfo qi = P.qinfo[t];
     const int n = (int)(qi.meta & kQueryCountMask);  // <= 128 for a deferred query
@@ -1735,8 +1850,13 @@ __global__ void __launch_bounds__(kEmitListThreads)
   __shared__ uint32_t wbuf[DEFER ? 1 : kEmitListThreads / 32][DEFER ? 1 : 32 * E];
   const int lane = threadIdx.x & 31;
   if (nwork_dev) nwork = *nwork_dev;
+  uint32_t begin = 0;
+  if (P.list_start) {  // one range of output ranks
+    begin = P.list_start[P.range];
+    nwork = P.list_start[P.range + 1];
+  }
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nwork; j += warps) {  // whole warps
+  for (uint32_t j = begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); j < nwork; j += warps) {  // whole warps
     const uint32_t t = work[j];
     EmitQuery q;
     emit_load(P, t, lane, q);
@@ -1744,6 +1864,62 @@ __global__ void __launch_bounds__(kEmitListThreads)
     emit_query<E, DEFER>(P, t, q, n, lane, DEFER ? nullptr : wbuf[threadIdx.x >> 5]);
   }
 }
+
+// Output rank -> processing rank map for emission range by range (padding
+// ranks hold no query).
+__global__ void k_emit_order(const uint32_t* qorder, const uint32_t* qrank, uint32_t np, uint32_t* order) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x) {
+    const uint32_t qin = qorder[t];
+    if (qin != kNone) order[qrank[qin]] = t;
+  }
+}
+
+// The download range of output rank r: the c with nq*c/C <= r < nq*(c+1)/C
+// (integer division, as the range bounds are cut).
+__device__ __forceinline__ uint32_t download_range(uint32_t r, uint32_t nq, uint32_t chunks) {
+  return (uint32_t)((((uint64_t)r + 1) * chunks - 1) / nq);
+}
+
+// A work list of processing ranks partitioned by download range (a counting
+// sort; the order inside a range is arbitrary, which the per-query emit does
+// not see).  part[0..C) counts, part[C..2C] the range starts, part[2C+1..3C]
+// the scatter cursors.
+__global__ void k_range_count(const uint32_t* list, const unsigned int* n_dev, const uint32_t* qorder,
+                              const uint32_t* qrank, uint32_t nq, uint32_t chunks, unsigned int* part) {
+  const unsigned int n = *n_dev;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    atomicAdd(&part[download_range(qrank[qorder[list[j]]], nq, chunks)], 1u);
+}
+
+__global__ void k_range_starts(uint32_t chunks, unsigned int* part) {
+  unsigned int sum = 0;
+  for (uint32_t c = 0; c < chunks; ++c) {
+    part[chunks + c] = sum;
+    part[2 * chunks + 1 + c] = sum;
+    sum += part[c];
+  }
+  part[2 * chunks] = sum;
+}
+
+__global__ void k_range_scatter(const uint32_t* list, const unsigned int* n_dev, const uint32_t* qorder,
+                                const uint32_t* qrank, uint32_t nq, uint32_t chunks, unsigned int* part,
+                                uint32_t* out) {
+  const unsigned int n = *n_dev;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t t = list[j];
+    const uint32_t c = download_range(qrank[qorder[t]], nq, chunks);
+    out[atomicAdd(&part[2 * chunks + 1 + c], 1u)] = t;
+  }
+}
+
+// First row of each range of output ranks [c * nq / chunks, ...), and the total.
+__global__ void k_chunk_rows(const unsigned long long* offsets, uint32_t nq, int chunks, unsigned long long* out) {
+  const int c = threadIdx.x;
+  if (c <= chunks) out[c] = offsets[(uint64_t)nq * (uint32_t)c / (uint32_t)chunks];
+}
+
+// The next range's fix-ups start after this range's.
+__global__ void k_fix_advance(unsigned int* fix_begin, const unsigned int* fix_count) { *fix_begin = *fix_count; }
 
 __global__ void k_fill_i32(int* out, uint32_t n, int v) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = v;
@@ -2209,6 +2385,9 @@ std::vector<unsigned long long>& last_stats() {
 
 namespace {
 
+// Ranges of output ranks whose rows are copied to the host as each completes.
+constexpr int kDownloadChunks = 8;
+
 struct Readback {
   unsigned long long rows;
   unsigned int heavy;  // these four are copied together from the `small` device counters
@@ -2219,6 +2398,7 @@ struct Readback {
   unsigned int query_bad;
   unsigned int fixups;
   unsigned int refine_left;  // heavy queries still unresolved after a refinement pass
+  unsigned long long chunk_rows[kDownloadChunks + 1];  // first row of each download range
 };
 
 Readback* pinned_readback() {
@@ -2716,7 +2896,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
                              uint32_t kmax, void* rows_dev, size_t rows_capacity, void** rows_alloc,
                              uint8_t* overflow_dev, cudaStream_t s, PhaseTimer* timer, const BatchSpec* bs = nullptr,
                              const SummarySpec* ss = nullptr, const PreparedQueries* pq = nullptr,
-                             bool witness = false) {
+                             bool witness = false, RowDownload* dl = nullptr) {
   // witness (k_max 1): one row per query at its input position, pre-filled
   // with the no-witness row; the nearest in-radius neighbour overwrites it.
   QueryResult res;
@@ -2866,6 +3046,18 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       check_readback(*rb);
       res.rows = rb->rows;
     } else {
+      // rows copied to the host range by range as they are emitted
+      bool chunked = dl != nullptr && dl->alloc != nullptr && rows_alloc != nullptr && !bs && !ss && !witness &&
+                     nq >= (uint32_t)kDownloadChunks * 1024u;
+      if (chunked) {
+        unsigned long long* chunk_dev =
+            static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (kDownloadChunks + 1), s));
+        refine_bufs.push_back(chunk_dev);
+        k_chunk_rows<<<1, 32, 0, s>>>(offsets, nq, kDownloadChunks, chunk_dev);
+        RTDL_LAUNCHED(1);
+        RTDL_CUDA_CHECK(cudaMemcpyAsync(rb->chunk_rows, chunk_dev, sizeof(unsigned long long) * (kDownloadChunks + 1),
+                                        cudaMemcpyDeviceToHost, s));
+      }
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, s));
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
@@ -2874,6 +3066,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       const Readback r = *rb;
       check_readback(r);
       res.rows = r.rows;
+      if (res.rows == 0) chunked = false;
       uint32_t mid = r.mid, big = r.big, generic = r.heavy;
       const uint32_t* generic_list = heavy_list;
       const uint32_t* generic_m = heavy_m;
@@ -2916,6 +3109,10 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       }
       k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, np, poff);
       RTDL_LAUNCHED(1);
+      if (chunked) {
+        const size_t row_size = predicate == kFrn ? 16 : 24;
+        dl->host = dl->alloc(row_size * res.rows, &dl->pinned);
+      }
       EmitParams E;
       E.S = sc->view();
       E.nq = np;
@@ -2927,6 +3124,81 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       E.sink.ranked = predicate == kFrn ? 0 : 1;
       E.fix_list = fix_list;
       E.fix_count = small + 4;
+      if (chunked) {
+        // Range by range in output order: each range's queries are emitted
+        // (the list kernels and k_emit skip queries outside it), its deferred
+        // queries fixed up, and the copy of its rows queued on the copy
+        // stream, which overlaps the emission of the ranges after it.  The
+        // generic queries' rows are written first.
+        if (generic > 0) launch_expand(generic, generic_list);
+        uint32_t* eorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
+        refine_bufs.push_back(eorder);
+        k_emit_order<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, np, eorder);
+        RTDL_LAUNCHED(1);
+        // the two list kernels' work, partitioned by range (list lengths in small[2], small[3])
+        constexpr uint32_t C = kDownloadChunks, kPart = 3 * C + 1;
+        unsigned int* part = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * 2 * kPart, s));
+        refine_bufs.push_back(part);
+        RTDL_CUDA_CHECK(cudaMemsetAsync(part, 0, sizeof(unsigned int) * 2 * kPart, s));
+        uint32_t* lists_by_range[2] = {nullptr, nullptr};
+        const uint32_t list_len[2] = {mid, big};
+        uint32_t* lists[2] = {mid_list, big_list};
+        for (int l = 0; l < 2; ++l) {
+          if (list_len[l] == 0) continue;
+          lists_by_range[l] = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * list_len[l], s));
+          refine_bufs.push_back(lists_by_range[l]);
+          const unsigned int grid = grid_for(list_len[l], 256);
+          k_range_count<<<grid, 256, 0, s>>>(lists[l], small + 2 + l, qp.qorder, qrank, nq, C, part + l * kPart);
+          k_range_starts<<<1, 1, 0, s>>>(C, part + l * kPart);
+          k_range_scatter<<<grid, 256, 0, s>>>(lists[l], small + 2 + l, qp.qorder, qrank, nq, C, part + l * kPart,
+                                               lists_by_range[l]);
+          RTDL_LAUNCHED(3);
+        }
+        E.order = eorder;
+        E.fix_begin = small + 5;
+        static thread_local cudaEvent_t ev_range[kDownloadChunks] = {};
+        unsigned long long first[kDownloadChunks + 1];
+        for (int c = 0; c <= kDownloadChunks; ++c) first[c] = r.chunk_rows[c];
+        if (first[kDownloadChunks] != res.rows) throw std::runtime_error("row ranges disagree with the row count");
+        const size_t row_size = predicate == kFrn ? 16 : 24;
+        for (int c = 0; c < (int)C; ++c) {
+          if (first[c + 1] == first[c]) continue;  // no rows in this range
+          E.out_lo = (uint32_t)((uint64_t)nq * (uint32_t)c / C);
+          E.out_hi = (uint32_t)((uint64_t)nq * (uint32_t)(c + 1) / C);
+          E.range = c;
+          // the list kernels stride over the range's part: grids sized for an even split
+          if (mid > 0) {
+            E.list_start = part + C;
+            k_emit_list<4, true><<<div_up((uint64_t)div_up(mid, C) * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(
+                E, lists_by_range[0], 0, nullptr);
+          }
+          if (big > 0) {
+            E.list_start = part + kPart + C;
+            k_emit_list<8, false><<<div_up((uint64_t)div_up(big, C) * 32, kEmitListThreads), kEmitListThreads, 0,
+                                    s>>>(E, lists_by_range[1], 0, nullptr);
+          }
+          E.list_start = nullptr;
+          k_emit<<<div_up((uint64_t)(E.out_hi - E.out_lo) * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
+          k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
+          k_fix_advance<<<1, 1, 0, s>>>(small + 5, small + 4);
+          RTDL_LAUNCHED(5);
+          if (!ev_range[c]) RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_range[c], cudaEventDisableTiming));
+          RTDL_CUDA_CHECK(cudaEventRecord(ev_range[c], s));
+          RTDL_CUDA_CHECK(cudaStreamWaitEvent(dl->copy, ev_range[c], 0));
+          RTDL_CUDA_CHECK(cudaMemcpyAsync(static_cast<char*>(dl->host) + first[c] * row_size,
+                                          static_cast<const char*>(rows_dev) + first[c] * row_size,
+                                          (first[c + 1] - first[c]) * row_size, cudaMemcpyDeviceToHost, dl->copy));
+          ++dl->copies;
+        }
+        if (timer) timer->mark("emit");
+        RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+        if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
+        if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
+        cleanup();
+        return res;
+      }
       // The list kernels (queries with 65..kSlab candidates: few warps, long
       // sorts) run on the second stream beside k_emit, so each fills the
       // other's partial waves; they write disjoint rows, and the fix-up waits
@@ -3228,7 +3500,7 @@ QueryResult run_nearest_witness(Scene* sc, const void* queries_dev, uint32_t nq,
 QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, double radius, uint32_t limit,
                                 void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev,
                                 cudaStream_t s, cudaStream_t aux, PhaseTimer* timer, Scene** scene_out,
-                                void** query_owned) {
+                                void** query_owned, RowDownload* download) {
   *scene_out = nullptr;
   *query_owned = nullptr;
   const size_t qbytes = (in.dim == 3 ? sizeof(RtdlPoint3D) : sizeof(RtdlPoint)) * (size_t)in.nq;
@@ -3277,7 +3549,7 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
   QueryResult r;
   try {
     r = run_radius_query(sc, q, in.nq, predicate, radius, limit, rows_dev, rows_capacity, rows_alloc, overflow_dev, s,
-                         timer, nullptr, nullptr, pq);
+                         timer, nullptr, nullptr, pq, false, download);
   } catch (...) {
     pq->raw = nullptr;
     destroy_query_set(pq);
@@ -3723,8 +3995,10 @@ void ensure_pass1_shared_memory() {
   if ((int)done.size() <= dev) done.resize(dev + 1, false);
   if (done[dev]) return;
   const int most = kMaxList * 256 * 8;
-  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
-  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, true, kWalkRope>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, false, kWalkRope>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, true, kWalkNear>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+  RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, false, kWalkNear>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
   RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
   RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
   RTDL_CUDA_CHECK(cudaFuncSetAttribute(k_pass1<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
@@ -3839,10 +4113,11 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
       }
       ensure_pass1_shared_memory();
       auto launch = [&](auto kernel) { kernel<<<blocks, threads, shm, s>>>(P); };
-      const bool packet = tuning().traversal != 1;  // "lane": one thread per query walks alone
+      const int walk = tuning().traversal == 1 ? kWalkLane : L >= kNearFirstMinList ? kWalkNear : kWalkRope;
       if (knn) {
-        if (stats) packet ? launch(k_pass1<true, true, true>) : launch(k_pass1<true, true>);
-        else packet ? launch(k_pass1<true, false, true>) : launch(k_pass1<true, false>);
+        if (walk == kWalkNear) stats ? launch(k_pass1<true, true, kWalkNear>) : launch(k_pass1<true, false, kWalkNear>);
+        else if (walk == kWalkRope) stats ? launch(k_pass1<true, true, kWalkRope>) : launch(k_pass1<true, false, kWalkRope>);
+        else stats ? launch(k_pass1<true, true>) : launch(k_pass1<true, false>);
       } else {
         if (stats) launch(k_pass1<false, true>);
         else launch(k_pass1<false, false>);
@@ -3908,6 +4183,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
     if (timer) timer->mark("emit");
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (rb->error & 8u) throw std::runtime_error("LBVH traversal stack overflow");
     if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
   } catch (...) {
     sync_quietly(s);
@@ -3954,7 +4230,7 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   P.qcodes = qp.qcodes;
   P.scodes = sc->codes;
   if (tuning().traversal != 1)
-    k_pass1<true, false, true><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
+    k_pass1<true, false, kWalkRope><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
   else
     k_pass1<true, false><<<div_up(nq, threads), threads, (size_t)threads * 8, s>>>(P);
   RTDL_LAUNCHED(1);
@@ -3973,9 +4249,10 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
   const Witness w = *hw;
   if (timer) timer->mark("reduce");
-  unsigned int bad[2] = {0, 0};
+  unsigned int bad[3] = {0, 0, 0};
   RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad[0], &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
   RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad[1], &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad[2], small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
   RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
   dev_free(counts, s);
   dev_free(flags, s);
@@ -3985,6 +4262,7 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   dev_free(best, s);
   free_prep(qp, s);
   throw_if_bad(bad[0] | bad[1]);
+  if (bad[2] & 8u) throw std::runtime_error("LBVH traversal stack overflow");
   HausdorffResult out;
   unsigned long long db = w.dist;
   memcpy(&out.distance, &db, sizeof(double));

@@ -147,8 +147,9 @@ def test_every_traversal_matches_oracle(gpu, traversal):
 
 @pytest.mark.parametrize("traversal", ["packet", "lane"])
 def test_knn_walks_match_oracle(gpu, traversal):
-    """The nearest-list walk in warp packets over density-class order (default)
-    and one thread per query in Morton order ("lane"): KNN rows and the
+    """The nearest-list walk in warp packets over density-class order (default:
+    pre-order for k < 4 and the Hausdorff nearest, nearer child first from
+    k = 4) and one thread per query in Morton order ("lane"): KNN rows and the
     Hausdorff nearest, on clustered 3D sets with a query count that leaves a
     partial last warp, and on a 2D lattice whose equal distances are broken
     by id."""
@@ -163,7 +164,7 @@ def test_knn_walks_match_oracle(gpu, traversal):
     try:
         for search, query in ((s, q), (s2, q2)):
             with rt.B200Scene(_pack(search)) as scene:
-                for k in (1, 5, 16, 40):
+                for k in (1, 3, 4, 16, 40):
                     v = scene.query(_pack(query), predicate="knn_rows", limit=k)
                     _assert_same_rows(v.to_numpy(), O.knn_rows(query, search, k=k, threads=8), True)
                     v.close()
@@ -412,3 +413,29 @@ def test_device_rows_path_heavy_and_generic_queries(gpu):
                                       limit=k_max, rows_address=rows.data_ptr(), rows_capacity=n) == n
             got = np.frombuffer(rows.cpu().numpy().tobytes(), dtype=FRN_ROW_DTYPE)[:n]
             _assert_same_rows(got, exp, False)
+
+
+@pytest.mark.parametrize("dim,ranked,k_max", [(3, False, 8), (3, False, 64), (3, True, 16), (2, False, 64), (2, True, 5)])
+def test_plain_call_rows_copied_range_by_range(gpu, dim, ranked, k_max):
+    """The plain per-call launch with 8,192 queries or more copies its rows to
+    the host range by range (eight ranges of queries in output order) while
+    later ranges are emitted.  Clustered queries give every emission kind
+    (warp lists, 65..kSlab lists, deferred fix-ups, refined heavy queries);
+    the first three eighths of the queries lie far from every point, so their
+    ranges hold no rows; coincident copies of a few points reach the generic
+    path."""
+    rng = np.random.default_rng(200 + 7 * k_max + dim)
+    centres = rng.random((12, dim if dim == 3 else 3))
+    s_pts = _clustered(rng, 60000, centres)[:, :dim]
+    s_pts = np.concatenate([s_pts, np.repeat(s_pts[:3], 300, axis=0)])  # 301 copies of three points
+    q_pts = _clustered(rng, 24000, centres)[:, :dim]
+    q_pts[: 24000 * 3 // 8] += 5.0  # no neighbours
+    q_pts[-100:] = s_pts[np.arange(100) % 3]  # queries on the coincident copies
+    s, q = _cols(s_pts), _cols(q_pts)
+    radius = 0.012
+    v = rt.runtime.fixed_radius_neighbors(_pack(q), _pack(s), radius=radius, k_max=k_max, ranked=ranked)
+    got = v.to_numpy()
+    v.close()
+    exp = O.fixed_radius_neighbors(q, s, radius=radius, k_max=k_max, ranked=ranked, threads=8, grid=True)
+    _assert_same_rows(got, exp, ranked)
+    assert got["query_id"].min() >= 24000 * 3 // 8

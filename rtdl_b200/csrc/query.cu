@@ -227,6 +227,12 @@ enum Stat { kStatNodes, kStatLeafPoints, kStatInRadius, kStatInserts, kStatShift
 // leaf only when its own bound reaches it, so lists and rows are the
 // per-lane walk's.
 constexpr int kWalkLane = 0, kWalkRope = 1, kWalkNear = 2;
+// Half-width of the Morton window that seeds a nearest list of length L
+// before its walk (2w points, inserted by every lane at once): a wider window
+// tightens the k-th bound the divergent walk starts from.  Measured on the
+// clustered 1M x 1M sets: k = 16 walk 5.20 / 4.79 / 4.55 / 4.73 ms at
+// w = L / 2L / 4L / 6L; k = 1 1.15 / 1.11 / 1.06 ms at w = 8 / 16 / 32.
+__host__ __device__ constexpr int seed_half_width(int L) { return L * 4 < 32 ? 32 : L * 4; }
 // Lists at least this long take kWalkNear (k = 4: both packet forms equal).
 constexpr int kNearFirstMinList = 4;
 template <bool KNN, bool STATS, int WALK = kWalkLane>
@@ -349,7 +355,7 @@ __global__ void __launch_bounds__(256) k_pass1(Pass1Params P) {
       if (__ldg(&P.scodes[mid]) < code) lo = mid + 1;
       else hi = mid;
     }
-    const int w = L < 8 ? 8 : L;
+    const int w = seed_half_width(L);
     int a = (int)lo - w;
     if (a < 0) a = 0;
     int b = a + 2 * w;
@@ -4052,7 +4058,7 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
   const bool all_heavy = knn && limit > (uint32_t)kMaxList;
   const int L = all_heavy ? 1 : (int)(limit < (uint32_t)kMaxList ? limit : (uint32_t)kMaxList);
   if (knn && !all_heavy && tuning().traversal != 1 && nq > 32)
-    order_by_density_class(sc, qp, nq, L < 8 ? 8 : L, s);
+    order_by_density_class(sc, qp, nq, seed_half_width(L), s);
   if (timer) timer->mark("query_prep");
 
   uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
@@ -4201,7 +4207,7 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   const int qstride = sc->dim == 3 ? 4 : 3;
   if (timer) timer->mark("start");
   QueryPrep qp = prepare_queries(sc, queries_dev, nq, false, 0.0, false, s);
-  if (tuning().traversal != 1 && nq > 32) order_by_density_class(sc, qp, nq, 8, s);
+  if (tuning().traversal != 1 && nq > 32) order_by_density_class(sc, qp, nq, seed_half_width(1), s);
   if (timer) timer->mark("query_prep");
   uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq, s));

@@ -1265,17 +1265,21 @@ def main(argv=None) -> int:
             lib.rtdl_b200_free_rows(rows)
             return count.value
 
-        for _ in range(2):
+        for _ in range(max(3, args.warmup)):
             e2e_call()
         barrier()
+        calls_ms = []
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
+            tc = time.perf_counter()
             assert e2e_call() == rows_total
+            calls_ms.append((time.perf_counter() - tc) * 1e3)
         t_local = time.perf_counter() - t0
         barrier()
         t_job = allreduce(t_local, dist.ReduceOp.MAX if dist else None)
         e2e = {"value": all_rows * e2e_steps / t_job, "unit": UNIT, "h2d_bytes_per_step": (N_BUILD + N_PROBE) * 32,
                "d2h_bytes_per_step": rows_total * 16, "ms_per_step": t_job / e2e_steps * 1e3,
+               "calls_ms": [round(v, 3) for v in calls_ms],
                "entry_point": "rtdl_b200_run_fixed_radius_neighbors_3d (pinned host buffers)"}
 
     # exactness of the timed rows against the oracle, then the KNN and Hausdorff legs (one GPU only)

@@ -376,15 +376,15 @@ int leaf_size_for(bool fixed_radius_only) {
   return fixed_radius_only ? 24 : 8;
 }
 
-cudaStream_t aux_stream() {
-  static thread_local std::map<int, cudaStream_t> streams;
+cudaStream_t aux_stream(int which) {
+  static thread_local std::map<std::pair<int, int>, cudaStream_t> streams;
   int dev = 0;
   RTDL_CUDA_CHECK(cudaGetDevice(&dev));
-  auto it = streams.find(dev);
+  auto it = streams.find({dev, which});
   if (it != streams.end()) return it->second;
   cudaStream_t s;
   RTDL_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  streams[dev] = s;
+  streams[{dev, which}] = s;
   return s;
 }
 }  // namespace rtdl_b200

@@ -357,8 +357,10 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
                                 void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev,
                                 cudaStream_t s, cudaStream_t aux, PhaseTimer* timer, Scene** scene_out,
                                 void** query_owned, RowDownload* download = nullptr);
-// A second stream of this thread on the current device (the query side of run_build_and_query).
-cudaStream_t aux_stream();
+// Further streams of this thread on the current device: 0 is the query side of
+// run_build_and_query and the row copies, 1 the heavy queries' refinement
+// beside the emit kernels.
+cudaStream_t aux_stream(int which = 0);
 // Leaf-bucket size of a scene build: the tuning's when set, else 24 for scenes
 // that serve only fixed-radius queries (larger buckets shorten the walk and the
 // collect tests a bucket's points with four loads in flight) and 8 for general

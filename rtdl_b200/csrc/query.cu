@@ -29,6 +29,7 @@
 //     sort in global memory, emit).
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <mutex>
 
 #include "internal.cuh"
@@ -547,7 +548,7 @@ struct QueryInfo {
 };
 constexpr uint32_t kQueryCountMask = 0xFFFFu;
 constexpr uint32_t kQueryGeneric = 1u << 16;   // more than kSlab candidates: generic path
-constexpr uint32_t kQueryBig = 1u << 17;       // 65..kSlab candidates: k_emit_list
+constexpr uint32_t kQueryBig = 1u << 17;       // 65..kSlab candidates, or refined: k_emit_list
 constexpr uint32_t kQueryOverflow = 1u << 18;  // more in-radius points than kmax
 constexpr int kQueryKmaxShift = 19;            // bits 19..25: kmax
 __device__ __forceinline__ int query_kmax(uint32_t meta) { return (int)((meta >> kQueryKmaxShift) & 127u); }
@@ -570,7 +571,7 @@ struct CollectParams {
   uint32_t* heavy_list;
   uint32_t* heavy_m;
   uint32_t* heavy_t;         // processing rank of each heavy_list entry (optional)
-  uint32_t* mid_list;        // processing ranks of the queries with 65..128 candidates
+  uint32_t* mid_list;        // processing ranks of the queries with 65..128 candidates (or refined, <= 128)
   uint32_t* big_list;        // processing ranks of the queries with 129..kSlab candidates
   unsigned int* small;       // [0] generic-path query count, [1] error bits, [2] mid_list length,
                              // [3] big_list length, [4] emit fixup queue length
@@ -1128,12 +1129,15 @@ __device__ __forceinline__ bool refine_update_one(const RefineUpdate& U, uint32_
   const uint32_t qin = U.qorder[t], c = U.cnt[j];
   const uint32_t kmax = U.prob_kmax ? U.prob_kmax[U.qprob ? U.qprob[qin] : 0u] : U.kmax;
   if (c >= kmax && c <= (uint32_t)kSlab) {  // resolved: the slab holds every point within rad
+    // A resolved query goes to a list kernel whatever its count (k_emit_list<4>
+    // sorts up to 128): k_emit may run while the refinement does, and it skips
+    // the query under both the collect's record (generic) and this one (big).
     uint8_t fl = (uint8_t)((U.flags[qin] & ~6u) | (c > 64u ? 4u : 0u));
     U.flags[qin] = fl;
-    U.qinfo[t].meta = c | ((fl & 1) ? kQueryOverflow : 0u) | (c > 64u ? kQueryBig : 0u) | (kmax << kQueryKmaxShift);
+    U.qinfo[t].meta = c | ((fl & 1) ? kQueryOverflow : 0u) | kQueryBig | (kmax << kQueryKmaxShift);
     if (c > 128u)
       U.big_list[atomicAdd(&U.small[3], 1u)] = t;
-    else if (c > 64u)
+    else
       U.mid_list[atomicAdd(&U.small[2], 1u)] = t;
     return false;
   }
@@ -1444,26 +1448,34 @@ __device__ __forceinline__ void emit_query(const EmitParams& P, uint32_t t, cons
 // the generic path get their rows from k_expand.
 constexpr int kEmitThreads = 256;
 
-__global__ void __launch_bounds__(kEmitThreads, 8) k_emit(EmitParams P) {
+// The grid fills the GPU once (emit_grid) and each warp strides over the
+// queries: a warp takes its next query as soon as it is done with one,
+// instead of short blocks of eight queries retiring and launching.
+constexpr int kEmitBlocksPerSm = 8;
+
+__global__ void __launch_bounds__(kEmitThreads, kEmitBlocksPerSm) k_emit(EmitParams P) {
   const int lane = threadIdx.x & 31;
-  const uint64_t t64 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint32_t t;
-  if (P.order) {  // one range of output ranks
-    if (t64 >= (uint64_t)(P.out_hi - P.out_lo)) return;  // whole warp
-    t = P.order[P.out_lo + (uint32_t)t64];
-  } else {
-    if (t64 >= P.nq) return;  // whole warp
-    t = (uint32_t)t64;
+  const uint32_t warps = gridDim.x * (kEmitThreads / 32);
+  const uint32_t total = P.order ? P.out_hi - P.out_lo : P.nq;  // P.order: one range of output ranks
+  for (uint32_t w = blockIdx.x * (kEmitThreads / 32) + (threadIdx.x >> 5); w < total; w += warps) {
+    const uint32_t t = P.order ? P.order[P.out_lo + w] : w;
+    EmitQuery q;
+    emit_load(P, t, lane, q);
+    const uint32_t meta = q.qi.meta;
+    const int n = (int)(meta & kQueryCountMask);
+    if ((meta & (kQueryGeneric | kQueryBig)) || n == 0) continue;
+    if (n <= 32)
+      emit_query<1, true>(P, t, q, n, lane, nullptr);
+    else
+      emit_query<2, true>(P, t, q, n, lane, nullptr);
   }
-  EmitQuery q;
-  emit_load(P, t, lane, q);
-  const uint32_t meta = q.qi.meta;
-  const int n = (int)(meta & kQueryCountMask);
-  if ((meta & (kQueryGeneric | kQueryBig)) || n == 0) return;
-  if (n <= 32)
-    emit_query<1, true>(P, t, q, n, lane, nullptr);
-  else
-    emit_query<2, true>(P, t, q, n, lane, nullptr);
+}
+
+// Blocks of k_emit for `queries` warps of work: one resident wave at most.
+inline unsigned int emit_grid(uint64_t queries) {
+  const uint64_t blocks = div_up(queries * 32, (uint64_t)kEmitThreads);
+  const uint64_t cap = (uint64_t)kSmCount * kEmitBlocksPerSm;
+  return (unsigned int)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
 
 // The queries the emit kernels queued, one warp per query: the sorted keys go
@@ -2682,7 +2694,7 @@ struct RefineOut {
 RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radius, uint32_t kmax, uint32_t H,
                        const uint32_t* heavy_list, const uint32_t* heavy_m, const uint32_t* heavy_t,
                        QueryInfo* qinfo, uint8_t* flags, uint32_t* mid_list, uint32_t* big_list, unsigned int* small,
-                       cudaStream_t s) {
+                       cudaStream_t s, const std::function<void()>& after_first_pass = {}) {
   RefineOut out;
   auto alloc = [&](size_t bytes) {
     void* p = dev_alloc(bytes ? bytes : 1, s);
@@ -2765,6 +2777,7 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     U.last = last ? 1 : 0;
     k_refine_update<<<div_up(n, 256), 256, 0, s>>>(U);
     RTDL_LAUNCHED(2);
+    if (pass == 0 && after_first_pass) after_first_pass();  // work the caller queues before the first wait
 
     RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->refine_left, next_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -3077,124 +3090,244 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       const uint32_t* generic_list = heavy_list;
       const uint32_t* generic_m = heavy_m;
       const double* generic_rad = nullptr;
-      if (r.heavy > 0) {
-        // queries with more than kSlab points in radius: collect again at smaller radii
+      auto emit_params = [&]() {
+        EmitParams E;
+        E.S = sc->view();
+        E.nq = np;
+        E.slab = slab;
+        E.qinfo = qinfo;
+        E.poff = poff;
+        E.sink.rows = rows_dev;
+        E.sink.capacity = rows_dev ? rows_capacity : 0;
+        E.sink.ranked = predicate == kFrn ? 0 : 1;
+        E.fix_list = fix_list;
+        E.fix_count = small + 4;
+        return E;
+      };
+      if (r.heavy > 0 && rows_alloc == nullptr && !witness) {
+        // Rows into a given device buffer: the emit does not wait for the heavy
+        // queries.  Three streams: the list kernels of the collect's 65..kSlab
+        // candidate queries (their counts are final) are queued first on the
+        // second stream, the first refinement pass on the third, then k_emit
+        // on this one; the refinement's later passes (each reads its count
+        // back to the host), the generic path and the list kernels of the
+        // queries it resolved follow on the third stream.  k_emit skips a
+        // heavy query whichever of its records it reads: the collect marked
+        // it generic, the pass that resolves it marks it for a list kernel
+        // and appends it to a list after the collect's entries.
+        cudaStream_t ls = aux_stream(0), rs = aux_stream(1);
+        static thread_local cudaEvent_t ev_offsets = nullptr, ev_lists = nullptr, ev_refined = nullptr;
+        if (!ev_offsets) {
+          RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_offsets, cudaEventDisableTiming));
+          RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_lists, cudaEventDisableTiming));
+          RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_refined, cudaEventDisableTiming));
+        }
+        k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, np, poff);
+        RTDL_LAUNCHED(1);
+        RTDL_CUDA_CHECK(cudaEventRecord(ev_offsets, s));
+        RTDL_CUDA_CHECK(cudaStreamWaitEvent(ls, ev_offsets, 0));
+        RTDL_CUDA_CHECK(cudaStreamWaitEvent(rs, ev_offsets, 0));
+        const EmitParams E = emit_params();
+        auto launch_lists = [&](uint32_t first_mid, uint32_t n_mid, uint32_t first_big, uint32_t n_big,
+                                cudaStream_t st) {
+          if (n_mid > 0) {
+            k_emit_list<4, true><<<div_up((uint64_t)n_mid * 32, kEmitListThreads), kEmitListThreads, 0, st>>>(
+                E, mid_list + first_mid, n_mid, nullptr);
+            RTDL_LAUNCHED(1);
+          }
+          if (n_big > 0) {
+            k_emit_list<8, false><<<div_up((uint64_t)n_big * 32, kEmitListThreads), kEmitListThreads, 0, st>>>(
+                E, big_list + first_big, n_big, nullptr);
+            RTDL_LAUNCHED(1);
+          }
+        };
+        launch_lists(0, r.mid, 0, r.big, ls);
+        RTDL_CUDA_CHECK(cudaEventRecord(ev_lists, ls));
         RefineOut ro = refine_heavy(C, qp, radius, kmax, r.heavy, heavy_list, heavy_m, heavy_t, qinfo, flags, mid_list,
-                                    big_list, small, s);
+                                    big_list, small, rs, [&]() {
+                                      k_emit<<<emit_grid(np), kEmitThreads, 0, s>>>(E);
+                                      RTDL_LAUNCHED(1);
+                                    });
         refine_bufs = ro.buffers;
         generic = ro.generic;
-        generic_list = ro.generic_qin;
-        generic_m = ro.generic_m;
-        generic_rad = ro.generic_rad;
-        mid = ro.mid;
-        big = ro.big;
-        if (timer) timer->mark("refine");
-      }
-      res.heavy = generic;
-      if (stats) {
-        last_stats()[kStatGenericQueries] = generic;
-        last_stats()[kStatLargeQueries] = mid + big;
-        last_stats()[kStatRefined] = r.heavy - generic;
-      }
-      if (generic > 0) {
-        // the gather is bounded by each query's smallest tested radius that holds its rows
-        g = run_generic_path(sc, qp, queries_dev, qstride, generic, generic_list, generic_m, kmax, false, small + 1, s,
-                             generic_rad);
-        if (timer) timer->mark("generic_path");
-      }
-      if (rows_alloc != nullptr) {
-        const size_t row_size = predicate == kFrn ? 16 : 24;
-        rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
-        rows_capacity = res.rows;
-        *rows_alloc = rows_dev;
-      }
-      if (witness && rows_dev) {
-        k_witness_fill<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, static_cast<RtdlFixedRadiusNeighborRow*>(rows_dev),
-                                                         rows_capacity);
-        RTDL_LAUNCHED(1);
-      }
-      k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, np, poff);
-      RTDL_LAUNCHED(1);
-      if (chunked) {
-        const size_t row_size = predicate == kFrn ? 16 : 24;
-        dl->host = dl->alloc(row_size * res.rows, &dl->pinned);
-      }
-      EmitParams E;
-      E.S = sc->view();
-      E.nq = np;
-      E.slab = slab;
-      E.qinfo = qinfo;
-      E.poff = poff;
-      E.sink.rows = rows_dev;
-      E.sink.capacity = rows_dev ? rows_capacity : 0;
-      E.sink.ranked = predicate == kFrn ? 0 : 1;
-      E.fix_list = fix_list;
-      E.fix_count = small + 4;
-      if (chunked) {
-        // Range by range in output order: each range's queries are emitted
-        // (the list kernels and k_emit skip queries outside it), its deferred
-        // queries fixed up, and the copy of its rows queued on the copy
-        // stream, which overlaps the emission of the ranges after it.  The
-        // generic queries' rows are written first.
-        if (generic > 0) launch_expand(generic, generic_list);
-        uint32_t* eorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
-        refine_bufs.push_back(eorder);
-        k_emit_order<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, np, eorder);
-        RTDL_LAUNCHED(1);
-        // the two list kernels' work, partitioned by range (list lengths in small[2], small[3])
-        constexpr uint32_t C = kDownloadChunks, kPart = 3 * C + 1;
-        unsigned int* part = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * 2 * kPart, s));
-        refine_bufs.push_back(part);
-        RTDL_CUDA_CHECK(cudaMemsetAsync(part, 0, sizeof(unsigned int) * 2 * kPart, s));
-        uint32_t* lists_by_range[2] = {nullptr, nullptr};
-        const uint32_t list_len[2] = {mid, big};
-        uint32_t* lists[2] = {mid_list, big_list};
-        for (int l = 0; l < 2; ++l) {
-          if (list_len[l] == 0) continue;
-          lists_by_range[l] = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * list_len[l], s));
-          refine_bufs.push_back(lists_by_range[l]);
-          const unsigned int grid = grid_for(list_len[l], 256);
-          k_range_count<<<grid, 256, 0, s>>>(lists[l], small + 2 + l, qp.qorder, qrank, nq, C, part + l * kPart);
-          k_range_starts<<<1, 1, 0, s>>>(C, part + l * kPart);
-          k_range_scatter<<<grid, 256, 0, s>>>(lists[l], small + 2 + l, qp.qorder, qrank, nq, C, part + l * kPart,
-                                               lists_by_range[l]);
-          RTDL_LAUNCHED(3);
+        res.heavy = generic;
+        if (stats) {
+          last_stats()[kStatGenericQueries] = generic;
+          last_stats()[kStatLargeQueries] = ro.mid + ro.big;
+          last_stats()[kStatRefined] = r.heavy - generic;
         }
-        E.order = eorder;
-        E.fix_begin = small + 5;
-        static thread_local cudaEvent_t ev_range[kDownloadChunks] = {};
-        unsigned long long first[kDownloadChunks + 1];
-        for (int c = 0; c <= kDownloadChunks; ++c) first[c] = r.chunk_rows[c];
-        if (first[kDownloadChunks] != res.rows) throw std::runtime_error("row ranges disagree with the row count");
-        const size_t row_size = predicate == kFrn ? 16 : 24;
-        for (int c = 0; c < (int)C; ++c) {
-          if (first[c + 1] == first[c]) continue;  // no rows in this range
-          E.out_lo = (uint32_t)((uint64_t)nq * (uint32_t)c / C);
-          E.out_hi = (uint32_t)((uint64_t)nq * (uint32_t)(c + 1) / C);
-          E.range = c;
-          // the list kernels stride over the range's part: grids sized for an even split
-          if (mid > 0) {
-            E.list_start = part + C;
-            k_emit_list<4, true><<<div_up((uint64_t)div_up(mid, C) * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(
-                E, lists_by_range[0], 0, nullptr);
+        // the gather is bounded by each query's smallest tested radius that holds its rows
+        if (generic > 0)
+          g = run_generic_path(sc, qp, queries_dev, qstride, generic, ro.generic_qin, ro.generic_m, kmax, false,
+                               small + 1, rs, ro.generic_rad);
+        launch_lists(r.mid, ro.mid - r.mid, r.big, ro.big - r.big, rs);
+        RTDL_CUDA_CHECK(cudaEventRecord(ev_refined, rs));
+        RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ev_lists, 0));
+        RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ev_refined, 0));
+        k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
+        RTDL_LAUNCHED(1);
+        if (generic > 0) launch_expand(generic, ro.generic_qin);
+        if (timer) timer->mark("emit");
+        RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+        if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
+        if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
+      } else {
+        if (r.heavy > 0) {
+          // queries with more than kSlab points in radius: collect again at smaller radii
+          RefineOut ro = refine_heavy(C, qp, radius, kmax, r.heavy, heavy_list, heavy_m, heavy_t, qinfo, flags, mid_list,
+                                      big_list, small, s);
+          refine_bufs = ro.buffers;
+          generic = ro.generic;
+          generic_list = ro.generic_qin;
+          generic_m = ro.generic_m;
+          generic_rad = ro.generic_rad;
+          mid = ro.mid;
+          big = ro.big;
+          if (timer) timer->mark("refine");
+        }
+        res.heavy = generic;
+        if (stats) {
+          last_stats()[kStatGenericQueries] = generic;
+          last_stats()[kStatLargeQueries] = mid + big;
+          last_stats()[kStatRefined] = r.heavy - generic;
+        }
+        if (generic > 0) {
+          // the gather is bounded by each query's smallest tested radius that holds its rows
+          g = run_generic_path(sc, qp, queries_dev, qstride, generic, generic_list, generic_m, kmax, false, small + 1, s,
+                               generic_rad);
+          if (timer) timer->mark("generic_path");
+        }
+        if (rows_alloc != nullptr) {
+          const size_t row_size = predicate == kFrn ? 16 : 24;
+          rows_dev = res.rows ? dev_alloc(row_size * res.rows, s) : nullptr;
+          rows_capacity = res.rows;
+          *rows_alloc = rows_dev;
+        }
+        if (witness && rows_dev) {
+          k_witness_fill<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, nq, static_cast<RtdlFixedRadiusNeighborRow*>(rows_dev),
+                                                           rows_capacity);
+          RTDL_LAUNCHED(1);
+        }
+        k_proc_offsets<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, offsets, np, poff);
+        RTDL_LAUNCHED(1);
+        if (chunked) {
+          const size_t row_size = predicate == kFrn ? 16 : 24;
+          dl->host = dl->alloc(row_size * res.rows, &dl->pinned);
+        }
+        EmitParams E = emit_params();
+        if (chunked) {
+          // Range by range in output order: each range's queries are emitted
+          // (the list kernels and k_emit skip queries outside it), its deferred
+          // queries fixed up, and the copy of its rows queued on the copy
+          // stream, which overlaps the emission of the ranges after it.  The
+          // generic queries' rows are written first.
+          if (generic > 0) launch_expand(generic, generic_list);
+          uint32_t* eorder = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq1, s));
+          refine_bufs.push_back(eorder);
+          k_emit_order<<<grid_for(np, 256), 256, 0, s>>>(qp.qorder, qrank, np, eorder);
+          RTDL_LAUNCHED(1);
+          // the two list kernels' work, partitioned by range (list lengths in small[2], small[3])
+          constexpr uint32_t C = kDownloadChunks, kPart = 3 * C + 1;
+          unsigned int* part = static_cast<unsigned int*>(dev_alloc(sizeof(unsigned int) * 2 * kPart, s));
+          refine_bufs.push_back(part);
+          RTDL_CUDA_CHECK(cudaMemsetAsync(part, 0, sizeof(unsigned int) * 2 * kPart, s));
+          uint32_t* lists_by_range[2] = {nullptr, nullptr};
+          const uint32_t list_len[2] = {mid, big};
+          uint32_t* lists[2] = {mid_list, big_list};
+          for (int l = 0; l < 2; ++l) {
+            if (list_len[l] == 0) continue;
+            lists_by_range[l] = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * list_len[l], s));
+            refine_bufs.push_back(lists_by_range[l]);
+            const unsigned int grid = grid_for(list_len[l], 256);
+            k_range_count<<<grid, 256, 0, s>>>(lists[l], small + 2 + l, qp.qorder, qrank, nq, C, part + l * kPart);
+            k_range_starts<<<1, 1, 0, s>>>(C, part + l * kPart);
+            k_range_scatter<<<grid, 256, 0, s>>>(lists[l], small + 2 + l, qp.qorder, qrank, nq, C, part + l * kPart,
+                                                 lists_by_range[l]);
+            RTDL_LAUNCHED(3);
           }
-          if (big > 0) {
-            E.list_start = part + kPart + C;
-            k_emit_list<8, false><<<div_up((uint64_t)div_up(big, C) * 32, kEmitListThreads), kEmitListThreads, 0,
-                                    s>>>(E, lists_by_range[1], 0, nullptr);
+          E.order = eorder;
+          E.fix_begin = small + 5;
+          static thread_local cudaEvent_t ev_range[kDownloadChunks] = {};
+          unsigned long long first[kDownloadChunks + 1];
+          for (int c = 0; c <= kDownloadChunks; ++c) first[c] = r.chunk_rows[c];
+          if (first[kDownloadChunks] != res.rows) throw std::runtime_error("row ranges disagree with the row count");
+          const size_t row_size = predicate == kFrn ? 16 : 24;
+          for (int c = 0; c < (int)C; ++c) {
+            if (first[c + 1] == first[c]) continue;  // no rows in this range
+            E.out_lo = (uint32_t)((uint64_t)nq * (uint32_t)c / C);
+            E.out_hi = (uint32_t)((uint64_t)nq * (uint32_t)(c + 1) / C);
+            E.range = c;
+            // the list kernels stride over the range's part: grids sized for an even split
+            if (mid > 0) {
+              E.list_start = part + C;
+              k_emit_list<4, true><<<div_up((uint64_t)div_up(mid, C) * 32, kEmitListThreads), kEmitListThreads, 0, s>>>(
+                  E, lists_by_range[0], 0, nullptr);
+            }
+            if (big > 0) {
+              E.list_start = part + kPart + C;
+              k_emit_list<8, false><<<div_up((uint64_t)div_up(big, C) * 32, kEmitListThreads), kEmitListThreads, 0,
+                                      s>>>(E, lists_by_range[1], 0, nullptr);
+            }
+            E.list_start = nullptr;
+            k_emit<<<emit_grid(E.out_hi - E.out_lo), kEmitThreads, 0, s>>>(E);
+            k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
+            k_fix_advance<<<1, 1, 0, s>>>(small + 5, small + 4);
+            RTDL_LAUNCHED(5);
+            if (!ev_range[c]) RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_range[c], cudaEventDisableTiming));
+            RTDL_CUDA_CHECK(cudaEventRecord(ev_range[c], s));
+            RTDL_CUDA_CHECK(cudaStreamWaitEvent(dl->copy, ev_range[c], 0));
+            RTDL_CUDA_CHECK(cudaMemcpyAsync(static_cast<char*>(dl->host) + first[c] * row_size,
+                                            static_cast<const char*>(rows_dev) + first[c] * row_size,
+                                            (first[c + 1] - first[c]) * row_size, cudaMemcpyDeviceToHost, dl->copy));
+            ++dl->copies;
           }
-          E.list_start = nullptr;
-          k_emit<<<div_up((uint64_t)(E.out_hi - E.out_lo) * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
-          k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
-          k_fix_advance<<<1, 1, 0, s>>>(small + 5, small + 4);
-          RTDL_LAUNCHED(5);
-          if (!ev_range[c]) RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_range[c], cudaEventDisableTiming));
-          RTDL_CUDA_CHECK(cudaEventRecord(ev_range[c], s));
-          RTDL_CUDA_CHECK(cudaStreamWaitEvent(dl->copy, ev_range[c], 0));
-          RTDL_CUDA_CHECK(cudaMemcpyAsync(static_cast<char*>(dl->host) + first[c] * row_size,
-                                          static_cast<const char*>(rows_dev) + first[c] * row_size,
-                                          (first[c + 1] - first[c]) * row_size, cudaMemcpyDeviceToHost, dl->copy));
-          ++dl->copies;
+          if (timer) timer->mark("emit");
+          RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+          RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+          RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
+          if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
+          if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
+          cleanup();
+          return res;
+        }
+        // The list kernels (queries with 65..kSlab candidates: few warps, long
+        // sorts) run on the second stream beside k_emit, so each fills the
+        // other's partial waves; they write disjoint rows, and the fix-up waits
+        // for both.
+        static thread_local cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+        const bool side = mid > 0 || big > 0;
+        cudaStream_t ls = s;
+        if (side) {
+          if (!ev_fork) {
+            RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+            RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+          }
+          ls = aux_stream();
+          RTDL_CUDA_CHECK(cudaEventRecord(ev_fork, s));
+          RTDL_CUDA_CHECK(cudaStreamWaitEvent(ls, ev_fork, 0));
+        }
+        if (mid > 0) {
+          k_emit_list<4, true><<<div_up((uint64_t)mid * 32, kEmitListThreads), kEmitListThreads, 0, ls>>>(E, mid_list,
+                                                                                                       mid, nullptr);
+          RTDL_LAUNCHED(1);
+        }
+        if (big > 0) {
+          k_emit_list<8, false><<<div_up((uint64_t)big * 32, kEmitListThreads), kEmitListThreads, 0, ls>>>(E, big_list,
+                                                                                                        big, nullptr);
+          RTDL_LAUNCHED(1);
+        }
+        k_emit<<<emit_grid(np), kEmitThreads, 0, s>>>(E);
+        RTDL_LAUNCHED(1);
+        if (side) {
+          RTDL_CUDA_CHECK(cudaEventRecord(ev_join, ls));
+          RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ev_join, 0));
+        }
+        k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
+        RTDL_LAUNCHED(1);
+        if (generic > 0) {
+          launch_expand(generic, generic_list);
         }
         if (timer) timer->mark("emit");
         RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
@@ -3202,52 +3335,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
         RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
         if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
         if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
-        cleanup();
-        return res;
       }
-      // The list kernels (queries with 65..kSlab candidates: few warps, long
-      // sorts) run on the second stream beside k_emit, so each fills the
-      // other's partial waves; they write disjoint rows, and the fix-up waits
-      // for both.
-      static thread_local cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-      const bool side = mid > 0 || big > 0;
-      cudaStream_t ls = s;
-      if (side) {
-        if (!ev_fork) {
-          RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-          RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
-        }
-        ls = aux_stream();
-        RTDL_CUDA_CHECK(cudaEventRecord(ev_fork, s));
-        RTDL_CUDA_CHECK(cudaStreamWaitEvent(ls, ev_fork, 0));
-      }
-      if (mid > 0) {
-        k_emit_list<4, true><<<div_up((uint64_t)mid * 32, kEmitListThreads), kEmitListThreads, 0, ls>>>(E, mid_list,
-                                                                                                     mid, nullptr);
-        RTDL_LAUNCHED(1);
-      }
-      if (big > 0) {
-        k_emit_list<8, false><<<div_up((uint64_t)big * 32, kEmitListThreads), kEmitListThreads, 0, ls>>>(E, big_list,
-                                                                                                      big, nullptr);
-        RTDL_LAUNCHED(1);
-      }
-      k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
-      RTDL_LAUNCHED(1);
-      if (side) {
-        RTDL_CUDA_CHECK(cudaEventRecord(ev_join, ls));
-        RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ev_join, 0));
-      }
-      k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
-      RTDL_LAUNCHED(1);
-      if (generic > 0) {
-        launch_expand(generic, generic_list);
-      }
-      if (timer) timer->mark("emit");
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-      RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-      if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
-      if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
     }
     if (ss) {
       const uint32_t blocks = div_up((uint64_t)nq * 32, kSummaryThreads);
@@ -3267,6 +3355,8 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     }
   } catch (...) {
     sync_quietly(s);
+    sync_quietly(aux_stream(0));  // the refinement and the list kernels may run there
+    sync_quietly(aux_stream(1));
     dev_free(summary_rows, s);
     cleanup();
     throw;
@@ -3701,7 +3791,7 @@ void graph_enqueue_request(SummaryGraph* g, uint32_t r, cudaStream_t s) {
   E.sink.ranked = 0;
   E.fix_list = g->fix_list;
   E.fix_count = small + 4;
-  k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
+  k_emit<<<emit_grid(np), kEmitThreads, 0, s>>>(E);
   k_emit_list<4, true><<<kStrideBlocks, kEmitListThreads, 0, s>>>(E, g->mid_list, 0, small + 2);
   k_emit_list<8, false><<<kStrideBlocks, kEmitListThreads, 0, s>>>(E, g->big_list, 0, small + 3);
   k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);
@@ -4579,7 +4669,7 @@ void batch_graph_enqueue(BatchGraph* g, uint32_t i, cudaStream_t s) {
   E.sink.ranked = 0;
   E.fix_list = g->fix_list;
   E.fix_count = small + 4;
-  k_emit<<<div_up((uint64_t)np * 32, kEmitThreads), kEmitThreads, 0, s>>>(E);
+  k_emit<<<emit_grid(np), kEmitThreads, 0, s>>>(E);
   k_emit_list<4, true><<<kStrideBlocks, kEmitListThreads, 0, s>>>(E, g->mid_list, 0, small + 2);
   k_emit_list<8, false><<<kStrideBlocks, kEmitListThreads, 0, s>>>(E, g->big_list, 0, small + 3);
   k_emit_fixup<<<kSmCount * 4, kFixupThreads, 0, s>>>(E);

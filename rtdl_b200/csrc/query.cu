@@ -1335,6 +1335,37 @@ __device__ __noinline__ void exact_fixup_sorted(uint32_t* buf, int n, int shift,
   }
 }
 
+// Only the first kk of a query's n sorted candidates become rows.  An element
+// whose truncated key is two units or more above that of element kk - 1
+// orders after every element up to kk - 1 exactly as well, so the exact
+// re-decision of near ties only has to cover the first m elements: those
+// within one unit of element kk - 1 or below it (m = n when kk = n).  `v`
+// holds the warp-sorted packed keys in the striped layout (padding
+// 0xFFFFFFFF); every lane returns the same m.
+template <int E, int SHIFT>
+__device__ __forceinline__ int exact_window(const uint32_t (&v)[E], int n, int kk, int lane) {
+  if (kk >= n) return n;
+  const int c = kk - 1;
+  uint32_t vc = v[0];
+#pragma unroll
+  for (int r = 1; r < E; ++r)
+    if ((c >> 5) == r) vc = v[r];
+  const uint32_t limit = (__shfl_sync(0xffffffffu, vc, c & 31) >> SHIFT) + 1u;
+  int m = 0;
+#pragma unroll
+  for (int r = 0; r < E; ++r) m += __popc(__ballot_sync(0xffffffffu, v[r] != 0xFFFFFFFFu && (v[r] >> SHIFT) <= limit));
+  return m;
+}
+
+// The window of exact_window for keys sorted in a shared-memory buffer (k_emit_fixup).
+__device__ __forceinline__ int exact_window_sorted(const uint32_t* keys, int n, int kk, int shift) {
+  if (kk >= n) return n;
+  const uint32_t limit = (keys[kk - 1] >> shift) + 1u;
+  int m = kk;
+  while (m < n && (keys[m] >> shift) <= limit) ++m;
+  return m;
+}
+
 // What a warp needs of one query before it sorts: three independent loads
 // (the query's record, its first row and slab entry `lane`), so a query costs
 // one memory round trip before the sort and one (the point gather) after it.
@@ -1377,14 +1408,17 @@ __device__ __forceinline__ void emit_query(const EmitParams& P, uint32_t t, cons
     }
   }
   warp_bitonic_striped<E>(v, lane);
-  // ambiguous neighbours: element i and i + 1 within one truncated unit
+  const int kmax = query_kmax(q.qi.meta);
+  const int kk = n < kmax ? n : kmax;
+  const int m = exact_window<E, SHIFT>(v, n, kk, lane);
+  // ambiguous neighbours inside the window: element i and i + 1 within one truncated unit
   bool amb = false;
 #pragma unroll
   for (int r = 0; r < E; ++r) {
     uint32_t nx = __shfl_down_sync(0xffffffffu, v[r], 1);
     const uint32_t wrap = __shfl_sync(0xffffffffu, v[r + 1 < E ? r + 1 : r], 0);
     if (lane == 31) nx = r + 1 < E ? wrap : 0xFFFFFFFFu;
-    amb |= nx != 0xFFFFFFFFu && (nx >> SHIFT) - (v[r] >> SHIFT) <= 1u;
+    amb |= ((r << 5) | lane) + 1 < m && (nx >> SHIFT) - (v[r] >> SHIFT) <= 1u;
   }
   const double ex = q.qi.ex, ey = q.qi.ey, ez = q.qi.ez;
   const int inexact = *P.S.inexact;
@@ -1400,15 +1434,13 @@ __device__ __forceinline__ void emit_query(const EmitParams& P, uint32_t t, cons
 #pragma unroll
       for (int r = 0; r < E; ++r) wbuf[(r << 5) | lane] = v[r];
       __syncwarp();
-      if (lane == 0) exact_fixup_sorted(wbuf, n, SHIFT, ent, P.S, inexact, ex, ey, ez);
+      if (lane == 0) exact_fixup_sorted(wbuf, m, SHIFT, ent, P.S, inexact, ex, ey, ez);
       __syncwarp();
 #pragma unroll
       for (int r = 0; r < E; ++r) v[r] = wbuf[(r << 5) | lane];
       __syncwarp();
     }
   }
-  const int kmax = query_kmax(q.qi.meta);
-  const int kk = n < kmax ? n : kmax;
 #pragma unroll
   for (int r = 0; r < E; ++r) {
     const int i = (r << 5) | lane;
@@ -1504,10 +1536,13 @@ __global__ void __launch_bounds__(kFixupThreads) k_emit_fixup(EmitParams P) {
     const uint32_t* src = deferred_keys(P.slab, t, n);
     for (int i = lane; i < n; i += 32) keys[i] = src[i];
     __syncwarp();
-    for (int pass = 0; pass < n; ++pass) {
+    const int kmax = query_kmax(qi.meta);
+    const int kk = n < kmax ? n : kmax;
+    const int w = exact_window_sorted(keys, n, kk, shift);  // the elements the first kk rows can come from
+    for (int pass = 0; pass < w; ++pass) {
       bool changed = false;
       for (int parity = 0; parity < 2; ++parity) {
-        for (int i = parity + 2 * lane; i + 1 < n; i += 64) {
+        for (int i = parity + 2 * lane; i + 1 < w; i += 64) {
           const uint32_t a = keys[i], b = keys[i + 1];
           if ((b >> shift) - (a >> shift) > 1u) continue;
           if (exact_before(qi.ex, qi.ey, qi.ez, P.S.pts, P.S.pts64, P.S.perm, inexact, (uint32_t)ent[b & mask],
@@ -1522,8 +1557,6 @@ __global__ void __launch_bounds__(kFixupThreads) k_emit_fixup(EmitParams P) {
       if (!__any_sync(0xffffffffu, changed)) break;
     }
     const unsigned long long base = P.poff[t];
-    const int kmax = query_kmax(qi.meta);
-    const int kk = n < kmax ? n : kmax;
     for (int i = lane; i < kk; i += 32) {
       const uint32_t idx = (uint32_t)ent[keys[i] & mask];
       const float4 p = __ldg(&P.S.pts[idx]);

@@ -230,12 +230,15 @@ enum Stat { kStatNodes, kStatLeafPoints, kStatInRadius, kStatInserts, kStatShift
 constexpr int kWalkLane = 0, kWalkRope = 1, kWalkNear = 2;
 // Half-width of the Morton window that seeds a nearest list of length L
 // before its walk (2w points, inserted by every lane at once): a wider window
-// tightens the k-th bound the divergent walk starts from.  Measured on the
-// clustered 1M x 1M sets: k = 16 walk 5.20 / 4.79 / 4.55 / 4.73 ms at
-// w = L / 2L / 4L / 6L; k = 1 1.15 / 1.11 / 1.06 ms at w = 8 / 16 / 32.
-__host__ __device__ constexpr int seed_half_width(int L) { return L * 4 < 32 ? 32 : L * 4; }
-// Lists at least this long take kWalkNear (k = 4: both packet forms equal).
-constexpr int kNearFirstMinList = 4;
+// tightens the k-th bound the divergent walk starts from, at the cost of the
+// window's own tests.  Measured on the clustered 1M x 1M sets (packets in
+// Morton order): k = 16 walk 3.69 / 3.69 / 3.71 / 3.84 ms at w = 2L / 3L /
+// 4L / 6L; k = 1 0.82 / 0.79 / 0.82 / 0.90 ms at w = 8 / 16 / 32 / 64 (the
+// 4M x 4M uniform 2D Hausdorff nearest: 1.48 / 1.52 / 1.68 / 2.08 ms).
+__host__ __device__ constexpr int seed_half_width(int L) { return L * 2 < 16 ? 16 : L * 2; }
+// Lists at least this long take kWalkNear (k = 4: 1.40 ms pre-order against
+// 1.46 ms nearer first).
+constexpr int kNearFirstMinList = 5;
 // Held to 64 registers (32 resident warps at 128 threads per block): the
 // k = 16 walk ran 2.8% faster than at its natural 72 (28 warps); at 48
 // registers the spills cost more than the occupancy gained.
@@ -2027,50 +2030,6 @@ __global__ void k_mark_all_heavy(const uint32_t* qorder, uint32_t nq, uint32_t n
     counts[qin] = k < n ? k : n;
     flags[qin] = 2;
     temp[qin] = (uint32_t)t;
-  }
-}
-
-// Density class of each query of a nearest search, by processing rank: the
-// FP32 exponent of the largest d2 over the seed window of 2w scene points
-// around the query's Morton code (the window the nearest walk seeds from, so
-// the class tracks the k-th bound the walk starts with).  Queries in a dense
-// cluster get small classes, queries in the sparse background large ones.
-__global__ void k_knn_class(const float4* qpts, const uint32_t* qorder, const uint32_t* qcodes, uint32_t nq,
-                            const float4* spts, const uint32_t* scodes, uint32_t ns, int w, uint32_t* cls,
-                            uint32_t* rank) {
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += gridDim.x * blockDim.x) {
-    const float4 q = qpts[qorder[t]];
-    const uint32_t code = qcodes[t];
-    uint32_t lo = 0, hi = ns;
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (__ldg(&scodes[mid]) < code) lo = mid + 1;
-      else hi = mid;
-    }
-    int a = (int)lo - w;
-    if (a < 0) a = 0;
-    int b = a + 2 * w;
-    if (b > (int)ns) {
-      b = (int)ns;
-      a = b - 2 * w < 0 ? 0 : b - 2 * w;
-    }
-    float far = 0.f;
-    for (int i = a; i < b; ++i) {
-      const float4 p = __ldg(&spts[i]);
-      const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-      far = fmaxf(far, fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
-    }
-    cls[t] = (__float_as_uint(far) >> 23) & 0xFFu;
-    rank[t] = t;
-  }
-}
-
-__global__ void k_permute_pair(const uint32_t* a, const uint32_t* b, const uint32_t* perm, uint32_t n, uint32_t* a_out,
-                               uint32_t* b_out) {
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    const uint32_t p = perm[j];
-    a_out[j] = a[p];
-    b_out[j] = b[p];
   }
 }
 
@@ -4138,31 +4097,6 @@ void ensure_pass1_shared_memory() {
   done[dev] = true;
 }
 
-// Nearest searches walk in warp packets; a packet mixing queries of a dense
-// cluster with queries of the sparse background walks the union of very
-// different k-th bounds.  The Morton processing order is therefore reordered,
-// stably, by the queries' density class: packets hold queries of alike bounds
-// and keep Morton order within a class.  Only the processing order changes
-// (each query's rows do not depend on it).
-void order_by_density_class(Scene* sc, QueryPrep& qp, uint32_t nq, int w, cudaStream_t s) {
-  uint32_t* cls = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* rank = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* order = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  uint32_t* codes = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
-  k_knn_class<<<grid_for(nq, 256), 256, 0, s>>>(qp.qpts, qp.qorder, qp.qcodes, nq, sc->pts, sc->codes, sc->n, w, cls,
-                                                rank);
-  RTDL_LAUNCHED(1);
-  radix_sort_pairs(cls, rank, nq, 0, 8, nullptr, &qp.qst->bad, s);
-  k_permute_pair<<<grid_for(nq, 256), 256, 0, s>>>(qp.qorder, qp.qcodes, rank, nq, order, codes);
-  RTDL_LAUNCHED(1);
-  dev_free(qp.qorder, s);
-  dev_free(qp.qcodes, s);
-  qp.qorder = order;
-  qp.qcodes = codes;
-  dev_free(cls, s);
-  dev_free(rank, s);
-}
-
 QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predicate, double radius, uint32_t limit,
                       void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev, cudaStream_t s,
                       PhaseTimer* timer) {
@@ -4183,8 +4117,6 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
   QueryPrep qp = prepare_queries(sc, queries_dev, nq, !knn, radius, true, s);
   const bool all_heavy = knn && limit > (uint32_t)kMaxList;
   const int L = all_heavy ? 1 : (int)(limit < (uint32_t)kMaxList ? limit : (uint32_t)kMaxList);
-  if (knn && !all_heavy && tuning().traversal != 1 && nq > 32)
-    order_by_density_class(sc, qp, nq, seed_half_width(L), s);
   if (timer) timer->mark("query_prep");
 
   uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
@@ -4333,7 +4265,6 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
   const int qstride = sc->dim == 3 ? 4 : 3;
   if (timer) timer->mark("start");
   QueryPrep qp = prepare_queries(sc, queries_dev, nq, false, 0.0, false, s);
-  if (tuning().traversal != 1 && nq > 32) order_by_density_class(sc, qp, nq, seed_half_width(1), s);
   if (timer) timer->mark("query_prep");
   uint32_t* counts = static_cast<uint32_t*>(dev_alloc(sizeof(uint32_t) * nq, s));
   uint8_t* flags = static_cast<uint8_t*>(dev_alloc(nq, s));

@@ -147,9 +147,9 @@ def test_every_traversal_matches_oracle(gpu, traversal):
 
 @pytest.mark.parametrize("traversal", ["packet", "lane"])
 def test_knn_walks_match_oracle(gpu, traversal):
-    """The nearest-list walk in warp packets over density-class order (default:
-    pre-order for k < 4 and the Hausdorff nearest, nearer child first from
-    k = 4) and one thread per query in Morton order ("lane"): KNN rows and the
+    """The nearest-list walk in warp packets of Morton-consecutive queries
+    (default: pre-order for k <= 4 and the Hausdorff nearest, nearer child
+    first from k = 5) and one thread per query in Morton order ("lane"): KNN rows and the
     Hausdorff nearest, on clustered 3D sets with a query count that leaves a
     partial last warp, and on a 2D lattice whose equal distances are broken
     by id."""

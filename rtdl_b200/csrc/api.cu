@@ -8,6 +8,7 @@
 // Rows handed to the caller live in pinned host buffers from a small pool, so
 // the device-to-host copy runs at full PCIe rate; rtdl_b200_free_rows returns
 // them to the pool.
+#include <algorithm>
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
@@ -306,11 +307,60 @@ void* rows_host_buffer(size_t bytes, bool* pinned) {
   return host;
 }
 
+// Query sets of two kRangeQueries or more are answered in ranges of their
+// input order (run_build_and_query_chunked, at most kMaxQueryRanges ranges of
+// at least kRangeQueries queries), so the copy of the rows to the host, which
+// bounds the call, starts after the first range's query.  Each range costs
+// a query's fixed overhead (about 0.5 ms): at 1,048,576 clustered queries
+// (30 M rows) a call took 11.5 ms in one piece, 10.6 ms in 4 ranges,
+// 12.6 ms in 8 and 19.7 ms in 16.
+constexpr size_t kRangeQueries = 1u << 17;
+constexpr int kMaxQueryRanges = 4;
+
+// The ranged form of run_rows_call: one host buffer with room for every
+// query's limit rows (pinned, from the pool) takes each range's rows.
+void run_rows_call_ranged(const void* q, size_t nq, const void* sp, size_t ns, int dim, int predicate, double radius,
+                          size_t limit, int ranges, void** rows_out, size_t* row_count_out) {
+  cudaStream_t s = library_stream(), copy = aux_stream(0);
+  PhaseTimer timer(s);
+  timer.mark("begin");
+  const size_t rec = record_size(dim);
+  const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
+  void* d_search = upload(sp, rec * ns, s);
+  timer.mark("upload");
+  Scene* sc = nullptr;
+  bool pinned = false;
+  void* host = nullptr;
+  try {
+    host = rows_host_buffer(row_size * nq * limit, &pinned);
+    BuildQueryInputs in{d_search, (uint32_t)ns, nullptr, q, (uint32_t)nq, dim};
+    QueryResult r = run_build_and_query_chunked(in, predicate, radius, (uint32_t)limit, s, copy, &timer, &sc, host,
+                                                (unsigned long long)nq * limit, ranges);
+    RTDL_CUDA_CHECK(cudaStreamSynchronize(s));  // s has waited for the copies
+    timer.mark("download");
+    timer.publish();
+    *rows_out = host;
+    *row_count_out = (size_t)r.rows;
+  } catch (...) {
+    sync_quietly(copy);
+    if (host && !(pinned && pinned_pool().put(host))) std::free(host);
+    destroy_scene(sc);
+    dev_free(d_search, s);
+    sync_quietly(s);
+    throw;
+  }
+  destroy_scene(sc);
+  dev_free(d_search, s);
+}
+
 // Plain per-call launch: upload, build, query, download.  Fixed-radius rows
 // are copied to the host range by range while later ranges are still being
 // emitted (the copy stream is this thread's second stream, idle by then).
 void run_rows_call(const void* q, size_t nq, const void* sp, size_t ns, int dim, int predicate, double radius,
                    size_t limit, void** rows_out, size_t* row_count_out) {
+  const int ranges = (int)std::min<size_t>(kMaxQueryRanges, nq / kRangeQueries);
+  if (predicate != kKnn && limit <= (size_t)kMaxList && ranges >= 2)
+    return run_rows_call_ranged(q, nq, sp, ns, dim, predicate, radius, limit, ranges, rows_out, row_count_out);
   cudaStream_t s = library_stream();
   PhaseTimer timer(s);
   timer.mark("begin");

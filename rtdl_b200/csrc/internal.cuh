@@ -348,6 +348,7 @@ struct BuildQueryInputs {
 // makes its stream wait for `copy` before it uses or releases the rows.
 struct RowDownload {
   void* (*alloc)(size_t bytes, bool* pinned) = nullptr;
+  void* host_fixed = nullptr;  // instead of `alloc`: the rows go here (pinned memory the caller holds)
   cudaStream_t copy = nullptr;
   void* host = nullptr;
   bool pinned = false;
@@ -357,6 +358,15 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
                                 void* rows_dev, size_t rows_capacity, void** rows_alloc, uint8_t* overflow_dev,
                                 cudaStream_t s, cudaStream_t aux, PhaseTimer* timer, Scene** scene_out,
                                 void** query_owned, RowDownload* download = nullptr);
+// The plain per-call form with rows to host memory, the queries taken in
+// `chunks` ranges of their input order so that the copy of each range's rows
+// overlaps the query of the next (rows land in host_rows, pinned memory of
+// host_capacity_rows rows held by the caller; `copy` carries the copies, and
+// work queued on `s` after the call follows them).  Query records are read
+// from in.query_host.
+QueryResult run_build_and_query_chunked(const BuildQueryInputs& in, int predicate, double radius, uint32_t limit,
+                                        cudaStream_t s, cudaStream_t copy, PhaseTimer* timer, Scene** scene_out,
+                                        void* host_rows, unsigned long long host_capacity_rows, int chunks);
 // Further streams of this thread on the current device: 0 is the query side of
 // run_build_and_query and the row copies, 1 the heavy queries' refinement
 // beside the emit kernels.

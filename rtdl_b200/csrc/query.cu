@@ -2414,11 +2414,63 @@ struct Readback {
   unsigned long long chunk_rows[kDownloadChunks + 1];  // first row of each download range
 };
 
+// Pinned and mapped into the device address space, so small reads of device
+// counters can be written into it by a kernel (SmallReads) instead of being
+// copied by the copy engine.
 Readback* pinned_readback() {
   thread_local Readback* rb = nullptr;
-  if (rb == nullptr) RTDL_CUDA_CHECK(cudaMallocHost(&rb, sizeof(Readback)));
+  if (rb == nullptr)
+    RTDL_CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&rb), sizeof(Readback),
+                                  cudaHostAllocMapped | cudaHostAllocPortable));
   return rb;
 }
+
+// Small reads of device counters into the thread's Readback, written by one
+// kernel of one warp.  Kernel stores do not queue behind copies: a call whose
+// rows are being copied to the host (the copy engine busy for milliseconds)
+// reads its counts at once instead of after those copies.  Sources and
+// fields are 4-byte words; the host reads the fields after the stream has
+// been synchronized.
+struct SmallRead {
+  static constexpr int kMax = 6;
+  const uint32_t* src[kMax];
+  uint32_t* dst[kMax];
+  uint32_t words[kMax];
+  int n;
+};
+
+__global__ void k_read_small(SmallRead r) {
+  for (int k = 0; k < r.n; ++k)
+    for (uint32_t i = threadIdx.x; i < r.words[k]; i += blockDim.x) r.dst[k][i] = r.src[k][i];
+}
+
+class SmallReads {
+ public:
+  explicit SmallReads(Readback* rb) : rb_(rb) {
+    void* alias = nullptr;
+    RTDL_CUDA_CHECK(cudaHostGetDevicePointer(&alias, rb, 0));
+    alias_ = static_cast<char*>(alias);
+    r_.n = 0;
+  }
+  // `field` is a member of the Readback given at construction.
+  void add(void* field, const void* dev, size_t bytes) {
+    if (r_.n == SmallRead::kMax) throw std::runtime_error("too many small reads in one launch");
+    r_.src[r_.n] = static_cast<const uint32_t*>(dev);
+    r_.dst[r_.n] = reinterpret_cast<uint32_t*>(alias_ + (static_cast<char*>(field) - reinterpret_cast<char*>(rb_)));
+    r_.words[r_.n] = (uint32_t)(bytes / 4);
+    ++r_.n;
+  }
+  void launch(cudaStream_t s) {
+    k_read_small<<<1, 32, 0, s>>>(r_);
+    RTDL_LAUNCHED(1);
+    r_.n = 0;
+  }
+
+ private:
+  Readback* rb_;
+  char* alias_;
+  SmallRead r_;
+};
 
 inline unsigned int grid_for(uint64_t n, int threads) {
   uint64_t b = (n + threads - 1) / threads;
@@ -2774,7 +2826,9 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
     RTDL_LAUNCHED(2);
     if (pass == 0 && after_first_pass) after_first_pass();  // work the caller queues before the first wait
 
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->refine_left, next_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    SmallReads reads(rb);
+    reads.add(&rb->refine_left, next_count, sizeof(unsigned int));
+    reads.launch(s);
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
     n = rb->refine_left;
     if (last) out.generic = n;
@@ -2783,7 +2837,9 @@ RefineOut refine_heavy(const CollectParams& C, const QueryPrep& qp, double radiu
   out.generic_qin = gen_qin;
   out.generic_m = gen_m;
   out.generic_rad = gen_rad;
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->mid, small + 2, sizeof(unsigned int) * 2, cudaMemcpyDeviceToHost, s));
+  SmallReads reads(rb);
+  reads.add(&rb->mid, small + 2, sizeof(unsigned int) * 2);
+  reads.launch(s);
   RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
   out.mid = rb->mid;
   out.big = rb->big;
@@ -3052,30 +3108,34 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
     const bool count_only = rows_alloc == nullptr && rows_dev == nullptr && !bs && !ss && !witness;
     Readback* rb = pinned_readback();
     if (count_only) {
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, s));
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+      SmallReads reads(rb);
+      reads.add(&rb->rows, offsets + nq, sizeof(unsigned long long));
+      reads.add(&rb->heavy, small, sizeof(unsigned int) * 4);
+      reads.add(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int));
+      reads.add(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int));
+      reads.launch(s);
       RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
       check_readback(*rb);
       res.rows = rb->rows;
     } else {
       // rows copied to the host range by range as they are emitted
-      bool chunked = dl != nullptr && dl->alloc != nullptr && rows_alloc != nullptr && !bs && !ss && !witness &&
+      bool chunked = dl != nullptr && (dl->alloc != nullptr || dl->host_fixed != nullptr) && rows_alloc != nullptr &&
+                     !bs && !ss && !witness &&
                      nq >= (uint32_t)kDownloadChunks * 1024u;
+      SmallReads reads(rb);
       if (chunked) {
         unsigned long long* chunk_dev =
             static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * (kDownloadChunks + 1), s));
         refine_bufs.push_back(chunk_dev);
         k_chunk_rows<<<1, 32, 0, s>>>(offsets, nq, kDownloadChunks, chunk_dev);
         RTDL_LAUNCHED(1);
-        RTDL_CUDA_CHECK(cudaMemcpyAsync(rb->chunk_rows, chunk_dev, sizeof(unsigned long long) * (kDownloadChunks + 1),
-                                        cudaMemcpyDeviceToHost, s));
+        reads.add(rb->chunk_rows, chunk_dev, sizeof(unsigned long long) * (kDownloadChunks + 1));
       }
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, s));
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-      RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+      reads.add(&rb->rows, offsets + nq, sizeof(unsigned long long));
+      reads.add(&rb->heavy, small, sizeof(unsigned int) * 4);
+      reads.add(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int));
+      reads.add(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int));
+      reads.launch(s);
       RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
       const Readback r = *rb;
       check_readback(r);
@@ -3163,8 +3223,10 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
         RTDL_LAUNCHED(1);
         if (generic > 0) launch_expand(generic, ro.generic_qin);
         if (timer) timer->mark("emit");
-        RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-        RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        SmallReads end_reads(rb);
+        end_reads.add(&rb->error, small + 1, sizeof(unsigned int));
+        end_reads.add(&rb->fixups, small + 4, sizeof(unsigned int));
+        end_reads.launch(s);
         RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
         if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
         if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
@@ -3209,7 +3271,12 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
         RTDL_LAUNCHED(1);
         if (chunked) {
           const size_t row_size = predicate == kFrn ? 16 : 24;
-          dl->host = dl->alloc(row_size * res.rows, &dl->pinned);
+          if (dl->host_fixed) {
+            dl->host = dl->host_fixed;
+            dl->pinned = true;
+          } else {
+            dl->host = dl->alloc(row_size * res.rows, &dl->pinned);
+          }
         }
         EmitParams E = emit_params();
         if (chunked) {
@@ -3279,8 +3346,10 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
             ++dl->copies;
           }
           if (timer) timer->mark("emit");
-          RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-          RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+          SmallReads end_reads(rb);
+          end_reads.add(&rb->error, small + 1, sizeof(unsigned int));
+          end_reads.add(&rb->fixups, small + 4, sizeof(unsigned int));
+          end_reads.launch(s);
           RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
           if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
           if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
@@ -3325,8 +3394,10 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
           launch_expand(generic, generic_list);
         }
         if (timer) timer->mark("emit");
-        RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->error, small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-        RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->fixups, small + 4, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        SmallReads end_reads(rb);
+        end_reads.add(&rb->error, small + 1, sizeof(unsigned int));
+        end_reads.add(&rb->fixups, small + 4, sizeof(unsigned int));
+        end_reads.launch(s);
         RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
         if (stats) last_stats()[kStatEmitFixups] = rb->fixups;
         if (rb->error & 6u) throw std::runtime_error("generic neighbor path produced an inconsistent candidate count");
@@ -3649,6 +3720,79 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
   pq->raw = nullptr;  // the caller's records (or *query_owned)
   destroy_query_set(pq);
   return r;
+}
+
+// Rows to host memory with the query set cut into `chunks` ranges of its input
+// order, answered one after another against one scene: each range's rows are
+// copied to their place in `host_rows` (the ranges' rows follow one another
+// in input order, as one call's would) range by range on `copy` while the
+// next range is collected and emitted on `s`.  The transfer of the rows,
+// which bounds such a call, so starts after the first range's query instead
+// of after the whole set's.  Each range is an ordinary query: its rows are
+// the rows a call with only those queries gives.
+QueryResult run_build_and_query_chunked(const BuildQueryInputs& in, int predicate, double radius, uint32_t limit,
+                                        cudaStream_t s, cudaStream_t copy, PhaseTimer* timer, Scene** scene_out,
+                                        void* host_rows, unsigned long long host_capacity_rows, int chunks) {
+  *scene_out = nullptr;
+  Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, leaf_size_for(predicate != kKnn));
+  *scene_out = sc;
+  if (timer) timer->mark("build");
+  const size_t rec = in.dim == 3 ? sizeof(RtdlPoint3D) : sizeof(RtdlPoint);
+  const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
+  QueryResult total;
+  // Every range keeps its device rows until all copies are done: a buffer
+  // released behind its copies would make the pool order the next range's
+  // allocation, and so its emission, after them.
+  std::vector<void*> range_rows;
+  auto release_rows = [&]() {
+    for (void* p : range_rows) dev_free(p, s);
+    range_rows.clear();
+  };
+  try {
+    for (int c = 0; c < chunks; ++c) {
+      const uint32_t q0 = (uint32_t)((uint64_t)in.nq * (uint32_t)c / (uint32_t)chunks);
+      const uint32_t q1 = (uint32_t)((uint64_t)in.nq * (uint32_t)(c + 1) / (uint32_t)chunks);
+      const uint32_t nqc = q1 - q0;
+      if (nqc == 0) continue;
+      if (total.rows + (unsigned long long)nqc * limit > host_capacity_rows)
+        throw std::runtime_error("host row buffer too small for the query ranges");
+      void* d_q = dev_alloc(rec * nqc, s);
+      void* d_rows = nullptr;
+      RowDownload dl;
+      dl.host_fixed = static_cast<char*>(host_rows) + total.rows * row_size;
+      dl.copy = copy;
+      QueryResult r;
+      try {
+        RTDL_CUDA_CHECK(cudaMemcpyAsync(d_q, static_cast<const char*>(in.query_host) + rec * q0, rec * nqc,
+                                        cudaMemcpyHostToDevice, s));
+        r = run_radius_query(sc, d_q, nqc, predicate, radius, limit, nullptr, 0, &d_rows, nullptr, s, nullptr, nullptr,
+                             nullptr, nullptr, false, &dl);
+        if (r.rows && dl.copies == 0)  // a range too small to be copied piecewise: one copy after its emit
+          RTDL_CUDA_CHECK(cudaMemcpyAsync(dl.host_fixed, d_rows, r.rows * row_size, cudaMemcpyDeviceToHost, s));
+      } catch (...) {
+        sync_quietly(copy);
+        dev_free(d_rows, s);
+        dev_free(d_q, s);
+        throw;
+      }
+      range_rows.push_back(d_rows);
+      dev_free(d_q, s);
+      total.rows += r.rows;
+      total.heavy += r.heavy;
+    }
+    if (timer) timer->mark("queries");
+    // the rows are released on `s` once it has waited for the copies
+    static thread_local cudaEvent_t ev_copied = nullptr;
+    if (!ev_copied) RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
+    RTDL_CUDA_CHECK(cudaEventRecord(ev_copied, copy));
+    RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ev_copied, 0));
+    release_rows();
+  } catch (...) {
+    sync_quietly(copy);
+    release_rows();
+    throw;
+  }
+  return total;
 }
 
 // ---- captured summary graphs ------------------------------------------------

@@ -85,6 +85,24 @@ def test_full_scale_fixed_radius_rows(gpu, clustered):
     assert _sha(rows) == ref["rows_sha256"], f"rows differ from the oracle's in queries {_first_bad_block(rows, per_q, ref)}"
 
 
+def test_full_scale_plain_call_rows(gpu, clustered):
+    """The plain per-call entry point with host records and host rows
+    (rtdl_b200_run_fixed_radius_neighbors_3d), the call the end-to-end
+    benchmark times: 1,048,576 queries are answered in eight ranges of their
+    input order whose rows are copied to the host while the next range runs.
+    The complete row set must equal the oracle's."""
+    probe, build = clustered
+    view = rt.runtime.fixed_radius_neighbors(rt.pack_points(records=probe), rt.pack_points(records=build),
+                                             radius=workloads.CLUSTERED_RADIUS, k_max=64)
+    rows = view.to_numpy()
+    view.close()
+    ref = DIGESTS["frn_1m"]
+    per_q = np.bincount(rows["query_id"], minlength=len(probe))
+    assert len(rows) == ref["rows"]
+    assert _sha(per_q.astype(np.uint32)) == ref["counts_sha256"]
+    assert _sha(rows) == ref["rows_sha256"], f"rows differ from the oracle's in queries {_first_bad_block(rows, per_q, ref)}"
+
+
 def test_full_scale_knn16_rows(gpu, clustered):
     probe, build = clustered
     with rt.B200Scene(rt.pack_points(records=build)) as scene:

@@ -2254,14 +2254,18 @@ struct ExpandParams {
   const uint32_t* qrank;      // with work_list: input index -> output rank
 };
 
-// A warp per query writes its rows with the exact FP64 distance: all queries in
-// output order, or the queries of `work_list`.
+// G consecutive threads per query (G = 32: a warp) write its rows with the
+// exact FP64 distance: all queries in output order, or the queries of
+// `work_list`.  G is at least the longest row list when it is known to be
+// short (nearest lists of k <= 16 rows), so a warp serves 32 / G queries and
+// their rows, consecutive in output order, with one set of stores.
+template <int G>
 __global__ void __launch_bounds__(kExpandThreads) k_expand(ExpandParams P) {
-  const int lane = threadIdx.x & 31;
-  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & (G - 1);
+  const uint64_t groups = ((uint64_t)gridDim.x * blockDim.x) / G;
   const bool ids_sorted = P.bands->ids_sorted != 0;
   const bool scene_inexact = *P.S.inexact != 0;
-  for (uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < P.nq; j += warps) {
+  for (uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G; j < P.nq; j += groups) {
     const uint32_t qin = P.work_list ? P.work_list[j] : (ids_sorted ? (uint32_t)j : P.oorder[j]);
     const uint32_t cnt = P.counts[qin];
     const uint8_t fl = P.flags[qin];
@@ -2274,7 +2278,7 @@ __global__ void __launch_bounds__(kExpandThreads) k_expand(ExpandParams P) {
     const uint32_t* src = P.work_list ? P.heavy_out + P.heavy_out_off[j]
                           : (fl & 2) ? P.heavy_out + P.heavy_out_off[P.temp[(size_t)qin * P.L]]
                                      : P.temp + (size_t)qin * P.L;
-    for (uint32_t s = lane; s < cnt; s += 32) {
+    for (uint32_t s = lane; s < cnt; s += G) {
       const uint32_t sidx = src[s];
       if (sidx >= P.S.n) {  // never expected: a generic-path slot without a candidate
         atomicOr(P.error, 4u);
@@ -3101,7 +3105,7 @@ QueryResult run_radius_query(Scene* sc, const void* queries_dev, uint32_t nq, in
       X.error = small + 1;
       X.work_list = list;
       X.qrank = qrank;
-      k_expand<<<grid_for((uint64_t)n_generic * 32, kExpandThreads), kExpandThreads, 0, s>>>(X);
+      k_expand<32><<<grid_for((uint64_t)n_generic * 32, kExpandThreads), kExpandThreads, 0, s>>>(X);
       RTDL_LAUNCHED(1);
     };
     // Rows only counted: the total is known after the scan (no refinement, no emit).
@@ -4342,10 +4346,12 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
     if (timer) timer->mark("scan");
 
     Readback* rb = pinned_readback();
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->rows, offsets + nq, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->heavy, small, sizeof(unsigned int) * 2, cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-    RTDL_CUDA_CHECK(cudaMemcpyAsync(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    SmallReads reads(rb);
+    reads.add(&rb->rows, offsets + nq, sizeof(unsigned long long));
+    reads.add(&rb->heavy, small, sizeof(unsigned int) * 2);
+    reads.add(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int));
+    reads.add(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int));
+    reads.launch(s);
     RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
     const Readback r = *rb;
     check_readback(r);
@@ -4384,8 +4390,17 @@ QueryResult run_query(Scene* sc, const void* queries_dev, uint32_t nq, int predi
       E.error = small + 1;
       E.work_list = nullptr;
       E.qrank = nullptr;
-      const unsigned int blocks = grid_for((uint64_t)nq * 32, kExpandThreads);
-      k_expand<<<blocks, kExpandThreads, 0, s>>>(E);
+      // lists of at most L rows unless some query took the generic path
+      const int group = (r.heavy > 0 || L > 16) ? 32 : L > 8 ? 16 : L > 4 ? 8 : L > 2 ? 4 : L > 1 ? 2 : 1;
+      const unsigned int blocks = grid_for((uint64_t)nq * group, kExpandThreads);
+      switch (group) {
+        case 1: k_expand<1><<<blocks, kExpandThreads, 0, s>>>(E); break;
+        case 2: k_expand<2><<<blocks, kExpandThreads, 0, s>>>(E); break;
+        case 4: k_expand<4><<<blocks, kExpandThreads, 0, s>>>(E); break;
+        case 8: k_expand<8><<<blocks, kExpandThreads, 0, s>>>(E); break;
+        case 16: k_expand<16><<<blocks, kExpandThreads, 0, s>>>(E); break;
+        default: k_expand<32><<<blocks, kExpandThreads, 0, s>>>(E); break;
+      }
       RTDL_LAUNCHED(1);
     }
     if (timer) timer->mark("emit");

@@ -4464,18 +4464,20 @@ HausdorffResult run_directed_hausdorff(Scene* sc, const void* queries_dev, uint3
                                           temp, nearest_dist_dev, nearest_id_dev, partial);
   k_witness_final<<<1, 32, 0, s>>>(partial, (int)blocks, best);
   RTDL_LAUNCHED(2);
+  // one read of the witness (into the record's row-range words) and the error words
   Readback* rb = pinned_readback();
-  Witness* hw = reinterpret_cast<Witness*>(rb);
-  static_assert(sizeof(Witness) <= sizeof(Readback), "readback buffer too small");
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(hw, best, sizeof(Witness), cudaMemcpyDeviceToHost, s));
+  static_assert(sizeof(Witness) <= sizeof(rb->chunk_rows), "readback record too small for the witness");
+  SmallReads reads(rb);
+  reads.add(rb->chunk_rows, best, sizeof(Witness));
+  reads.add(&rb->scene_bad, &sc->stats->bad, sizeof(unsigned int));
+  reads.add(&rb->query_bad, &qp.qst->bad, sizeof(unsigned int));
+  reads.add(&rb->error, small + 1, sizeof(unsigned int));
+  reads.launch(s);
   RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
-  const Witness w = *hw;
+  Witness w;
+  memcpy(&w, rb->chunk_rows, sizeof(Witness));
+  const unsigned int bad[3] = {rb->scene_bad, rb->query_bad, rb->error};
   if (timer) timer->mark("reduce");
-  unsigned int bad[3] = {0, 0, 0};
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad[0], &sc->stats->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad[1], &qp.qst->bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-  RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad[2], small + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-  RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
   dev_free(counts, s);
   dev_free(flags, s);
   dev_free(temp, s);

@@ -3738,49 +3738,92 @@ QueryResult run_build_and_query_chunked(const BuildQueryInputs& in, int predicat
                                         cudaStream_t s, cudaStream_t copy, PhaseTimer* timer, Scene** scene_out,
                                         void* host_rows, unsigned long long host_capacity_rows, int chunks) {
   *scene_out = nullptr;
-  Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, leaf_size_for(predicate != kKnn));
-  *scene_out = sc;
-  if (timer) timer->mark("build");
   const size_t rec = in.dim == 3 ? sizeof(RtdlPoint3D) : sizeof(RtdlPoint);
   const size_t row_size = predicate == kFrn ? sizeof(RtdlFixedRadiusNeighborRow) : sizeof(RtdlKnnNeighborRow);
-  QueryResult total;
+  // Each range's query set is uploaded and prepared (Morton order, its own
+  // statistics) on a third stream one range ahead: the first range's beside
+  // the scene build, every later one beside the query of the range before it.
+  cudaStream_t ps = aux_stream(1);
+  std::vector<PreparedQueries*> sets(chunks, nullptr);
+  std::vector<cudaEvent_t> ready(chunks, nullptr);
+  auto range_of = [&](int c, uint32_t& q0, uint32_t& n) {
+    q0 = (uint32_t)((uint64_t)in.nq * (uint32_t)c / (uint32_t)chunks);
+    n = (uint32_t)((uint64_t)in.nq * (uint32_t)(c + 1) / (uint32_t)chunks) - q0;
+  };
+  auto prepare_range = [&](int c) {
+    uint32_t q0, n;
+    range_of(c, q0, n);
+    void* d_q = dev_alloc(rec * n, ps);
+    RTDL_CUDA_CHECK(cudaMemcpyAsync(d_q, static_cast<const char*>(in.query_host) + rec * q0, rec * n,
+                                    cudaMemcpyHostToDevice, ps));
+    PreparedQueries* pq = nullptr;
+    try {
+      pq = prepare_query_set(d_q, n, in.dim, ps);  // owns d_q from here
+    } catch (...) {
+      dev_free(d_q, ps);
+      throw;
+    }
+    sets[c] = pq;
+    RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ready[c], cudaEventDisableTiming));
+    RTDL_CUDA_CHECK(cudaEventRecord(ready[c], ps));
+  };
   // Every range keeps its device rows until all copies are done: a buffer
   // released behind its copies would make the pool order the next range's
   // allocation, and so its emission, after them.
   std::vector<void*> range_rows;
-  auto release_rows = [&]() {
+  auto release = [&]() {
+    sync_quietly(ps);
+    for (int c = 0; c < chunks; ++c) {
+      if (sets[c]) {
+        sets[c]->stream = s;
+        destroy_query_set(sets[c]);
+        sets[c] = nullptr;
+      }
+      if (ready[c]) {
+        note_cleanup_error(cudaEventDestroy(ready[c]), "cudaEventDestroy");
+        ready[c] = nullptr;
+      }
+    }
     for (void* p : range_rows) dev_free(p, s);
     range_rows.clear();
   };
+  QueryResult total;
   try {
+    // the query side waits for what the caller queued on s (the search set's upload)
+    static thread_local cudaEvent_t ev_start = nullptr;
+    if (!ev_start) RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
+    RTDL_CUDA_CHECK(cudaEventRecord(ev_start, s));
+    RTDL_CUDA_CHECK(cudaStreamWaitEvent(ps, ev_start, 0));
+    prepare_range(0);
+    Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, leaf_size_for(predicate != kKnn));
+    *scene_out = sc;
+    if (timer) timer->mark("build");
     for (int c = 0; c < chunks; ++c) {
-      const uint32_t q0 = (uint32_t)((uint64_t)in.nq * (uint32_t)c / (uint32_t)chunks);
-      const uint32_t q1 = (uint32_t)((uint64_t)in.nq * (uint32_t)(c + 1) / (uint32_t)chunks);
-      const uint32_t nqc = q1 - q0;
-      if (nqc == 0) continue;
+      uint32_t q0, nqc;
+      range_of(c, q0, nqc);
       if (total.rows + (unsigned long long)nqc * limit > host_capacity_rows)
         throw std::runtime_error("host row buffer too small for the query ranges");
-      void* d_q = dev_alloc(rec * nqc, s);
+      RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ready[c], 0));
+      PreparedQueries* pq = sets[c];
+      pq->stream = s;  // from here the set is used and released on s
+      if (c + 1 < chunks) prepare_range(c + 1);
       void* d_rows = nullptr;
       RowDownload dl;
       dl.host_fixed = static_cast<char*>(host_rows) + total.rows * row_size;
       dl.copy = copy;
       QueryResult r;
       try {
-        RTDL_CUDA_CHECK(cudaMemcpyAsync(d_q, static_cast<const char*>(in.query_host) + rec * q0, rec * nqc,
-                                        cudaMemcpyHostToDevice, s));
-        r = run_radius_query(sc, d_q, nqc, predicate, radius, limit, nullptr, 0, &d_rows, nullptr, s, nullptr, nullptr,
-                             nullptr, nullptr, false, &dl);
+        r = run_radius_query(sc, nullptr, nqc, predicate, radius, limit, nullptr, 0, &d_rows, nullptr, s, nullptr,
+                             nullptr, nullptr, pq, false, &dl);
         if (r.rows && dl.copies == 0)  // a range too small to be copied piecewise: one copy after its emit
           RTDL_CUDA_CHECK(cudaMemcpyAsync(dl.host_fixed, d_rows, r.rows * row_size, cudaMemcpyDeviceToHost, s));
       } catch (...) {
-        sync_quietly(copy);
-        dev_free(d_rows, s);
-        dev_free(d_q, s);
+        if (d_rows) range_rows.push_back(d_rows);
         throw;
       }
       range_rows.push_back(d_rows);
-      dev_free(d_q, s);
+      destroy_query_set(pq);
+      sets[c] = nullptr;
       total.rows += r.rows;
       total.heavy += r.heavy;
     }
@@ -3790,10 +3833,11 @@ QueryResult run_build_and_query_chunked(const BuildQueryInputs& in, int predicat
     if (!ev_copied) RTDL_CUDA_CHECK(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
     RTDL_CUDA_CHECK(cudaEventRecord(ev_copied, copy));
     RTDL_CUDA_CHECK(cudaStreamWaitEvent(s, ev_copied, 0));
-    release_rows();
+    release();
   } catch (...) {
     sync_quietly(copy);
-    release_rows();
+    sync_quietly(s);
+    release();
     throw;
   }
   return total;

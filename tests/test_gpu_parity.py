@@ -441,8 +441,8 @@ def test_plain_call_rows_copied_range_by_range(gpu, dim, ranked, k_max):
     assert got["query_id"].min() >= 24000 * 3 // 8
 
 
-@pytest.mark.parametrize("ranked,k_max", [(False, 64), (True, 12)])
-def test_plain_call_query_ranges(gpu, ranked, k_max):
+@pytest.mark.parametrize("dim,ranked,k_max", [(3, False, 64), (3, True, 12), (2, False, 32)])
+def test_plain_call_query_ranges(gpu, dim, ranked, k_max):
     """From 262,144 queries on, the plain per-call launch answers its queries
     in ranges of their input order (here three) and copies each range's rows
     to the host while the next range runs.  Rows must equal the oracle's
@@ -450,16 +450,16 @@ def test_plain_call_query_ranges(gpu, ranked, k_max):
     a multiple of three), a stretch of queries without neighbours across a
     boundary, dense clusters with list queries and refined heavy queries,
     and queries on coincident points that reach the generic path."""
-    rng = np.random.default_rng(314 + k_max)
+    rng = np.random.default_rng(314 + k_max + dim)
     centres = rng.random((16, 3))
-    s_pts = _clustered(rng, 120000, centres)
+    s_pts = _clustered(rng, 120000, centres)[:, :dim]
     s_pts = np.concatenate([s_pts, np.repeat(s_pts[:2], 400, axis=0)])  # 401 copies of two points
     nq = 400003
-    q_pts = _clustered(rng, nq, centres)
+    q_pts = _clustered(rng, nq, centres)[:, :dim]
     q_pts[nq // 4: nq // 2] += 5.0  # no neighbours, across the first range boundary
     q_pts[-50:] = s_pts[np.arange(50) % 2]  # queries on the coincident copies
     s, q = _cols(s_pts), _cols(q_pts)
-    radius = 0.01
+    radius = 0.01 if dim == 3 else 0.002
     v = rt.runtime.fixed_radius_neighbors(_pack(q), _pack(s), radius=radius, k_max=k_max, ranked=ranked)
     got = v.to_numpy()
     v.close()

@@ -369,7 +369,7 @@ QueryResult run_build_and_query_chunked(const BuildQueryInputs& in, int predicat
                                         void* host_rows, unsigned long long host_capacity_rows, int chunks);
 // Further streams of this thread on the current device: 0 is the query side of
 // run_build_and_query and the row copies, 1 the heavy queries' refinement
-// beside the emit kernels.
+// beside the emit kernels and the query ranges' preparation one range ahead.
 cudaStream_t aux_stream(int which = 0);
 // Leaf-bucket size of a scene build: the tuning's when set, else 24 for scenes
 // that serve only fixed-radius queries (larger buckets shorten the walk and the

@@ -239,6 +239,11 @@ __host__ __device__ constexpr int seed_half_width(int L) { return L * 2 < 16 ? 1
 // Lists at least this long take kWalkNear (k = 4: 1.40 ms pre-order against
 // 1.46 ms nearer first).
 constexpr int kNearFirstMinList = 5;
+// A leaf at most this many lanes need is visited point-major (visit_leaf_pm):
+// the walk of lists of k <= 4 took 0.67 instead of 0.80 ms at k = 1 with 4
+// (the 4M x 4M Hausdorff nearest 1.39 instead of 1.52 ms), at k = 16 3.63
+// instead of 3.69 ms with 2 and 3.85 ms with 4.
+__host__ __device__ constexpr int point_major_max(int L) { return L <= 4 ? 4 : 2; }
 // Held to 64 registers (32 resident warps at 128 threads per block): the
 // k = 16 walk ran 2.8% faster than at its natural 72 (28 warps); at 48
 // registers the spills cost more than the occupancy gained.
@@ -344,6 +349,44 @@ __global__ void __launch_bounds__(256, 4) k_pass1(Pass1Params P) {
     }
   };
 
+  // Point-major visit of a leaf few lanes need (nearest lists): lane j holds
+  // point first + j and the needing lanes are taken in turn; a point passes
+  // when it may order before that lane's current last entry (the FP32 side
+  // of `before`, a superset of what it accepts), and the owning lane then
+  // inserts the passing points one by one, exactly as visit_leaf would.
+  auto visit_leaf_pm = [&](int first, int cnt, unsigned int needers) {
+    const bool has = lane < cnt;
+    const uint32_t pi = (uint32_t)(first + (has ? lane : 0));
+    const float4 p = __ldg(&S.pts[pi]);
+    while (needers) {
+      const int q = __ffs(needers) - 1;
+      needers &= needers - 1u;
+      const float qx = __shfl_sync(0xffffffffu, c.qx, q), qy = __shfl_sync(0xffffffffu, c.qy, q),
+                  qz = __shfl_sync(0xffffffffu, c.qz, q);
+      const float kl = __shfl_sync(0xffffffffu, klast, q);
+      const bool full_list = __shfl_sync(0xffffffffu, (int)(len == L), q) != 0;
+      const int wlo = __shfl_sync(0xffffffffu, win_lo, q), whi = __shfl_sync(0xffffffffu, win_hi, q);
+      const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+      const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      bool pass = has && !((int)pi >= wlo && (int)pi < whi);
+      if (full_list) pass = pass && d2 - kl <= key_tol(c, fmaxf(d2, kl));
+      unsigned int passing = __ballot_sync(0xffffffffu, pass);
+      if (STATS && lane == q) st_points += cnt;
+      while (passing) {
+        const int j = __ffs(passing) - 1;
+        passing &= passing - 1u;
+        const float key = __shfl_sync(0xffffffffu, d2, j);
+        if (lane == q) {
+          const uint32_t idx = (uint32_t)(first + j);
+          if (!(len == L && !before(c, key, idx, klast, ilast))) {
+            insert(key, idx);
+            ++count;
+          }
+        }
+      }
+    }
+  };
+
   auto box_ok = [&](float kb) -> bool {
     if (!KNN && kb > B.box_hi2) return false;
     const bool full = KNN ? (len == L) : prune;
@@ -401,7 +444,9 @@ __global__ void __launch_bounds__(256, 4) k_pass1(Pass1Params P) {
           ++cur;  // internal node: its left child is the next record
           continue;
         }
-        if (need) visit_leaf(leaf_first(hit), leaf_count(hit));
+        const unsigned int nm = __ballot_sync(0xffffffffu, need);
+        if (KNN && __popc(nm) <= point_major_max(L)) visit_leaf_pm(leaf_first(hit), leaf_count(hit), nm);
+        else if (need) visit_leaf(leaf_first(hit), leaf_count(hit));
       }
       cur = __float_as_int(b.w);
     }
@@ -434,7 +479,9 @@ __global__ void __launch_bounds__(256, 4) k_pass1(Pass1Params P) {
       const int hit = __float_as_int(a.w);
       bool descended = false;
       if (hit < 0) {
-        if (need) visit_leaf(leaf_first(hit), leaf_count(hit));
+        const unsigned int nm = __ballot_sync(0xffffffffu, need);
+        if (KNN && __popc(nm) <= point_major_max(L)) visit_leaf_pm(leaf_first(hit), leaf_count(hit), nm);
+        else if (need) visit_leaf(leaf_first(hit), leaf_count(hit));
       } else {
         const int left = cur + 1;
         const float4 la = __ldg(&S.nodes[2 * left]), lb = __ldg(&S.nodes[2 * left + 1]);

@@ -632,10 +632,8 @@ RTDL_B200_API int rtdl_b200_get_last_query_stats(unsigned long long* values_out,
 RTDL_B200_API int rtdl_b200_get_launch_count(unsigned long long* count_out);
 
 /* Tuning knobs; the autotuner sets these.  leaf_size: points per LBVH leaf
- * bucket (1..32, applies to scenes built afterwards; 0, the default: 24 for
- * scenes that serve only fixed-radius queries -- the prepared fixed-radius
- * scene, problem batches, the per-call fixed_radius_neighbors and
- * bounded_knn_rows -- and 8 for general scenes); block_threads: 64, 128
+ * bucket (1..32, applies to scenes built afterwards; 0, the default: 24);
+ * block_threads: 64, 128
  * or 256; traversal: 0 = one warp walks the tree for 32 neighbouring queries
  * (packet), 1 = one thread per query, 2 = packet with the query's bounding
  * cube tested at internal nodes, 3 = packet whose leaf buckets are tested

@@ -37,7 +37,7 @@ BLOCK_THREADS = (128, 256)
 
 @dataclass(frozen=True)
 class Config:
-    leaf_size: int = 0  # 0: by the scene's use (see set_tuning)
+    leaf_size: int = 0  # 0: the library default (see set_tuning)
     traversal: str = "packet_hybrid"
     block_threads: int = 128
 

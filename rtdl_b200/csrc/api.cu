@@ -421,9 +421,9 @@ struct PreparedHandle {
 
 }  // namespace
 
-int leaf_size_for(bool fixed_radius_only) {
+int scene_leaf_size() {
   if (tuning().leaf_size > 0) return tuning().leaf_size;
-  return fixed_radius_only ? 24 : 8;
+  return 24;
 }
 
 cudaStream_t aux_stream(int which) {
@@ -629,7 +629,7 @@ int rtdl_b200_run_k_closest_hits_3d(const RtdlPoint3D* query_points, size_t quer
 namespace rtdl_b200 {
 namespace {
 int scene_create_impl(const void* points, size_t count, int dimension, int points_on_device, void* stream,
-                      bool fixed_radius_only, void** scene_out, char* error_out, size_t error_size) {
+                      void** scene_out, char* error_out, size_t error_size) {
   return guarded([&]() {
     if (!scene_out) throw std::runtime_error("scene_out must not be null");
     *scene_out = nullptr;
@@ -648,7 +648,7 @@ int scene_create_impl(const void* points, size_t count, int dimension, int point
     }
     Scene* sc = nullptr;
     try {
-      sc = build_scene(d_points, (uint32_t)count, dimension, s, leaf_size_for(fixed_radius_only));
+      sc = build_scene(d_points, (uint32_t)count, dimension, s, scene_leaf_size());
       unsigned int bad = 0;
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
       RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -668,7 +668,7 @@ int scene_create_impl(const void* points, size_t count, int dimension, int point
 
 int rtdl_b200_scene_create(const void* points, size_t count, int dimension, int points_on_device, void* stream,
                            void** scene_out, char* error_out, size_t error_size) {
-  return scene_create_impl(points, count, dimension, points_on_device, stream, false, scene_out, error_out,
+  return scene_create_impl(points, count, dimension, points_on_device, stream, scene_out, error_out,
                            error_size);
 }
 
@@ -771,7 +771,7 @@ int rtdl_b200_batch_create(const void* points, const unsigned long long* point_o
         owned = upload(points, record_size(dimension) * count, s);
         d_points = owned;
       }
-      sc = build_scene_batch(d_points, point_offsets, problems, dimension, s, leaf_size_for(true));
+      sc = build_scene_batch(d_points, point_offsets, problems, dimension, s, scene_leaf_size());
       unsigned int bad = 0;
       RTDL_CUDA_CHECK(cudaMemcpyAsync(&bad, &sc->stats->bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
       RTDL_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1018,7 +1018,7 @@ int rtdl_b200_prepare_fixed_radius_neighbors_3d(const RtdlPoint3D* search_points
     *prepared_out = nullptr;
     void* scene = nullptr;
     char err[1024];
-    if (scene_create_impl(search_points, search_count, 3, 0, nullptr, true, &scene, err, sizeof(err)) != 0)
+    if (scene_create_impl(search_points, search_count, 3, 0, nullptr, &scene, err, sizeof(err)) != 0)
       throw std::runtime_error(err);
     static_cast<Scene*>(scene)->max_radius = max_radius;
     *prepared_out = scene;
@@ -1351,7 +1351,7 @@ int prepare_count_scene(const void* points, size_t count, int dim, int on_device
                         bool device_columns, void** prepared_out, char* error_out, size_t error_size) {
   void* scene = nullptr;
   char err[1024];
-  if (scene_create_impl(points, count, dim, on_device, nullptr, true, &scene, err, sizeof(err)) != 0) {
+  if (scene_create_impl(points, count, dim, on_device, nullptr, &scene, err, sizeof(err)) != 0) {
     if (error_out && error_size) {
       std::strncpy(error_out, err, error_size - 1);
       error_out[error_size - 1] = 0;
@@ -1384,7 +1384,7 @@ int rtdl_b200_run_fixed_radius_count_threshold(const RtdlPoint* query_points, si
     void* d_query = nullptr;
     Scene* sc = nullptr;
     try {
-      sc = build_scene(d_search, (uint32_t)search_count, 2, s, leaf_size_for(true));
+      sc = build_scene(d_search, (uint32_t)search_count, 2, s, scene_leaf_size());
       d_query = upload(query_points, sizeof(RtdlPoint) * query_count, s);
       count_rows_to_host(sc, d_query, (uint32_t)query_count, radius, (uint32_t)threshold, rows_out, row_count_out, s);
     } catch (...) {
@@ -1676,7 +1676,7 @@ int rtdl_b200_prepare_point_group_nearest_witness_2d(const RtdlPoint* search_poi
     RTDL_CUDA_CHECK(cudaGetDevice(&dev));
     ensure_pool_configured(dev);
     *prepared_out = point_group_create(search_points, search_count, groups, group_count, max_radius,
-                                       leaf_size_for(true), library_stream());
+                                       scene_leaf_size(), library_stream());
   }, error_out, error_size);
 }
 

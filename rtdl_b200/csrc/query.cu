@@ -239,11 +239,11 @@ __host__ __device__ constexpr int seed_half_width(int L) { return L * 2 < 16 ? 1
 // Lists at least this long take kWalkNear (k = 4: 1.40 ms pre-order against
 // 1.46 ms nearer first).
 constexpr int kNearFirstMinList = 5;
-// A leaf at most this many lanes need is visited point-major (visit_leaf_pm):
-// the walk of lists of k <= 4 took 0.67 instead of 0.80 ms at k = 1 with 4
-// (the 4M x 4M Hausdorff nearest 1.39 instead of 1.52 ms), at k = 16 3.63
-// instead of 3.69 ms with 2 and 3.85 ms with 4.
-__host__ __device__ constexpr int point_major_max(int L) { return L <= 4 ? 4 : 2; }
+// A leaf at most this many lanes need is visited point-major (visit_leaf_pm).
+// With 24-point buckets: k = 1 walk 0.56 ms with 8 (0.60 with 4), the 4M x 4M
+// Hausdorff nearest 1.21 ms (1.23), k = 16 3.44 ms with 4 (3.48 with 2); with
+// 8-point buckets lane-major visits of every leaf took 0.79, 1.52 and 3.69 ms.
+__host__ __device__ constexpr int point_major_max(int L) { return L <= 4 ? 8 : 4; }
 // Held to 64 registers (32 resident warps at 128 threads per block): the
 // k = 16 walk ran 2.8% faster than at its natural 72 (28 warps); at 48
 // registers the spills cost more than the occupancy gained.
@@ -3725,7 +3725,7 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
       RTDL_CUDA_CHECK(cudaMemcpyAsync(*query_owned, in.query_host, qbytes, cudaMemcpyHostToDevice, s));
       q = *query_owned;
     }
-    Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, leaf_size_for(predicate != kKnn));
+    Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, scene_leaf_size());
     *scene_out = sc;
     if (timer) timer->mark("build");
     return run_query(sc, q, in.nq, predicate, radius, limit, rows_dev, rows_capacity, rows_alloc, overflow_dev, s,
@@ -3740,7 +3740,7 @@ QueryResult run_build_and_query(const BuildQueryInputs& in, int predicate, doubl
   }
   RTDL_CUDA_CHECK(cudaEventRecord(ev_start, s));
   RTDL_CUDA_CHECK(cudaStreamWaitEvent(aux, ev_start, 0));  // whatever the caller queued on s comes first
-  Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, leaf_size_for(true));
+  Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, scene_leaf_size());
   *scene_out = sc;
   const void* q = in.query_dev;
   if (in.query_host) {  // a pageable copy holds the host; the build is already queued
@@ -3842,7 +3842,7 @@ QueryResult run_build_and_query_chunked(const BuildQueryInputs& in, int predicat
     RTDL_CUDA_CHECK(cudaEventRecord(ev_start, s));
     RTDL_CUDA_CHECK(cudaStreamWaitEvent(ps, ev_start, 0));
     prepare_range(0);
-    Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, leaf_size_for(predicate != kKnn));
+    Scene* sc = build_scene(in.search_dev, in.ns, in.dim, s, scene_leaf_size());
     *scene_out = sc;
     if (timer) timer->mark("build");
     for (int c = 0; c < chunks; ++c) {

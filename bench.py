@@ -606,27 +606,23 @@ def batch_workload(args) -> dict:
     d_probe = torch.from_numpy(concat_records(probes).view(np.uint8)).to(dev)
     del probs
     chunks = _plan_chunks(nb, nq, 32 << 20, 8 << 20)
-    # autotune (leaf size and block size; batches always walk in warp packets) on the median-size problem
     from dataclasses import asdict
 
     from rtdl_b200.autotune import Autotuner
 
-    med = int(np.argsort(nb * nq)[len(nb) // 2])
-    tuner = Autotuner(repeats=2, traversals=("packet_hybrid", "packet"))
-    tune_key, tune_cfg = tuner.tune(d_build.data_ptr() + 32 * int(boff[med]), int(nb[med]),
-                                    d_probe.data_ptr() + 32 * int(qoff[med]), int(nq[med]), dimension=3,
-                                    radius=float(radius[med]), k_max=int(kmax[med]), stream=sh)
+    def one_batch(ci, rows_buf, cap):
+        a, b = chunks[ci]
+        ba, qa = int(boff[a]), int(qoff[a])
+        with B200ProblemBatch(None, dimension=3, stream=sh,
+                              device_points=(d_build.data_ptr() + 32 * ba, boff[a:b + 1] - boff[a])) as batch:
+            return batch.fixed_radius_neighbors_device(
+                d_probe.data_ptr() + 32 * qa, qoff[a:b + 1] - qoff[a], radius=radius[a:b], k_max=kmax[a:b],
+                rows_address=rows_buf.data_ptr() if rows_buf is not None else None, rows_capacity=cap, stream=sh)
 
     def batch_step(rows_buf, cap, sizes_out=None):
         total = 0
-        for ci, (a, b) in enumerate(chunks):
-            ba, qa = int(boff[a]), int(qoff[a])
-            with B200ProblemBatch(None, dimension=3, stream=sh,
-                                  device_points=(d_build.data_ptr() + 32 * ba, boff[a:b + 1] - boff[a])) as batch:
-                offs = batch.fixed_radius_neighbors_device(
-                    d_probe.data_ptr() + 32 * qa, qoff[a:b + 1] - qoff[a], radius=radius[a:b], k_max=kmax[a:b],
-                    rows_address=rows_buf.data_ptr() if rows_buf is not None else None,
-                    rows_capacity=cap, stream=sh)
+        for ci in range(len(chunks)):
+            offs = one_batch(ci, rows_buf, cap)
             if sizes_out is not None:
                 sizes_out.append(offs)
             total += int(offs[-1])
@@ -653,6 +649,12 @@ def batch_workload(args) -> dict:
     rows_total = batch_step(None, 0, chunk_sizes)
     max_chunk_rows = max(int(o[-1]) for o in chunk_sizes)
     rows_buf = torch.empty(max_chunk_rows * 16, dtype=torch.uint8, device=dev)
+    # autotune (leaf size, block size; batches always walk in warp packets) on one whole batch, the largest
+    big = int(np.argmax([int(o[-1]) for o in chunk_sizes]))
+    tuner = Autotuner(repeats=2, traversals=("packet_hybrid", "packet"))
+
+    tune_key, tune_cfg = tuner.tune_callable(f"problem batch {big} of {len(chunks)}",
+                                             lambda: one_batch(big, rows_buf, max_chunk_rows), stream=stream)
     assert plain_step(None, 0, plain_sizes) == rows_total
     plain_buf = torch.empty(max(plain_sizes) * 16, dtype=torch.uint8, device=dev)
     for _ in range(args.warmup):
@@ -1302,7 +1304,8 @@ def main(argv=None) -> int:
                      "step": "one build + query per batch of problems", "config": b["config"],
                      "plain_per_call": b["plain_per_call"], "speedup_vs_plain": b["speedup_vs_plain"],
                      "graph": b.get("graph"), "speedup_graph_vs_plain": b.get("speedup_graph_vs_plain"),
-                     "exactness": b["exactness"], "roofline": b["roofline"], "gpu_launches": b["gpu_launches"]}
+                     "exactness": b["exactness"], "roofline": b["roofline"], "gpu_launches": b["gpu_launches"],
+                     "autotune": {"tuned_on": b["autotune"]["shape_class"], "config": b["autotune"]["config"]}}
         v = serve_workload(sub)
         serve = {"metric": v["metric"], "value": v["value"], "unit": v["unit"], "config": v["config"],
                  "served": v["served"], "plain_per_call": v["plain_per_call"],

@@ -113,6 +113,33 @@ class Autotuner:
         winner.apply()
         return key, winner
 
+    def tune_callable(self, key: str, run, *, stream=None, force: bool = False) -> tuple[str, Config]:
+        """Times ``run()`` with CUDA events on ``stream`` (a torch stream; default the current one) under
+        every candidate, caches the fastest under ``key``, applies it and returns (key, config).  For a
+        workload no single plain call stands for, such as one whole problem batch."""
+        import torch
+
+        if not force and key in self.cache:
+            return key, self.apply(key)
+        timings = {}
+        for cfg in self.candidates:
+            cfg.apply()
+            best = math.inf
+            for _ in range(self.repeats + 1):  # the first run warms the allocator
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                cur = stream if stream is not None else torch.cuda.current_stream()
+                a.record(cur)
+                run()
+                b.record(cur)
+                b.synchronize()
+                best = min(best, a.elapsed_time(b))
+            timings[f"{cfg.leaf_size}/{cfg.traversal}/{cfg.block_threads}"] = best
+        winner = min(self.candidates, key=lambda c: timings[f"{c.leaf_size}/{c.traversal}/{c.block_threads}"])
+        self._store(key, winner, timings)
+        winner.apply()
+        return key, winner
+
     @staticmethod
     def _run(build_address, build_count, query_address, query_count, dimension, radius, k_max, rows_address,
              capacity, stream):

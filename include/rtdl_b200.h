@@ -632,7 +632,7 @@ RTDL_B200_API int rtdl_b200_get_last_query_stats(unsigned long long* values_out,
 RTDL_B200_API int rtdl_b200_get_launch_count(unsigned long long* count_out);
 
 /* Tuning knobs; the autotuner sets these.  leaf_size: points per LBVH leaf
- * bucket (1..32, applies to scenes built afterwards; 0, the default: 24);
+ * bucket (1..32, applies to scenes built afterwards; 0, the default: 32);
  * block_threads: 64, 128
  * or 256; traversal: 0 = one warp walks the tree for 32 neighbouring queries
  * (packet), 1 = one thread per query, 2 = packet with the query's bounding

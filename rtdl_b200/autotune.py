@@ -30,7 +30,7 @@ import numpy as np
 from . import _native
 from .runtime import B200Scene, set_tuning
 
-LEAF_SIZES = (8, 16, 24)
+LEAF_SIZES = (8, 16, 24, 32)
 TRAVERSALS = ("packet_hybrid", "packet", "packet_cube", "packet_points", "lane")
 BLOCK_THREADS = (128, 256)
 

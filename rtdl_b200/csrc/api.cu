@@ -423,7 +423,7 @@ struct PreparedHandle {
 
 int scene_leaf_size() {
   if (tuning().leaf_size > 0) return tuning().leaf_size;
-  return 24;
+  return 32;
 }
 
 cudaStream_t aux_stream(int which) {

@@ -371,11 +371,13 @@ QueryResult run_build_and_query_chunked(const BuildQueryInputs& in, int predicat
 // run_build_and_query and the row copies, 1 the heavy queries' refinement
 // beside the emit kernels and the query ranges' preparation one range ahead.
 cudaStream_t aux_stream(int which = 0);
-// Leaf-bucket size of a scene build: the tuning's when set, else 24.  Larger
-// buckets shorten the walks: the fixed-radius collect tests a bucket's points
-// with four loads in flight, and the nearest walks visit a bucket few lanes
-// need a lane per point (k = 16 walk 3.44 ms at 24 points against 3.65 ms at
-// 8, the 4M x 4M Hausdorff nearest 1.21 against 1.39 ms).
+// Leaf-bucket size of a scene build: the tuning's when set, else 32, the
+// largest a leaf reference holds.  Larger buckets shorten the walks: the
+// fixed-radius collect tests a bucket's points with four loads in flight
+// (0.69 ms at 32 points, 0.73 at 24, 0.76 at 20 on the clustered 1M x 1M
+// sets), and the nearest walks visit a bucket few lanes need a lane per point
+// (k = 16 walk 3.44 ms at 32 or 24 points against 3.65 ms at 8, the 4M x 4M
+// Hausdorff nearest 1.21 against 1.39 ms).
 int scene_leaf_size();
 
 // Ranked-summary aggregates of several (radius, k_max) requests over one

@@ -1523,7 +1523,7 @@ def hausdorff_distance(points_a, points_b, *, dimension: int | None = None) -> d
 
 def set_tuning(*, leaf_size: int = 0, block_threads: int = 128, traversal: str = "packet_hybrid") -> None:
     """Set the kernel tuning knobs (see ``rtdl_b200_set_tuning``); ``leaf_size`` 0 keeps the default
-    leaf bucket size (24 points)."""
+    leaf bucket size (32 points)."""
     modes = {"packet": 0, "lane": 1, "packet_cube": 2, "packet_points": 3, "packet_hybrid": 4}
     if traversal not in modes:
         raise ValueError("traversal must be 'packet', 'lane', 'packet_cube', 'packet_points' or 'packet_hybrid'")

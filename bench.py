@@ -992,8 +992,6 @@ def run_summary(args) -> int:
 
     torch.cuda.set_device(0)
     rt.set_device(0)
-    # these scenes serve only fixed-radius queries: the leaf buckets of a prepared fixed-radius scene
-    rt.set_tuning(leaf_size=24)
     golden = json.loads((ROOT / "tests" / "golden" / "rtnn_ranked_summary_262144.json").read_text())
     radius, k_max = golden["radius"], golden["k_max"]
     dev = torch.device("cuda", 0)

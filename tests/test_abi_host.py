@@ -239,3 +239,52 @@ def test_autotune_shape_classes_and_cache(tmp_path):
     t._store("d3-b20-q20-m5", Config(16, "lane", 256), {"16/lane/256": 1.0})
     assert Autotuner(tmp_path / "c.json").lookup("d3-b20-q20-m5") == Config(16, "lane", 256)
     assert t.lookup("missing") is None
+
+
+def test_autotune_callable_picks_caches_and_applies_the_fastest(tmp_path, monkeypatch):
+    """tune_callable's host logic without a GPU: CUDA events are replaced by a
+    clock that charges each run the time the active candidate costs; the
+    fastest candidate must win, be cached under the key (file included), be
+    applied last, and a second call must come from the cache without runs."""
+    import rtdl_b200.autotune as at
+
+    applied = []
+    monkeypatch.setattr(at.Config, "apply", lambda self: applied.append(self))
+    cost = {c: 10.0 + i for i, c in enumerate(at.Autotuner().candidates)}
+    fastest = at.Config(24, "packet", 256)
+    cost[fastest] = 1.0
+
+    class FakeEvent:
+        clock = 0.0
+
+        def __init__(self, enable_timing=False):
+            self.t = None
+
+        def record(self, stream=None):
+            self.t = FakeEvent.clock
+
+        def synchronize(self):
+            pass
+
+        def elapsed_time(self, end):
+            return end.t - self.t
+
+    runs = []
+
+    def run():
+        runs.append(applied[-1])
+        FakeEvent.clock += cost[applied[-1]]
+
+    import torch
+
+    monkeypatch.setattr(torch.cuda, "Event", FakeEvent)
+    tuner = at.Autotuner(tmp_path / "t.json", repeats=2)
+    key, cfg = tuner.tune_callable("problem batch 0 of 1", run, stream=object())
+    assert (key, cfg) == ("problem batch 0 of 1", fastest)
+    assert applied[-1] == fastest
+    assert len(runs) == 3 * len(tuner.candidates)  # one warm-up run and two timed runs each
+    assert tuner.cache[key]["ms"]["24/packet/256"] == 1.0
+    assert at.Autotuner(tmp_path / "t.json").lookup(key) == fastest
+    n_runs = len(runs)
+    assert tuner.tune_callable(key, run, stream=object()) == (key, fastest)
+    assert len(runs) == n_runs and applied[-1] == fastest
